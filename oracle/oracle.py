@@ -1,0 +1,164 @@
+"""ctypes bindings of the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+* :class:`Oracle` loads ``oracle/_build/libmiso_oracle.so``, the C
+  restatement of MISO's explicit MHD step (oracle/miso_oracle.c);
+* :class:`Reference` loads ``oracle/_ref/libmiso_ref.so``, the reference's own
+  host integrator compiled from its headers (oracle/ref_harness.cpp).
+
+Both expose the same calls on a :class:`miso_b200.problems.Problem`-like
+object (grid, config, sign) and a ``(9, I, J, K)`` float64 array.  Only the
+tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use
+this module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libmiso_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmiso_ref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [("i_size", ctypes.c_int), ("j_size", ctypes.c_int), ("k_size", ctypes.c_int),
+                ("margin", ctypes.c_int),
+                ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+                ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
+                ("z_min", ctypes.c_double), ("z_max", ctypes.c_double),
+                ("periodic", ctypes.c_int * 3),
+                ("sign", ctypes.c_double * 54),
+                ("gm", ctypes.c_double), ("cfl_number", ctypes.c_double),
+                ("ep", ctypes.c_double), ("fh", ctypes.c_double),
+                ("cs_fac", ctypes.c_double), ("ca_fac", ctypes.c_double),
+                ("vv_fac", ctypes.c_double)]
+
+
+def make_desc(grid, config, sign=None) -> Desc:
+    d = Desc()
+    d.i_size, d.j_size, d.k_size, d.margin = grid.i_size, grid.j_size, grid.k_size, grid.margin
+    d.x_min, d.x_max = grid.x_min, grid.x_max
+    d.y_min, d.y_max = grid.y_min, grid.y_max
+    d.z_min, d.z_max = grid.z_min, grid.z_max
+    p = config["domain"]["periodic"]
+    d.periodic[0], d.periodic[1], d.periodic[2] = int(p["x"]), int(p["y"]), int(p["z"])
+    s = np.ones((3, 2, 9)) if sign is None else np.asarray(sign, dtype=np.float64)
+    for n, v in enumerate(s.reshape(-1)):
+        d.sign[n] = float(v)
+    d.gm = config["eos"]["gm"]
+    d.cfl_number = config["mhd"]["cfl_number"]
+    av = config["mhd"]["artificial_viscosity"]
+    d.ep, d.fh = av["ep"], av["fh"]
+    d.cs_fac, d.ca_fac, d.vv_fac = av["cs_fac"], av["ca_fac"], av["vv_fac"]
+    return d
+
+
+def _ptrs(q: np.ndarray):
+    assert q.dtype == np.float64 and q.flags.c_contiguous and q.shape[0] == 9
+    arr = (_dp * 9)()
+    for f in range(9):
+        arr[f] = q[f].ctypes.data_as(_dp)
+    return arr
+
+
+def build():
+    """Compile the restatement (and the reference build where its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if os.path.isdir("/root/reference/miso/include"):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+class _Lib:
+    prefix = ""
+    path = ""
+
+    def __init__(self):
+        if not os.path.exists(self.path):
+            raise FileNotFoundError(f"{self.path} is not built (run make -C oracle)")
+        lib = ctypes.CDLL(self.path)
+        P = self.prefix
+        self._run = getattr(lib, P + "run")
+        self._run.argtypes = [ctypes.POINTER(Desc), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+        self._run.restype = ctypes.c_int
+        self._cfl = getattr(lib, P + "cfl")
+        self._cfl.argtypes = [ctypes.POINTER(Desc), ctypes.c_void_p]
+        self._cfl.restype = ctypes.c_double
+        self._stage = getattr(lib, P + "stage")
+        self._stage.argtypes = [ctypes.POINTER(Desc), ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                ctypes.c_double]
+        self._stage.restype = ctypes.c_int
+        self._av = getattr(lib, P + "av")
+        self._av.argtypes = [ctypes.POINTER(Desc), ctypes.c_void_p, ctypes.c_double]
+        self._av.restype = ctypes.c_int
+        self._fill = getattr(lib, P + "fill_ghosts")
+        self._fill.argtypes = [ctypes.POINTER(Desc), ctypes.c_void_p]
+        self._fill.restype = ctypes.c_int
+        self._mind = getattr(lib, P + "min_dxyz")
+        self._mind.argtypes = [ctypes.POINTER(Desc)]
+        self._mind.restype = ctypes.c_double
+        self.lib = lib
+
+    def run(self, prob, q: np.ndarray, nsteps: int, fill_first: bool = True):
+        """Advance ``q`` in place by ``nsteps`` (cfl + update); returns the dts."""
+        d = make_desc(prob.grid, prob.config, prob.sign)
+        dts = np.zeros(max(nsteps, 1))
+        rc = self._run(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p), nsteps,
+                       int(fill_first), dts.ctypes.data_as(_dp))
+        if rc:
+            raise RuntimeError(f"{self.prefix}run failed: {rc}")
+        return dts[:nsteps]
+
+    def cfl(self, prob, q):
+        d = make_desc(prob.grid, prob.config, prob.sign)
+        return self._cfl(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p))
+
+    def stage(self, prob, orgn, argm, rslt, dt, ch2, tau):
+        d = make_desc(prob.grid, prob.config, prob.sign)
+        rc = self._stage(ctypes.byref(d), ctypes.cast(_ptrs(orgn), ctypes.c_void_p),
+                         ctypes.cast(_ptrs(argm), ctypes.c_void_p),
+                         ctypes.cast(_ptrs(rslt), ctypes.c_void_p), dt, ch2, tau)
+        if rc:
+            raise RuntimeError(f"{self.prefix}stage failed: {rc}")
+
+    def av(self, prob, q, dt):
+        d = make_desc(prob.grid, prob.config, prob.sign)
+        rc = self._av(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p), dt)
+        if rc:
+            raise RuntimeError(f"{self.prefix}av failed: {rc}")
+
+    def fill_ghosts(self, prob, q):
+        d = make_desc(prob.grid, prob.config, prob.sign)
+        rc = self._fill(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p))
+        if rc:
+            raise RuntimeError(f"{self.prefix}fill_ghosts failed: {rc}")
+
+    def min_dxyz(self, prob):
+        d = make_desc(prob.grid, prob.config, prob.sign)
+        return self._mind(ctypes.byref(d))
+
+
+class Oracle(_Lib):
+    prefix = "miso_oracle_"
+    path = ORACLE_SO
+
+
+class Reference(_Lib):
+    prefix = "miso_ref_"
+    path = REF_SO
+
+    def symmetric_index(self, i, i_total, i_margin, outer):
+        f = self.lib.miso_ref_symmetric_index
+        f.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(ctypes.c_int)] * 2
+        g, t = ctypes.c_int(), ctypes.c_int()
+        f(i, i_total, i_margin, int(outer), ctypes.byref(g), ctypes.byref(t))
+        return g.value, t.value
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)

@@ -1,0 +1,225 @@
+/*
+ * ref_harness.cpp -- drives the reference's OWN host integrator
+ * (miso::mhd::Integrator<double, backend::Host>, compiled from the MISO
+ * headers where they lie) behind the same C entry points as the oracle
+ * restatement, so tests can check the restatement against the reference
+ * bit for bit.  Built by oracle/Makefile into oracle/_ref/libmiso_ref.so.
+ * TEST INFRASTRUCTURE ONLY: nothing in the product loads it.
+ *
+ * The boundary functor mirrors the demos' "outflow" condition
+ * (demo/mhd1d_shock_tube/src/main.cpp:85-162): on every physical (non
+ * periodic) face, boundary_condition::symmetric is applied to all 9 fields
+ * with the per-field sign given in the descriptor.  Periodic faces are
+ * handled by the reference's HaloExchanger through single-rank MPI.
+ */
+#include <miso/boundary_condition.hpp>
+#include <miso/eos.hpp>
+#include <miso/mhd_integrator.hpp>
+#include <miso/mhd_model_base.hpp>
+
+#include <cstdio>
+#include <filesystem>
+#include <fstream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <unistd.h>
+
+#include "miso_oracle.h"
+
+using namespace miso;
+using Real = double;
+using B = backend::Host;
+
+namespace {
+
+struct DescBC {
+  mpi::Shape &shape;
+  double sign[3][2][9];
+
+  DescBC(mpi::Shape &s, const miso_oracle_desc &d) : shape(s) {
+    std::memcpy(sign, d.sign, sizeof(sign));
+  }
+
+  void apply(mhd::FieldsView<Real> qq, GridView<const Real> grid) const {
+    namespace bc = miso::boundary_condition;
+    Array3DView<Real> *f[9] = {&qq.ro, &qq.vx, &qq.vy, &qq.vz, &qq.bx,
+                               &qq.by, &qq.bz, &qq.ei, &qq.ph};
+    const Direction dirs[3] = {Direction::X, Direction::Y, Direction::Z};
+    const Side sides[2] = {Side::INNER, Side::OUTER};
+    for (int a = 0; a < 3; ++a)
+      for (int s = 0; s < 2; ++s)
+        if (bc::is_physical_boundary(dirs[a], sides[s], shape))
+          for (int v = 0; v < 9; ++v)
+            bc::symmetric(B{}, *f[v], grid, sign[a][s][v] < 0 ? Sign::Neg : Sign::Pos,
+                          dirs[a], sides[s]);
+  }
+};
+
+struct Session {
+  std::unique_ptr<Env> env;
+  std::string path;
+  std::unique_ptr<Config> config;
+  std::unique_ptr<mpi::Shape> shape;
+  std::unique_ptr<Grid<Real, B>> grid;
+  std::unique_ptr<mhd::ExecContext<Real, B>> ctx;
+  std::unique_ptr<mhd::Integrator<Real, B>> integ;
+  std::unique_ptr<eos::IdealEOS<Real>> eos;
+  std::unique_ptr<DescBC> bc;
+  mhd::EmptySourceTerm<Real> src;
+
+  explicit Session(const miso_oracle_desc &d) {
+    static Env *global_env = new Env();
+    (void)global_env;
+    char tmpl[] = "/tmp/miso_ref_cfgXXXXXX";
+    int fd = mkstemp(tmpl);
+    if (fd < 0) throw std::runtime_error("mkstemp failed");
+    close(fd);
+    path = tmpl;
+    std::ostringstream y;
+    y.precision(17);
+    y << "io:\n  enabled: false\n  continue: false\n  save_dir: ./\n";
+    y << "grid:\n  i_size: " << d.i_size << "\n  j_size: " << d.j_size
+      << "\n  k_size: " << d.k_size << "\n  margin: " << d.margin << "\n  x_min: " << d.x_min
+      << "\n  x_max: " << d.x_max << "\n  y_min: " << d.y_min << "\n  y_max: " << d.y_max
+      << "\n  z_min: " << d.z_min << "\n  z_max: " << d.z_max << "\n";
+    y << "mpi:\n  x_procs: 1\n  y_procs: 1\n  z_procs: 1\n";
+    y << "domain:\n  periodic:\n    x: " << (d.periodic[0] ? "true" : "false")
+      << "\n    y: " << (d.periodic[1] ? "true" : "false")
+      << "\n    z: " << (d.periodic[2] ? "true" : "false") << "\n";
+    y << "mhd:\n  cfl_number: " << d.cfl_number << "\n  artificial_viscosity:\n    ep: " << d.ep
+      << "\n    fh: " << d.fh << "\n    cs_fac: " << d.cs_fac << "\n    ca_fac: " << d.ca_fac
+      << "\n    vv_fac: " << d.vv_fac << "\n";
+    y << "eos:\n  gm: " << d.gm << "\n";
+    {
+      std::ofstream f(path);
+      f << y.str();
+    }
+    config.reset(new Config(path));
+    shape.reset(new mpi::Shape(*config));
+    grid.reset(new Grid<Real, B>(d.i_size, d.j_size, d.k_size, d.margin, d.x_min, d.x_max,
+                                 d.y_min, d.y_max, d.z_min, d.z_max));
+    ctx.reset(new mhd::ExecContext<Real, B>(*shape, *grid));
+    integ.reset(new mhd::Integrator<Real, B>(*config, *grid, *ctx));
+    eos.reset(new eos::IdealEOS<Real>(d.gm));
+    bc.reset(new DescBC(*shape, d));
+  }
+  ~Session() { std::remove(path.c_str()); }
+};
+
+void to_fields(mhd::Fields<Real, B> &qq, double *const q[9]) {
+  Array3D<Real, B> *f[9] = {&qq.ro, &qq.vx, &qq.vy, &qq.vz, &qq.bx,
+                            &qq.by, &qq.bz, &qq.ei, &qq.ph};
+  for (int v = 0; v < 9; ++v)
+    std::memcpy(f[v]->data(), q[v], sizeof(double) * f[v]->size());
+}
+
+void from_fields(const mhd::Fields<Real, B> &qq, double *const q[9]) {
+  const Array3D<Real, B> *f[9] = {&qq.ro, &qq.vx, &qq.vy, &qq.vz, &qq.bx,
+                                  &qq.by, &qq.bz, &qq.ei, &qq.ph};
+  for (int v = 0; v < 9; ++v)
+    std::memcpy(q[v], f[v]->data(), sizeof(double) * f[v]->size());
+}
+
+} // namespace
+
+extern "C" {
+
+int miso_ref_run(const miso_oracle_desc *d, double *const q[9], int nsteps, int fill_first,
+                 double *dt_out) {
+  try {
+    Session s(*d);
+    mhd::Fields<Real, B> qq(*s.grid);
+    to_fields(qq, q);
+    if (fill_first) s.integ->apply_boundary_condition(*s.bc, qq);
+    for (int n = 0; n < nsteps; ++n) {
+      const Real dt = s.integ->cfl(qq, *s.eos);
+      if (dt_out) dt_out[n] = dt;
+      s.integ->update(dt, *s.eos, *s.bc, s.src, qq);
+    }
+    from_fields(qq, q);
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "miso_ref_run: %s\n", e.what());
+    return -1;
+  }
+}
+
+double miso_ref_cfl(const miso_oracle_desc *d, double *const q[9]) {
+  try {
+    Session s(*d);
+    mhd::Fields<Real, B> qq(*s.grid);
+    to_fields(qq, q);
+    return s.integ->cfl(qq, *s.eos);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "miso_ref_cfl: %s\n", e.what());
+    return -1.0;
+  }
+}
+
+int miso_ref_stage(const miso_oracle_desc *d, double *const orgn[9], double *const argm[9],
+                   double *const rslt[9], double dt, double ch_divb_square,
+                   double tau_divb) {
+  try {
+    Session s(*d);
+    mhd::Fields<Real, B> o(*s.grid), a(*s.grid), r(*s.grid);
+    to_fields(o, orgn);
+    to_fields(a, argm);
+    to_fields(r, rslt);
+    s.integ->ch_divb_square = ch_divb_square;
+    s.integ->tau_divb = tau_divb;
+    s.integ->update_sc4(dt, *s.eos, s.src, o, a, r);
+    from_fields(r, rslt);
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "miso_ref_stage: %s\n", e.what());
+    return -1;
+  }
+}
+
+int miso_ref_av(const miso_oracle_desc *d, double *const q[9], double dt) {
+  try {
+    Session s(*d);
+    mhd::Fields<Real, B> qq(*s.grid);
+    to_fields(qq, q);
+    s.integ->apply_artificial_viscosity(dt, *s.eos, *s.bc, qq);
+    from_fields(qq, q);
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "miso_ref_av: %s\n", e.what());
+    return -1;
+  }
+}
+
+int miso_ref_fill_ghosts(const miso_oracle_desc *d, double *const q[9]) {
+  try {
+    Session s(*d);
+    mhd::Fields<Real, B> qq(*s.grid);
+    to_fields(qq, q);
+    s.integ->apply_boundary_condition(*s.bc, qq);
+    from_fields(qq, q);
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "miso_ref_fill_ghosts: %s\n", e.what());
+    return -1;
+  }
+}
+
+double miso_ref_min_dxyz(const miso_oracle_desc *d) {
+  try {
+    Session s(*d);
+    return s.grid->min_dxyz;
+  } catch (const std::exception &e) {
+    return -1.0;
+  }
+}
+
+/* Symmetric-boundary index helper of the reference (boundary_condition.hpp:77-90),
+ * exposed for the index known-answer test. */
+void miso_ref_symmetric_index(int i, int i_total, int i_margin, int outer, int *ghst,
+                              int *trgt) {
+  boundary_condition::symmetric_index(i, i_total, i_margin, *ghst, *trgt,
+                                      outer ? Side::OUTER : Side::INNER);
+}
+
+} // extern "C"

@@ -1,0 +1,143 @@
+/*
+ * miso_b200.h -- C ABI of libmiso_b200.so, the B200 (sm_100a) implementation
+ * of MISO's explicit ideal-MHD time step.
+ *
+ * Every call returns an int status (MISO_B200_OK = 0, negative on error) and
+ * never aborts the process; miso_b200_last_error() gives a message.  One
+ * handle is driven by one host thread; all device work of a handle is
+ * ordered on one CUDA stream (the caller's, or one the handle creates).
+ *
+ * Field order everywhere: ro, vx, vy, vz, bx, by, bz, ei, ph -- the
+ * reference's primitive variables (miso/include/miso/mhd_fields.hpp:17-18),
+ * each an (i_total, j_total, k_total) array with k fastest
+ * (miso/include/miso/array3d.hpp:54-60) and `margin` ghost cells on every
+ * axis of size > 1 (miso/include/miso/grid.hpp:67-90).
+ */
+#ifndef MISO_B200_H
+#define MISO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MISO_B200_OK 0
+#define MISO_B200_ERR_ARG (-1)      /* invalid argument or descriptor */
+#define MISO_B200_ERR_CUDA (-2)     /* a CUDA call failed */
+#define MISO_B200_ERR_NONFINITE (-3) /* non-positive/non-finite ro or ei seen by the CFL pass */
+#define MISO_B200_ERR_STATE (-4)    /* call not valid in the handle's current state */
+#define MISO_B200_ERR_NOMEM (-5)    /* device allocation failed */
+
+#define MISO_B200_FP64 0        /* primitive FP64 state, bit-faithful to the reference */
+#define MISO_B200_FP32_SPLIT 1  /* conserved FP32 hi/lo state, FP32 RHS and viscosity */
+
+/* Grid and boundary description.  Replaces the serial constructor
+ * Grid<Real, backend::Host>(i_size, ..., z_max) (miso/include/miso/grid.hpp:316-337),
+ * domain.periodic.{x,y,z} (miso/include/miso/mpi_util.hpp:79-86) and the
+ * demos' symmetric "outflow" boundary functor
+ * (demo/mhd1d_shock_tube/src/main.cpp:85-162 calling
+ * boundary_condition::symmetric, miso/include/miso/boundary_condition.hpp:109-136). */
+typedef struct miso_b200_grid_desc {
+  int i_size, j_size, k_size; /* interior cells per axis (size 1 = degenerate axis) */
+  int margin;                 /* ghost width on non-degenerate axes; the stencil needs 2 */
+  double x_min, x_max, y_min, y_max, z_min, z_max;
+  int periodic[3];            /* 1 = periodic wrap; 0 = mirror (symmetric) faces */
+  double sign[3][2][9];       /* mirror sign per axis, side (0 inner, 1 outer), field */
+} miso_b200_grid_desc;
+
+/* Physics and numerics parameters: the keys the reference's integrator reads
+ * (eos.gm, eos.hpp:17; mhd.cfl_number, mhd_integrator_host.hpp:52;
+ * mhd.artificial_viscosity.*, mhd_artificial_viscosity_host.hpp:40-44). */
+typedef struct miso_b200_params {
+  double gm;
+  double cfl_number;
+  double ep, fh;
+  double cs_fac, ca_fac, vv_fac;
+  int precision; /* MISO_B200_FP64 or MISO_B200_FP32_SPLIT */
+} miso_b200_params;
+
+typedef struct miso_b200_handle miso_b200_handle;
+
+/* Create a solver for one grid on the current CUDA device.  `stream` is a
+ * cudaStream_t (NULL: the handle creates its own).  Replaces the
+ * construction of Integrator<Real, backend::CUDA> with its workspaces
+ * (miso/include/miso/mhd_integrator_cuda.cuh:328-339) and of Fields qq
+ * (miso/include/miso/mhd.hpp:22-25). */
+int miso_b200_create(const miso_b200_grid_desc *grid, const miso_b200_params *params,
+                     void *stream, miso_b200_handle **out);
+
+/* Release every device buffer of the handle. */
+int miso_b200_destroy(miso_b200_handle *h);
+
+/* Copy the 9 primitive fields in (q[f] host or device pointers, full arrays
+ * including ghosts).  Replaces Fields<Real, CUDA>::copy_from(host Fields)
+ * (miso/include/miso/mhd_fields.hpp:150-160).  Synchronises the stream. */
+int miso_b200_upload(miso_b200_handle *h, const double *const q[9]);
+
+/* Copy the 9 primitive fields out (FP32_SPLIT: converted from the conserved
+ * hi/lo state to FP64 primitives).  Replaces Fields<Real, Host>::copy_from(CUDA
+ * Fields) (miso/include/miso/mhd_fields.hpp:83-96).  Synchronises the stream. */
+int miso_b200_download(miso_b200_handle *h, double *const q[9]);
+
+/* Fill every ghost cell from its periodic or mirror image.  Replaces
+ * Integrator::apply_boundary_condition(bc, qq) for the built-in boundaries
+ * (miso/include/miso/mhd_integrator_cuda.cuh:396-401). */
+int miso_b200_fill_ghosts(miso_b200_handle *h);
+
+/* CFL time step, returned to the host (synchronises).  Replaces
+ * Integrator::cfl(qq, eos) (miso/include/miso/mhd_integrator_cuda.cuh:450-478,
+ * host twin mhd_integrator_host.hpp:303-334).  The result is also kept on
+ * the device for miso_b200_update_device(). */
+int miso_b200_cfl(miso_b200_handle *h, double *dt_out);
+
+/* Advance one step with a host-given dt: 4 Runge-Kutta stages, 3 artificial
+ * viscosity sweeps, ghost fills.  Replaces Integrator::update(dt, eos, bc,
+ * src, qq) (miso/include/miso/mhd_integrator_cuda.cuh:481-487; host twin
+ * mhd_integrator_host.hpp:344-350).  Asynchronous. */
+int miso_b200_update(miso_b200_handle *h, double dt);
+
+/* Advance one step with the dt left on the device by the last CFL pass
+ * (no host round trip).  Asynchronous. */
+int miso_b200_update_device(miso_b200_handle *h);
+
+/* Run `nsteps` of ModelBase::update() -- cfl then update
+ * (miso/include/miso/mhd_model_base.hpp:57-62) -- with dt kept on the device.
+ * With use_graph != 0 one step is captured in a CUDA graph on first use and
+ * replayed.  Asynchronous. */
+int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph);
+
+/* Wait for the handle's stream; reports device-side error flags. */
+int miso_b200_sync(miso_b200_handle *h);
+
+/* dt of the last CFL pass as held on the device (synchronises). */
+int miso_b200_last_dt(miso_b200_handle *h, double *dt_out);
+
+/* FP64 global monitors of the current state: out[0..7] = sum ro dV,
+ * sum ro*vx dV, sum ro*vy dV, sum ro*vz dV, sum Et dV, sum |div B| dV,
+ * max |div B|, sum ph^2 dV (interior cells, dV = product of the spacings of
+ * the non-degenerate axes).  Synchronises. */
+int miso_b200_monitors(miso_b200_handle *h, double out[8]);
+
+/* Device pointers of the FP64 primitive state arrays (FP64 form only), valid
+ * until the next call that steps or destroys the handle.  Gives user code
+ * the reference's FieldsView for custom boundary work
+ * (miso/include/miso/mhd_fields.hpp:17-34). */
+int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
+
+/* Bytes of device memory the handle holds. */
+int miso_b200_device_bytes(miso_b200_handle *h, size_t *bytes);
+
+/* Number of kernels the library enqueued on the handle's stream so far. */
+int miso_b200_launch_count(miso_b200_handle *h, long long *count);
+
+/* Message of the last error on this handle (or of the last failed create when h is NULL). */
+const char *miso_b200_last_error(miso_b200_handle *h);
+
+/* Library version string. */
+const char *miso_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,97 @@
+"""ctypes binding of libmiso_b200.so (the C ABI of include/miso_b200.h).
+
+The library is loaded from ``miso_b200/lib/`` (built in-tree by
+``miso_b200.build``).  There is no fallback: if the shared library is
+missing, importing the solver raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libmiso_b200.so")
+
+OK = 0
+ERR_ARG = -1
+ERR_CUDA = -2
+ERR_NONFINITE = -3
+ERR_STATE = -4
+ERR_NOMEM = -5
+
+FP64 = 0
+FP32_SPLIT = 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("i_size", ctypes.c_int), ("j_size", ctypes.c_int), ("k_size", ctypes.c_int),
+                ("margin", ctypes.c_int),
+                ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+                ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
+                ("z_min", ctypes.c_double), ("z_max", ctypes.c_double),
+                ("periodic", ctypes.c_int * 3),
+                ("sign", ctypes.c_double * 54)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("gm", ctypes.c_double), ("cfl_number", ctypes.c_double),
+                ("ep", ctypes.c_double), ("fh", ctypes.c_double),
+                ("cs_fac", ctypes.c_double), ("ca_fac", ctypes.c_double),
+                ("vv_fac", ctypes.c_double), ("precision", ctypes.c_int)]
+
+
+# name -> (restype, argtypes); the exported set must match include/miso_b200.h
+SIGNATURES = {
+    "miso_b200_create": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(Params),
+                                        ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "miso_b200_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_fill_ghosts": (ctypes.c_int, [ctypes.c_void_p]),
+    "miso_b200_cfl": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "miso_b200_update": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "miso_b200_update_device": (ctypes.c_int, [ctypes.c_void_p]),
+    "miso_b200_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "miso_b200_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "miso_b200_last_dt": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "miso_b200_monitors": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "miso_b200_fields_view": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_device_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
+    "miso_b200_launch_count": (ctypes.c_int, [ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_longlong)]),
+    "miso_b200_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "miso_b200_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load():
+    """Load the shared library once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m miso_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class MisoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def check(code: int, handle=None):
+    if code != OK:
+        lib = load()
+        msg = lib.miso_b200_last_error(handle)
+        raise MisoError(code, msg.decode() if msg else "")

@@ -1,0 +1,680 @@
+// C ABI of libmiso_b200.so (declared in include/miso_b200.h): handle
+// lifetime, device buffers, step sequencing, CUDA-graph capture, monitors.
+//
+// Step sequence (Integrator::update, mhd_integrator_host.hpp:344-350):
+//   divb parameters -> 4 RK stages (258-277), each followed by a ghost fill
+//   -> characteristic speed -> AV sweeps x, y, z (280-300), each followed by a
+//   ghost fill.
+// The reference copies whole field sets between stages (Fields::copy_from,
+// mhd_fields.hpp:161-172); here three field sets rotate instead, so a step
+// makes no device-to-device copies.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/miso_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+#include "kernels_s32.h"
+
+using namespace miso_b200;
+
+namespace {
+
+std::string g_create_error;
+std::mutex g_create_mu;
+
+constexpr size_t ALIGN = 256;
+
+size_t round_up(size_t x) { return (x + ALIGN - 1) / ALIGN * ALIGN; }
+
+// FP64 monitors: per-block partial sums of 8 quantities (interior cells).
+template <bool SPLIT>
+__global__ void __launch_bounds__(256)
+monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
+               FieldPtrs<const float> lo, double *__restrict__ partial) {
+  const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (long long lin = blockIdx.x * (long long)blockDim.x + threadIdx.x; lin < nint;
+       lin += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(lin % g.n[2]) + g.m[2];
+    const long long r1 = lin / g.n[2];
+    const int j = (int)(r1 % g.n[1]) + g.m[1];
+    const int i = (int)(r1 / g.n[1]) + g.m[0];
+    const long long c = i * g.st[0] + j * g.st[1] + k;
+    double u[NF];
+    if (SPLIT) {
+      for (int f = 0; f < NF; ++f) u[f] = (double)hi.f[f][c] + (double)lo.f[f][c];
+    } else {
+      const double ro = q.f[RO][c], vx = q.f[VX][c], vy = q.f[VY][c], vz = q.f[VZ][c];
+      const double bx = q.f[BX][c], by = q.f[BY][c], bz = q.f[BZ][c];
+      u[RO] = ro;
+      u[MX] = ro * vx;
+      u[MY] = ro * vy;
+      u[MZ] = ro * vz;
+      u[BX] = bx;
+      u[BY] = by;
+      u[BZ] = bz;
+      u[ET] = ro * q.f[EI][c] + 0.5 * ro * (vx * vx + vy * vy + vz * vz) +
+              PII8 * (bx * bx + by * by + bz * bz);
+      u[PH] = q.f[PH][c];
+    }
+    double divb = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      if (!g.s[d]) continue;
+      const long long s = g.st[d];
+      double p2, p1, m1, m2;
+      if (SPLIT) {
+        const float *h = hi.f[BX + d], *l = lo.f[BX + d];
+        p2 = (double)h[c + 2 * s] + l[c + 2 * s];
+        p1 = (double)h[c + s] + l[c + s];
+        m1 = (double)h[c - s] + l[c - s];
+        m2 = (double)h[c - 2 * s] + l[c - 2 * s];
+      } else {
+        const double *b = q.f[BX + d];
+        p2 = b[c + 2 * s];
+        p1 = b[c + s];
+        m1 = b[c - s];
+        m2 = b[c - 2 * s];
+      }
+      divb += (-p2 + 8.0 * p1 - 8.0 * m1 + m2) * INV12 * g.dsi[d];
+    }
+    acc[0] += u[RO];
+    acc[1] += u[MX];
+    acc[2] += u[MY];
+    acc[3] += u[MZ];
+    acc[4] += u[ET];
+    acc[5] += fabs(divb);
+    acc[6] = fmax(acc[6], fabs(divb));
+    acc[7] += u[PH] * u[PH];
+  }
+  __shared__ double red[8][256];
+  for (int q8 = 0; q8 < 8; ++q8) red[q8][threadIdx.x] = acc[q8];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      for (int q8 = 0; q8 < 8; ++q8) {
+        if (q8 == 6)
+          red[q8][threadIdx.x] = fmax(red[q8][threadIdx.x], red[q8][threadIdx.x + w]);
+        else
+          red[q8][threadIdx.x] += red[q8][threadIdx.x + w];
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int q8 = 0; q8 < 8; ++q8) partial[blockIdx.x * 8 + q8] = red[q8][0];
+}
+
+__global__ void set_scalars_kernel(StepScalars *sc, StepScalars v) {
+  const unsigned int err = sc->err;
+  *sc = v;
+  sc->err = err;
+}
+
+}  // namespace
+
+struct miso_b200_handle {
+  Geom g{};
+  miso_b200_params p{};
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+
+  void *block = nullptr;  // one allocation holds every device buffer
+  size_t bytes = 0;
+
+  // FP64 form: three rotating field sets + characteristic speed
+  double *q64[3][NF] = {};
+  double *cc64 = nullptr;
+  // FP32-split form: hi/lo state (two sets, swapped by the AV sweeps), two
+  // stage buffers, characteristic speed, FP64 staging for upload/download
+  float *hi[2][NF] = {}, *lo[2][NF] = {};
+  float *stg[2][NF] = {};
+  float *cc32 = nullptr;
+  double *io64[NF] = {};
+  int cur = 0;  // which hi/lo set holds the state
+
+  float *partial = nullptr;
+  int nparts = 0;
+  double *mon_partial = nullptr;
+  int mon_blocks = 0;
+  StepScalars *sc = nullptr;
+
+  double min_dxyz = 0.0, cfl_dx = 0.0;
+  long long launches = 0;
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_steps = 0;          // steps captured in the graph (1 or 2)
+  long long graph_kernels = 0;  // kernels per graph launch
+
+  int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+  }
+  int cuda(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return MISO_B200_OK;
+    return fail(MISO_B200_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+  int check_launch(const char *what) { return cuda(cudaGetLastError(), what); }
+
+  bool split() const { return p.precision == MISO_B200_FP32_SPLIT; }
+
+  FieldPtrs<double> f64(int set) {
+    FieldPtrs<double> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = q64[set][f];
+    return r;
+  }
+  FieldPtrs<const double> c64(int set) {
+    FieldPtrs<const double> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = q64[set][f];
+    return r;
+  }
+  template <typename T>
+  static FieldPtrs<const T> cst(const FieldPtrs<T> &a) {
+    FieldPtrs<const T> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = a.f[f];
+    return r;
+  }
+  FieldPtrs<float> H(int s) {
+    FieldPtrs<float> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = hi[s][f];
+    return r;
+  }
+  FieldPtrs<float> L(int s) {
+    FieldPtrs<float> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = lo[s][f];
+    return r;
+  }
+  FieldPtrs<float> S(int s) {
+    FieldPtrs<float> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = stg[s][f];
+    return r;
+  }
+  FieldPtrs<double> IO() {
+    FieldPtrs<double> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = io64[f];
+    return r;
+  }
+
+  // ghost fill of one field set (the split form fills hi and lo together)
+  int fill64(int set) {
+    launch_fill_ghosts<double>(g, f64(set), NF, sms, stream);
+    launches += g.s[0] + g.s[1] + g.s[2];
+    return check_launch("fill_ghosts");
+  }
+  int fill_split(int s) {
+    launch_fill_ghosts<float>(g, H(s), NF, sms, stream);
+    launch_fill_ghosts<float>(g, L(s), NF, sms, stream);
+    launches += 2 * (g.s[0] + g.s[1] + g.s[2]);
+    return check_launch("fill_ghosts");
+  }
+  int fill_stage(int s) {
+    launch_fill_ghosts<float>(g, S(s), NF, sms, stream);
+    launches += g.s[0] + g.s[1] + g.s[2];
+    return check_launch("fill_ghosts");
+  }
+
+  int fill_state() { return split() ? fill_split(cur) : fill64(0); }
+
+  // host-side step scalars exactly as Integrator::divb_parameters_set and
+  // runge_kutta_4step form them (host libm exp, as the reference's host path)
+  StepScalars host_scalars(double dt) const {
+    StepScalars v{};
+    v.dt = dt;
+    v.dts[0] = dt / 4.0;
+    v.dts[1] = dt / 3.0;
+    v.dts[2] = dt / 2.0;
+    v.dts[3] = dt;
+    volatile double ch = 0.8 * p.cfl_number * min_dxyz / dt;
+    v.ch2 = ch * ch;
+    v.tau = 2.0 * dt;
+    for (int s = 0; s < 4; ++s) v.ph_decay[s] = std::exp(-v.dts[s] / v.tau);
+    return v;
+  }
+
+  int enqueue_cfl() {
+    if (split()) {
+      launch_s32_cfl_partial(g, cst(H(cur)), partial, nparts, sc, p.gm, cfl_dx, stream);
+      launch_cfl_finalize(partial, nparts, sc, p.cfl_number, min_dxyz, stream);
+    } else {
+      launch_fp64_cfl(g, c64(0), partial, sc, p.gm, p.cfl_number, cfl_dx, min_dxyz, sms, stream);
+    }
+    launches += 2;
+    return check_launch("cfl");
+  }
+
+  int enqueue_update() {
+    int rc;
+    if (!split()) {
+      // RK: qq(0) -> A(1) -> B(2) -> A -> B
+      const int seq_a[4] = {0, 1, 2, 1};
+      const int seq_r[4] = {1, 2, 1, 2};
+      for (int s = 0; s < 4; ++s) {
+        launch_fp64_rhs_stage(g, c64(0), c64(seq_a[s]), f64(seq_r[s]), sc, s, p.gm, sms, stream);
+        launches++;
+        if ((rc = check_launch("rhs_stage"))) return rc;
+        if ((rc = fill64(seq_r[s]))) return rc;
+      }
+      // AV on B(2): x: B -> qq, y: qq -> A, z: A -> qq
+      launch_fp64_char_velocity(g, c64(2), cc64, p.gm, p.cs_fac, p.vv_fac, p.ca_fac, sms,
+                                stream);
+      launches++;
+      const int src[3] = {2, 0, 1}, dst[3] = {0, 1, 0};
+      for (int d = 0; d < 3; ++d) {
+        launch_fp64_av_sweep(g, c64(src[d]), f64(dst[d]), cc64, sc, d, p.ep, p.fh, sms, stream);
+        launches++;
+        if ((rc = check_launch("av_sweep"))) return rc;
+        if ((rc = fill64(dst[d]))) return rc;
+      }
+      return MISO_B200_OK;
+    }
+    // FP32 split: stage 0 reads hi, stages write stg[0], stg[1], stg[0];
+    // stage 3 accumulates into hi/lo of the current set.
+    const int c = cur;
+    for (int s = 0; s < 4; ++s) {
+      FieldPtrs<const float> prev = s == 0 ? cst(H(c)) : cst(S((s - 1) & 1));
+      FieldPtrs<float> out = s < 3 ? S(s & 1) : S(0);
+      launch_s32_rk_stage(g, prev, H(c), L(c), out, sc, s, p.gm, sms, stream);
+      launches++;
+      if ((rc = check_launch("rk_stage"))) return rc;
+      if (s < 3) {
+        if ((rc = fill_stage(s & 1))) return rc;
+      } else {
+        if ((rc = fill_split(c))) return rc;
+      }
+    }
+    launch_s32_char_velocity(g, cst(H(c)), cc32, p.gm, p.cs_fac, p.vv_fac, p.ca_fac, sms, stream);
+    launches++;
+    for (int d = 0; d < 3; ++d) {
+      if (!g.s[d]) continue;  // a degenerate sweep leaves the conserved state unchanged
+      launch_s32_av_sweep(g, cst(H(cur)), cst(L(cur)), H(cur ^ 1), L(cur ^ 1), cc32, sc, d, p.ep,
+                          p.fh, sms, stream);
+      launches++;
+      if ((rc = check_launch("av_sweep"))) return rc;
+      cur ^= 1;
+      if ((rc = fill_split(cur))) return rc;
+    }
+    return MISO_B200_OK;
+  }
+
+  int read_err() {
+    unsigned int e = 0;
+    int rc = cuda(cudaMemcpyAsync(&e, &sc->err, sizeof e, cudaMemcpyDeviceToHost, stream),
+                  "read error flags");
+    if (rc) return rc;
+    if ((rc = cuda(cudaStreamSynchronize(stream), "synchronize"))) return rc;
+    if (e & ERRBIT_NONFINITE) {
+      unsigned int zero = 0;
+      cudaMemcpy(&sc->err, &zero, sizeof zero, cudaMemcpyHostToDevice);
+      return fail(MISO_B200_ERR_NONFINITE,
+                  "non-positive or non-finite density / internal energy in the CFL pass");
+    }
+    return MISO_B200_OK;
+  }
+};
+
+static bool valid_axis(int size, int margin) { return size >= 1 && (size == 1 || size >= margin); }
+
+extern "C" {
+
+const char *miso_b200_version(void) { return "miso_b200 0.1 (sm_100a)"; }
+
+const char *miso_b200_last_error(miso_b200_handle *h) {
+  if (!h) {
+    std::lock_guard<std::mutex> lk(g_create_mu);
+    return g_create_error.c_str();
+  }
+  return h->err.c_str();
+}
+
+int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, void *stream,
+                     miso_b200_handle **out) {
+  auto create_fail = [](int code, const std::string &msg) {
+    std::lock_guard<std::mutex> lk(g_create_mu);
+    g_create_error = msg;
+    return code;
+  };
+  if (!gd || !pp || !out) return create_fail(MISO_B200_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (gd->margin < 2)
+    return create_fail(MISO_B200_ERR_ARG, "margin must be >= 2 for the 4th-order stencil");
+  const int sz[3] = {gd->i_size, gd->j_size, gd->k_size};
+  const double lo[3] = {gd->x_min, gd->y_min, gd->z_min};
+  const double hi[3] = {gd->x_max, gd->y_max, gd->z_max};
+  for (int a = 0; a < 3; ++a) {
+    if (!valid_axis(sz[a], gd->margin))
+      return create_fail(MISO_B200_ERR_ARG, "invalid grid size");
+    if (!(lo[a] < hi[a])) return create_fail(MISO_B200_ERR_ARG, "invalid grid range");
+  }
+  if (!(pp->gm > 1.0) || !(pp->cfl_number > 0.0) || !(pp->ep >= 0.0) || !(pp->fh >= 0.0))
+    return create_fail(MISO_B200_ERR_ARG, "invalid physics parameters");
+  if (pp->precision != MISO_B200_FP64 && pp->precision != MISO_B200_FP32_SPLIT)
+    return create_fail(MISO_B200_ERR_ARG, "unknown precision");
+
+  auto *h = new miso_b200_handle();
+  h->p = *pp;
+  Geom &g = h->g;
+  double ds[3];
+  for (int a = 0; a < 3; ++a) {
+    g.n[a] = sz[a];
+    g.s[a] = sz[a] > 1 ? 1 : 0;
+    g.m[a] = gd->margin * g.s[a];
+    g.t[a] = sz[a] + 2 * g.m[a];
+    g.periodic[a] = gd->periodic[a] ? 1 : 0;
+    // grid.hpp:22-31 and 67-99: uniform spacing; degenerate axes 1e30 / 0
+    const double sp = (hi[a] - lo[a]) / (double)sz[a];
+    ds[a] = g.s[a] ? sp : 1.e30;
+    g.dsi[a] = g.s[a] ? 1.0 / sp : 0.0;
+    for (int side = 0; side < 2; ++side)
+      for (int f = 0; f < NF; ++f) g.sign[a][side][f] = (float)(gd->sign[a][side][f] < 0 ? -1 : 1);
+  }
+  g.st[2] = 1;
+  g.st[1] = g.t[2];
+  g.st[0] = (long long)g.t[1] * g.t[2];
+  g.cells = (long long)g.t[0] * g.t[1] * g.t[2];
+  // grid.hpp:241 and mhd_integrator_host.hpp:323-325, through float
+  const float m3 = fminf(fminf((float)ds[0], (float)ds[1]), (float)ds[2]);
+  h->min_dxyz = (double)m3;
+  h->cfl_dx = pp->cfl_number * (double)m3;
+
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
+  if (e != cudaSuccess) {
+    delete h;
+    return create_fail(MISO_B200_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  }
+  if (stream) {
+    h->stream = (cudaStream_t)stream;
+  } else {
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete h;
+      return create_fail(MISO_B200_ERR_CUDA, "stream creation failed");
+    }
+    h->own_stream = true;
+  }
+
+  h->nparts = cfl_partial_blocks(h->sms);
+  h->mon_blocks = h->sms * 2;
+  const size_t cells = (size_t)g.cells;
+  size_t total = 0;
+  std::vector<std::pair<void **, size_t>> plan;
+  auto add = [&](void **p, size_t b) {
+    plan.emplace_back(p, b);
+    total += round_up(b);
+  };
+  if (!h->split()) {
+    for (int s = 0; s < 3; ++s)
+      for (int f = 0; f < NF; ++f) add((void **)&h->q64[s][f], cells * sizeof(double));
+    add((void **)&h->cc64, cells * sizeof(double));
+  } else {
+    for (int s = 0; s < 2; ++s)
+      for (int f = 0; f < NF; ++f) {
+        add((void **)&h->hi[s][f], cells * sizeof(float));
+        add((void **)&h->lo[s][f], cells * sizeof(float));
+      }
+    for (int s = 0; s < 2; ++s)
+      for (int f = 0; f < NF; ++f) add((void **)&h->stg[s][f], cells * sizeof(float));
+    add((void **)&h->cc32, cells * sizeof(float));
+  }
+  add((void **)&h->partial, sizeof(float) * h->nparts);
+  add((void **)&h->mon_partial, sizeof(double) * 8 * h->mon_blocks);
+  add((void **)&h->sc, sizeof(StepScalars));
+  e = cudaMalloc(&h->block, total);
+  if (e != cudaSuccess) {
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return create_fail(MISO_B200_ERR_NOMEM, "device allocation of " + std::to_string(total) +
+                                                " bytes failed");
+  }
+  h->bytes = total;
+  size_t off = 0;
+  for (auto &pb : plan) {
+    *pb.first = (char *)h->block + off;
+    off += round_up(pb.second);
+  }
+  if (h->split()) {
+    // The FP64 upload/download staging overlays the 18 consecutive FP32
+    // stage arrays (18 * 4 bytes >= 9 * 8 bytes per cell), which hold no
+    // state between steps.
+    for (int f = 0; f < NF; ++f) h->io64[f] = (double *)h->stg[0][0] + (size_t)f * cells;
+  }
+  e = cudaMemsetAsync(h->block, 0, total, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    cudaFree(h->block);
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return create_fail(MISO_B200_ERR_CUDA, "device memset failed");
+  }
+  *out = h;
+  return MISO_B200_OK;
+}
+
+int miso_b200_destroy(miso_b200_handle *h) {
+  if (!h) return MISO_B200_ERR_ARG;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->block) cudaFree(h->block);
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return MISO_B200_OK;
+}
+
+int miso_b200_upload(miso_b200_handle *h, const double *const q[9]) {
+  if (!h || !q) return MISO_B200_ERR_ARG;
+  const size_t bytes = (size_t)h->g.cells * sizeof(double);
+  int rc;
+  for (int f = 0; f < NF; ++f) {
+    if (!q[f]) return h->fail(MISO_B200_ERR_ARG, "null field pointer %d", f);
+    double *dst = h->split() ? h->io64[f] : h->q64[0][f];
+    if ((rc = h->cuda(cudaMemcpyAsync(dst, q[f], bytes, cudaMemcpyDefault, h->stream), "upload")))
+      return rc;
+  }
+  if (h->split()) {
+    FieldPtrs<const double> src;
+    for (int f = 0; f < NF; ++f) src.f[f] = h->io64[f];
+    h->cur = 0;
+    launch_s32_to_split(h->g.cells, src, h->H(0), h->L(0), h->sms, h->stream);
+    h->launches++;
+    if ((rc = h->check_launch("to_split"))) return rc;
+  }
+  return h->cuda(cudaStreamSynchronize(h->stream), "upload synchronize");
+}
+
+int miso_b200_download(miso_b200_handle *h, double *const q[9]) {
+  if (!h || !q) return MISO_B200_ERR_ARG;
+  const size_t bytes = (size_t)h->g.cells * sizeof(double);
+  int rc;
+  if (h->split()) {
+    launch_s32_from_split(h->g.cells, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->IO(), h->sms,
+                          h->stream);
+    h->launches++;
+    if ((rc = h->check_launch("from_split"))) return rc;
+  }
+  for (int f = 0; f < NF; ++f) {
+    if (!q[f]) return h->fail(MISO_B200_ERR_ARG, "null field pointer %d", f);
+    const double *src = h->split() ? h->io64[f] : h->q64[0][f];
+    if ((rc = h->cuda(cudaMemcpyAsync(q[f], src, bytes, cudaMemcpyDefault, h->stream),
+                      "download")))
+      return rc;
+  }
+  return h->cuda(cudaStreamSynchronize(h->stream), "download synchronize");
+}
+
+int miso_b200_fill_ghosts(miso_b200_handle *h) {
+  if (!h) return MISO_B200_ERR_ARG;
+  return h->fill_state();
+}
+
+int miso_b200_cfl(miso_b200_handle *h, double *dt_out) {
+  if (!h || !dt_out) return MISO_B200_ERR_ARG;
+  int rc = h->enqueue_cfl();
+  if (rc) return rc;
+  StepScalars v;
+  if ((rc = h->cuda(cudaMemcpyAsync(&v, h->sc, sizeof v, cudaMemcpyDeviceToHost, h->stream),
+                    "read dt")))
+    return rc;
+  if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cfl synchronize"))) return rc;
+  if (v.err & ERRBIT_NONFINITE) return h->read_err();
+  *dt_out = v.dt;
+  return MISO_B200_OK;
+}
+
+int miso_b200_update(miso_b200_handle *h, double dt) {
+  if (!h) return MISO_B200_ERR_ARG;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return h->fail(MISO_B200_ERR_ARG, "dt must be > 0");
+  set_scalars_kernel<<<1, 1, 0, h->stream>>>(h->sc, h->host_scalars(dt));
+  h->launches++;
+  int rc = h->check_launch("set_scalars");
+  if (rc) return rc;
+  return h->enqueue_update();
+}
+
+int miso_b200_update_device(miso_b200_handle *h) {
+  if (!h) return MISO_B200_ERR_ARG;
+  return h->enqueue_update();
+}
+
+int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
+  if (!h || nsteps < 0) return MISO_B200_ERR_ARG;
+  int rc;
+  if (!use_graph) {
+    for (int n = 0; n < nsteps; ++n) {
+      if ((rc = h->enqueue_cfl())) return rc;
+      if ((rc = h->enqueue_update())) return rc;
+    }
+    return MISO_B200_OK;
+  }
+  // The split form swaps its hi/lo sets once per AV sweep; when a step
+  // swaps an odd number of times the captured graph covers two steps so
+  // that it starts and ends on the same set.
+  if (!h->graph_exec) {
+    const int before = h->cur;
+    const long long l0 = h->launches;
+    if ((rc = h->cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal),
+                      "begin capture")))
+      return rc;
+    int steps = 1;
+    rc = h->enqueue_cfl();
+    if (!rc) rc = h->enqueue_update();
+    if (!rc && h->cur != before) {
+      steps = 2;
+      rc = h->enqueue_cfl();
+      if (!rc) rc = h->enqueue_update();
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    h->cur = before;
+    const long long kernels = h->launches - l0;
+    h->launches = l0;
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if ((rc = h->cuda(e, "end capture"))) return rc;
+    h->graph = graph;
+    if ((rc = h->cuda(cudaGraphInstantiate(&h->graph_exec, graph, 0), "graph instantiate")))
+      return rc;
+    h->graph_steps = steps;
+    h->graph_kernels = kernels;
+  }
+  if (nsteps % h->graph_steps)
+    return h->fail(MISO_B200_ERR_ARG, "nsteps must be a multiple of %d", h->graph_steps);
+  for (int n = 0; n < nsteps; n += h->graph_steps) {
+    if ((rc = h->cuda(cudaGraphLaunch(h->graph_exec, h->stream), "graph launch"))) return rc;
+    h->launches += h->graph_kernels;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_sync(miso_b200_handle *h) {
+  if (!h) return MISO_B200_ERR_ARG;
+  return h->read_err();
+}
+
+int miso_b200_last_dt(miso_b200_handle *h, double *dt_out) {
+  if (!h || !dt_out) return MISO_B200_ERR_ARG;
+  StepScalars v;
+  int rc = h->cuda(cudaMemcpyAsync(&v, h->sc, sizeof v, cudaMemcpyDeviceToHost, h->stream),
+                   "read dt");
+  if (rc) return rc;
+  if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "synchronize"))) return rc;
+  *dt_out = v.dt;
+  return MISO_B200_OK;
+}
+
+int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
+  if (!h || !out) return MISO_B200_ERR_ARG;
+  FieldPtrs<const double> q{};
+  FieldPtrs<const float> hs{}, ls{};
+  if (h->split()) {
+    hs = h->cst(h->H(h->cur));
+    ls = h->cst(h->L(h->cur));
+    monitor_kernel<true><<<h->mon_blocks, 256, 0, h->stream>>>(h->g, q, hs, ls, h->mon_partial);
+  } else {
+    q = h->c64(0);
+    monitor_kernel<false><<<h->mon_blocks, 256, 0, h->stream>>>(h->g, q, hs, ls, h->mon_partial);
+  }
+  h->launches++;
+  int rc = h->check_launch("monitors");
+  if (rc) return rc;
+  std::vector<double> part((size_t)h->mon_blocks * 8);
+  if ((rc = h->cuda(cudaMemcpyAsync(part.data(), h->mon_partial, part.size() * sizeof(double),
+                                    cudaMemcpyDeviceToHost, h->stream),
+                    "read monitors")))
+    return rc;
+  if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "monitors synchronize"))) return rc;
+  double dv = 1.0;
+  for (int a = 0; a < 3; ++a)
+    if (h->g.s[a]) dv *= 1.0 / h->g.dsi[a];
+  for (int q8 = 0; q8 < 8; ++q8) out[q8] = 0.0;
+  for (int b = 0; b < h->mon_blocks; ++b)
+    for (int q8 = 0; q8 < 8; ++q8) {
+      const double v = part[(size_t)b * 8 + q8];
+      if (q8 == 6)
+        out[6] = std::fmax(out[6], v);
+      else
+        out[q8] += v;
+    }
+  for (int q8 = 0; q8 < 8; ++q8)
+    if (q8 != 6) out[q8] *= dv;
+  return MISO_B200_OK;
+}
+
+int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]) {
+  if (!h || !ptrs) return MISO_B200_ERR_ARG;
+  if (h->split())
+    return h->fail(MISO_B200_ERR_STATE, "fields_view needs the FP64 form");
+  for (int f = 0; f < NF; ++f) ptrs[f] = h->q64[0][f];
+  return MISO_B200_OK;
+}
+
+int miso_b200_device_bytes(miso_b200_handle *h, size_t *bytes) {
+  if (!h || !bytes) return MISO_B200_ERR_ARG;
+  *bytes = h->bytes;
+  return MISO_B200_OK;
+}
+
+int miso_b200_launch_count(miso_b200_handle *h, long long *count) {
+  if (!h || !count) return MISO_B200_ERR_ARG;
+  *count = h->launches;
+  return MISO_B200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,30 @@
+// Host-side launch entry points of the device kernels (internal to the
+// library; the public interface is include/miso_b200.h).
+#pragma once
+
+#include "common.cuh"
+
+namespace miso_b200 {
+
+// ---- FP64 form (bit-faithful to the reference's double host path) ----
+void launch_fp64_rhs_stage(const Geom &g, const FieldPtrs<const double> &o,
+                           const FieldPtrs<const double> &a, const FieldPtrs<double> &r,
+                           const StepScalars *sc, int stage, double gm, int sms,
+                           cudaStream_t st);
+void launch_fp64_char_velocity(const Geom &g, const FieldPtrs<const double> &q, double *cc,
+                               double gm, double cs_fac, double vv_fac, double ca_fac, int sms,
+                               cudaStream_t st);
+void launch_fp64_av_sweep(const Geom &g, const FieldPtrs<const double> &q,
+                          const FieldPtrs<double> &r, const double *cc, const StepScalars *sc,
+                          int dir, double ep, double fh, int sms, cudaStream_t st);
+int cfl_partial_blocks(int sms);
+void launch_fp64_cfl(const Geom &g, const FieldPtrs<const double> &q, float *partial,
+                     StepScalars *sc, double gm, double cfl_number, double cfl_dx,
+                     double min_dxyz, int sms, cudaStream_t st);
+void launch_cfl_finalize(const float *partial, int nparts, StepScalars *sc, double cfl_number,
+                         double min_dxyz, cudaStream_t st);
+template <typename T>
+void launch_fill_ghosts(const Geom &g, const FieldPtrs<T> &q, int nfields, int sms,
+                        cudaStream_t st);
+
+}  // namespace miso_b200

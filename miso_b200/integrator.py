@@ -1,0 +1,208 @@
+"""Host-side mirror of the reference's integrator interface over the C ABI.
+
+``Integrator`` stands where ``mhd::Integrator<Real, backend::CUDA>`` stands
+in the reference (miso/include/miso/mhd_integrator_cuda.cuh:291-501):
+
+* ``Integrator(config, grid)``            -- constructor (lines 328-339)
+* ``cfl(qq=None, eos=None) -> dt``        -- Integrator::cfl (450-478)
+* ``update(dt, eos, bc, src, qq=None)``   -- Integrator::update (481-487)
+* ``apply_boundary_condition(bc, qq)``    -- (396-401)
+
+and ``MHD`` mirrors ``mhd::MHD`` (miso/include/miso/mhd.hpp:15-50), which owns
+the fields and forwards ``cfl``/``update``.  The equation of state, the
+boundary condition and the source term are the built-in ones the reference's
+MHD demos use: ideal gas with ``eos.gm``; periodic faces where
+``domain.periodic`` says so and the symmetric mirror (per-field sign) on the
+other faces; no source.  Every call goes through ``libmiso_b200.so``;
+nothing here computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .config import merge_defaults
+from .grid import Grid
+
+PRECISIONS = {"fp64": _lib.FP64, "fp32_split": _lib.FP32_SPLIT}
+
+
+class IdealEOS:
+    """Ideal-gas equation of state (miso/include/miso/eos.hpp:13-45)."""
+
+    def __init__(self, gm: float):
+        self.gm = float(gm)
+
+
+class BuiltinBoundary:
+    """Periodic / symmetric-mirror faces (the reference's HaloExchanger for
+    periodic axes plus boundary_condition::symmetric on the others)."""
+
+    def __init__(self, sign=None):
+        self.sign = np.ones((3, 2, 9)) if sign is None else np.asarray(sign, dtype=np.float64)
+
+
+class EmptySourceTerm:
+    """No source terms (miso/include/miso/mhd_model_base.hpp:131-155)."""
+
+
+def _field_ptrs(q):
+    """9 pointers into a (9, I, J, K) float64 array (numpy, host) or a torch
+    tensor (host or CUDA)."""
+    arr = (ctypes.c_void_p * 9)()
+    if isinstance(q, np.ndarray):
+        if q.dtype != np.float64 or not q.flags.c_contiguous or q.shape[0] != 9:
+            raise ValueError("fields must be a C-contiguous (9, I, J, K) float64 array")
+        for f in range(9):
+            arr[f] = q[f].ctypes.data
+        return arr
+    # torch tensor
+    if q.dtype.__str__() != "torch.float64" or not q.is_contiguous() or q.shape[0] != 9:
+        raise ValueError("fields must be a contiguous (9, I, J, K) float64 tensor")
+    for f in range(9):
+        arr[f] = q[f].data_ptr()
+    return arr
+
+
+class Integrator:
+    """One grid advanced on the current CUDA device."""
+
+    def __init__(self, config: dict, grid: Grid, sign=None, precision: str = "fp64",
+                 stream: int | None = None):
+        cfg = merge_defaults(config)
+        self.config = cfg
+        self.grid = grid
+        self.precision = precision
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        self.eos = IdealEOS(cfg["eos"]["gm"])
+        self.bc = BuiltinBoundary(sign)
+        self.src = EmptySourceTerm()
+        lib = _lib.load()
+        gd = _lib.GridDesc()
+        gd.i_size, gd.j_size, gd.k_size, gd.margin = (grid.i_size, grid.j_size, grid.k_size,
+                                                      grid.margin)
+        gd.x_min, gd.x_max, gd.y_min, gd.y_max = grid.x_min, grid.x_max, grid.y_min, grid.y_max
+        gd.z_min, gd.z_max = grid.z_min, grid.z_max
+        per = cfg["domain"]["periodic"]
+        gd.periodic[0], gd.periodic[1], gd.periodic[2] = (int(per["x"]), int(per["y"]),
+                                                          int(per["z"]))
+        for n, v in enumerate(self.bc.sign.reshape(-1)):
+            gd.sign[n] = float(v)
+        pp = _lib.Params()
+        av = cfg["mhd"]["artificial_viscosity"]
+        pp.gm = cfg["eos"]["gm"]
+        pp.cfl_number = cfg["mhd"]["cfl_number"]
+        pp.ep, pp.fh = av["ep"], av["fh"]
+        pp.cs_fac, pp.ca_fac, pp.vv_fac = av["cs_fac"], av["ca_fac"], av["vv_fac"]
+        pp.precision = PRECISIONS[precision]
+        h = ctypes.c_void_p()
+        _lib.check(lib.miso_b200_create(ctypes.byref(gd), ctypes.byref(pp),
+                                        ctypes.c_void_p(stream or 0), ctypes.byref(h)), None)
+        self._h = h
+        self._lib = lib
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.miso_b200_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, code):
+        _lib.check(code, self._h)
+
+    # -- data movement --------------------------------------------------------
+    def upload(self, q):
+        """Copy the 9 primitive fields in (numpy host array or torch tensor)."""
+        self._check(self._lib.miso_b200_upload(self._h, _field_ptrs(q)))
+
+    def download(self, out=None) -> np.ndarray:
+        """Copy the 9 primitive fields out as a (9, I, J, K) float64 array."""
+        if out is None:
+            out = np.empty((9,) + self.grid.shape, dtype=np.float64)
+        self._check(self._lib.miso_b200_download(self._h, _field_ptrs(out)))
+        return out
+
+    # -- the reference's integrator interface ---------------------------------
+    def apply_boundary_condition(self, bc=None, qq=None):
+        self._check(self._lib.miso_b200_fill_ghosts(self._h))
+
+    def cfl(self, qq=None, eos=None) -> float:
+        dt = ctypes.c_double()
+        self._check(self._lib.miso_b200_cfl(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def update(self, dt: float, eos=None, bc=None, src=None, qq=None):
+        self._check(self._lib.miso_b200_update(self._h, float(dt)))
+
+    # -- device-resident stepping --------------------------------------------
+    def update_device(self):
+        """One step with the dt of the last CFL pass, no host round trip."""
+        self._check(self._lib.miso_b200_update_device(self._h))
+
+    def run(self, nsteps: int, graph: bool = True):
+        """nsteps of (cfl, update) with dt kept on the device."""
+        self._check(self._lib.miso_b200_run(self._h, int(nsteps), int(bool(graph))))
+
+    def sync(self):
+        self._check(self._lib.miso_b200_sync(self._h))
+
+    def last_dt(self) -> float:
+        dt = ctypes.c_double()
+        self._check(self._lib.miso_b200_last_dt(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def monitors(self) -> dict:
+        out = (ctypes.c_double * 8)()
+        self._check(self._lib.miso_b200_monitors(self._h, out))
+        keys = ("mass", "mom_x", "mom_y", "mom_z", "energy", "divb_l1", "divb_max", "ph2")
+        return dict(zip(keys, list(out)))
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_size_t()
+        self._check(self._lib.miso_b200_device_bytes(self._h, ctypes.byref(b)))
+        return b.value
+
+    def launch_count(self) -> int:
+        c = ctypes.c_longlong()
+        self._check(self._lib.miso_b200_launch_count(self._h, ctypes.byref(c)))
+        return c.value
+
+
+class MHD:
+    """Fields + integrator for one grid (miso/include/miso/mhd.hpp:15-50)."""
+
+    def __init__(self, config: dict, grid: Grid, sign=None, precision: str = "fp64"):
+        self.grid = grid
+        self.integrator = Integrator(config, grid, sign=sign, precision=precision)
+
+    def apply_initial_condition(self, q):
+        """Upload initial fields and fill the ghosts (mhd.hpp:28-35)."""
+        self.integrator.upload(q)
+        self.integrator.apply_boundary_condition()
+
+    def cfl(self, eos=None) -> float:
+        return self.integrator.cfl()
+
+    def update(self, dt, eos=None, bc=None, src=None):
+        self.integrator.update(dt)
+
+    def step(self) -> float:
+        """ModelBase::update (mhd_model_base.hpp:57-62): cfl then update."""
+        dt = self.cfl()
+        self.update(dt)
+        return dt

@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the MISO MHD time step on B200.
+
+Workload (default): 3-D decaying MHD turbulence, 512^3 interior cells,
+periodic, gamma = 5/3, rho = 1, p = 1/gamma, seeded solenoidal v and B with
+1 <= |k| <= 4, E(k) ~ k^-2, Mach 0.5, beta 1 -- advanced in the FP32
+split-precision form.  One "step" is one full time step of the reference's
+ModelBase::update(): CFL reduction, 4 Runge-Kutta stages, 3 artificial-
+viscosity sweeps and the ghost fills.  The metric is cell-updates per second
+(interior cells x steps / device seconds).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank advances its own grid (independent replicas, weak
+scaling; the time is the maximum over ranks).  ``--impl reference`` times
+the reference's own CPU integrator (oracle/_ref, built from the MISO
+sources) on the host cores instead.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s/GPU (FP32-split vs FP64) and % HBM roofline at stated L1 err vs FP64"
+UNIT = "Gcell-updates/s"
+# algorithmic bytes per interior cell per step (canonical 7-pass structure:
+# 9 fields, perfect stencil reuse, derived quantities never stored)
+ALG_BYTES = {"fp32_split": 912.0, "fp64": 1248.0}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
+    ap.add_argument("--precision", choices=["fp32_split", "fp64"], default="fp32_split")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-n", type=int, default=64, help="reference CPU sample grid size per core")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# peaks, clocks
+# ---------------------------------------------------------------------------
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        with open(self.tmp.name) as f:
+            rows = [r.strip().split(",") for r in f if r.strip()]
+        os.unlink(self.tmp.name)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for nm, val in zip(names, r[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref, else the oracle restatement)
+# ---------------------------------------------------------------------------
+def _cpu_worker(args):
+    n, steps, warm, seed = args
+    from oracle import oracle as om
+    from miso_b200 import problems as P
+    lib = om.Reference() if om.reference_available() else om.Oracle()
+    prob = P.turbulence(n, seed=seed)
+    q = prob.q.copy()
+    lib.fill_ghosts(prob, q)
+    if warm:
+        lib.run(prob, q, warm, fill_first=False)
+    t = time.perf_counter()
+    lib.run(prob, q, steps, fill_first=False)
+    return time.perf_counter() - t
+
+
+def cpu_reference(n: int, steps: int, warm: int, procs: int):
+    """Reference host integrator on `procs` host cores, one independent
+    `n`^3 sample per core (the reference is single-threaded per rank)."""
+    from oracle import oracle as om
+    kind = "reference" if om.reference_available() else "port"
+    if procs == 1:
+        el = [_cpu_worker((n, steps, warm, 0))]
+    else:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            el = pool.map(_cpu_worker, [(n, steps, warm, r) for r in range(procs)])
+    value = procs * n ** 3 * steps / max(el) / 1e9
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
+            "sample": f"turbulence {n}^3 FP64, {steps} steps per core after {warm} warm-up, "
+                      f"{procs} independent process(es)"}
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+
+    from miso_b200 import problems as P
+    from miso_b200.integrator import Integrator
+
+    rank, world, local = dist_init()
+    torch.cuda.set_device(local)
+    n, K, W = args.n, args.steps, args.warmup
+    prob = P.turbulence(n, seed=0)
+    cells = prob.grid.n_interior
+    stream = torch.cuda.Stream()
+
+    def timed_run(integ, steps, graph):
+        """Device time of `steps` steps on the library's stream (CUDA events)."""
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        integ.run(steps, graph=graph)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        integ.sync()
+        barrier(world)
+        return max_over_ranks(e0.elapsed_time(e1), world)
+
+    # ---- split (or chosen) precision: warm-up, timed region, breakdown
+    integ = Integrator(prob.config, prob.grid, precision=args.precision,
+                       stream=stream.cuda_stream)
+    integ.upload(prob.q)
+    integ.apply_boundary_condition()
+    integ.run(W, graph=False)
+    integ.sync()
+    sampler = ClockSampler(local)
+    integ.set_timing(True)
+    l0 = integ.launch_count()
+    sampler.start()
+    ms = timed_run(integ, K, graph=False)
+    clocks = sampler.stop()
+    launches = integ.launch_count() - l0
+    report = integ.timing_report()
+    integ.set_timing(False)
+    value = world * cells * K / (ms / 1e3) / 1e9
+    state_split = integ.download() if not args.no_fp64 else None
+
+    # graph replay of the same step (production path)
+    ms_graph = timed_run(integ, K if K % 2 == 0 else K + 1, graph=True)
+    ms_graph_step = ms_graph / (K if K % 2 == 0 else K + 1)
+
+    # ---- e2e through the reference-facing API: cfl() -> host dt -> update(dt)
+    # -> monitors() (the step's result read back), every step
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        dt = integ.cfl()
+        integ.update(dt)
+        integ.monitors()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = {"value": world * cells * K / e2e_s / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": 96, "d2h_bytes_per_step": 96 + 8 * 8 * 2 * sms,
+           "path": "Integrator.cfl() -> update(dt) -> monitors() per step, host dt"}
+    integ.close()
+
+    # ---- FP64 comparison on the same workload (same steps)
+    fp64 = None
+    if not args.no_fp64 and args.precision != "fp64":
+        i64 = Integrator(prob.config, prob.grid, precision="fp64", stream=stream.cuda_stream)
+        i64.upload(prob.q)
+        i64.apply_boundary_condition()
+        i64.run(W, graph=False)
+        i64.sync()
+        ms64 = timed_run(i64, K, graph=False)
+        v64 = world * cells * K / (ms64 / 1e3) / 1e9
+        st64 = i64.download()
+        i64.close()
+        inner = (slice(None),) + prob.grid.interior
+        a, b = state_split[inner], st64[inner]
+        gm = prob.config["eos"]["gm"]
+
+        def l1(x, y):
+            return float(np.sum(np.abs(x - y)) / np.sum(np.abs(y)))
+        fp64 = {"value": v64, "ms_per_step": ms64 / K,
+                "split_speedup": value / v64,
+                "l1_vs_fp64_after_steps": W + K,
+                "l1_rho": l1(a[P.RO], b[P.RO]),
+                "l1_p": l1(a[P.RO] * a[P.EI] * (gm - 1), b[P.RO] * b[P.EI] * (gm - 1)),
+                "l1_B": l1(a[P.BX:P.BZ + 1], b[P.BX:P.BZ + 1])}
+
+    # ---- roofline of the dominant kernel
+    peak, peak_src = hbm_peak()
+    dom = max(report.items(), key=lambda kv: kv[1]["ms"])
+    dname, d = dom
+    achieved = (d["bytes"] / d["launches"]) / (d["ms"] / d["launches"] / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(f"{args.precision}:{dname}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+                "traffic": traffic,
+                "step_frac": value / world * ALG_BYTES[args.precision] / peak,
+                "alg_bytes_per_cell_step": ALG_BYTES[args.precision]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference(96, 3, 0, 1)
+        except Exception as exc:  # the checker may be absent on a stripped box
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "unavailable",
+                   "sample": f"{type(exc).__name__}: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32_split" else "f64",
+            "data": "synthetic (seeded solenoidal Fourier modes)",
+            "config": {"workload": f"3D decaying MHD turbulence {n}^3 periodic, "
+                                   f"{args.precision}, gamma 5/3, Mach 0.5, beta 1",
+                       "precision": args.precision, "cells_per_gpu": cells,
+                       "l2": "inputs larger than L2 (state > 1 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "ms_per_step_graph": ms_graph_step,
+            "gpu_launches": launches,
+            "kernels": {k: {"launches": v["launches"], "ms_per_step": v["ms"] / K,
+                            "GBps": v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] else None}
+                        for k, v in report.items()},
+            "roofline": roofline, "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    n = args.cpu_n
+    res = cpu_reference(n, args.steps, args.warmup, procs)
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded solenoidal Fourier modes)",
+            "config": {"workload": f"3D decaying MHD turbulence {args.n}^3 periodic "
+                                   f"(CPU sample {n}^3 per core)",
+                       "precision": "fp64 (reference host path)"},
+            "cpu_baseline": res,
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

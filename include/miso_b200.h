@@ -125,6 +125,24 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]);
  * (miso/include/miso/mhd_fields.hpp:17-34). */
 int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
 
+/* Kernel variant of one kernel class on the 3-D FP32-split path:
+ * kernel_class 0 = Runge-Kutta stage, 1/2/3 = viscosity sweep x/y/z;
+ * variant 0 = tiled (TMA plane tiles / streaming lines / warp-shuffle rows),
+ * 1 = flat (one thread per cell).  Both compute the same step; the
+ * autotuner (miso_b200/autotune.py) times them and keeps the faster.
+ * ERR_STATE on grids that use the simple per-cell kernels only. */
+int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant);
+int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant);
+
+/* Enable (1) or disable (0) per-kernel CUDA-event timing on the handle's
+ * stream (outside graph replays); clears the accumulated totals. */
+int miso_b200_set_timing(miso_b200_handle *h, int enable);
+
+/* Per-kernel totals since the last miso_b200_set_timing(), as JSON text
+ * {"name": {"launches": n, "ms": total, "bytes": algorithmic bytes}, ...}.
+ * Synchronises. */
+int miso_b200_timing_report(miso_b200_handle *h, char *buf, size_t len);
+
 /* Bytes of device memory the handle holds. */
 int miso_b200_device_bytes(miso_b200_handle *h, size_t *bytes);
 

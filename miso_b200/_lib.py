@@ -61,6 +61,11 @@ SIGNATURES = {
     "miso_b200_device_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
     "miso_b200_launch_count": (ctypes.c_int, [ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_longlong)]),
+    "miso_b200_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "miso_b200_get_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_int)]),
+    "miso_b200_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "miso_b200_timing_report": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "miso_b200_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "miso_b200_version": (ctypes.c_char_p, []),
 }

@@ -26,8 +26,12 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-Xptxas", "-warn-spills", "-I" + INCLUDE, "-I" + CSRC]
 # per-file extra flags
+FAST32 = ["--ftz=true", "--prec-div=false", "--prec-sqrt=false"]
 EXTRA = {
     "fp64_kernels.cu": ["--fmad=false"],
+    "fp32s_kernels.cu": FAST32,
+    "s32_tiled.cu": FAST32,
+    "s32_flat.cu": FAST32,
 }
 
 

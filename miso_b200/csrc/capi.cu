@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -20,6 +21,8 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "kernels_s32.h"
+#include "s32_tiled.h"
+#include "s32_flat.h"
 
 using namespace miso_b200;
 
@@ -142,7 +145,29 @@ struct miso_b200_handle {
   int cur = 0;  // which hi/lo set holds the state
 
   float *partial = nullptr;
-  int nparts = 0;
+  int nparts = 0;         // CFL partial minima used by the FP64 / untiled passes
+  int nparts_alloc = 0;   // capacity of `partial`
+
+  // tiled FP32-split path (3-D grids)
+  bool tiled = false;
+  alignas(64) unsigned char tm_hi[2][128];   // RK plane-tile maps of hi[set] (4-D: k, j, i, field)
+  alignas(64) unsigned char tm_stg[2][128];  // RK plane-tile maps of stg[set]
+  alignas(64) unsigned char tm_avh[2][128];  // AV line maps of hi[set]
+  alignas(64) unsigned char tm_avl[2][128];  // AV line maps of lo[set]
+  alignas(64) unsigned char tm_avc[128];     // AV line map of the characteristic speed
+  long long pitch = 0;                       // elements between consecutive field arrays
+  int rk_L = 64, rk_tiles_j = 0, rk_tiles_k = 0, rk_items = 0, rk_grid = 0;
+  int av_L = 64, av_grid = 0, z_grid = 0;
+  // The flat kernels run exactly one resident wave (grid = resident blocks)
+  // and stride over tiles in order, so the CTAs in flight always cover one
+  // contiguous band of planes and stencil neighbours are reused from L2.
+  int flat_grid = 0;
+  int z_parts = 0;  // CFL partial minima written by the last z sweep
+  bool partials_valid = false;  // `partial` holds CFL minima of the current state
+  // kernel variant per class on the 3-D split path: 0 = tiled (TMA plane
+  // tiles / streaming lines), 1 = flat (one thread per cell)
+  int rk_var = 0;
+  int av_var[3] = {0, 0, 0};
   double *mon_partial = nullptr;
   int mon_blocks = 0;
   StepScalars *sc = nullptr;
@@ -153,7 +178,64 @@ struct miso_b200_handle {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;          // steps captured in the graph (1 or 2)
+  int graph_cur = 0;            // hi/lo set the captured graph starts from
   long long graph_kernels = 0;  // kernels per graph launch
+
+  // Optional per-kernel CUDA-event timing (never active inside a graph
+  // capture): each timed launch is bracketed by two events on the stream.
+  struct Pending {
+    const char *name;
+    double bytes;
+    cudaEvent_t a, b;
+  };
+  struct Acc {
+    long long n = 0;
+    double ms = 0.0, bytes = 0.0;
+  };
+  bool timing = false, capturing = false;
+  std::vector<Pending> pend;
+  std::vector<cudaEvent_t> pool;
+  std::map<std::string, Acc> acc;
+
+  cudaEvent_t ev() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  int tb() {
+    if (!timing || capturing) return -1;
+    Pending pd{nullptr, 0.0, ev(), ev()};
+    cudaEventRecord(pd.a, stream);
+    pend.push_back(pd);
+    return (int)pend.size() - 1;
+  }
+  void te(int slot, const char *name, double bytes) {
+    ++launches;
+    if (slot < 0) return;
+    pend[slot].name = name;
+    pend[slot].bytes = bytes;
+    cudaEventRecord(pend[slot].b, stream);
+  }
+  void harvest() {
+    for (auto &pd : pend) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, pd.a, pd.b);
+      Acc &x = acc[pd.name ? pd.name : "?"];
+      x.n++;
+      x.ms += ms;
+      x.bytes += pd.bytes;
+      pool.push_back(pd.a);
+      pool.push_back(pd.b);
+    }
+    pend.clear();
+  }
+  double interior() const { return (double)g.n[0] * g.n[1] * g.n[2]; }
+  double ghost_cells() const { return (double)g.cells - interior(); }
 
   int fail(int code, const char *fmt, ...) {
     char buf[512];
@@ -203,6 +285,9 @@ struct miso_b200_handle {
     for (int f = 0; f < NF; ++f) r.f[f] = stg[s][f];
     return r;
   }
+  FSet fs(float *const (&arr)[NF]) const { return FSet{arr[0], pitch}; }
+  CFSet cfs(float *const (&arr)[NF]) const { return CFSet{arr[0], pitch}; }
+
   FieldPtrs<double> IO() {
     FieldPtrs<double> r;
     for (int f = 0; f < NF; ++f) r.f[f] = io64[f];
@@ -211,19 +296,25 @@ struct miso_b200_handle {
 
   // ghost fill of one field set (the split form fills hi and lo together)
   int fill64(int set) {
+    const int t = tb();
     launch_fill_ghosts<double>(g, f64(set), NF, sms, stream);
-    launches += g.s[0] + g.s[1] + g.s[2];
+    te(t, "fill_ghosts", ghost_cells() * NF * 16.0);
+    launches += g.s[0] + g.s[1] + g.s[2] - 1;
     return check_launch("fill_ghosts");
   }
   int fill_split(int s) {
+    const int t = tb();
     launch_fill_ghosts<float>(g, H(s), NF, sms, stream);
     launch_fill_ghosts<float>(g, L(s), NF, sms, stream);
-    launches += 2 * (g.s[0] + g.s[1] + g.s[2]);
+    te(t, "fill_ghosts", ghost_cells() * NF * 16.0);
+    launches += 2 * (g.s[0] + g.s[1] + g.s[2]) - 1;
     return check_launch("fill_ghosts");
   }
   int fill_stage(int s) {
+    const int t = tb();
     launch_fill_ghosts<float>(g, S(s), NF, sms, stream);
-    launches += g.s[0] + g.s[1] + g.s[2];
+    te(t, "fill_ghosts", ghost_cells() * NF * 8.0);
+    launches += g.s[0] + g.s[1] + g.s[2] - 1;
     return check_launch("fill_ghosts");
   }
 
@@ -246,13 +337,29 @@ struct miso_b200_handle {
   }
 
   int enqueue_cfl() {
+    const int t = tb();
+    if (split() && tiled) {
+      if (!partials_valid) {
+        launch_s32_cfl_partial(g, cst(H(cur)), partial, z_grid, sc, p.gm, cfl_dx, stream);
+        te(t, "cfl", interior() * 32.0);
+        const int t2 = tb();
+        launch_cfl_finalize(partial, z_grid, sc, p.cfl_number, min_dxyz, stream);
+        te(t2, "cfl_finalize", 0.0);
+      } else {
+        launch_cfl_finalize(partial, z_parts, sc, p.cfl_number, min_dxyz, stream);
+        te(t, "cfl_finalize", 0.0);
+      }
+      return check_launch("cfl");
+    }
     if (split()) {
       launch_s32_cfl_partial(g, cst(H(cur)), partial, nparts, sc, p.gm, cfl_dx, stream);
       launch_cfl_finalize(partial, nparts, sc, p.cfl_number, min_dxyz, stream);
+      te(t, "cfl", interior() * 32.0);
     } else {
       launch_fp64_cfl(g, c64(0), partial, sc, p.gm, p.cfl_number, cfl_dx, min_dxyz, sms, stream);
+      te(t, "cfl", interior() * 64.0);
     }
-    launches += 2;
+    launches += 1;
     return check_launch("cfl");
   }
 
@@ -263,32 +370,37 @@ struct miso_b200_handle {
       const int seq_a[4] = {0, 1, 2, 1};
       const int seq_r[4] = {1, 2, 1, 2};
       for (int s = 0; s < 4; ++s) {
+        const int t = tb();
         launch_fp64_rhs_stage(g, c64(0), c64(seq_a[s]), f64(seq_r[s]), sc, s, p.gm, sms, stream);
-        launches++;
+        te(t, "rk_stage", interior() * (s == 0 ? 144.0 : 216.0));
         if ((rc = check_launch("rhs_stage"))) return rc;
         if ((rc = fill64(seq_r[s]))) return rc;
       }
       // AV on B(2): x: B -> qq, y: qq -> A, z: A -> qq
+      int t = tb();
       launch_fp64_char_velocity(g, c64(2), cc64, p.gm, p.cs_fac, p.vv_fac, p.ca_fac, sms,
                                 stream);
-      launches++;
+      te(t, "char_velocity", (double)g.cells * 72.0);
       const int src[3] = {2, 0, 1}, dst[3] = {0, 1, 0};
       for (int d = 0; d < 3; ++d) {
+        t = tb();
         launch_fp64_av_sweep(g, c64(src[d]), f64(dst[d]), cc64, sc, d, p.ep, p.fh, sms, stream);
-        launches++;
+        te(t, "av_sweep", interior() * 152.0);
         if ((rc = check_launch("av_sweep"))) return rc;
         if ((rc = fill64(dst[d]))) return rc;
       }
       return MISO_B200_OK;
     }
+    if (tiled) return enqueue_update_tiled();
     // FP32 split: stage 0 reads hi, stages write stg[0], stg[1], stg[0];
     // stage 3 accumulates into hi/lo of the current set.
     const int c = cur;
     for (int s = 0; s < 4; ++s) {
       FieldPtrs<const float> prev = s == 0 ? cst(H(c)) : cst(S((s - 1) & 1));
       FieldPtrs<float> out = s < 3 ? S(s & 1) : S(0);
+      const int t = tb();
       launch_s32_rk_stage(g, prev, H(c), L(c), out, sc, s, p.gm, sms, stream);
-      launches++;
+      te(t, "rk_stage", interior() * (s == 0 ? 72.0 : s < 3 ? 108.0 : 180.0));
       if ((rc = check_launch("rk_stage"))) return rc;
       if (s < 3) {
         if ((rc = fill_stage(s & 1))) return rc;
@@ -296,17 +408,87 @@ struct miso_b200_handle {
         if ((rc = fill_split(c))) return rc;
       }
     }
+    int t = tb();
     launch_s32_char_velocity(g, cst(H(c)), cc32, p.gm, p.cs_fac, p.vv_fac, p.ca_fac, sms, stream);
-    launches++;
+    te(t, "char_velocity", (double)g.cells * 40.0);
     for (int d = 0; d < 3; ++d) {
       if (!g.s[d]) continue;  // a degenerate sweep leaves the conserved state unchanged
+      t = tb();
       launch_s32_av_sweep(g, cst(H(cur)), cst(L(cur)), H(cur ^ 1), L(cur ^ 1), cc32, sc, d, p.ep,
                           p.fh, sms, stream);
-      launches++;
+      te(t, "av_sweep", interior() * 148.0);
       if ((rc = check_launch("av_sweep"))) return rc;
       cur ^= 1;
       if ((rc = fill_split(cur))) return rc;
     }
+    return MISO_B200_OK;
+  }
+
+  // Tiled FP32-split step: 4 RK stage launches and 3 viscosity sweeps; ghost
+  // images, the characteristic speed and the next step's CFL minima are
+  // written by those kernels themselves.
+  int enqueue_update_tiled() {
+    int rc;
+    const int c = cur;
+    for (int st = 0; st < 4; ++st) {
+      RkArgs a;
+      a.g = g;
+      a.u0 = cfs(hi[c]);
+      a.hi = fs(hi[c]);
+      a.lo = fs(lo[c]);
+      a.out = fs(stg[st & 1]);
+      a.cc = cc32;
+      a.sc = sc;
+      a.err = &sc->err;
+      a.gm = (float)p.gm;
+      a.gm1 = (float)(p.gm - 1.0);
+      a.cs_fac = (float)p.cs_fac;
+      a.vv_fac = (float)p.vv_fac;
+      a.ca_fac = (float)p.ca_fac;
+      a.L = rk_L;
+      a.tiles_j = rk_tiles_j;
+      a.tiles_k = rk_tiles_k;
+      a.items = rk_items;
+      const void *tm = st == 0 ? (const void *)tm_hi[c] : (const void *)tm_stg[(st - 1) & 1];
+      const int t = tb();
+      if (rk_var == 1)
+        launch_s32_rk_flat(st == 0 ? cfs(hi[c]) : cfs(stg[(st - 1) & 1]), a, st, flat_grid,
+                           stream);
+      else
+        launch_s32_rk_tiled(tm, a, st, rk_grid, stream);
+      te(t, "rk_stage", interior() * (st == 0 ? 72.0 : st < 3 ? 108.0 : 184.0));
+      if ((rc = check_launch("rk_stage"))) return rc;
+    }
+    for (int d = 0; d < 3; ++d) {
+      AvArgs a;
+      a.g = g;
+      a.hi = cfs(hi[cur]);
+      a.lo = cfs(lo[cur]);
+      a.hi2 = fs(hi[cur ^ 1]);
+      a.lo2 = fs(lo[cur ^ 1]);
+      a.cc = cc32;
+      a.sc = sc;
+      a.err = &sc->err;
+      a.partial = d == 2 ? partial : nullptr;
+      a.ep = (float)p.ep;
+      a.fh = (float)p.fh;
+      a.gm = (float)p.gm;
+      a.gm1 = (float)(p.gm - 1.0);
+      a.cfl_dx = (float)cfl_dx;
+      a.L = av_L;
+      const int t = tb();
+      if (av_var[d] == 1)
+        launch_s32_av_flat(a, d, flat_grid, stream);
+      else if (d < 2)
+        launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, av_grid, stream);
+      else
+        launch_s32_av_z(a, z_grid, stream);
+      te(t, "av_sweep", interior() * 148.0);
+      if ((rc = check_launch("av_sweep"))) return rc;
+      cur ^= 1;
+    }
+    z_parts = av_var[2] == 1 ? flat_grid : z_grid;
+    partials_valid = true;
     return MISO_B200_OK;
   }
 
@@ -378,8 +560,13 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
     const double sp = (hi[a] - lo[a]) / (double)sz[a];
     ds[a] = g.s[a] ? sp : 1.e30;
     g.dsi[a] = g.s[a] ? 1.0 / sp : 0.0;
-    for (int side = 0; side < 2; ++side)
-      for (int f = 0; f < NF; ++f) g.sign[a][side][f] = (float)(gd->sign[a][side][f] < 0 ? -1 : 1);
+    for (int side = 0; side < 2; ++side) {
+      g.negmask[a][side] = 0;
+      for (int f = 0; f < NF; ++f) {
+        g.sign[a][side][f] = (float)(gd->sign[a][side][f] < 0 ? -1 : 1);
+        if (!g.periodic[a] && gd->sign[a][side][f] < 0) g.negmask[a][side] |= (unsigned short)(1u << f);
+      }
+    }
   }
   g.st[2] = 1;
   g.st[1] = g.t[2];
@@ -409,6 +596,9 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   }
 
   h->nparts = cfl_partial_blocks(h->sms);
+  h->z_grid = 8 * h->sms;
+  h->av_grid = 16 * h->sms;
+  h->nparts_alloc = h->nparts > h->z_grid ? h->nparts : h->z_grid;
   h->mon_blocks = h->sms * 2;
   const size_t cells = (size_t)g.cells;
   size_t total = 0;
@@ -422,16 +612,17 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
       for (int f = 0; f < NF; ++f) add((void **)&h->q64[s][f], cells * sizeof(double));
     add((void **)&h->cc64, cells * sizeof(double));
   } else {
-    for (int s = 0; s < 2; ++s)
-      for (int f = 0; f < NF; ++f) {
-        add((void **)&h->hi[s][f], cells * sizeof(float));
-        add((void **)&h->lo[s][f], cells * sizeof(float));
-      }
+    // each set of 9 arrays is contiguous with one pitch, so a 4-D tensor
+    // map (k, j, i, field) can address it
+    for (int s = 0; s < 2; ++s) {
+      for (int f = 0; f < NF; ++f) add((void **)&h->hi[s][f], cells * sizeof(float));
+      for (int f = 0; f < NF; ++f) add((void **)&h->lo[s][f], cells * sizeof(float));
+    }
     for (int s = 0; s < 2; ++s)
       for (int f = 0; f < NF; ++f) add((void **)&h->stg[s][f], cells * sizeof(float));
     add((void **)&h->cc32, cells * sizeof(float));
   }
-  add((void **)&h->partial, sizeof(float) * h->nparts);
+  add((void **)&h->partial, sizeof(float) * h->nparts_alloc);
   add((void **)&h->mon_partial, sizeof(double) * 8 * h->mon_blocks);
   add((void **)&h->sc, sizeof(StepScalars));
   e = cudaMalloc(&h->block, total);
@@ -453,6 +644,29 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
     // state between steps.
     for (int f = 0; f < NF; ++f) h->io64[f] = (double *)h->stg[0][0] + (size_t)f * cells;
   }
+  h->pitch = (long long)(round_up(cells * sizeof(float)) / sizeof(float));
+  if (h->split() && s32_tiled_supported(g) && !getenv("MISO_B200_UNTILED")) {
+    const size_t pb = round_up(cells * sizeof(float));
+    bool ok = s32_configure() == 0;
+    for (int s = 0; s < 2 && ok; ++s) {
+      ok = s32_make_tmap(g, h->hi[s][0], pb, 0, h->tm_hi[s]) == 0 &&
+           s32_make_tmap(g, h->stg[s][0], pb, 0, h->tm_stg[s]) == 0 &&
+           s32_make_tmap(g, h->hi[s][0], pb, 1, h->tm_avh[s]) == 0 &&
+           s32_make_tmap(g, h->lo[s][0], pb, 1, h->tm_avl[s]) == 0;
+    }
+    if (ok) ok = s32_make_tmap_cc(g, h->cc32, h->tm_avc) == 0;
+    if (ok) {
+      h->tiled = true;
+      s32_rk_items(g, h->rk_L, h->rk_tiles_j, h->rk_tiles_k, h->rk_items);
+      const int per_sm = 2;
+      h->rk_grid = h->rk_items < per_sm * h->sms ? h->rk_items : per_sm * h->sms;
+      h->av_grid = 3 * h->sms;
+      h->flat_grid = 3 * h->sms;  // 256 threads x 80 registers: 3 resident CTAs per SM
+      if (const char *v = getenv("MISO_B200_RK")) h->rk_var = strcmp(v, "flat") == 0 ? 1 : 0;
+      if (const char *v = getenv("MISO_B200_AV"))
+        for (int d = 0; d < 3 && v[d]; ++d) h->av_var[d] = v[d] == 'f' ? 1 : 0;
+    }
+  }
   e = cudaMemsetAsync(h->block, 0, total, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
@@ -468,6 +682,8 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
 int miso_b200_destroy(miso_b200_handle *h) {
   if (!h) return MISO_B200_ERR_ARG;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  h->harvest();
+  for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->block) cudaFree(h->block);
@@ -490,6 +706,7 @@ int miso_b200_upload(miso_b200_handle *h, const double *const q[9]) {
     FieldPtrs<const double> src;
     for (int f = 0; f < NF; ++f) src.f[f] = h->io64[f];
     h->cur = 0;
+    h->partials_valid = false;
     launch_s32_to_split(h->g.cells, src, h->H(0), h->L(0), h->sms, h->stream);
     h->launches++;
     if ((rc = h->check_launch("to_split"))) return rc;
@@ -561,15 +778,33 @@ int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
     }
     return MISO_B200_OK;
   }
+  // The tiled split path computes the next step's CFL minima inside the last
+  // viscosity sweep; a captured step assumes they are present, so a state
+  // that has not been stepped yet takes one eager step first.
+  if (h->tiled && !h->partials_valid && nsteps > 0) {
+    if ((rc = h->enqueue_cfl())) return rc;
+    if ((rc = h->enqueue_update())) return rc;
+    --nsteps;
+  }
+  if (nsteps == 0) return MISO_B200_OK;
   // The split form swaps its hi/lo sets once per AV sweep; when a step
   // swaps an odd number of times the captured graph covers two steps so
   // that it starts and ends on the same set.
+  if (h->graph_exec && h->graph_cur != h->cur) {
+    // captured for the other hi/lo set: capture again
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
   if (!h->graph_exec) {
     const int before = h->cur;
+    const bool valid_before = h->partials_valid;
     const long long l0 = h->launches;
     if ((rc = h->cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal),
                       "begin capture")))
       return rc;
+    h->capturing = true;
     int steps = 1;
     rc = h->enqueue_cfl();
     if (!rc) rc = h->enqueue_update();
@@ -580,7 +815,9 @@ int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
     }
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    h->capturing = false;
     h->cur = before;
+    h->partials_valid = valid_before;
     const long long kernels = h->launches - l0;
     h->launches = l0;
     if (rc) {
@@ -593,12 +830,17 @@ int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
       return rc;
     h->graph_steps = steps;
     h->graph_kernels = kernels;
+    h->graph_cur = before;
   }
-  if (nsteps % h->graph_steps)
-    return h->fail(MISO_B200_ERR_ARG, "nsteps must be a multiple of %d", h->graph_steps);
-  for (int n = 0; n < nsteps; n += h->graph_steps) {
+  const int reps = nsteps / h->graph_steps, rem = nsteps % h->graph_steps;
+  for (int n = 0; n < reps; ++n) {
     if ((rc = h->cuda(cudaGraphLaunch(h->graph_exec, h->stream), "graph launch"))) return rc;
     h->launches += h->graph_kernels;
+  }
+  if (reps > 0 && h->tiled) h->partials_valid = true;
+  for (int n = 0; n < rem; ++n) {
+    if ((rc = h->enqueue_cfl())) return rc;
+    if ((rc = h->enqueue_update())) return rc;
   }
   return MISO_B200_OK;
 }
@@ -662,6 +904,63 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]) {
   if (h->split())
     return h->fail(MISO_B200_ERR_STATE, "fields_view needs the FP64 form");
   for (int f = 0; f < NF; ++f) ptrs[f] = h->q64[0][f];
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
+  if (!h || kernel_class < 0 || kernel_class > 3 || variant < 0 || variant > 1)
+    return MISO_B200_ERR_ARG;
+  if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "kernel variants apply to 3-D split grids");
+  if (kernel_class == 0)
+    h->rk_var = variant;
+  else
+    h->av_var[kernel_class - 1] = variant;
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant) {
+  if (!h || !variant || kernel_class < 0 || kernel_class > 3) return MISO_B200_ERR_ARG;
+  if (!h->tiled) {
+    *variant = -1;
+    return MISO_B200_OK;
+  }
+  *variant = kernel_class == 0 ? h->rk_var : h->av_var[kernel_class - 1];
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_timing(miso_b200_handle *h, int enable) {
+  if (!h) return MISO_B200_ERR_ARG;
+  int rc = h->cuda(cudaStreamSynchronize(h->stream), "synchronize");
+  if (rc) return rc;
+  h->harvest();
+  h->acc.clear();
+  h->timing = enable != 0;
+  return MISO_B200_OK;
+}
+
+int miso_b200_timing_report(miso_b200_handle *h, char *buf, size_t len) {
+  if (!h || !buf || len == 0) return MISO_B200_ERR_ARG;
+  int rc = h->cuda(cudaStreamSynchronize(h->stream), "synchronize");
+  if (rc) return rc;
+  h->harvest();
+  std::string out = "{";
+  bool first = true;
+  for (auto &kv : h->acc) {
+    char item[256];
+    snprintf(item, sizeof item, "%s\"%s\": {\"launches\": %lld, \"ms\": %.6f, \"bytes\": %.1f}",
+             first ? "" : ", ", kv.first.c_str(), kv.second.n, kv.second.ms, kv.second.bytes);
+    out += item;
+    first = false;
+  }
+  out += "}";
+  if (out.size() + 1 > len) return h->fail(MISO_B200_ERR_ARG, "buffer too small");
+  memcpy(buf, out.c_str(), out.size() + 1);
   return MISO_B200_OK;
 }
 

@@ -34,6 +34,7 @@ struct Geom {
   double dsi[3];    // inverse spacing per axis (0 on a degenerate axis)
   int periodic[3];
   float sign[3][2][NF];  // mirror sign on non-periodic faces
+  unsigned short negmask[3][2];  // bit f set where sign[a][side][f] < 0 (0 on periodic axes)
 };
 
 // Per-step scalars, resident in device memory so a whole step can run
@@ -53,6 +54,7 @@ struct StepScalars {
 };
 
 constexpr unsigned int ERRBIT_NONFINITE = 1u;
+constexpr unsigned int ERRBIT_TIMEOUT = 2u;  // a bounded device-side wait ran out
 
 // utility.hpp:91-124: util::min2/max2/min3/max3 only have float overloads,
 // so double operands are rounded to float and the float result widened

@@ -1,0 +1,728 @@
+// Tiled FP32 split-precision kernels for 3-D grids (every axis of size > 1).
+//
+// Runge-Kutta stage (rk_tiled_kernel):
+//   A CTA owns a TJ x TK tile of (j, k) columns and marches along i over a
+//   chunk of planes.  Each plane of the previous stage state -- 9 conserved
+//   fields on the tile plus a 2-cell halo in j and k -- arrives in shared
+//   memory by one TMA bulk-tensor copy (4-D tensor map: k, j, i, field),
+//   NBUF planes in flight.  Every point's flux vectors along y and z are
+//   formed once per plane and kept in shared memory for the 4th-order
+//   differences; the flux along the march axis goes into a 5-plane register
+//   queue, and each difference is formed as (F[-2] - F[+2]) + 8 (F[+1] -
+//   F[-1]), exactly zero for a locally constant flux.  Results are written
+//   with their ghost images (periodic wrap / mirror), so no ghost-fill pass
+//   runs; the last stage also writes the characteristic speed.
+//
+// Artificial viscosity:
+//   x and y sweeps (av_line_kernel) stream along their axis: a CTA of 128
+//   threads owns 128 consecutive k cells of one line; per plane one TMA
+//   copy each brings hi, lo and the characteristic speed (k box of 132
+//   cells), and a register queue carries the limiter slopes and face
+//   fluxes, so each face flux and each slope is evaluated once.  The z
+//   sweep (contiguous axis, av_z_kernel) exchanges neighbours with warp
+//   shuffles and folds the CFL candidate of the new state into per-block
+//   minima.
+//
+// Physics as in fp32s_kernels.cu (flux form of mhd_integrator_host.hpp:
+// 57-247; limiter.hpp:11-37; mhd_artificial_viscosity_host.hpp:51-348).
+#include <cuda.h>
+
+#include "common.cuh"
+#include "s32_tiled.h"
+#include "s32_common.cuh"
+
+namespace miso_b200 {
+namespace s32t {
+
+// ---------------------------------------------------------------------------
+// mbarrier / TMA
+// ---------------------------------------------------------------------------
+constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s: far beyond any copy
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bounded wait for phase `parity`; false on timeout.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  const unsigned a = smem_u32(bar);
+  const long long t0 = clock64();
+  while (true) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > WAIT_CYCLES) return false;
+  }
+}
+__device__ __forceinline__ void tma4(const CUtensorMap *tm, void *dst, unsigned long long *bar,
+                                     int c0, int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"((unsigned long long)tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma3(const CUtensorMap *tm, void *dst, unsigned long long *bar,
+                                     int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"((unsigned long long)tm), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// RK stage kernel
+// ---------------------------------------------------------------------------
+constexpr int TJ = 8, TK = 32, HJ = TJ + 4, HK = TK + 4;
+constexpr int NTHR = TJ * TK;  // 256
+constexpr int NBUF = 3;
+constexpr int PLANE_BYTES = NF * HJ * HK * 4;                  // TMA bytes per plane
+constexpr int PLANE_STRIDE = (PLANE_BYTES + 127) / 128 * 128;  // 128-byte aligned buffers
+
+struct __align__(128) RkSmem {
+  unsigned char plane[NBUF][PLANE_STRIDE];
+  float fy[NF][HJ][TK];
+  float fz[NF][TJ][HK];
+  unsigned long long bar[NBUF];
+  int abort;
+};
+
+struct March {
+  float F1[NF], F2[NF], F3[NF], F4[NF];  // x flux at planes q-1 .. q-4
+  float Dyz1[NF], Dyz2[NF];              // y+z differences of cells q-1, q-2
+};
+
+template <int STAGE>
+__device__ __forceinline__ void rk_plane(const RkArgs &a, RkSmem &sm, const float *pl, March &ms,
+                                         int q, int i_start, int i_end, int jj, int kk,
+                                         int tid, float ch2, float dt, float decay) {
+  const int ty = tid / TK, tx = tid % TK;
+  const Geom &g = a.g;
+  const float wx = (float)(g.dsi[0] * INV12);
+  const float wy = (float)(g.dsi[1] * INV12);
+  const float wz = (float)(g.dsi[2] * INV12);
+  float Fn[NF];
+  const bool need_yz = q >= i_start && q < i_end;
+  {
+    float u[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) u[f] = pl[(f * HJ + ty + 2) * HK + tx + 2];
+    PrimF p;
+    prim(u, a.gm1, p);
+    if (need_yz) {
+      float F[NF];
+      flux_dir<1>(u, p, ch2, F);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) sm.fy[f][ty + 2][tx] = F[f];
+      flux_dir<2>(u, p, ch2, F);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) sm.fz[f][ty][tx + 2] = F[f];
+    }
+    flux_dir<0>(u, p, ch2, Fn);
+  }
+  // halo fluxes (y rows above/below, z columns left/right)
+  if (need_yz && tid < 4 * TK + 4 * TJ) {
+    float uh[NF], Fh[NF];
+    PrimF ph;
+    if (tid < 4 * TK) {
+      const int r = tid / TK, col = tid % TK;
+      const int row = r < 2 ? r : TJ + r;  // 0, 1, TJ+2, TJ+3
+#pragma unroll
+      for (int f = 0; f < NF; ++f) uh[f] = pl[(f * HJ + row) * HK + col + 2];
+      prim(uh, a.gm1, ph);
+      flux_dir<1>(uh, ph, ch2, Fh);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) sm.fy[f][row][col] = Fh[f];
+    } else {
+      const int e = tid - 4 * TK;
+      const int row = e / 4, c = e % 4;
+      const int col = c < 2 ? c : TK + c;  // 0, 1, TK+2, TK+3
+#pragma unroll
+      for (int f = 0; f < NF; ++f) uh[f] = pl[(f * HJ + row + 2) * HK + col];
+      prim(uh, a.gm1, ph);
+      flux_dir<2>(uh, ph, ch2, Fh);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) sm.fz[f][row][col] = Fh[f];
+    }
+  }
+  __syncthreads();  // (A) fluxes visible; the plane buffer is free
+  float Dyz[NF];
+  if (need_yz) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const float dy = (sm.fy[f][ty][tx] - sm.fy[f][ty + 4][tx]) +
+                       8.0f * (sm.fy[f][ty + 3][tx] - sm.fy[f][ty + 1][tx]);
+      const float dz = (sm.fz[f][ty][tx] - sm.fz[f][ty][tx + 4]) +
+                       8.0f * (sm.fz[f][ty][tx + 3] - sm.fz[f][ty][tx + 1]);
+      Dyz[f] = wy * dy + wz * dz;
+    }
+  }
+  // output of the centre cell c = q-2
+  const int c = q - 2;
+  const int jg = jj + ty, kg = kk + tx;
+  if (c >= i_start && c < i_end && jg < g.n[1] && kg < g.n[2]) {
+    float D[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+      D[f] = wx * ((ms.F4[f] - Fn[f]) + 8.0f * (ms.F1[f] - ms.F3[f])) + ms.Dyz2[f];
+    const int cell = cell_of(g, c, jg, kg);
+    const bool nb = near_boundary(g, c, jg, kg);
+    Img im;
+    if (nb) make_img(g, c, jg, kg, im);
+    if (STAGE < 3) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const float u0 = __ldg(a.u0.p + f * a.u0.pitch + cell);
+        float v = u0 - dt * D[f];
+        if (f == PH) v *= decay;
+        store_cell(a.out.p + f * a.out.pitch, cell, nb, im, f, v);
+      }
+    } else {
+      float sv[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        float *hp = a.hi.p + f * a.hi.pitch;
+        float *lp = a.lo.p + f * a.lo.pitch;
+        const float h = hp[cell], l = lp[cell];
+        float e;
+        if (f == PH) {
+          float t;
+          two_sum(h, l - dt * D[f], sv[f], t);
+          const float pr = sv[f] * decay;
+          const float pe = fmaf(sv[f], decay, -pr);
+          two_sum(pr, pe + t * decay, sv[f], e);
+        } else {
+          two_sum(h, l - dt * D[f], sv[f], e);
+        }
+        store_cell(hp, cell, nb, im, f, sv[f]);
+        store_cell(lp, cell, nb, im, f, e);
+      }
+      float cs, vv, ca, ein;
+      speeds(sv, a.gm, a.gm1, cs, vv, ca, ein);
+      store_cell(a.cc, cell, nb, im, NF, cs * a.cs_fac + vv * a.vv_fac + ca * a.ca_fac);
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    ms.F4[f] = ms.F3[f];
+    ms.F3[f] = ms.F2[f];
+    ms.F2[f] = ms.F1[f];
+    ms.F1[f] = Fn[f];
+    ms.Dyz2[f] = ms.Dyz1[f];
+    ms.Dyz1[f] = need_yz ? Dyz[f] : 0.0f;
+  }
+}
+
+struct Item {
+  int tj, tk, i_start, i_end;
+};
+
+__device__ __forceinline__ Item item_of(const RkArgs &a, int it) {
+  Item r;
+  const int per_chunk = a.tiles_j * a.tiles_k;
+  const int ch = it / per_chunk, rem = it % per_chunk;
+  r.tj = rem / a.tiles_k;
+  r.tk = rem % a.tiles_k;
+  r.i_start = ch * a.L;
+  r.i_end = min(a.g.n[0], r.i_start + a.L);
+  return r;
+}
+
+// Producer cursor over the (item, plane) sequence of this CTA.
+struct RkCursor {
+  int it, q;
+  Item cur;
+  __device__ void begin(const RkArgs &a) {
+    it = blockIdx.x;
+    if (it < a.items) {
+      cur = item_of(a, it);
+      q = cur.i_start - 2;
+    }
+  }
+  __device__ bool valid(const RkArgs &a) const { return it < a.items; }
+  __device__ void next(const RkArgs &a) {
+    if (++q > cur.i_end + 1) {
+      it += gridDim.x;
+      if (it < a.items) {
+        cur = item_of(a, it);
+        q = cur.i_start - 2;
+      }
+    }
+  }
+};
+
+template <int STAGE>
+__global__ void __launch_bounds__(NTHR, 2)
+rk_tiled_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  RkSmem &sm = *reinterpret_cast<RkSmem *>(smem_raw);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int b = 0; b < NBUF; ++b) mbar_init(&sm.bar[b], 1);
+    sm.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if ((int)blockIdx.x >= a.items) return;
+  const float ch2 = (float)a.sc->ch2;
+  const float dt = (float)a.sc->dts[STAGE];
+  const float decay = (float)a.sc->ph_decay[STAGE];
+
+  RkCursor prod;
+  long long issued = 0;
+  if (tid == 0) {
+    prod.begin(a);
+    for (int b = 0; b < NBUF && prod.valid(a); ++b) {
+      mbar_expect_tx(&sm.bar[b], PLANE_BYTES);
+      tma4(&tm, sm.plane[b], &sm.bar[b], prod.cur.tk * TK, prod.cur.tj * TJ, prod.q + a.g.m[0], 0);
+      prod.next(a);
+      ++issued;
+    }
+  }
+  long long seq = 0;
+  March ms;
+  for (int it = blockIdx.x; it < a.items; it += gridDim.x) {
+    const Item itm = item_of(a, it);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      ms.F1[f] = ms.F2[f] = ms.F3[f] = ms.F4[f] = 0.0f;
+      ms.Dyz1[f] = ms.Dyz2[f] = 0.0f;
+    }
+    for (int q = itm.i_start - 2; q <= itm.i_end + 1; ++q, ++seq) {
+      const int b = (int)(seq % NBUF);
+      if (tid == 0 && !mbar_wait(&sm.bar[b], (unsigned)((seq / NBUF) & 1))) sm.abort = 1;
+      __syncthreads();
+      if (sm.abort) {
+        if (tid == 0) {
+          atomicOr(a.err, ERRBIT_TIMEOUT);
+          // drain the copies still in flight (bounded) before the CTA exits
+          for (long long s2 = seq + 1; s2 < issued; ++s2)
+            mbar_wait(&sm.bar[s2 % NBUF], (unsigned)((s2 / NBUF) & 1));
+        }
+        return;
+      }
+      const float *pl = reinterpret_cast<const float *>(sm.plane[b]);
+      rk_plane<STAGE>(a, sm, pl, ms, q, itm.i_start, itm.i_end, itm.tj * TJ, itm.tk * TK, tid,
+                      ch2, dt, decay);
+      // every thread is past barrier (A) inside rk_plane: the plane buffer
+      // is free; refill it with the plane NBUF ahead
+      if (tid == 0 && prod.valid(a)) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&sm.bar[b], PLANE_BYTES);
+        tma4(&tm, sm.plane[b], &sm.bar[b], prod.cur.tk * TK, prod.cur.tj * TJ,
+             prod.q + a.g.m[0], 0);
+        prod.next(a);
+        ++issued;
+      }
+      __syncthreads();  // (B) fy/fz reads done before the next plane's writes
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Artificial viscosity
+// ---------------------------------------------------------------------------
+// ---- x / y line sweep ----
+constexpr int LK = 128;       // k cells per CTA
+constexpr int LBOX = LK + 4;  // k box of the TMA copies
+constexpr int LNB = 6;        // slots (3 planes in use, 3 in flight)
+constexpr int L_HI = 0;
+constexpr int L_LO = (NF * LBOX * 4 + 127) / 128 * 128;
+constexpr int L_CC = L_LO + L_LO;
+constexpr int L_SLOT = L_CC + (LBOX * 4 + 127) / 128 * 128;
+constexpr unsigned L_TX = 2 * NF * LBOX * 4 + LBOX * 4;  // bytes per slot fill
+
+struct __align__(128) LineSmem {
+  unsigned char slot[LNB][L_SLOT];
+  unsigned long long bar[LNB];
+  int abort;
+};
+
+struct LineItem {
+  int kb, u, t0, t1;
+};
+
+template <int DIR>
+__device__ __forceinline__ LineItem line_item(const AvArgs &a, int it, int kblocks, int nu) {
+  LineItem r;
+  r.kb = it % kblocks;
+  const int r1 = it / kblocks;
+  r.u = r1 % nu;
+  const int ch = r1 / nu;
+  r.t0 = ch * a.L;
+  r.t1 = min(a.g.n[DIR], r.t0 + a.L);
+  return r;
+}
+
+template <int DIR>
+struct LineCursor {
+  int it, p;
+  LineItem cur;
+  __device__ void begin(const AvArgs &a, int kblocks, int nu, int items) {
+    it = blockIdx.x;
+    if (it < items) {
+      cur = line_item<DIR>(a, it, kblocks, nu);
+      p = cur.t0 - 2;
+    }
+  }
+  __device__ bool valid(int items) const { return it < items; }
+  __device__ void next(const AvArgs &a, int kblocks, int nu, int items) {
+    if (++p > cur.t1 + 1) {
+      it += gridDim.x;
+      if (it < items) {
+        cur = line_item<DIR>(a, it, kblocks, nu);
+        p = cur.t0 - 2;
+      }
+    }
+  }
+};
+
+template <int DIR>
+__device__ __forceinline__ void line_issue(const CUtensorMap *thi, const CUtensorMap *tlo,
+                                           const CUtensorMap *tcc, LineSmem &sm, int s,
+                                           const Geom &g, const LineItem &it, int p) {
+  unsigned char *sl = sm.slot[s];
+  const int k0 = it.kb * LK;
+  const int cj = DIR == 0 ? it.u + g.m[1] : p + g.m[1];
+  const int ci = DIR == 0 ? p + g.m[0] : it.u + g.m[0];
+  mbar_expect_tx(&sm.bar[s], L_TX);
+  tma4(thi, sl + L_HI, &sm.bar[s], k0, cj, ci, 0);
+  tma4(tlo, sl + L_LO, &sm.bar[s], k0, cj, ci, 0);
+  tma3(tcc, sl + L_CC, &sm.bar[s], k0, cj, ci);
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(LK, 3)
+av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CUtensorMap tlo,
+               const __grid_constant__ CUtensorMap tcc, const AvArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  LineSmem &sm = *reinterpret_cast<LineSmem *>(smem_raw);
+  const Geom &g = a.g;
+  constexpr int OTH = DIR == 0 ? 1 : 0;
+  const int tid = threadIdx.x;
+  const int nk = g.n[2], nu = g.n[OTH];
+  const int kblocks = (nk + LK - 1) / LK;
+  const int chunks = (g.n[DIR] + a.L - 1) / a.L;
+  const int items = kblocks * nu * chunks;
+  if (tid == 0) {
+    for (int b = 0; b < LNB; ++b) mbar_init(&sm.bar[b], 1);
+    sm.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if ((int)blockIdx.x >= items) return;
+  const float fac = (float)(g.dsi[DIR] * a.sc->dt);
+  LineCursor<DIR> prod;
+  long long issued = 0;
+  if (tid == 0) {
+    prod.begin(a, kblocks, nu, items);
+    for (int s = 0; s < LNB && prod.valid(items); ++s) {
+      line_issue<DIR>(&thi, &tlo, &tcc, sm, s, g, prod.cur, prod.p);
+      prod.next(a, kblocks, nu, items);
+      ++issued;
+    }
+  }
+  long long seq = 0;
+  float wm2[NW], wm1[NW], w0[NW], w1[NW], dq0[NW], F0[NW];
+  float ccm1 = 0.f, cc0 = 0.f, cc1 = 0.f;
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    const LineItem li = line_item<DIR>(a, it, kblocks, nu);
+    const int k = li.kb * LK + tid;
+    const bool active = k < nk;
+    for (int p = li.t0 - 2; p <= li.t1 + 1; ++p, ++seq) {
+      const int s = (int)(seq % LNB);
+      if (tid == 0 && !mbar_wait(&sm.bar[s], (unsigned)((seq / LNB) & 1))) sm.abort = 1;
+      __syncthreads();
+      if (sm.abort) {
+        if (tid == 0) {
+          atomicOr(a.err, ERRBIT_TIMEOUT);
+          for (long long s2 = seq + 1; s2 < issued; ++s2)
+            mbar_wait(&sm.bar[s2 % LNB], (unsigned)((s2 / LNB) & 1));
+        }
+        return;
+      }
+      const float *shi = reinterpret_cast<const float *>(sm.slot[s] + L_HI);
+      const float *scc = reinterpret_cast<const float *>(sm.slot[s] + L_CC);
+      float u[NF], wp[NW];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) u[f] = shi[f * LBOX + tid + 2];
+      limited_vars(u, wp);
+      const float ccp = scc[tid + 2];
+      const int r = p - li.t0;  // -2 .. t1-t0+1
+      if (r == -2) {
+#pragma unroll
+        for (int n = 0; n < NW; ++n) wm2[n] = wp[n];
+      } else if (r == -1) {
+#pragma unroll
+        for (int n = 0; n < NW; ++n) wm1[n] = wp[n];
+        ccm1 = ccp;
+      } else if (r == 0) {
+#pragma unroll
+        for (int n = 0; n < NW; ++n) w0[n] = wp[n];
+        cc0 = ccp;
+      } else if (r == 1) {
+#pragma unroll
+        for (int n = 0; n < NW; ++n) {
+          w1[n] = wp[n];
+          const float dqm = dqq_eval(wm2[n], wm1[n], w0[n], a.ep);
+          dq0[n] = dqq_eval(wm1[n], w0[n], w1[n], a.ep);
+          F0[n] = flux_core(wm1[n], w0[n], dqm, dq0[n], 0.5f * (ccm1 + cc0), a.fh);
+        }
+        cc1 = ccp;
+      } else {
+        // centre cell t = p - 2; its plane sits two slots back
+        const int t = p - 2;
+        const int sc_ = (int)((seq - 2) % LNB);
+        const float *chi = reinterpret_cast<const float *>(sm.slot[sc_] + L_HI);
+        const float *clo = reinterpret_cast<const float *>(sm.slot[sc_] + L_LO);
+        float dF[NW];
+#pragma unroll
+        for (int n = 0; n < NW; ++n) {
+          const float dq1 = dqq_eval(w0[n], w1[n], wp[n], a.ep);
+          const float F1 = flux_core(w0[n], w1[n], dq0[n], dq1, 0.5f * (cc0 + cc1), a.fh);
+          dF[n] = F1 - F0[n];
+          F0[n] = F1;
+          dq0[n] = dq1;
+          w0[n] = w1[n];
+          w1[n] = wp[n];
+        }
+        cc0 = cc1;
+        cc1 = ccp;
+        if (active) {
+          const int x0 = DIR == 0 ? t : li.u;
+          const int x1 = DIR == 0 ? li.u : t;
+          const int cell = cell_of(g, x0, x1, k);
+          const bool nb = near_boundary(g, x0, x1, k);
+          Img im;
+          if (nb) make_img(g, x0, x1, k, im);
+#pragma unroll
+          for (int n = 0; n < NW; ++n) {
+            const int f = field_of(n);
+            float sv, e;
+            two_sum(chi[f * LBOX + tid + 2], clo[f * LBOX + tid + 2] - dF[n] * fac, sv, e);
+            store_cell(a.hi2.p + f * a.hi2.pitch, cell, nb, im, f, sv);
+            store_cell(a.lo2.p + f * a.lo2.pitch, cell, nb, im, f, e);
+          }
+        }
+      }
+      __syncthreads();  // every thread is done with the slot of plane p-2
+      if (tid == 0 && seq >= 2 && prod.valid(items)) {
+        const int fs = (int)((seq - 2) % LNB);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        line_issue<DIR>(&thi, &tlo, &tcc, sm, fs, g, prod.cur, prod.p);
+        prod.next(a, kblocks, nu, items);
+        ++issued;
+      }
+    }
+  }
+}
+
+// ---- z sweep (contiguous axis) ----
+// Each warp loads 32 consecutive cells of a row and updates the inner 28;
+// neighbours come from warp shuffles.  The CFL candidate of the new state
+// is folded into a per-block minimum.
+__global__ void __launch_bounds__(128)
+av_z_kernel(const AvArgs a) {
+  const Geom &g = a.g;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nk = g.n[2];
+  const int segs = (nk + 27) / 28;
+  const int rows = g.n[0] * g.n[1];
+  const int work = rows * segs;
+  const float fac = (float)(g.dsi[2] * a.sc->dt);
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  float best = 1.e10f;
+  bool bad = false;
+  for (int wi = blockIdx.x * (blockDim.x >> 5) + wid; wi < work; wi += warps) {
+    const int sg = wi % segs;
+    const int row = wi / segs;
+    const int j = row % g.n[1];
+    const int i = row / g.n[1];
+    const int k = sg * 28 + lane - 2;  // interior k of this lane
+    const int kc = min(k, nk + 1);     // stay inside the array (ghosts reach nk+1)
+    const int c = cell_of(g, i, j, kc);
+    float u[NF], w[NW];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) u[f] = __ldg(a.hi.p + f * a.hi.pitch + c);
+    limited_vars(u, w);
+    const float cc = __ldg(a.cc + c);
+    const float cc_up = __shfl_down_sync(0xffffffffu, cc, 1);
+    float dF[NW];
+#pragma unroll
+    for (int n = 0; n < NW; ++n) {
+      const float wm = __shfl_up_sync(0xffffffffu, w[n], 1);
+      const float wp = __shfl_down_sync(0xffffffffu, w[n], 1);
+      const float dq = dqq_eval(wm, w[n], wp, a.ep);
+      const float dq_up = __shfl_down_sync(0xffffffffu, dq, 1);
+      const float Fup = flux_core(w[n], wp, dq, dq_up, 0.5f * (cc + cc_up), a.fh);
+      const float Fdw = __shfl_up_sync(0xffffffffu, Fup, 1);
+      dF[n] = Fup - Fdw;
+    }
+    if (lane >= 2 && lane < 30 && k < nk) {
+      const bool nb = near_boundary(g, i, j, k);
+      Img im;
+      if (nb) make_img(g, i, j, k, im);
+      float s[NF];
+#pragma unroll
+      for (int n = 0; n < NW; ++n) {
+        const int f = field_of(n);
+        float e;
+        two_sum(u[f], __ldg(a.lo.p + f * a.lo.pitch + c) - dF[n] * fac, s[f], e);
+        store_cell(a.hi2.p + f * a.hi2.pitch, c, nb, im, f, s[f]);
+        store_cell(a.lo2.p + f * a.lo2.pitch, c, nb, im, f, e);
+      }
+      if (a.partial) {
+        // CFL candidate of the new state (mhd_integrator_host.hpp:303-334)
+        float cs, vv, ca, ein;
+        speeds(s, a.gm, a.gm1, cs, vv, ca, ein);
+        const float tv = cs + vv + ca;
+        best = fminf(best, a.cfl_dx / tv);
+        bad |= !(s[RO] > 0.0f) || !(ein >= 0.0f) || !isfinite(tv);
+      }
+    }
+  }
+  if (a.partial) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    __shared__ float red[4];
+    if (lane == 0) red[wid] = best;
+    if (bad) atomicOr(a.err, ERRBIT_NONFINITE);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float b = red[0];
+      for (int w2 = 1; w2 < (int)(blockDim.x >> 5); ++w2) b = fminf(b, red[w2]);
+      a.partial[blockIdx.x] = b;
+    }
+  }
+}
+
+}  // namespace s32t
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+bool s32_tiled_supported(const Geom &g) {
+  if (!g.s[0] || !g.s[1] || !g.s[2]) return false;
+  if (g.m[0] != 2 || g.m[1] != 2 || g.m[2] != 2) return false;
+  if ((g.t[2] * 4) % 16) return false;  // TMA row pitch: multiple of 16 bytes
+  for (int a = 0; a < 3; ++a)
+    if (g.n[a] < 2 * g.m[a]) return false;  // one ghost image per axis side
+  if (g.cells >= (1LL << 31) / 9) return false;  // 32-bit cell offsets
+  return encode_fn() != nullptr;
+}
+
+int s32_make_tmap(const Geom &g, const float *field0, size_t pitch_bytes, int kind,
+                  void *tm_out) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return -1;
+  cuuint64_t dims[4] = {(cuuint64_t)g.t[2], (cuuint64_t)g.t[1], (cuuint64_t)g.t[0], NF};
+  cuuint64_t strides[3] = {(cuuint64_t)g.t[2] * 4, (cuuint64_t)g.t[2] * g.t[1] * 4,
+                           (cuuint64_t)pitch_bytes};
+  cuuint32_t box_rk[4] = {s32t::HK, s32t::HJ, 1, NF};
+  cuuint32_t box_av[4] = {s32t::LBOX, 1, 1, NF};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = fn((CUtensorMap *)tm_out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)field0,
+                  dims, strides, kind == 0 ? box_rk : box_av, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -2;
+}
+
+int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return -1;
+  cuuint64_t dims[3] = {(cuuint64_t)g.t[2], (cuuint64_t)g.t[1], (cuuint64_t)g.t[0]};
+  cuuint64_t strides[2] = {(cuuint64_t)g.t[2] * 4, (cuuint64_t)g.t[2] * g.t[1] * 4};
+  cuuint32_t box[3] = {s32t::LBOX, 1, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn((CUtensorMap *)tm_out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)cc, dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -2;
+}
+
+int s32_configure() {
+  const int rk = (int)sizeof(s32t::RkSmem);
+  const int ln = (int)sizeof(s32t::LineSmem);
+  cudaError_t e = cudaSuccess;
+#define MISO_SET(k, b) \
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b)
+  MISO_SET(s32t::rk_tiled_kernel<0>, rk);
+  MISO_SET(s32t::rk_tiled_kernel<1>, rk);
+  MISO_SET(s32t::rk_tiled_kernel<2>, rk);
+  MISO_SET(s32t::rk_tiled_kernel<3>, rk);
+  MISO_SET(s32t::av_line_kernel<0>, ln);
+  MISO_SET(s32t::av_line_kernel<1>, ln);
+#undef MISO_SET
+  return e == cudaSuccess ? 0 : -1;
+}
+
+void s32_rk_items(const Geom &g, int L, int &tiles_j, int &tiles_k, int &items) {
+  tiles_j = (g.n[1] + s32t::TJ - 1) / s32t::TJ;
+  tiles_k = (g.n[2] + s32t::TK - 1) / s32t::TK;
+  const int chunks = (g.n[0] + L - 1) / L;
+  items = tiles_j * tiles_k * chunks;
+}
+
+void launch_s32_rk_tiled(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st) {
+  const CUtensorMap &m = *(const CUtensorMap *)tm;
+  const size_t smem = sizeof(s32t::RkSmem);
+  switch (stage) {
+    case 0: s32t::rk_tiled_kernel<0><<<grid, s32t::NTHR, smem, st>>>(m, a); break;
+    case 1: s32t::rk_tiled_kernel<1><<<grid, s32t::NTHR, smem, st>>>(m, a); break;
+    case 2: s32t::rk_tiled_kernel<2><<<grid, s32t::NTHR, smem, st>>>(m, a); break;
+    default: s32t::rk_tiled_kernel<3><<<grid, s32t::NTHR, smem, st>>>(m, a); break;
+  }
+}
+
+void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
+                        int dir, int grid, cudaStream_t st) {
+  const CUtensorMap &h = *(const CUtensorMap *)tm_hi;
+  const CUtensorMap &l = *(const CUtensorMap *)tm_lo;
+  const CUtensorMap &c = *(const CUtensorMap *)tm_cc;
+  const size_t smem = sizeof(s32t::LineSmem);
+  if (dir == 0)
+    s32t::av_line_kernel<0><<<grid, s32t::LK, smem, st>>>(h, l, c, a);
+  else
+    s32t::av_line_kernel<1><<<grid, s32t::LK, smem, st>>>(h, l, c, a);
+}
+
+void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st) {
+  s32t::av_z_kernel<<<grid, 128, 0, st>>>(a);
+}
+
+}  // namespace miso_b200

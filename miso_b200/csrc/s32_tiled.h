@@ -1,0 +1,59 @@
+// Tiled FP32 split-precision kernels for 3-D grids (internal to the library).
+#pragma once
+
+#include "common.cuh"
+
+namespace miso_b200 {
+
+// Nine arrays laid out at a common pitch (elements) from p.
+struct FSet {
+  float *p;
+  long long pitch;
+};
+struct CFSet {
+  const float *p;
+  long long pitch;
+};
+
+// Arguments of one Runge-Kutta stage launch.
+struct RkArgs {
+  Geom g;
+  CFSet u0;     // U^n (hi words), read at the cell itself
+  FSet hi, lo;  // stage 3: state updated in place
+  FSet out;     // stages 0-2: stage state written here
+  float *cc;    // stage 3: characteristic speed of the new state
+  const StepScalars *sc;
+  unsigned int *err;
+  float gm, gm1, cs_fac, vv_fac, ca_fac;
+  int L;  // planes per work item along i
+  int tiles_j, tiles_k, items;
+};
+
+// Arguments of one artificial-viscosity sweep launch.
+struct AvArgs {
+  Geom g;
+  CFSet hi, lo;
+  FSet hi2, lo2;
+  const float *cc;
+  const StepScalars *sc;
+  unsigned int *err;
+  float *partial;  // z sweep: per-block CFL minima of the new state (nullable)
+  float ep, fh, gm, gm1, cfl_dx;
+  int L;  // cells per work item along the sweep axis (x, y sweeps)
+};
+
+bool s32_tiled_supported(const Geom &g);
+// 4-D tensor maps (k, j, i, field) over 9 arrays at `pitch_bytes`:
+//   kind 0: RK plane tile (k 36, j 12, i 1, 9 fields)
+//   kind 1: AV line (k 132, j 1, i 1, 9 fields)
+int s32_make_tmap(const Geom &g, const float *field0, size_t pitch_bytes, int kind, void *tm_out);
+// 3-D tensor map of one array for the AV line (k 132, j 1, i 1)
+int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out);
+int s32_configure();
+void s32_rk_items(const Geom &g, int L, int &tiles_j, int &tiles_k, int &items);
+void launch_s32_rk_tiled(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st);
+void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
+                        int dir, int grid, cudaStream_t st);
+void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);
+
+}  // namespace miso_b200

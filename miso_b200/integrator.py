@@ -172,6 +172,23 @@ class Integrator:
         keys = ("mass", "mom_x", "mom_y", "mom_z", "energy", "divb_l1", "divb_max", "ph2")
         return dict(zip(keys, list(out)))
 
+    def set_variant(self, kernel_class: int, variant: int):
+        self._check(self._lib.miso_b200_set_variant(self._h, int(kernel_class), int(variant)))
+
+    def get_variant(self, kernel_class: int) -> int:
+        v = ctypes.c_int()
+        self._check(self._lib.miso_b200_get_variant(self._h, int(kernel_class), ctypes.byref(v)))
+        return v.value
+
+    def set_timing(self, enable: bool):
+        self._check(self._lib.miso_b200_set_timing(self._h, int(bool(enable))))
+
+    def timing_report(self) -> dict:
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self._lib.miso_b200_timing_report(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     def device_bytes(self) -> int:
         b = ctypes.c_size_t()
         self._check(self._lib.miso_b200_device_bytes(self._h, ctypes.byref(b)))

@@ -285,8 +285,16 @@ struct miso_b200_handle {
     for (int f = 0; f < NF; ++f) r.f[f] = stg[s][f];
     return r;
   }
-  FSet fs(float *const (&arr)[NF]) const { return FSet{arr[0], pitch}; }
-  CFSet cfs(float *const (&arr)[NF]) const { return CFSet{arr[0], pitch}; }
+  FSet fs(float *const (&arr)[NF]) const {
+    FSet r;
+    for (int f = 0; f < NF; ++f) r.f[f] = arr[f];
+    return r;
+  }
+  CFSet cfs(float *const (&arr)[NF]) const {
+    CFSet r;
+    for (int f = 0; f < NF; ++f) r.f[f] = arr[f];
+    return r;
+  }
 
   FieldPtrs<double> IO() {
     FieldPtrs<double> r;

@@ -21,28 +21,33 @@ using namespace s32t;
 
 constexpr int BK = 32, BJ = 8;
 
-struct Tile {
-  int i, j, k;
+// Work item: a 32 x 8 (k, j) column tile over a chunk of L planes along i.
+// Items are chunk-major, and the grid is one resident wave, so the CTAs in
+// flight cover one band of planes; a thread marches down its column and the
+// planes it touched a step earlier are still in L1.
+struct Item {
+  int j, k, i0, i1;
 };
 
-__device__ __forceinline__ bool tile_cell(const Geom &g, long long t, Tile &c) {
-  const int tk = (g.n[2] + BK - 1) / BK, tj = (g.n[1] + BJ - 1) / BJ;
-  const int kt = (int)(t % tk);
-  const long long r = t / tk;
-  const int jt = (int)(r % tj);
-  c.i = (int)(r / tj);
-  c.j = jt * BJ + threadIdx.y;
-  c.k = kt * BK + threadIdx.x;
-  return c.j < g.n[1] && c.k < g.n[2];
+__device__ __forceinline__ int item_count(const Geom &g, int L) {
+  return ((g.n[2] + BK - 1) / BK) * ((g.n[1] + BJ - 1) / BJ) * ((g.n[0] + L - 1) / L);
 }
 
-__device__ __forceinline__ long long tile_count(const Geom &g) {
-  return (long long)((g.n[2] + BK - 1) / BK) * ((g.n[1] + BJ - 1) / BJ) * g.n[0];
+__device__ __forceinline__ Item item_of(const Geom &g, int it, int L) {
+  const int tk = (g.n[2] + BK - 1) / BK, tj = (g.n[1] + BJ - 1) / BJ;
+  const int per = tk * tj;
+  const int ch = it / per, rem = it % per;
+  Item r;
+  r.j = (rem / tk) * BJ + (int)threadIdx.y;
+  r.k = (rem % tk) * BK + (int)threadIdx.x;
+  r.i0 = ch * L;
+  r.i1 = min(g.n[0], r.i0 + L);
+  return r;
 }
 
 __device__ __forceinline__ void load_state(const CFSet &s, int c, float u[NF]) {
 #pragma unroll
-  for (int f = 0; f < NF; ++f) u[f] = __ldg(s.p + f * s.pitch + c);
+  for (int f = 0; f < NF; ++f) u[f] = __ldg(s.f[f] + c);
 }
 
 template <int D>
@@ -79,33 +84,36 @@ rk_flat_kernel(const CFSet prev, const RkArgs a) {
   const float wy = (float)(g.dsi[1] * INV12);
   const float wz = (float)(g.dsi[2] * INV12);
   const int Si = (int)g.st[0], Sj = (int)g.st[1];
-  const long long ntiles = tile_count(g);
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    Tile tc;
-    if (!tile_cell(g, t, tc)) continue;
-    const int cell = cell_of(g, tc.i, tc.j, tc.k);
+  const int items = item_count(g, a.L);
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    const Item itm = item_of(g, it, a.L);
+    if (itm.j >= g.n[1] || itm.k >= g.n[2]) continue;
+    const bool nbjk = itm.j < g.m[1] || itm.j >= g.n[1] - g.m[1] || itm.k < g.m[2] ||
+                      itm.k >= g.n[2] - g.m[2];
+    int cell = cell_of(g, itm.i0, itm.j, itm.k);
+    for (int i = itm.i0; i < itm.i1; ++i, cell += Si) {
     float D[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) D[f] = 0.0f;
     diff_dir<2>(prev, cell, 1, wz, a.gm1, ch2, D);
     diff_dir<1>(prev, cell, Sj, wy, a.gm1, ch2, D);
     diff_dir<0>(prev, cell, Si, wx, a.gm1, ch2, D);
-    const bool nb = near_boundary(g, tc.i, tc.j, tc.k);
+    const bool nb = nbjk || i < g.m[0] || i >= g.n[0] - g.m[0];
     Img im;
-    if (nb) make_img(g, tc.i, tc.j, tc.k, im);
+    if (nb) make_img(g, i, itm.j, itm.k, im);
     if (STAGE < 3) {
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
-        float v = __ldg(a.u0.p + f * a.u0.pitch + cell) - dt * D[f];
+        float v = __ldg(a.u0.f[f] + cell) - dt * D[f];
         if (f == PH) v *= decay;
-        store_cell(a.out.p + f * a.out.pitch, cell, nb, im, f, v);
+        store_cell(a.out.f[f], cell, nb, im, f, v);
       }
     } else {
       float sv[NF];
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
-        float *hp = a.hi.p + f * a.hi.pitch;
-        float *lp = a.lo.p + f * a.lo.pitch;
+        float *hp = a.hi.f[f];
+        float *lp = a.lo.f[f];
         const float h = hp[cell], l = lp[cell];
         float e;
         if (f == PH) {
@@ -124,6 +132,7 @@ rk_flat_kernel(const CFSet prev, const RkArgs a) {
       speeds(sv, a.gm, a.gm1, cs, vv, ca, ein);
       store_cell(a.cc, cell, nb, im, NF, cs * a.cs_fac + vv * a.vv_fac + ca * a.ca_fac);
     }
+    }
   }
 }
 
@@ -134,13 +143,17 @@ av_flat_kernel(const AvArgs a) {
   const Geom &g = a.g;
   const int S = (int)g.st[DIR];
   const float fac = (float)(g.dsi[DIR] * a.sc->dt);
-  const long long ntiles = tile_count(g);
+  const int Si = (int)g.st[0];
+  const int items = item_count(g, a.L);
   float best = 1.e10f;
   bool bad = false;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    Tile tc;
-    if (!tile_cell(g, t, tc)) continue;
-    const int cell = cell_of(g, tc.i, tc.j, tc.k);
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    const Item itm = item_of(g, it, a.L);
+    if (itm.j >= g.n[1] || itm.k >= g.n[2]) continue;
+    const bool nbjk = itm.j < g.m[1] || itm.j >= g.n[1] - g.m[1] || itm.k < g.m[2] ||
+                      itm.k >= g.n[2] - g.m[2];
+    int cell = cell_of(g, itm.i0, itm.j, itm.k);
+    for (int i = itm.i0; i < itm.i1; ++i, cell += Si) {
     float w[5][NW];
     float hic[NF];
 #pragma unroll
@@ -155,9 +168,9 @@ av_flat_kernel(const AvArgs a) {
     }
     const float ccl = __ldg(a.cc + cell - S), ccc = __ldg(a.cc + cell), ccr = __ldg(a.cc + cell + S);
     const float cdw = 0.5f * (ccl + ccc), cup = 0.5f * (ccc + ccr);
-    const bool nb = near_boundary(g, tc.i, tc.j, tc.k);
+    const bool nb = nbjk || i < g.m[0] || i >= g.n[0] - g.m[0];
     Img im;
-    if (nb) make_img(g, tc.i, tc.j, tc.k, im);
+    if (nb) make_img(g, i, itm.j, itm.k, im);
     float s[NF];
 #pragma unroll
     for (int n = 0; n < NW; ++n) {
@@ -168,9 +181,9 @@ av_flat_kernel(const AvArgs a) {
       const float fup = flux_core(w[2][n], w[3][n], d1, d2, cup, a.fh);
       const int f = field_of(n);
       float e;
-      two_sum(hic[f], __ldg(a.lo.p + f * a.lo.pitch + cell) - (fup - fdw) * fac, s[f], e);
-      store_cell(a.hi2.p + f * a.hi2.pitch, cell, nb, im, f, s[f]);
-      store_cell(a.lo2.p + f * a.lo2.pitch, cell, nb, im, f, e);
+      two_sum(hic[f], __ldg(a.lo.f[f] + cell) - (fup - fdw) * fac, s[f], e);
+      store_cell(a.hi2.f[f], cell, nb, im, f, s[f]);
+      store_cell(a.lo2.f[f], cell, nb, im, f, e);
     }
     if (DIR == 2 && a.partial) {
       float cs, vv, ca, ein;
@@ -178,6 +191,7 @@ av_flat_kernel(const AvArgs a) {
       const float tv = cs + vv + ca;
       best = fminf(best, a.cfl_dx / tv);
       bad |= !(s[RO] > 0.0f) || !(ein >= 0.0f) || !isfinite(tv);
+    }
     }
   }
   if (DIR == 2 && a.partial) {

@@ -186,17 +186,17 @@ __device__ __forceinline__ void rk_plane(const RkArgs &a, RkSmem &sm, const floa
     if (STAGE < 3) {
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
-        const float u0 = __ldg(a.u0.p + f * a.u0.pitch + cell);
+        const float u0 = __ldg(a.u0.f[f] + cell);
         float v = u0 - dt * D[f];
         if (f == PH) v *= decay;
-        store_cell(a.out.p + f * a.out.pitch, cell, nb, im, f, v);
+        store_cell(a.out.f[f], cell, nb, im, f, v);
       }
     } else {
       float sv[NF];
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
-        float *hp = a.hi.p + f * a.hi.pitch;
-        float *lp = a.lo.p + f * a.lo.pitch;
+        float *hp = a.hi.f[f];
+        float *lp = a.lo.f[f];
         const float h = hp[cell], l = lp[cell];
         float e;
         if (f == PH) {
@@ -283,7 +283,7 @@ rk_tiled_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
   const float decay = (float)a.sc->ph_decay[STAGE];
 
   RkCursor prod;
-  long long issued = 0;
+  int issued = 0;
   if (tid == 0) {
     prod.begin(a);
     for (int b = 0; b < NBUF && prod.valid(a); ++b) {
@@ -293,7 +293,7 @@ rk_tiled_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
       ++issued;
     }
   }
-  long long seq = 0;
+  int seq = 0;
   March ms;
   for (int it = blockIdx.x; it < a.items; it += gridDim.x) {
     const Item itm = item_of(a, it);
@@ -310,7 +310,7 @@ rk_tiled_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
         if (tid == 0) {
           atomicOr(a.err, ERRBIT_TIMEOUT);
           // drain the copies still in flight (bounded) before the CTA exits
-          for (long long s2 = seq + 1; s2 < issued; ++s2)
+          for (int s2 = seq + 1; s2 < issued; ++s2)
             mbar_wait(&sm.bar[s2 % NBUF], (unsigned)((s2 / NBUF) & 1));
         }
         return;
@@ -427,7 +427,7 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
   if ((int)blockIdx.x >= items) return;
   const float fac = (float)(g.dsi[DIR] * a.sc->dt);
   LineCursor<DIR> prod;
-  long long issued = 0;
+  int issued = 0;
   if (tid == 0) {
     prod.begin(a, kblocks, nu, items);
     for (int s = 0; s < LNB && prod.valid(items); ++s) {
@@ -436,7 +436,7 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
       ++issued;
     }
   }
-  long long seq = 0;
+  int seq = 0;
   float wm2[NW], wm1[NW], w0[NW], w1[NW], dq0[NW], F0[NW];
   float ccm1 = 0.f, cc0 = 0.f, cc1 = 0.f;
   for (int it = blockIdx.x; it < items; it += gridDim.x) {
@@ -450,7 +450,7 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
       if (sm.abort) {
         if (tid == 0) {
           atomicOr(a.err, ERRBIT_TIMEOUT);
-          for (long long s2 = seq + 1; s2 < issued; ++s2)
+          for (int s2 = seq + 1; s2 < issued; ++s2)
             mbar_wait(&sm.bar[s2 % LNB], (unsigned)((s2 / LNB) & 1));
         }
         return;
@@ -514,8 +514,8 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
             const int f = field_of(n);
             float sv, e;
             two_sum(chi[f * LBOX + tid + 2], clo[f * LBOX + tid + 2] - dF[n] * fac, sv, e);
-            store_cell(a.hi2.p + f * a.hi2.pitch, cell, nb, im, f, sv);
-            store_cell(a.lo2.p + f * a.lo2.pitch, cell, nb, im, f, e);
+            store_cell(a.hi2.f[f], cell, nb, im, f, sv);
+            store_cell(a.lo2.f[f], cell, nb, im, f, e);
           }
         }
       }
@@ -557,7 +557,7 @@ av_z_kernel(const AvArgs a) {
     const int c = cell_of(g, i, j, kc);
     float u[NF], w[NW];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) u[f] = __ldg(a.hi.p + f * a.hi.pitch + c);
+    for (int f = 0; f < NF; ++f) u[f] = __ldg(a.hi.f[f] + c);
     limited_vars(u, w);
     const float cc = __ldg(a.cc + c);
     const float cc_up = __shfl_down_sync(0xffffffffu, cc, 1);
@@ -581,9 +581,9 @@ av_z_kernel(const AvArgs a) {
       for (int n = 0; n < NW; ++n) {
         const int f = field_of(n);
         float e;
-        two_sum(u[f], __ldg(a.lo.p + f * a.lo.pitch + c) - dF[n] * fac, s[f], e);
-        store_cell(a.hi2.p + f * a.hi2.pitch, c, nb, im, f, s[f]);
-        store_cell(a.lo2.p + f * a.lo2.pitch, c, nb, im, f, e);
+        two_sum(u[f], __ldg(a.lo.f[f] + c) - dF[n] * fac, s[f], e);
+        store_cell(a.hi2.f[f], c, nb, im, f, s[f]);
+        store_cell(a.lo2.f[f], c, nb, im, f, e);
       }
       if (a.partial) {
         // CFL candidate of the new state (mhd_integrator_host.hpp:303-334)

@@ -5,15 +5,9 @@
 
 namespace miso_b200 {
 
-// Nine arrays laid out at a common pitch (elements) from p.
-struct FSet {
-  float *p;
-  long long pitch;
-};
-struct CFSet {
-  const float *p;
-  long long pitch;
-};
+// The 9 field arrays of one state set.
+using FSet = FieldPtrs<float>;
+using CFSet = FieldPtrs<const float>;
 
 // Arguments of one Runge-Kutta stage launch.
 struct RkArgs {

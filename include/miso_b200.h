@@ -149,7 +149,27 @@ int miso_b200_device_bytes(miso_b200_handle *h, size_t *bytes);
 /* Number of kernels the library enqueued on the handle's stream so far. */
 int miso_b200_launch_count(miso_b200_handle *h, long long *count);
 
-/* Message of the last error on this handle (or of the last failed create when h is NULL). */
+/* Allocation-free CFL time step.  No counterpart in the reference: it is an
+ * extra entry point for callers that must not let a library allocate device
+ * memory -- code running while a stream is captured into a CUDA graph,
+ * loops that must not synchronise the device (cudaMalloc may), hosts that
+ * own all device memory through their own pool or budget.  It computes the
+ * same float-rounded CFL time step as miso_b200_cfl() over the interior of
+ * 9 caller-owned DEVICE arrays q[] (FP64 primitives ro, vx, vy, vz, bx, by,
+ * bz, ei, ph in the layout above) and returns it in *dt_out (host), with no
+ * handle and no cudaMalloc/cudaFree: its scratch is a 65,792-byte array in
+ * the library's device memory, held by every GPU that loads the library
+ * until the process exits.  Grids of more than 268,435,456 interior cells
+ * are rejected with MISO_B200_ERR_ARG.  The first call on a device looks up
+ * that device's scratch address, so make it before any stream capture.
+ * Every call shares the one scratch array: calls whose work overlaps on the
+ * GPU (other threads, other streams) race and must be serialised by the
+ * caller.  Synchronises `stream` (a cudaStream_t, NULL = default stream). */
+int miso_b200_cfl_noalloc(const miso_b200_grid_desc *grid, const miso_b200_params *params,
+                          const double *const q[9], void *stream, double *dt_out);
+
+/* Message of the last error on this handle (or, when h is NULL, of the last
+ * failed create or miso_b200_cfl_noalloc call). */
 const char *miso_b200_last_error(miso_b200_handle *h);
 
 /* Library version string. */

@@ -66,6 +66,9 @@ SIGNATURES = {
                                              ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "miso_b200_timing_report": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "miso_b200_cfl_noalloc": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(Params),
+                                             ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p,
+                                             _dp]),
     "miso_b200_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "miso_b200_version": (ctypes.c_char_p, []),
 }

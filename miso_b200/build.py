@@ -29,6 +29,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 FAST32 = ["--ftz=true", "--prec-div=false", "--prec-sqrt=false"]
 EXTRA = {
     "fp64_kernels.cu": ["--fmad=false"],
+    "noalloc.cu": ["--fmad=false"],
     "fp32s_kernels.cu": FAST32,
     "s32_tiled.cu": FAST32,
     "s32_flat.cu": FAST32,

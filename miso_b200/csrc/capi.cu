@@ -518,6 +518,12 @@ struct miso_b200_handle {
 
 static bool valid_axis(int size, int margin) { return size >= 1 && (size == 1 || size >= margin); }
 
+// Error text of handle-less calls (read back through miso_b200_last_error(NULL)).
+void miso_b200_set_global_error(const std::string &msg) {
+  std::lock_guard<std::mutex> lk(g_create_mu);
+  g_create_error = msg;
+}
+
 extern "C" {
 
 const char *miso_b200_version(void) { return "miso_b200 0.1 (sm_100a)"; }

@@ -66,6 +66,42 @@ def _field_ptrs(q):
     return arr
 
 
+def make_descs(config: dict, grid: Grid, sign=None, precision: str = "fp64"):
+    """C-ABI grid descriptor and parameter block for a configuration."""
+    cfg = merge_defaults(config)
+    gd = _lib.GridDesc()
+    gd.i_size, gd.j_size, gd.k_size, gd.margin = (grid.i_size, grid.j_size, grid.k_size,
+                                                  grid.margin)
+    gd.x_min, gd.x_max, gd.y_min, gd.y_max = grid.x_min, grid.x_max, grid.y_min, grid.y_max
+    gd.z_min, gd.z_max = grid.z_min, grid.z_max
+    per = cfg["domain"]["periodic"]
+    gd.periodic[0], gd.periodic[1], gd.periodic[2] = (int(per["x"]), int(per["y"]),
+                                                      int(per["z"]))
+    sg = np.ones((3, 2, 9)) if sign is None else np.asarray(sign, dtype=np.float64)
+    for n, v in enumerate(sg.reshape(-1)):
+        gd.sign[n] = float(v)
+    pp = _lib.Params()
+    av = cfg["mhd"]["artificial_viscosity"]
+    pp.gm = cfg["eos"]["gm"]
+    pp.cfl_number = cfg["mhd"]["cfl_number"]
+    pp.ep, pp.fh = av["ep"], av["fh"]
+    pp.cs_fac, pp.ca_fac, pp.vv_fac = av["cs_fac"], av["ca_fac"], av["vv_fac"]
+    pp.precision = PRECISIONS[precision]
+    return gd, pp
+
+
+def cfl_noalloc(config: dict, grid: Grid, q, stream: int | None = None) -> float:
+    """CFL time step of caller-owned device fields (a CUDA (9, I, J, K)
+    float64 tensor) through the allocation-free entry point
+    miso_b200_cfl_noalloc: no handle, no device allocation."""
+    lib = _lib.load()
+    gd, pp = make_descs(config, grid)
+    dt = ctypes.c_double()
+    _lib.check(lib.miso_b200_cfl_noalloc(ctypes.byref(gd), ctypes.byref(pp), _field_ptrs(q),
+                                         ctypes.c_void_p(stream or 0), ctypes.byref(dt)), None)
+    return dt.value
+
+
 class Integrator:
     """One grid advanced on the current CUDA device."""
 

@@ -214,3 +214,22 @@ def orszag_tang_batch(count: int = 32, n_min: int = 128, n_max: int = 1024, seed
     """``count`` Orszag-Tang grids of random sizes U{n_min..n_max}^2."""
     rng = np.random.default_rng(seed)
     return [orszag_tang(int(n)) for n in rng.integers(n_min, n_max + 1, size=count)]
+
+
+def sod(n: int = 128, axis: int = 0, gm: float = 1.4, cfl: float = 0.5) -> Problem:
+    """Hydrodynamic Sod shock tube (B = 0) along ``axis`` on [0, 1], mirror
+    faces: (rho, p) = (1, 1) for x < 0.5 and (0.125, 0.1) beyond, at rest --
+    the configuration of the reference's shock-tube test
+    (miso/tests/serial/test_hd1d_shock_tube/config/config_x.yaml)."""
+    sizes = [1, 1, 1]
+    sizes[axis] = n
+    g = Grid(*sizes, 2, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+    q = _alloc(g)
+    coord = (g.x, g.y, g.z)[axis]
+    shape = [1, 1, 1]
+    shape[axis] = -1
+    left = (coord < 0.5).reshape(shape)
+    q[RO] = np.where(left, 1.0, 0.125)
+    q[EI] = np.where(left, 1.0 / (gm - 1.0) / 1.0, 0.1 / (gm - 1.0) / 0.125)
+    cfgd = make_config(gm, periodic=(False, False, False), cfl_number=cfl)
+    return Problem(f"sod_{n}_{'xyz'[axis]}", g, cfgd, q)

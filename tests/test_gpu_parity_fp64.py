@@ -106,3 +106,52 @@ def test_fp64_orszag_tang_256(oracle):
     a, b = interior(prob, out), interior(prob, ref)
     assert int(np.sum(a != b)) == 0
     assert rel_l1(a[0], b[0]) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_split"])
+def test_sod_accuracy_gpu(precision):
+    """The reference's shock-tube statement (test_hd1d_shock_tube.cpp:21-82)
+    on the device: relative L1 of density and velocity against the exact
+    Sod solution below 5e-2 at t = 0.2."""
+    from sod_exact import sample
+    prob = P.sod(128)
+    integ = Integrator(prob.config, prob.grid, precision=precision)
+    integ.upload(prob.q)
+    integ.apply_boundary_condition()
+    t = 0.0
+    while t < 0.2:
+        dt = integ.cfl()
+        integ.update(dt)
+        t += dt
+    q = integ.download()
+    integ.close()
+    r_ex, u_ex, _ = sample(prob.grid.x, t, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1, 1.4)
+    ro, vx = q[P.RO].reshape(-1), q[P.VX].reshape(-1)
+    assert np.sum(np.abs(ro - r_ex)) / np.sum(ro) < 5e-2
+    assert np.sum(np.abs(vx - u_ex)) / np.sum(vx) < 5e-2
+
+
+def test_nonfinite_state_is_reported():
+    """A negative density is reported as MISO_B200_ERR_NONFINITE by the CFL
+    pass (a status code; no device fault)."""
+    from miso_b200 import _lib
+    prob = P.orszag_tang(32)
+    q = prob.q.copy()
+    q[P.RO, 10, 10, 0] = -1.0
+    for precision in ("fp64", "fp32_split"):
+        integ = Integrator(prob.config, prob.grid, precision=precision)
+        integ.upload(q)
+        integ.apply_boundary_condition()
+        with pytest.raises(_lib.MisoError) as exc:
+            integ.cfl()
+        assert exc.value.code == _lib.ERR_NONFINITE
+        integ.close()
+
+
+def test_bad_dt_is_rejected():
+    from miso_b200 import _lib
+    prob = P.orszag_tang(16)
+    with Integrator(prob.config, prob.grid) as integ:
+        with pytest.raises(_lib.MisoError) as exc:
+            integ.update(-1.0)
+        assert exc.value.code == _lib.ERR_ARG

@@ -134,6 +134,10 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant);
 int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant);
 
+/* Planes per work item along the march axis for the Runge-Kutta and the
+ * x/y viscosity kernels of the 3-D FP32-split path (defaults 64). */
+int miso_b200_set_chunks(miso_b200_handle *h, int rk_chunk, int av_chunk);
+
 /* Enable (1) or disable (0) per-kernel CUDA-event timing on the handle's
  * stream (outside graph replays); clears the accumulated totals. */
 int miso_b200_set_timing(miso_b200_handle *h, int enable);
@@ -148,6 +152,38 @@ int miso_b200_device_bytes(miso_b200_handle *h, size_t *bytes);
 
 /* Number of kernels the library enqueued on the handle's stream so far. */
 int miso_b200_launch_count(miso_b200_handle *h, long long *count);
+
+/* ---------------------------------------------------------------------------
+ * Batched solver: `count` independent grids (any mix of 1-D, 2-D and 3-D,
+ * uneven sizes, their own parameters) advanced together.  Every pass of a
+ * step is one persistent launch over a list of 256-cell tiles of all
+ * instances; each instance keeps its own time step (per-instance CFL
+ * minimum).  No counterpart in the reference, which runs one grid per
+ * process (mhd_model_base.hpp:89-116); each instance follows the same
+ * update as miso_b200_update.  All instances share params[0].precision.
+ * ------------------------------------------------------------------------- */
+typedef struct miso_b200_batch miso_b200_batch;
+
+int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
+                           const miso_b200_params *params, void *stream,
+                           miso_b200_batch **out);
+int miso_b200_batch_destroy(miso_b200_batch *b);
+/* Copy instance `index`'s 9 primitive fields in / out (host or device pointers). */
+int miso_b200_batch_upload(miso_b200_batch *b, int index, const double *const q[9]);
+int miso_b200_batch_download(miso_b200_batch *b, int index, double *const q[9]);
+/* Fill every instance's ghost cells from their images. */
+int miso_b200_batch_fill_ghosts(miso_b200_batch *b);
+/* nsteps of (per-instance cfl, update); with use_graph a step is captured
+ * once and replayed.  Asynchronous. */
+int miso_b200_batch_run(miso_b200_batch *b, int nsteps, int use_graph);
+/* Wait for the batch's stream; reports device-side error flags. */
+int miso_b200_batch_sync(miso_b200_batch *b);
+/* Time step of each instance's last step (count values; synchronises). */
+int miso_b200_batch_dt(miso_b200_batch *b, double *dt);
+/* Interior cells of all instances, tiles in the work list, kernels enqueued. */
+int miso_b200_batch_info(miso_b200_batch *b, long long *interior_cells, int *tiles,
+                         long long *launches);
+const char *miso_b200_batch_last_error(miso_b200_batch *b);
 
 /* Allocation-free CFL time step.  No counterpart in the reference: it is an
  * extra entry point for callers that must not let a library allocate device

@@ -62,6 +62,7 @@ SIGNATURES = {
     "miso_b200_launch_count": (ctypes.c_int, [ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_longlong)]),
     "miso_b200_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "miso_b200_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_get_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -69,6 +70,22 @@ SIGNATURES = {
     "miso_b200_cfl_noalloc": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(Params),
                                              ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p,
                                              _dp]),
+    "miso_b200_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(GridDesc),
+                                              ctypes.POINTER(Params), ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "miso_b200_batch_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_batch_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_batch_fill_ghosts": (ctypes.c_int, [ctypes.c_void_p]),
+    "miso_b200_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "miso_b200_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "miso_b200_batch_dt": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "miso_b200_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                            ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_longlong)]),
+    "miso_b200_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "miso_b200_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "miso_b200_version": (ctypes.c_char_p, []),
 }

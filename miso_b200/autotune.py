@@ -1,0 +1,107 @@
+"""Autotuner for the 3-D FP32-split kernels.
+
+For one grid shape it times, on the device and on the live state, every
+kernel variant of each kernel class -- the Runge-Kutta stage and the x, y
+and z viscosity sweeps, each as a tiled kernel (TMA plane tiles, streaming
+lines, warp-shuffle rows) or a flat one (one thread per cell) -- and a few
+work-item lengths along the march axis, and keeps the fastest of each.
+Results are cached in a JSON file keyed by precision, grid shape and SM
+count ($MISO_B200_TUNE_CACHE, default ~/.cache/miso_b200/tune.json), so a
+later run of the same shape skips the search.
+
+Timing runs whole steps, so the state advances by the steps tuned; tune
+before the run it is meant for (bench.py tunes during its warm-up).
+"""
+from __future__ import annotations
+
+import json
+import os
+
+CLASSES = {"rk_stage": 0, "av_x": 1, "av_y": 2, "av_z": 3}
+CHUNKS = (32, 64, 128)
+
+
+def cache_path() -> str:
+    return os.environ.get("MISO_B200_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "miso_b200",
+                                       "tune.json"))
+
+
+def _key(integ) -> str:
+    import torch
+    g = integ.grid
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    return f"{integ.precision}:{g.i_size}x{g.j_size}x{g.k_size}:sm{sms}"
+
+
+def _load():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _save(cache):
+    path = cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        with open(path, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+    except OSError:
+        pass
+
+
+def _times(integ, steps):
+    integ.run(1, graph=False)
+    integ.sync()
+    integ.set_timing(True)
+    integ.run(steps, graph=False)
+    rep = integ.timing_report()
+    integ.set_timing(False)
+    return {k: v["ms"] / v["launches"] for k, v in rep.items()}
+
+
+def apply(integ, choice: dict):
+    for name, kc in CLASSES.items():
+        integ.set_variant(kc, int(choice[name]))
+    integ.set_chunks(int(choice["rk_chunk"]), int(choice["av_chunk"]))
+
+
+def autotune(integ, steps: int = 2, use_cache: bool = True) -> dict:
+    """Pick and apply the fastest kernel variants for `integ` (a 3-D
+    FP32-split Integrator); returns the choice with the per-class times."""
+    if integ.get_variant(0) < 0:
+        return {}  # grid served by the per-cell kernels only
+    cache = _load() if use_cache else {}
+    key = _key(integ)
+    if key in cache:
+        apply(integ, cache[key])
+        return dict(cache[key], cached=True)
+    best = {}
+    for var in (0, 1):
+        for kc in CLASSES.values():
+            integ.set_variant(kc, var)
+        for name, ms in _times(integ, steps).items():
+            if name in CLASSES and (name not in best or ms < best[name][1]):
+                best[name] = (var, ms)
+    choice = {name: v for name, (v, _) in best.items()}
+    for name, kc in CLASSES.items():
+        integ.set_variant(kc, choice[name])
+    # work-item lengths for the winning variants
+    chunk_best = None
+    for rk_chunk in CHUNKS:
+        for av_chunk in CHUNKS:
+            integ.set_chunks(rk_chunk, av_chunk)
+            t = _times(integ, 1)
+            total = t.get("rk_stage", 0) * 4 + t.get("av_x", 0) + t.get("av_y", 0) + \
+                t.get("av_z", 0)
+            if chunk_best is None or total < chunk_best[0]:
+                chunk_best = (total, rk_chunk, av_chunk)
+    choice["rk_chunk"], choice["av_chunk"] = chunk_best[1], chunk_best[2]
+    choice["ms"] = {name: ms for name, (_, ms) in best.items()}
+    apply(integ, choice)
+    cache[key] = choice
+    if use_cache:
+        _save(cache)
+    return choice

@@ -30,6 +30,8 @@ FAST32 = ["--ftz=true", "--prec-div=false", "--prec-sqrt=false"]
 EXTRA = {
     "fp64_kernels.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
+    "batch64.cu": ["--fmad=false"],
+    "batch32.cu": FAST32,
     "fp32s_kernels.cu": FAST32,
     "s32_tiled.cu": FAST32,
     "s32_flat.cu": FAST32,

@@ -1,0 +1,66 @@
+// Batched advance of many independent grids (internal to the library).
+//
+// All instances of a batch live in the same field arrays, one after the
+// other; a table gives each instance its geometry, parameters and the
+// element offset of its cell 0.  The interior cells of every instance are
+// cut into tiles of BATCH_TILE consecutive cells; every pass of the step is
+// ONE launch of a persistent grid that walks the tile list, so instances of
+// any size share the GPU evenly.  Each instance keeps its own time step:
+// the CFL pass reduces per tile and folds the tile minima per instance
+// (segmented minimum).
+#pragma once
+
+#include "common.cuh"
+
+namespace miso_b200 {
+
+constexpr int BATCH_TILE = 256;  // cells per tile = threads per CTA
+
+struct BatchInst {
+  Geom g;
+  long long base;  // element offset of this instance's cell 0 in every array
+  long long nint;  // interior cells
+  double gm, cfl_number, ep, fh, cs_fac, ca_fac, vv_fac;
+  double min_dxyz, cfl_dx;
+};
+
+struct BatchTile {
+  int inst;   // instance index
+  int start;  // first interior linear index of the tile
+};
+
+struct BatchArgs {
+  const BatchInst *insts;
+  const BatchTile *tiles;
+  int ntiles;
+  int count;
+  StepScalars *sc;       // per instance
+  unsigned int *dtmin;   // per instance: float bits of the running CFL minimum
+  unsigned int *err;     // error bits (shared)
+};
+
+// FP64 (primitive state, bit-faithful per cell to the single-grid kernels)
+void b64_cfl(const BatchArgs &a, const FieldPtrs<const double> &q, int grid, cudaStream_t st);
+void b_finalize(const BatchArgs &a, cudaStream_t st);
+void b64_rhs(const BatchArgs &a, const FieldPtrs<const double> &o,
+             const FieldPtrs<const double> &ar, const FieldPtrs<double> &r, int stage, int grid,
+             cudaStream_t st);
+void b64_cc(const BatchArgs &a, const FieldPtrs<const double> &q, double *cc, int grid,
+            cudaStream_t st);
+void b64_av(const BatchArgs &a, const FieldPtrs<const double> &q, const FieldPtrs<double> &r,
+            const double *cc, int dir, int grid, cudaStream_t st);
+void b64_fill(const BatchArgs &a, const FieldPtrs<double> &q, int grid, cudaStream_t st);
+
+// FP32 split (conserved hi/lo state)
+void b32_cfl(const BatchArgs &a, const FieldPtrs<const float> &hi, int grid, cudaStream_t st);
+void b32_rk(const BatchArgs &a, const FieldPtrs<const float> &prev,
+            const FieldPtrs<const float> &u0, const FieldPtrs<float> &hi,
+            const FieldPtrs<float> &lo, const FieldPtrs<float> &out, float *cc, int stage,
+            int grid, cudaStream_t st);
+void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
+            const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc, int dir,
+            int grid, cudaStream_t st);
+void b32_fill(const BatchArgs &a, const FieldPtrs<float> &q, int nfields, int grid,
+              cudaStream_t st);
+
+}  // namespace miso_b200

@@ -1,0 +1,468 @@
+// C ABI of the batched solver (include/miso_b200.h, miso_b200_batch_*):
+// many independent grids -- uneven sizes, their own parameters and time
+// steps -- advanced together, one persistent launch per pass, a step
+// captured once in a CUDA graph and replayed.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/miso_b200.h"
+#include "batch.h"
+#include "common.cuh"
+#include "kernels_s32.h"
+
+using namespace miso_b200;
+
+void miso_b200_set_global_error(const std::string &msg);  // capi.cu
+
+namespace {
+constexpr size_t ALIGN = 256;
+size_t round_up(size_t x) { return (x + ALIGN - 1) / ALIGN * ALIGN; }
+}  // namespace
+
+struct miso_b200_batch {
+  int count = 0;
+  bool split = false;
+  int sms = 148, grid = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+
+  std::vector<BatchInst> insts;
+  long long total = 0;       // elements per field array (all instances)
+  long long max_cells = 0;   // largest instance (cells incl. ghosts)
+  int ntiles = 0;
+  bool sweep[3] = {false, false, false};  // some instance is non-degenerate along d
+
+  void *block = nullptr;
+  size_t bytes = 0;
+  BatchInst *d_insts = nullptr;
+  BatchTile *d_tiles = nullptr;
+  StepScalars *d_sc = nullptr;
+  unsigned int *d_dtmin = nullptr;
+  unsigned int *d_err = nullptr;
+  // FP64
+  double *q64[3][NF] = {};
+  double *cc64 = nullptr;
+  // FP32 split
+  float *hi[2][NF] = {}, *lo[2][NF] = {}, *stg[2][NF] = {};
+  float *cc32 = nullptr;
+  double *io64[NF] = {};
+  int cur = 0;
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_steps = 0, graph_cur = 0;
+  long long launches = 0, graph_kernels = 0;
+
+  int fail(int code, const std::string &m) {
+    err = m;
+    return code;
+  }
+  int cuda(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return MISO_B200_OK;
+    return fail(MISO_B200_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+  BatchArgs args() const {
+    BatchArgs a;
+    a.insts = d_insts;
+    a.tiles = d_tiles;
+    a.ntiles = ntiles;
+    a.count = count;
+    a.sc = d_sc;
+    a.dtmin = d_dtmin;
+    a.err = d_err;
+    return a;
+  }
+  template <typename T>
+  static FieldPtrs<const T> cst(T *const (&arr)[NF]) {
+    FieldPtrs<const T> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = arr[f];
+    return r;
+  }
+  template <typename T>
+  static FieldPtrs<T> mut(T *const (&arr)[NF]) {
+    FieldPtrs<T> r;
+    for (int f = 0; f < NF; ++f) r.f[f] = arr[f];
+    return r;
+  }
+
+  int enqueue_step() {
+    const BatchArgs a = args();
+    if (!split) {
+      b64_cfl(a, cst(q64[0]), grid, stream);
+      b_finalize(a, stream);
+      const int seq_a[4] = {0, 1, 2, 1}, seq_r[4] = {1, 2, 1, 2};
+      for (int s = 0; s < 4; ++s)
+        b64_rhs(a, cst(q64[0]), cst(q64[seq_a[s]]), mut(q64[seq_r[s]]), s, grid, stream);
+      b64_cc(a, cst(q64[2]), cc64, grid, stream);
+      // every sweep runs, degenerate ones included: in FP64 the reference's
+      // degenerate sweep is a round-off step of its own
+      const int src[3] = {2, 0, 1}, dst[3] = {0, 1, 0};
+      for (int d = 0; d < 3; ++d)
+        b64_av(a, cst(q64[src[d]]), mut(q64[dst[d]]), cc64, d, grid, stream);
+      launches += 2 + 4 + 1 + 3;
+    } else {
+      b32_cfl(a, cst(hi[cur]), grid, stream);
+      b_finalize(a, stream);
+      const int c = cur;
+      for (int s = 0; s < 4; ++s) {
+        FieldPtrs<const float> prev = s == 0 ? cst(hi[c]) : cst(stg[(s - 1) & 1]);
+        b32_rk(a, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]), mut(stg[s & 1]), cc32, s, grid,
+               stream);
+      }
+      launches += 2 + 4;
+      for (int d = 0; d < 3; ++d) {
+        if (!sweep[d]) continue;  // degenerate for every instance: the state is unchanged
+        b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d, grid,
+               stream);
+        cur ^= 1;
+        ++launches;
+      }
+    }
+    return cuda(cudaGetLastError(), "batch step");
+  }
+
+  int read_err() {
+    unsigned int e = 0;
+    int rc = cuda(cudaMemcpyAsync(&e, d_err, sizeof e, cudaMemcpyDeviceToHost, stream), "read");
+    if (rc) return rc;
+    if ((rc = cuda(cudaStreamSynchronize(stream), "synchronize"))) return rc;
+    if (e) {
+      cudaMemsetAsync(d_err, 0, sizeof e, stream);
+      cudaStreamSynchronize(stream);
+      if (e & ERRBIT_NONFINITE)
+        return fail(MISO_B200_ERR_NONFINITE,
+                    "non-positive or non-finite density / internal energy in a CFL pass");
+    }
+    return MISO_B200_OK;
+  }
+};
+
+extern "C" {
+
+int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
+                           const miso_b200_params *params, void *stream,
+                           miso_b200_batch **out) {
+  auto bad = [](int code, const std::string &m) {
+    miso_b200_set_global_error("miso_b200_batch_create: " + m);
+    return code;
+  };
+  if (count < 1 || !grids || !params || !out) return bad(MISO_B200_ERR_ARG, "null argument");
+  *out = nullptr;
+  auto *b = new miso_b200_batch();
+  b->count = count;
+  b->split = params[0].precision == MISO_B200_FP32_SPLIT;
+  long long off = 0;
+  std::vector<BatchTile> tiles;
+  for (int n = 0; n < count; ++n) {
+    const miso_b200_grid_desc &gd = grids[n];
+    const miso_b200_params &pp = params[n];
+    if (pp.precision != params[0].precision) {
+      delete b;
+      return bad(MISO_B200_ERR_ARG, "all instances of a batch share one precision");
+    }
+    if (gd.margin != 2 || !(pp.gm > 1.0) || !(pp.cfl_number > 0.0) || !(pp.ep >= 0.0) ||
+        !(pp.fh >= 0.0)) {
+      delete b;
+      return bad(MISO_B200_ERR_ARG, "invalid margin or parameters of instance " +
+                                        std::to_string(n));
+    }
+    BatchInst in{};
+    Geom &g = in.g;
+    const int sz[3] = {gd.i_size, gd.j_size, gd.k_size};
+    const double lo[3] = {gd.x_min, gd.y_min, gd.z_min};
+    const double hi[3] = {gd.x_max, gd.y_max, gd.z_max};
+    double ds[3];
+    for (int a = 0; a < 3; ++a) {
+      if (sz[a] < 1 || (sz[a] > 1 && sz[a] < 2 * gd.margin) || !(lo[a] < hi[a])) {
+        delete b;
+        return bad(MISO_B200_ERR_ARG, "invalid size or range of instance " + std::to_string(n));
+      }
+      g.n[a] = sz[a];
+      g.s[a] = sz[a] > 1 ? 1 : 0;
+      g.m[a] = gd.margin * g.s[a];
+      g.t[a] = sz[a] + 2 * g.m[a];
+      g.periodic[a] = gd.periodic[a] ? 1 : 0;
+      const double sp = (hi[a] - lo[a]) / (double)sz[a];
+      ds[a] = g.s[a] ? sp : 1.e30;
+      g.dsi[a] = g.s[a] ? 1.0 / sp : 0.0;
+      for (int side = 0; side < 2; ++side) {
+        g.negmask[a][side] = 0;
+        for (int f = 0; f < NF; ++f) {
+          g.sign[a][side][f] = (float)(gd.sign[a][side][f] < 0 ? -1 : 1);
+          if (!g.periodic[a] && gd.sign[a][side][f] < 0)
+            g.negmask[a][side] |= (unsigned short)(1u << f);
+        }
+      }
+      if (g.s[a]) b->sweep[a] = true;
+    }
+    g.st[2] = 1;
+    g.st[1] = g.t[2];
+    g.st[0] = (long long)g.t[1] * g.t[2];
+    g.cells = (long long)g.t[0] * g.t[1] * g.t[2];
+    in.base = off;
+    in.nint = (long long)g.n[0] * g.n[1] * g.n[2];
+    in.gm = pp.gm;
+    in.cfl_number = pp.cfl_number;
+    in.ep = pp.ep;
+    in.fh = pp.fh;
+    in.cs_fac = pp.cs_fac;
+    in.ca_fac = pp.ca_fac;
+    in.vv_fac = pp.vv_fac;
+    const float m3 = fminf(fminf((float)ds[0], (float)ds[1]), (float)ds[2]);
+    in.min_dxyz = (double)m3;
+    in.cfl_dx = pp.cfl_number * (double)m3;
+    b->insts.push_back(in);
+    for (long long s = 0; s < in.nint; s += BATCH_TILE) tiles.push_back(BatchTile{n, (int)s});
+    off += (g.cells + 63) / 64 * 64;  // instances start on 256-byte (FP32) boundaries
+    if (g.cells > b->max_cells) b->max_cells = g.cells;
+  }
+  b->total = off;
+  b->ntiles = (int)tiles.size();
+
+  cudaError_t e = cudaSuccess;
+  int dev = 0;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) {
+    delete b;
+    return bad(MISO_B200_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  }
+  b->grid = b->sms * 8;
+  if (stream) {
+    b->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete b;
+      return bad(MISO_B200_ERR_CUDA, "stream creation failed");
+    }
+    b->own_stream = true;
+  }
+  const size_t cells = (size_t)b->total;
+  std::vector<std::pair<void **, size_t>> plan;
+  size_t total = 0;
+  auto add = [&](void **p, size_t bytes) {
+    plan.emplace_back(p, bytes);
+    total += round_up(bytes);
+  };
+  add((void **)&b->d_insts, sizeof(BatchInst) * count);
+  add((void **)&b->d_tiles, sizeof(BatchTile) * tiles.size());
+  add((void **)&b->d_sc, sizeof(StepScalars) * count);
+  add((void **)&b->d_dtmin, sizeof(unsigned int) * count);
+  add((void **)&b->d_err, sizeof(unsigned int));
+  if (!b->split) {
+    for (int s = 0; s < 3; ++s)
+      for (int f = 0; f < NF; ++f) add((void **)&b->q64[s][f], cells * sizeof(double));
+    add((void **)&b->cc64, cells * sizeof(double));
+  } else {
+    for (int s = 0; s < 2; ++s) {
+      for (int f = 0; f < NF; ++f) add((void **)&b->hi[s][f], cells * sizeof(float));
+      for (int f = 0; f < NF; ++f) add((void **)&b->lo[s][f], cells * sizeof(float));
+    }
+    for (int s = 0; s < 2; ++s)
+      for (int f = 0; f < NF; ++f) add((void **)&b->stg[s][f], cells * sizeof(float));
+    add((void **)&b->cc32, cells * sizeof(float));
+  }
+  e = cudaMalloc(&b->block, total);
+  if (e != cudaSuccess) {
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return bad(MISO_B200_ERR_NOMEM, "device allocation of " + std::to_string(total) +
+                                        " bytes failed");
+  }
+  b->bytes = total;
+  size_t o = 0;
+  for (auto &pb : plan) {
+    *pb.first = (char *)b->block + o;
+    o += round_up(pb.second);
+  }
+  if (b->split)  // FP64 staging of one instance over the stage arrays (no state between steps)
+    for (int f = 0; f < NF; ++f) b->io64[f] = (double *)b->stg[0][0] + (size_t)f * b->max_cells;
+  e = cudaMemsetAsync(b->block, 0, total, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_insts, b->insts.data(), sizeof(BatchInst) * count,
+                        cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(),
+                        cudaMemcpyHostToDevice, b->stream);
+  std::vector<unsigned int> init(count);
+  const float big = 1.e10f;
+  unsigned int bits;
+  memcpy(&bits, &big, sizeof bits);
+  for (auto &v : init) v = bits;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_dtmin, init.data(), sizeof(unsigned int) * count,
+                        cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) {
+    cudaFree(b->block);
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return bad(MISO_B200_ERR_CUDA, std::string("batch set-up: ") + cudaGetErrorString(e));
+  }
+  *out = b;
+  return MISO_B200_OK;
+}
+
+int miso_b200_batch_destroy(miso_b200_batch *b) {
+  if (!b) return MISO_B200_ERR_ARG;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->block) cudaFree(b->block);
+  if (b->own_stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return MISO_B200_OK;
+}
+
+int miso_b200_batch_upload(miso_b200_batch *b, int index, const double *const q[9]) {
+  if (!b || !q || index < 0 || index >= b->count) return MISO_B200_ERR_ARG;
+  const BatchInst &in = b->insts[index];
+  const size_t bytes = (size_t)in.g.cells * sizeof(double);
+  int rc;
+  for (int f = 0; f < NF; ++f) {
+    if (!q[f]) return b->fail(MISO_B200_ERR_ARG, "null field pointer");
+    double *dst = b->split ? b->io64[f] : b->q64[0][f] + in.base;
+    if ((rc = b->cuda(cudaMemcpyAsync(dst, q[f], bytes, cudaMemcpyDefault, b->stream), "upload")))
+      return rc;
+  }
+  if (b->split) {
+    FieldPtrs<const double> src;
+    FieldPtrs<float> h, l;
+    for (int f = 0; f < NF; ++f) {
+      src.f[f] = b->io64[f];
+      h.f[f] = b->hi[b->cur][f] + in.base;
+      l.f[f] = b->lo[b->cur][f] + in.base;
+    }
+    launch_s32_to_split(in.g.cells, src, h, l, b->sms, b->stream);
+    if ((rc = b->cuda(cudaGetLastError(), "to_split"))) return rc;
+  }
+  return b->cuda(cudaStreamSynchronize(b->stream), "upload synchronize");
+}
+
+int miso_b200_batch_download(miso_b200_batch *b, int index, double *const q[9]) {
+  if (!b || !q || index < 0 || index >= b->count) return MISO_B200_ERR_ARG;
+  const BatchInst &in = b->insts[index];
+  const size_t bytes = (size_t)in.g.cells * sizeof(double);
+  int rc;
+  if (b->split) {
+    FieldPtrs<const float> h, l;
+    FieldPtrs<double> dst;
+    for (int f = 0; f < NF; ++f) {
+      h.f[f] = b->hi[b->cur][f] + in.base;
+      l.f[f] = b->lo[b->cur][f] + in.base;
+      dst.f[f] = b->io64[f];
+    }
+    launch_s32_from_split(in.g.cells, h, l, dst, b->sms, b->stream);
+    if ((rc = b->cuda(cudaGetLastError(), "from_split"))) return rc;
+  }
+  for (int f = 0; f < NF; ++f) {
+    if (!q[f]) return b->fail(MISO_B200_ERR_ARG, "null field pointer");
+    const double *src = b->split ? b->io64[f] : b->q64[0][f] + in.base;
+    if ((rc = b->cuda(cudaMemcpyAsync(q[f], src, bytes, cudaMemcpyDefault, b->stream),
+                      "download")))
+      return rc;
+  }
+  return b->cuda(cudaStreamSynchronize(b->stream), "download synchronize");
+}
+
+int miso_b200_batch_fill_ghosts(miso_b200_batch *b) {
+  if (!b) return MISO_B200_ERR_ARG;
+  const BatchArgs a = b->args();
+  if (!b->split) {
+    b64_fill(a, b->mut(b->q64[0]), b->grid, b->stream);
+  } else {
+    b32_fill(a, b->mut(b->hi[b->cur]), NF, b->grid, b->stream);
+    b32_fill(a, b->mut(b->lo[b->cur]), NF, b->grid, b->stream);
+  }
+  return b->cuda(cudaGetLastError(), "fill_ghosts");
+}
+
+int miso_b200_batch_run(miso_b200_batch *b, int nsteps, int use_graph) {
+  if (!b || nsteps < 0) return MISO_B200_ERR_ARG;
+  int rc;
+  if (!use_graph) {
+    for (int n = 0; n < nsteps; ++n)
+      if ((rc = b->enqueue_step())) return rc;
+    return MISO_B200_OK;
+  }
+  if (b->graph_exec && b->graph_cur != b->cur) {
+    cudaGraphExecDestroy(b->graph_exec);
+    cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+  }
+  if (!b->graph_exec) {
+    const int before = b->cur;
+    const long long l0 = b->launches;
+    if ((rc = b->cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal),
+                      "begin capture")))
+      return rc;
+    int steps = 1;
+    rc = b->enqueue_step();
+    if (!rc && b->cur != before) {
+      steps = 2;
+      rc = b->enqueue_step();
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    b->cur = before;
+    const long long kernels = b->launches - l0;
+    b->launches = l0;
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if ((rc = b->cuda(e, "end capture"))) return rc;
+    b->graph = g;
+    if ((rc = b->cuda(cudaGraphInstantiate(&b->graph_exec, g, 0), "graph instantiate")))
+      return rc;
+    b->graph_steps = steps;
+    b->graph_cur = before;
+    b->graph_kernels = kernels;
+  }
+  const int reps = nsteps / b->graph_steps, rem = nsteps % b->graph_steps;
+  for (int n = 0; n < reps; ++n) {
+    if ((rc = b->cuda(cudaGraphLaunch(b->graph_exec, b->stream), "graph launch"))) return rc;
+    b->launches += b->graph_kernels;
+  }
+  for (int n = 0; n < rem; ++n)
+    if ((rc = b->enqueue_step())) return rc;
+  return MISO_B200_OK;
+}
+
+int miso_b200_batch_sync(miso_b200_batch *b) {
+  if (!b) return MISO_B200_ERR_ARG;
+  return b->read_err();
+}
+
+int miso_b200_batch_dt(miso_b200_batch *b, double *dt) {
+  if (!b || !dt) return MISO_B200_ERR_ARG;
+  std::vector<StepScalars> sc(b->count);
+  int rc = b->cuda(cudaMemcpyAsync(sc.data(), b->d_sc, sizeof(StepScalars) * b->count,
+                                   cudaMemcpyDeviceToHost, b->stream),
+                   "read dt");
+  if (rc) return rc;
+  if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "synchronize"))) return rc;
+  for (int n = 0; n < b->count; ++n) dt[n] = sc[n].dt;
+  return MISO_B200_OK;
+}
+
+int miso_b200_batch_info(miso_b200_batch *b, long long *interior_cells, int *tiles,
+                         long long *launches) {
+  if (!b) return MISO_B200_ERR_ARG;
+  long long n = 0;
+  for (auto &in : b->insts) n += in.nint;
+  if (interior_cells) *interior_cells = n;
+  if (tiles) *tiles = b->ntiles;
+  if (launches) *launches = b->launches;
+  return MISO_B200_OK;
+}
+
+const char *miso_b200_batch_last_error(miso_b200_batch *b) { return b ? b->err.c_str() : ""; }
+
+}  // extern "C"

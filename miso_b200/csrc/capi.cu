@@ -491,7 +491,7 @@ struct miso_b200_handle {
         launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, av_grid, stream);
       else
         launch_s32_av_z(a, z_grid, stream);
-      te(t, "av_sweep", interior() * 148.0);
+      te(t, d == 0 ? "av_x" : d == 1 ? "av_y" : "av_z", interior() * 148.0);
       if ((rc = check_launch("av_sweep"))) return rc;
       cur ^= 1;
     }
@@ -929,6 +929,22 @@ int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
     h->rk_var = variant;
   else
     h->av_var[kernel_class - 1] = variant;
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_chunks(miso_b200_handle *h, int rk_chunk, int av_chunk) {
+  if (!h || rk_chunk < 1 || av_chunk < 1) return MISO_B200_ERR_ARG;
+  if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "chunk lengths apply to 3-D split grids");
+  h->rk_L = rk_chunk;
+  h->av_L = av_chunk;
+  s32_rk_items(h->g, h->rk_L, h->rk_tiles_j, h->rk_tiles_k, h->rk_items);
+  h->rk_grid = h->rk_items < 2 * h->sms ? h->rk_items : 2 * h->sms;
   if (h->graph_exec) {
     cudaGraphExecDestroy(h->graph_exec);
     cudaGraphDestroy(h->graph);

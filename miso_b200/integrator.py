@@ -211,6 +211,9 @@ class Integrator:
     def set_variant(self, kernel_class: int, variant: int):
         self._check(self._lib.miso_b200_set_variant(self._h, int(kernel_class), int(variant)))
 
+    def set_chunks(self, rk_chunk: int, av_chunk: int):
+        self._check(self._lib.miso_b200_set_chunks(self._h, int(rk_chunk), int(av_chunk)))
+
     def get_variant(self, kernel_class: int) -> int:
         v = ctypes.c_int()
         self._check(self._lib.miso_b200_get_variant(self._h, int(kernel_class), ctypes.byref(v)))

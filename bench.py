@@ -235,7 +235,6 @@ def run_b200(args):
     report = integ.timing_report()
     integ.set_timing(False)
     value = world * cells * K / (ms / 1e3) / 1e9
-    state_split = integ.download() if not args.no_fp64 else None
 
     # graph replay of the same step (production path)
     ms_graph = timed_run(integ, K if K % 2 == 0 else K + 1, graph=True)
@@ -256,6 +255,33 @@ def run_b200(args):
     e2e = {"value": world * cells * K / e2e_s / 1e9, "unit": UNIT,
            "h2d_bytes_per_step": 96, "d2h_bytes_per_step": 96 + 8 * 8 * 2 * sms,
            "path": "Integrator.cfl() -> update(dt) -> monitors() per step, host dt"}
+
+    # ---- the same step with the whole FP64 primitive state crossing PCIe
+    # both ways every step (pinned host fields, upload -> cfl -> update ->
+    # download): what a caller holding its fields on the host pays per step
+    host_fields = None
+    try:
+        hb = torch.empty((9,) + tuple(prob.grid.shape), dtype=torch.float64, pin_memory=True)
+        hbn = hb.numpy()
+        integ.download(out=hbn)
+        Kh = 2
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(Kh):
+            integ.upload(hbn)
+            dt = integ.cfl()
+            integ.update(dt)
+            integ.download(out=hbn)
+        torch.cuda.synchronize()
+        hs = max_over_ranks(time.perf_counter() - t0, world)
+        fb = hbn.nbytes
+        host_fields = {"value": world * cells * Kh / hs / 1e9, "unit": UNIT, "steps": Kh,
+                       "h2d_bytes_per_step": fb + 96, "d2h_bytes_per_step": fb + 8,
+                       "path": "upload(host fp64) -> cfl() -> update(dt) -> download() per step"}
+        del hb, hbn
+    except Exception as exc:  # pinned host memory may be short on a small host
+        host_fields = {"value": None, "unit": UNIT, "skipped": f"{type(exc).__name__}: {exc}"}
     integ.close()
 
     # ---- FP64 comparison on the same workload (same steps)
@@ -270,6 +296,20 @@ def run_b200(args):
         v64 = world * cells * K / (ms64 / 1e3) / 1e9
         st64 = i64.download()
         i64.close()
+        # the same W + K steps in the split form from the same initial state,
+        # with the tuned kernel variants (the timed integrator above also
+        # advanced through the tuner's steps)
+        isp = Integrator(prob.config, prob.grid, precision=args.precision,
+                         stream=stream.cuda_stream)
+        if tuning:
+            from miso_b200.autotune import apply as apply_tuning
+            apply_tuning(isp, tuning)
+        isp.upload(prob.q)
+        isp.apply_boundary_condition()
+        isp.run(W + K, graph=False)
+        isp.sync()
+        state_split = isp.download()
+        isp.close()
         inner = (slice(None),) + prob.grid.interior
         a, b = state_split[inner], st64[inner]
         gm = prob.config["eos"]["gm"]
@@ -305,7 +345,7 @@ def run_b200(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference(96, 3, 0, 1)
+            cpu = cpu_reference(96, 4, 0, 1)
         except Exception as exc:  # the checker may be absent on a stripped box
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "unavailable",
                    "sample": f"{type(exc).__name__}: {exc}"}
@@ -327,7 +367,7 @@ def run_b200(args):
             "kernels": {k: {"launches": v["launches"], "ms_per_step": v["ms"] / K,
                             "GBps": v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] else None}
                         for k, v in report.items()},
-            "roofline": roofline, "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu,
+            "roofline": roofline, "e2e": e2e, "e2e_host_fields": host_fields, "fp64": fp64, "cpu_baseline": cpu,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -28,6 +28,7 @@ extern "C" {
 #define MISO_B200_ERR_NONFINITE (-3) /* non-positive/non-finite ro or ei seen by the CFL pass */
 #define MISO_B200_ERR_STATE (-4)    /* call not valid in the handle's current state */
 #define MISO_B200_ERR_NOMEM (-5)    /* device allocation failed */
+#define MISO_B200_ERR_TIMEOUT (-6)  /* a bounded device-side wait (TMA copy) ran out */
 
 #define MISO_B200_FP64 0        /* primitive FP64 state, bit-faithful to the reference */
 #define MISO_B200_FP32_SPLIT 1  /* conserved FP32 hi/lo state, FP32 RHS and viscosity */
@@ -128,8 +129,10 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
 /* Kernel variant of one kernel class on the 3-D FP32-split path:
  * kernel_class 0 = Runge-Kutta stage, 1/2/3 = viscosity sweep x/y/z;
  * variant 0 = tiled (TMA plane tiles / streaming lines / warp-shuffle rows),
- * 1 = flat (one thread per cell).  Both compute the same step; the
- * autotuner (miso_b200/autotune.py) times them and keeps the faster.
+ * 1 = flat (one thread per cell), 2 (Runge-Kutta stage only, the default)
+ * = pipelined TMA planes with packed FP32x2 differences.  All compute the
+ * same step; the autotuner (miso_b200/autotune.py) times them and keeps the
+ * fastest.
  * ERR_STATE on grids that use the simple per-cell kernels only. */
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant);
 int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant);

@@ -18,6 +18,7 @@ ERR_CUDA = -2
 ERR_NONFINITE = -3
 ERR_STATE = -4
 ERR_NOMEM = -5
+ERR_TIMEOUT = -6
 
 FP64 = 0
 FP32_SPLIT = 1

@@ -3,7 +3,8 @@
 For one grid shape it times, on the device and on the live state, every
 kernel variant of each kernel class -- the Runge-Kutta stage and the x, y
 and z viscosity sweeps, each as a tiled kernel (TMA plane tiles, streaming
-lines, warp-shuffle rows) or a flat one (one thread per cell) -- and a few
+lines, warp-shuffle rows) or a flat one (one thread per cell), and for the
+Runge-Kutta stage also the pipelined plane kernel -- and a few
 work-item lengths along the march axis, and keeps the fastest of each.
 Results are cached in a JSON file keyed by precision, grid shape and SM
 count ($MISO_B200_TUNE_CACHE, default ~/.cache/miso_b200/tune.json), so a
@@ -18,6 +19,8 @@ import json
 import os
 
 CLASSES = {"rk_stage": 0, "av_x": 1, "av_y": 2, "av_z": 3}
+# variants per class: RK 0 tiled, 1 flat, 2 pipelined planes; AV 0 tiled, 1 flat
+VARIANTS = {"rk_stage": (0, 1, 2), "av_x": (0, 1), "av_y": (0, 1), "av_z": (0, 1)}
 CHUNKS = (32, 64, 128)
 
 
@@ -79,11 +82,13 @@ def autotune(integ, steps: int = 2, use_cache: bool = True) -> dict:
         apply(integ, cache[key])
         return dict(cache[key], cached=True)
     best = {}
-    for var in (0, 1):
-        for kc in CLASSES.values():
-            integ.set_variant(kc, var)
+    for var in range(max(len(v) for v in VARIANTS.values())):
+        for name, kc in CLASSES.items():
+            if var in VARIANTS[name]:
+                integ.set_variant(kc, var)
         for name, ms in _times(integ, steps).items():
-            if name in CLASSES and (name not in best or ms < best[name][1]):
+            if name in CLASSES and var in VARIANTS[name] and \
+                    (name not in best or ms < best[name][1]):
                 best[name] = (var, ms)
     choice = {name: v for name, (v, _) in best.items()}
     for name, kc in CLASSES.items():

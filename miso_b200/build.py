@@ -35,6 +35,7 @@ EXTRA = {
     "fp32s_kernels.cu": FAST32,
     "s32_tiled.cu": FAST32,
     "s32_flat.cu": FAST32,
+    "s32_rk.cu": FAST32,
 }
 
 

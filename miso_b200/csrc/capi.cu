@@ -165,8 +165,9 @@ struct miso_b200_handle {
   int z_parts = 0;  // CFL partial minima written by the last z sweep
   bool partials_valid = false;  // `partial` holds CFL minima of the current state
   // kernel variant per class on the 3-D split path: 0 = tiled (TMA plane
-  // tiles / streaming lines), 1 = flat (one thread per cell)
-  int rk_var = 0;
+  // tiles / streaming lines), 1 = flat (one thread per cell), 2 (RK only) =
+  // pipelined TMA planes with packed FP32x2 differences
+  int rk_var = 2;
   int av_var[3] = {0, 0, 0};
   double *mon_partial = nullptr;
   int mon_blocks = 0;
@@ -462,6 +463,8 @@ struct miso_b200_handle {
       if (rk_var == 1)
         launch_s32_rk_flat(st == 0 ? cfs(hi[c]) : cfs(stg[(st - 1) & 1]), a, st, flat_grid,
                            stream);
+      else if (rk_var == 2)
+        launch_s32_rk_pipe(tm, a, st, rk_grid, stream);
       else
         launch_s32_rk_tiled(tm, a, st, rk_grid, stream);
       te(t, "rk_stage", interior() * (st == 0 ? 72.0 : st < 3 ? 108.0 : 184.0));
@@ -506,9 +509,12 @@ struct miso_b200_handle {
                   "read error flags");
     if (rc) return rc;
     if ((rc = cuda(cudaStreamSynchronize(stream), "synchronize"))) return rc;
-    if (e & ERRBIT_NONFINITE) {
+    if (e & (ERRBIT_NONFINITE | ERRBIT_TIMEOUT)) {
       unsigned int zero = 0;
       cudaMemcpy(&sc->err, &zero, sizeof zero, cudaMemcpyHostToDevice);
+      if (e & ERRBIT_TIMEOUT)
+        return fail(MISO_B200_ERR_TIMEOUT,
+                    "a device-side wait for a TMA copy ran out; the step's result is invalid");
       return fail(MISO_B200_ERR_NONFINITE,
                   "non-positive or non-finite density / internal energy in the CFL pass");
     }
@@ -661,7 +667,7 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   h->pitch = (long long)(round_up(cells * sizeof(float)) / sizeof(float));
   if (h->split() && s32_tiled_supported(g) && !getenv("MISO_B200_UNTILED")) {
     const size_t pb = round_up(cells * sizeof(float));
-    bool ok = s32_configure() == 0;
+    bool ok = s32_configure() == 0 && s32_rk_pipe_configure() == 0;
     for (int s = 0; s < 2 && ok; ++s) {
       ok = s32_make_tmap(g, h->hi[s][0], pb, 0, h->tm_hi[s]) == 0 &&
            s32_make_tmap(g, h->stg[s][0], pb, 0, h->tm_stg[s]) == 0 &&
@@ -676,7 +682,8 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
       h->rk_grid = h->rk_items < per_sm * h->sms ? h->rk_items : per_sm * h->sms;
       h->av_grid = 3 * h->sms;
       h->flat_grid = 3 * h->sms;  // 256 threads x 80 registers: 3 resident CTAs per SM
-      if (const char *v = getenv("MISO_B200_RK")) h->rk_var = strcmp(v, "flat") == 0 ? 1 : 0;
+      if (const char *v = getenv("MISO_B200_RK"))
+        h->rk_var = strcmp(v, "flat") == 0 ? 1 : strcmp(v, "tiled") == 0 ? 0 : 2;
       if (const char *v = getenv("MISO_B200_AV"))
         for (int d = 0; d < 3 && v[d]; ++d) h->av_var[d] = v[d] == 'f' ? 1 : 0;
     }
@@ -762,7 +769,7 @@ int miso_b200_cfl(miso_b200_handle *h, double *dt_out) {
                     "read dt")))
     return rc;
   if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cfl synchronize"))) return rc;
-  if (v.err & ERRBIT_NONFINITE) return h->read_err();
+  if (v.err & (ERRBIT_NONFINITE | ERRBIT_TIMEOUT)) return h->read_err();
   *dt_out = v.dt;
   return MISO_B200_OK;
 }
@@ -922,7 +929,8 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]) {
 }
 
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
-  if (!h || kernel_class < 0 || kernel_class > 3 || variant < 0 || variant > 1)
+  if (!h || kernel_class < 0 || kernel_class > 3 || variant < 0 ||
+      variant > (kernel_class == 0 ? 2 : 1))
     return MISO_B200_ERR_ARG;
   if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "kernel variants apply to 3-D split grids");
   if (kernel_class == 0)

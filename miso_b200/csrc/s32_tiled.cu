@@ -30,59 +30,10 @@
 #include "common.cuh"
 #include "s32_tiled.h"
 #include "s32_common.cuh"
+#include "tma.cuh"
 
 namespace miso_b200 {
 namespace s32t {
-
-// ---------------------------------------------------------------------------
-// mbarrier / TMA
-// ---------------------------------------------------------------------------
-constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s: far beyond any copy
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-// Bounded wait for phase `parity`; false on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
-  const unsigned a = smem_u32(bar);
-  const long long t0 = clock64();
-  while (true) {
-    unsigned done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (clock64() - t0 > WAIT_CYCLES) return false;
-  }
-}
-__device__ __forceinline__ void tma4(const CUtensorMap *tm, void *dst, unsigned long long *bar,
-                                     int c0, int c1, int c2, int c3) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
-      "l"((unsigned long long)tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tma3(const CUtensorMap *tm, void *dst, unsigned long long *bar,
-                                     int c0, int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"((unsigned long long)tm), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-      : "memory");
-}
 
 // ---------------------------------------------------------------------------
 // RK stage kernel

@@ -46,6 +46,10 @@ int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out);
 int s32_configure();
 void s32_rk_items(const Geom &g, int L, int &tiles_j, int &tiles_k, int &items);
 void launch_s32_rk_tiled(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st);
+// Pipelined RK stage (s32_rk.cu): same tensor map and work items as the
+// tiled kernel, one barrier per plane, packed FP32x2 differences.
+int s32_rk_pipe_configure();
+void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st);
 void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
                         int dir, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);

@@ -22,6 +22,9 @@ struct BatchInst {
   long long nint;  // interior cells
   double gm, cfl_number, ep, fh, cs_fac, ca_fac, vv_fac;
   double min_dxyz, cfl_dx;
+  // block-tile axes of the FP32 kernels: R = the last non-degenerate axis
+  // (unit stride), C = the one before it, P = the first of three (-1: none)
+  int ax_r, ax_c, ax_p;
 };
 
 struct BatchTile {
@@ -29,10 +32,19 @@ struct BatchTile {
   int start;  // first interior linear index of the tile
 };
 
+// Block tile of the FP32 kernels: BATCH_TC x BATCH_TR interior cells in the
+// (C, R) axes at one P coordinate (1 x BATCH_TILE for 1-D instances).
+constexpr int BATCH_TC = 8, BATCH_TR = 32;
+struct BlockTile {
+  int inst, p, c0, r0;
+};
+
 struct BatchArgs {
   const BatchInst *insts;
   const BatchTile *tiles;
   int ntiles;
+  const BlockTile *btiles;  // FP32 block tiles
+  int nbtiles;
   int count;
   StepScalars *sc;       // per instance
   unsigned int *dtmin;   // per instance: float bits of the running CFL minimum
@@ -62,5 +74,7 @@ void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtr
             int grid, cudaStream_t st);
 void b32_fill(const BatchArgs &a, const FieldPtrs<float> &q, int nfields, int grid,
               cudaStream_t st);
+// resident CTAs of the block-tile kernels on `sms` SMs (their persistent grid)
+int b32_block_grid(int sms);
 
 }  // namespace miso_b200

@@ -102,36 +102,188 @@ cfl_kernel(BatchArgs a, FieldPtrs<const float> hi) {
   }
 }
 
-// Runge-Kutta stage `stage` for every instance (see rk_flat_kernel).
-__global__ void __launch_bounds__(BATCH_TILE)
-rk_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float> u0,
-          FieldPtrs<float> hi, FieldPtrs<float> lo, FieldPtrs<float> out, float *cc, int stage) {
-  __shared__ TileState ts;
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    load_tile(a, t, ts);
-    const BatchInst &in = ts.inst;
-    const long long lin = ts.start + threadIdx.x;
-    if (lin < in.nint) {
-      const Geom &g = in.g;
-      int x0, x1, x2;
-      const long long c = decode(g, lin, x0, x1, x2);
-      const StepScalars &sc = a.sc[ts.idx];
-      const float ch2 = (float)sc.ch2, dt = (float)sc.dts[stage];
-      const float decay = (float)sc.ph_decay[stage];
-      const float gm1 = (float)(in.gm - 1.0);
-      float D[NF];
+// ---------------------------------------------------------------------------
+// Block-tile kernels.  A tile is BATCH_TC x BATCH_TR interior cells in the
+// instance's (C, R) axes at one P coordinate, or 1 x BATCH_TILE cells of a
+// 1-D instance.  The tile's input state with a 2-cell halo along R and C is
+// staged in shared memory once; flux vectors (RK) and limited variables
+// (viscosity) along R and C are formed once per point there, so each cell
+// reads its neighbours from shared memory.  The P axis of 3-D instances
+// keeps per-cell neighbour evaluation from global memory.
+// ---------------------------------------------------------------------------
+constexpr int TC = BATCH_TC, TR = BATCH_TR;
+constexpr int U_PTS = (TC + 4) * (TR + 4) > BATCH_TILE + 4 ? (TC + 4) * (TR + 4) : BATCH_TILE + 4;
+constexpr int FR_PTS = TC * (TR + 4) > BATCH_TILE + 4 ? TC * (TR + 4) : BATCH_TILE + 4;
+constexpr int FC_PTS = (TC + 4) * TR;
+constexpr int W_PTS = (TC + 4) * TR > U_PTS ? (TC + 4) * TR : U_PTS;
+
+struct BlockGeo {
+  BatchInst in;
+  int idx;
+  int tc, tr;            // tile extent (TC x TR, or 1 x BATCH_TILE)
+  int nc, nr;            // cells of the tile inside the interior
+  int hc;                // halo width along C (0 when the instance has no C axis)
+  long long cell0;       // element index (instance-relative) of the tile's first cell
+  long long sP, sC, sR;  // strides of the P, C, R axes (0 when absent)
+  int oC, oR;            // total coordinate of the tile origin along C, R
+  int tC, tR;            // total extent along C, R
+  int x[3];              // interior coordinates of the tile origin per array axis
+};
+
+__device__ __forceinline__ void load_block(const BatchArgs &a, int t, BlockGeo &bg) {
+  if (threadIdx.x == 0) {
+    const BlockTile bt = a.btiles[t];
+    bg.idx = bt.inst;
+    bg.in = a.insts[bt.inst];
+    const Geom &g = bg.in.g;
+    const int R = bg.in.ax_r, C = bg.in.ax_c, P = bg.in.ax_p;
+    bg.tc = C >= 0 ? TC : 1;
+    bg.tr = C >= 0 ? TR : BATCH_TILE;
+    bg.hc = C >= 0 ? 2 : 0;
+    bg.nr = min(bg.tr, g.n[R] - bt.r0);
+    bg.nc = C >= 0 ? min(bg.tc, g.n[C] - bt.c0) : 1;
+    bg.sR = g.st[R];
+    bg.sC = C >= 0 ? g.st[C] : 0;
+    bg.sP = P >= 0 ? g.st[P] : 0;
+    bg.oR = bt.r0 + g.m[R];
+    bg.oC = C >= 0 ? bt.c0 + g.m[C] : 0;
+    bg.tR = g.t[R];
+    bg.tC = C >= 0 ? g.t[C] : 1;
+    bg.x[0] = bg.x[1] = bg.x[2] = 0;
+    bg.x[R] = bt.r0;
+    if (C >= 0) bg.x[C] = bt.c0;
+    if (P >= 0) bg.x[P] = bt.p;
+    bg.cell0 = (P >= 0 ? (long long)(bt.p + g.m[P]) * bg.sP : 0) + (long long)bg.oC * bg.sC +
+               (long long)bg.oR * bg.sR;
+  }
+  __syncthreads();
+}
+
+// element index of tile point (c, r) in halo coordinates (c in [0, tc+2hc),
+// r in [0, tr+4)), clamped into the instance's array
+__device__ __forceinline__ long long block_point(const BlockGeo &bg, int c, int r) {
+  const int ct = min(max(bg.oC + c - bg.hc, 0), bg.tC - 1);
+  const int rt = min(max(bg.oR + r - 2, 0), bg.tR - 1);
+  return bg.cell0 + (long long)(ct - bg.oC) * bg.sC + (long long)(rt - bg.oR) * bg.sR;
+}
+
+template <int D>
+__device__ __forceinline__ void flux_pt(const float (&U)[NF][U_PTS], int m, float gm1, float ch2,
+                                        float F[NF]) {
+  float u[NF];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) D[f] = 0.0f;
-      if (g.s[0]) diff_dir<0>(prev, in.base, c, g.st[0], (float)(g.dsi[0] * INV12), gm1, ch2, D);
-      if (g.s[1]) diff_dir<1>(prev, in.base, c, g.st[1], (float)(g.dsi[1] * INV12), gm1, ch2, D);
-      if (g.s[2]) diff_dir<2>(prev, in.base, c, 1, (float)(g.dsi[2] * INV12), gm1, ch2, D);
-      const bool nb = near_boundary(g, x0, x1, x2);
+  for (int f = 0; f < NF; ++f) u[f] = U[f][m];
+  PrimF p;
+  prim(u, gm1, p);
+  flux_dir<D>(u, p, ch2, F);
+}
+
+__device__ __forceinline__ void flux_pt_axis(const float (&U)[NF][U_PTS], int m, int axis,
+                                             float gm1, float ch2, float F[NF]) {
+  if (axis == 0)
+    flux_pt<0>(U, m, gm1, ch2, F);
+  else if (axis == 1)
+    flux_pt<1>(U, m, gm1, ch2, F);
+  else
+    flux_pt<2>(U, m, gm1, ch2, F);
+}
+
+// 4th-order difference along the P axis (axis 0 of a 3-D instance) from
+// global memory, as the per-cell kernels form it
+__device__ __forceinline__ void diff_p(const FieldPtrs<const float> &s, long long base,
+                                       long long c, long long S, float w, float gm1, float ch2,
+                                       float acc[NF]) {
+  diff_dir<0>(s, base, c, S, w, gm1, ch2, acc);
+}
+
+// Runge-Kutta stage `stage` for every instance (flux form; see rk_flat_kernel).
+__global__ void __launch_bounds__(BATCH_TILE, 3)
+rk_block_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float> u0,
+                FieldPtrs<float> hi, FieldPtrs<float> lo, FieldPtrs<float> out, float *cc,
+                int stage) {
+  __shared__ BlockGeo bg;
+  __shared__ float U[NF][U_PTS];
+  __shared__ float FR[NF][FR_PTS];
+  __shared__ float FC[NF][FC_PTS];
+  const int tid = threadIdx.x;
+  for (int t = blockIdx.x; t < a.nbtiles; t += gridDim.x) {
+    load_block(a, t, bg);
+    const BatchInst &in = bg.in;
+    const Geom &g = in.g;
+    const int R = in.ax_r, C = in.ax_c, P = in.ax_p;
+    const StepScalars &sc = a.sc[bg.idx];
+    const float ch2 = (float)sc.ch2, dt = (float)sc.dts[stage];
+    const float decay = (float)sc.ph_decay[stage];
+    const float gm1 = (float)(in.gm - 1.0);
+    const int W = bg.tr + 4, H = bg.tc + 2 * bg.hc;
+    const int tcl = tid / bg.tr, trl = tid % bg.tr;
+    const bool mine = tcl < bg.nc && trl < bg.nr;
+    const long long c = bg.cell0 + (long long)tcl * bg.sC + (long long)trl * bg.sR;
+    // centre values of this thread's cell, loaded before the staging waits
+    float A0[NF], A1[NF];
+    if (mine) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        if (stage < 3) {
+          A0[f] = __ldg(u0.f[f] + in.base + c);
+        } else {
+          A0[f] = hi.f[f][in.base + c];
+          A1[f] = lo.f[f][in.base + c];
+        }
+      }
+    }
+    // 1. stage input with halos
+    for (int m = tid; m < H * W; m += BATCH_TILE) {
+      const long long e = in.base + block_point(bg, m / W, m % W);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) U[f][m] = __ldg(prev.f[f] + e);
+    }
+    __syncthreads();
+    // 2. flux vectors along R (tile rows, R halo) and C (tile columns, C halo)
+    for (int m = tid; m < bg.tc * W; m += BATCH_TILE) {
+      float F[NF];
+      flux_pt_axis(U, m + bg.hc * W, R, gm1, ch2, F);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) FR[f][m] = F[f];
+    }
+    if (C >= 0) {
+      for (int m = tid; m < H * bg.tr; m += BATCH_TILE) {
+        const int c = m / bg.tr, r = m % bg.tr;
+        float F[NF];
+        flux_pt_axis(U, c * W + r + 2, C, gm1, ch2, F);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) FC[f][m] = F[f];
+      }
+    }
+    __syncthreads();
+    // 3. the tile's cells
+    if (mine) {
+      const float wR = (float)(g.dsi[R] * INV12);
+      float D[NF];
+      {
+        const int m = tcl * W + trl;
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+          D[f] = wR * ((FR[f][m] - FR[f][m + 4]) + 8.0f * (FR[f][m + 3] - FR[f][m + 1]));
+      }
+      if (C >= 0) {
+        const float wC = (float)(g.dsi[C] * INV12);
+        const int m = tcl * bg.tr + trl, S = bg.tr;
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+          D[f] += wC * ((FC[f][m] - FC[f][m + 4 * S]) + 8.0f * (FC[f][m + 3 * S] - FC[f][m + S]));
+      }
+      if (P >= 0) diff_p(prev, in.base, c, bg.sP, (float)(g.dsi[P] * INV12), gm1, ch2, D);
+      int xs[3] = {bg.x[0], bg.x[1], bg.x[2]};
+      xs[R] += trl;
+      if (C >= 0) xs[C] += tcl;
+      const bool nb = near_boundary(g, xs[0], xs[1], xs[2]);
       Img im;
-      if (nb) make_img(g, x0, x1, x2, im);
+      if (nb) make_img(g, xs[0], xs[1], xs[2], im);
       if (stage < 3) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-          float v = __ldg(u0.f[f] + in.base + c) - dt * D[f];
+          float v = A0[f] - dt * D[f];
           if (f == PH) v *= decay;
           store_cell(out.f[f] + in.base, c, nb, im, f, v);
         }
@@ -141,7 +293,7 @@ rk_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float> u0,
         for (int f = 0; f < NF; ++f) {
           float *hp = hi.f[f] + in.base;
           float *lp = lo.f[f] + in.base;
-          const float h = hp[c], l = lp[c];
+          const float h = A0[f], l = A1[f];
           float e;
           if (f == PH) {
             float tt;
@@ -165,50 +317,108 @@ rk_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float> u0,
   }
 }
 
-// One viscosity sweep along `dir` for every instance.  An instance for which
-// `dir` is degenerate gets an exact copy (every difference is zero).
-__global__ void __launch_bounds__(BATCH_TILE)
-av_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
-          FieldPtrs<float> hi2, FieldPtrs<float> lo2, const float *cc, int dir) {
-  __shared__ TileState ts;
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    load_tile(a, t, ts);
-    const BatchInst &in = ts.inst;
-    const long long lin = ts.start + threadIdx.x;
-    if (lin < in.nint) {
-      const Geom &g = in.g;
-      int x0, x1, x2;
-      const long long c = decode(g, lin, x0, x1, x2);
-      const long long S = g.st[dir] * g.s[dir];
-      const float fac = (float)(g.dsi[dir] * a.sc[ts.idx].dt);
-      const float ep = (float)in.ep, fh = (float)in.fh;
-      float w[5][NW], hic[NF];
-#pragma unroll
-      for (int p = 0; p < 5; ++p) {
-        float u[NF];
-        load_u(hi, in.base, c + (p - 2) * S, u);
-        limited_vars(u, w[p]);
-        if (p == 2) {
-#pragma unroll
-          for (int f = 0; f < NF; ++f) hic[f] = u[f];
-        }
-      }
-      const float ccl = __ldg(cc + in.base + c - S), ccc = __ldg(cc + in.base + c);
-      const float ccr = __ldg(cc + in.base + c + S);
-      const float cdw = 0.5f * (ccl + ccc), cup = 0.5f * (ccc + ccr);
-      const bool nb = near_boundary(g, x0, x1, x2);
-      Img im;
-      if (nb) make_img(g, x0, x1, x2, im);
+// One viscosity sweep along `dir` for every instance.  Along R or C the
+// limited variables of the tile (halo 2 along the sweep) and the
+// characteristic speed (halo 1) are staged in shared memory; along P (3-D)
+// the cell reads its neighbours from global memory; an instance for which
+// `dir` is degenerate gets its state copied (every difference is zero).
+__global__ void __launch_bounds__(BATCH_TILE, 3)
+av_block_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
+                FieldPtrs<float> hi2, FieldPtrs<float> lo2, const float *cc, int dir) {
+  __shared__ BlockGeo bg;
+  __shared__ float Wv[NW][W_PTS];
+  __shared__ float CCs[W_PTS];
+  const int tid = threadIdx.x;
+  for (int t = blockIdx.x; t < a.nbtiles; t += gridDim.x) {
+    load_block(a, t, bg);
+    const BatchInst &in = bg.in;
+    const Geom &g = in.g;
+    const int R = in.ax_r, C = in.ax_c;
+    const bool along_r = dir == R, along_c = dir == C && C >= 0;
+    const bool staged = along_r || along_c;
+    // staged region: rows x cols with a 2-cell halo along the sweep axis
+    const int rows = along_c ? bg.tc + 4 : bg.tc;
+    const int cols = along_r ? bg.tr + 4 : bg.tr;
+    const int tcl = tid / bg.tr, trl = tid % bg.tr;
+    const bool mine = tcl < bg.nc && trl < bg.nr;
+    const long long c = bg.cell0 + (long long)tcl * bg.sC + (long long)trl * bg.sR;
+    float H0[NW], L0[NW];  // centre hi / lo in limited-variable order
+    if (mine) {
 #pragma unroll
       for (int n = 0; n < NW; ++n) {
-        const float d0 = dqq_eval(w[0][n], w[1][n], w[2][n], ep);
-        const float d1 = dqq_eval(w[1][n], w[2][n], w[3][n], ep);
-        const float d2 = dqq_eval(w[2][n], w[3][n], w[4][n], ep);
-        const float fdw = flux_core(w[1][n], w[2][n], d0, d1, cdw, fh);
-        const float fup = flux_core(w[2][n], w[3][n], d1, d2, cup, fh);
+        H0[n] = __ldg(hi.f[field_of(n)] + in.base + c);
+        L0[n] = __ldg(lo.f[field_of(n)] + in.base + c);
+      }
+    }
+    if (staged) {
+      for (int m = tid; m < rows * cols; m += BATCH_TILE) {
+        const int c = m / cols, r = m % cols;
+        // halo coordinates: C halo only when sweeping C, R halo only along R
+        const long long e = in.base + block_point(bg, c + (along_c ? 0 : bg.hc), r + (along_r ? 0 : 2));
+        float u[NF], w[NW];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) u[f] = __ldg(hi.f[f] + e);
+        limited_vars(u, w);
+#pragma unroll
+        for (int n = 0; n < NW; ++n) Wv[n][m] = w[n];
+        CCs[m] = __ldg(cc + e);
+      }
+    }
+    __syncthreads();
+    if (mine) {
+      int xs[3] = {bg.x[0], bg.x[1], bg.x[2]};
+      xs[R] += trl;
+      if (C >= 0) xs[C] += tcl;
+      const bool nb = near_boundary(g, xs[0], xs[1], xs[2]);
+      Img im;
+      if (nb) make_img(g, xs[0], xs[1], xs[2], im);
+      const float fac = (float)(g.dsi[dir] * a.sc[bg.idx].dt);
+      const float ep = (float)in.ep, fh = (float)in.fh;
+      float dF[NW];
+      if (staged) {
+        // centre at (tcl + 2, trl) along C or (tcl, trl + 2) along R
+        const int S = along_r ? 1 : cols;
+        const int m0 = along_r ? tcl * cols + trl + 2 : (tcl + 2) * cols + trl;
+        const float cdw = 0.5f * (CCs[m0 - S] + CCs[m0]);
+        const float cup = 0.5f * (CCs[m0] + CCs[m0 + S]);
+#pragma unroll
+        for (int n = 0; n < NW; ++n) {
+          const float w0 = Wv[n][m0 - 2 * S], w1 = Wv[n][m0 - S], w2 = Wv[n][m0];
+          const float w3 = Wv[n][m0 + S], w4 = Wv[n][m0 + 2 * S];
+          const float d0 = dqq_eval(w0, w1, w2, ep);
+          const float d1 = dqq_eval(w1, w2, w3, ep);
+          const float d2 = dqq_eval(w2, w3, w4, ep);
+          dF[n] = flux_core(w2, w3, d1, d2, cup, fh) - flux_core(w1, w2, d0, d1, cdw, fh);
+        }
+      } else if (g.s[dir]) {
+        const long long S = g.st[dir];
+        float w[5][NW];
+#pragma unroll
+        for (int p = 0; p < 5; ++p) {
+          float u[NF];
+          load_u(hi, in.base, c + (p - 2) * S, u);
+          limited_vars(u, w[p]);
+        }
+        const float ccl = __ldg(cc + in.base + c - S), ccc = __ldg(cc + in.base + c);
+        const float ccr = __ldg(cc + in.base + c + S);
+        const float cdw = 0.5f * (ccl + ccc), cup = 0.5f * (ccc + ccr);
+#pragma unroll
+        for (int n = 0; n < NW; ++n) {
+          const float d0 = dqq_eval(w[0][n], w[1][n], w[2][n], ep);
+          const float d1 = dqq_eval(w[1][n], w[2][n], w[3][n], ep);
+          const float d2 = dqq_eval(w[2][n], w[3][n], w[4][n], ep);
+          dF[n] = flux_core(w[2][n], w[3][n], d1, d2, cup, fh) -
+                  flux_core(w[1][n], w[2][n], d0, d1, cdw, fh);
+        }
+      } else {
+#pragma unroll
+        for (int n = 0; n < NW; ++n) dF[n] = 0.0f;
+      }
+#pragma unroll
+      for (int n = 0; n < NW; ++n) {
         const int f = field_of(n);
         float s, e;
-        two_sum(hic[f], __ldg(lo.f[f] + in.base + c) - (fup - fdw) * fac, s, e);
+        two_sum(H0[n], L0[n] - dF[n] * fac, s, e);
         store_cell(hi2.f[f] + in.base, c, nb, im, f, s);
         store_cell(lo2.f[f] + in.base, c, nb, im, f, e);
       }
@@ -250,12 +460,22 @@ void b32_rk(const BatchArgs &a, const FieldPtrs<const float> &prev,
             const FieldPtrs<const float> &u0, const FieldPtrs<float> &hi,
             const FieldPtrs<float> &lo, const FieldPtrs<float> &out, float *cc, int stage,
             int grid, cudaStream_t st) {
-  b32::rk_kernel<<<grid, BATCH_TILE, 0, st>>>(a, prev, u0, hi, lo, out, cc, stage);
+  b32::rk_block_kernel<<<grid, BATCH_TILE, 0, st>>>(a, prev, u0, hi, lo, out, cc, stage);
 }
 void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
             const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc, int dir,
             int grid, cudaStream_t st) {
-  b32::av_kernel<<<grid, BATCH_TILE, 0, st>>>(a, hi, lo, hi2, lo2, cc, dir);
+  b32::av_block_kernel<<<grid, BATCH_TILE, 0, st>>>(a, hi, lo, hi2, lo2, cc, dir);
+}
+int b32_block_grid(int sms) {
+  int rk = 0, av = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rk, b32::rk_block_kernel, BATCH_TILE, 0) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&av, b32::av_block_kernel, BATCH_TILE, 0) !=
+          cudaSuccess)
+    return 2 * sms;
+  const int per = rk < av ? rk : av;
+  return (per > 0 ? per : 1) * sms;
 }
 void b32_fill(const BatchArgs &a, const FieldPtrs<float> &q, int nfields, int grid,
               cudaStream_t st) {

@@ -35,12 +35,15 @@ struct miso_b200_batch {
   long long total = 0;       // elements per field array (all instances)
   long long max_cells = 0;   // largest instance (cells incl. ghosts)
   int ntiles = 0;
+  int nbtiles = 0;
+  int bgrid = 0;  // persistent grid of the FP32 block-tile kernels
   bool sweep[3] = {false, false, false};  // some instance is non-degenerate along d
 
   void *block = nullptr;
   size_t bytes = 0;
   BatchInst *d_insts = nullptr;
   BatchTile *d_tiles = nullptr;
+  BlockTile *d_btiles = nullptr;
   StepScalars *d_sc = nullptr;
   unsigned int *d_dtmin = nullptr;
   unsigned int *d_err = nullptr;
@@ -71,6 +74,8 @@ struct miso_b200_batch {
     a.insts = d_insts;
     a.tiles = d_tiles;
     a.ntiles = ntiles;
+    a.btiles = d_btiles;
+    a.nbtiles = nbtiles;
     a.count = count;
     a.sc = d_sc;
     a.dtmin = d_dtmin;
@@ -111,13 +116,13 @@ struct miso_b200_batch {
       const int c = cur;
       for (int s = 0; s < 4; ++s) {
         FieldPtrs<const float> prev = s == 0 ? cst(hi[c]) : cst(stg[(s - 1) & 1]);
-        b32_rk(a, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]), mut(stg[s & 1]), cc32, s, grid,
+        b32_rk(a, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]), mut(stg[s & 1]), cc32, s, bgrid,
                stream);
       }
       launches += 2 + 4;
       for (int d = 0; d < 3; ++d) {
         if (!sweep[d]) continue;  // degenerate for every instance: the state is unchanged
-        b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d, grid,
+        b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d, bgrid,
                stream);
         cur ^= 1;
         ++launches;
@@ -158,6 +163,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   b->split = params[0].precision == MISO_B200_FP32_SPLIT;
   long long off = 0;
   std::vector<BatchTile> tiles;
+  std::vector<BlockTile> btiles;
   for (int n = 0; n < count; ++n) {
     const miso_b200_grid_desc &gd = grids[n];
     const miso_b200_params &pp = params[n];
@@ -216,13 +222,32 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
     const float m3 = fminf(fminf((float)ds[0], (float)ds[1]), (float)ds[2]);
     in.min_dxyz = (double)m3;
     in.cfl_dx = pp.cfl_number * (double)m3;
+    // block-tile axes: R = last non-degenerate axis (unit stride), C the one
+    // before it, P the first of three
+    int nd[3], nnd = 0;
+    for (int a = 0; a < 3; ++a)
+      if (g.s[a]) nd[nnd++] = a;
+    in.ax_r = nnd > 0 ? nd[nnd - 1] : 2;
+    in.ax_c = nnd > 1 ? nd[nnd - 2] : -1;
+    in.ax_p = nnd > 2 ? nd[0] : -1;
     b->insts.push_back(in);
     for (long long s = 0; s < in.nint; s += BATCH_TILE) tiles.push_back(BatchTile{n, (int)s});
+    {
+      const int nr = g.n[in.ax_r];
+      const int nc = in.ax_c >= 0 ? g.n[in.ax_c] : 1;
+      const int np = in.ax_p >= 0 ? g.n[in.ax_p] : 1;
+      const int tr = in.ax_c >= 0 ? BATCH_TR : BATCH_TILE;
+      const int tc = in.ax_c >= 0 ? BATCH_TC : 1;
+      for (int pp2 = 0; pp2 < np; ++pp2)
+        for (int c0 = 0; c0 < nc; c0 += tc)
+          for (int r0 = 0; r0 < nr; r0 += tr) btiles.push_back(BlockTile{n, pp2, c0, r0});
+    }
     off += (g.cells + 63) / 64 * 64;  // instances start on 256-byte (FP32) boundaries
     if (g.cells > b->max_cells) b->max_cells = g.cells;
   }
   b->total = off;
   b->ntiles = (int)tiles.size();
+  b->nbtiles = (int)btiles.size();
 
   cudaError_t e = cudaSuccess;
   int dev = 0;
@@ -233,6 +258,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
     return bad(MISO_B200_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
   }
   b->grid = b->sms * 8;
+  b->bgrid = b32_block_grid(b->sms);
   if (stream) {
     b->stream = (cudaStream_t)stream;
   } else {
@@ -251,6 +277,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   };
   add((void **)&b->d_insts, sizeof(BatchInst) * count);
   add((void **)&b->d_tiles, sizeof(BatchTile) * tiles.size());
+  add((void **)&b->d_btiles, sizeof(BlockTile) * btiles.size());
   add((void **)&b->d_sc, sizeof(StepScalars) * count);
   add((void **)&b->d_dtmin, sizeof(unsigned int) * count);
   add((void **)&b->d_err, sizeof(unsigned int));
@@ -288,6 +315,9 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
                         cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(),
+                        cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_btiles, btiles.data(), sizeof(BlockTile) * btiles.size(),
                         cudaMemcpyHostToDevice, b->stream);
   std::vector<unsigned int> init(count);
   const float big = 1.e10f;

@@ -465,6 +465,7 @@ struct miso_b200_handle {
                            stream);
       else if (rk_var == 2)
         launch_s32_rk_pipe(tm, a, st, rk_grid, stream);
+
       else
         launch_s32_rk_tiled(tm, a, st, rk_grid, stream);
       te(t, "rk_stage", interior() * (st == 0 ? 72.0 : st < 3 ? 108.0 : 184.0));

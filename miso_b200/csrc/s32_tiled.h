@@ -50,6 +50,7 @@ void launch_s32_rk_tiled(const void *tm, const RkArgs &a, int stage, int grid, c
 // tiled kernel, one barrier per plane, packed FP32x2 differences.
 int s32_rk_pipe_configure();
 void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st);
+
 void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
                         int dir, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);

@@ -69,9 +69,11 @@ void b32_rk(const BatchArgs &a, const FieldPtrs<const float> &prev,
             const FieldPtrs<const float> &u0, const FieldPtrs<float> &hi,
             const FieldPtrs<float> &lo, const FieldPtrs<float> &out, float *cc, int stage,
             int grid, cudaStream_t st);
+// fuse_cfl: also fold the next step's CFL candidate of the new state into
+// the per-instance minima (the last sweep of a step)
 void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
             const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc, int dir,
-            int grid, cudaStream_t st);
+            int fuse_cfl, int grid, cudaStream_t st);
 void b32_fill(const BatchArgs &a, const FieldPtrs<float> &q, int nfields, int grid,
               cudaStream_t st);
 // resident CTAs of the block-tile kernels on `sms` SMs (their persistent grid)

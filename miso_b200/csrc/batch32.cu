@@ -324,10 +324,12 @@ rk_block_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float>
 // `dir` is degenerate gets its state copied (every difference is zero).
 __global__ void __launch_bounds__(BATCH_TILE, 3)
 av_block_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
-                FieldPtrs<float> hi2, FieldPtrs<float> lo2, const float *cc, int dir) {
+                FieldPtrs<float> hi2, FieldPtrs<float> lo2, const float *cc, int dir,
+                int fuse_cfl) {
   __shared__ BlockGeo bg;
   __shared__ float Wv[NW][W_PTS];
   __shared__ float CCs[W_PTS];
+  __shared__ float red[BATCH_TILE / 32];
   const int tid = threadIdx.x;
   for (int t = blockIdx.x; t < a.nbtiles; t += gridDim.x) {
     load_block(a, t, bg);
@@ -342,6 +344,7 @@ av_block_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> l
     const int tcl = tid / bg.tr, trl = tid % bg.tr;
     const bool mine = tcl < bg.nc && trl < bg.nr;
     const long long c = bg.cell0 + (long long)tcl * bg.sC + (long long)trl * bg.sR;
+    float best = 1.e10f;
     float H0[NW], L0[NW];  // centre hi / lo in limited-variable order
     if (mine) {
 #pragma unroll
@@ -414,16 +417,36 @@ av_block_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> l
 #pragma unroll
         for (int n = 0; n < NW; ++n) dF[n] = 0.0f;
       }
+      float sv[NF];
 #pragma unroll
       for (int n = 0; n < NW; ++n) {
         const int f = field_of(n);
-        float s, e;
-        two_sum(H0[n], L0[n] - dF[n] * fac, s, e);
-        store_cell(hi2.f[f] + in.base, c, nb, im, f, s);
+        float e;
+        two_sum(H0[n], L0[n] - dF[n] * fac, sv[f], e);
+        store_cell(hi2.f[f] + in.base, c, nb, im, f, sv[f]);
         store_cell(lo2.f[f] + in.base, c, nb, im, f, e);
       }
+      if (fuse_cfl) {
+        // CFL candidate of the new state for the next step (as cfl_kernel)
+        float cs, vv, ca, ein;
+        speeds(sv, (float)in.gm, (float)(in.gm - 1.0), cs, vv, ca, ein);
+        const float tv = cs + vv + ca;
+        best = fminf(best, (float)in.cfl_dx / tv);
+        if (!(sv[RO] > 0.0f) || !(ein >= 0.0f) || !isfinite(tv)) atomicOr(a.err, ERRBIT_NONFINITE);
+      }
+    }
+    if (fuse_cfl) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
+      if ((tid & 31) == 0) red[tid >> 5] = best;
     }
     __syncthreads();
+    if (fuse_cfl && tid == 0) {
+      float b = red[0];
+      for (int w = 1; w < BATCH_TILE / 32; ++w) b = fminf(b, red[w]);
+      // non-negative floats order as their bit patterns
+      atomicMin(a.dtmin + bg.idx, __float_as_uint(b));
+    }
   }
 }
 
@@ -464,8 +487,8 @@ void b32_rk(const BatchArgs &a, const FieldPtrs<const float> &prev,
 }
 void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
             const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc, int dir,
-            int grid, cudaStream_t st) {
-  b32::av_block_kernel<<<grid, BATCH_TILE, 0, st>>>(a, hi, lo, hi2, lo2, cc, dir);
+            int fuse_cfl, int grid, cudaStream_t st) {
+  b32::av_block_kernel<<<grid, BATCH_TILE, 0, st>>>(a, hi, lo, hi2, lo2, cc, dir, fuse_cfl);
 }
 int b32_block_grid(int sms) {
   int rk = 0, av = 0;

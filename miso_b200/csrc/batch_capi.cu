@@ -55,6 +55,9 @@ struct miso_b200_batch {
   float *cc32 = nullptr;
   double *io64[NF] = {};
   int cur = 0;
+  // FP32: the per-instance CFL minima of the current state were folded in
+  // by the last sweep of the previous step (no separate CFL pass needed)
+  bool cfl_valid = false;
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -111,7 +114,10 @@ struct miso_b200_batch {
         b64_av(a, cst(q64[src[d]]), mut(q64[dst[d]]), cc64, d, grid, stream);
       launches += 2 + 4 + 1 + 3;
     } else {
-      b32_cfl(a, cst(hi[cur]), grid, stream);
+      if (!cfl_valid) {
+        b32_cfl(a, cst(hi[cur]), grid, stream);
+        ++launches;
+      }
       b_finalize(a, stream);
       const int c = cur;
       for (int s = 0; s < 4; ++s) {
@@ -119,14 +125,18 @@ struct miso_b200_batch {
         b32_rk(a, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]), mut(stg[s & 1]), cc32, s, bgrid,
                stream);
       }
-      launches += 2 + 4;
+      launches += 1 + 4;
+      int last = -1;
+      for (int d = 0; d < 3; ++d)
+        if (sweep[d]) last = d;
       for (int d = 0; d < 3; ++d) {
         if (!sweep[d]) continue;  // degenerate for every instance: the state is unchanged
-        b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d, bgrid,
-               stream);
+        b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d,
+               d == last ? 1 : 0, bgrid, stream);
         cur ^= 1;
         ++launches;
       }
+      cfl_valid = last >= 0;
     }
     return cuda(cudaGetLastError(), "batch step");
   }
@@ -351,6 +361,7 @@ int miso_b200_batch_destroy(miso_b200_batch *b) {
 
 int miso_b200_batch_upload(miso_b200_batch *b, int index, const double *const q[9]) {
   if (!b || !q || index < 0 || index >= b->count) return MISO_B200_ERR_ARG;
+  b->cfl_valid = false;
   const BatchInst &in = b->insts[index];
   const size_t bytes = (size_t)in.g.cells * sizeof(double);
   int rc;
@@ -402,6 +413,7 @@ int miso_b200_batch_download(miso_b200_batch *b, int index, double *const q[9]) 
 
 int miso_b200_batch_fill_ghosts(miso_b200_batch *b) {
   if (!b) return MISO_B200_ERR_ARG;
+  b->cfl_valid = false;
   const BatchArgs a = b->args();
   if (!b->split) {
     b64_fill(a, b->mut(b->q64[0]), b->grid, b->stream);
@@ -419,6 +431,12 @@ int miso_b200_batch_run(miso_b200_batch *b, int nsteps, int use_graph) {
     for (int n = 0; n < nsteps; ++n)
       if ((rc = b->enqueue_step())) return rc;
     return MISO_B200_OK;
+  }
+  // the captured step relies on the CFL minima folded in by the previous
+  // step's last sweep: run one step eagerly first when they are missing
+  if (b->split && !b->cfl_valid && nsteps > 0) {
+    if ((rc = b->enqueue_step())) return rc;
+    --nsteps;
   }
   if (b->graph_exec && b->graph_cur != b->cur) {
     cudaGraphExecDestroy(b->graph_exec);

@@ -69,3 +69,21 @@ def test_batch_graph_equals_eager():
             outs.append([b.download(i) for i in range(len(probs))])
     for a, c in zip(*outs):
         assert np.array_equal(a, c)
+
+
+def test_batch_split_fused_cfl_equals_cfl_pass():
+    """The FP32 batch folds each step's CFL minima into its last viscosity
+    sweep; after a ghost fill (which drops them) the next step runs the
+    separate CFL pass.  Both give the same time steps and states, bit for
+    bit."""
+    probs = mixed()
+    with Batch(probs, "fp32_split") as b1, Batch(probs, "fp32_split") as b2:
+        for b in (b1, b2):
+            b.upload_all()
+        b1.run(4, graph=True)
+        b2.run(3, graph=True)
+        b2.fill_ghosts()
+        b2.run(1, graph=False)
+        assert np.array_equal(b1.dt(), b2.dt())
+        for i in range(len(probs)):
+            assert np.array_equal(b1.download(i), b2.download(i)), probs[i].name

@@ -81,6 +81,15 @@ int miso_b200_upload(miso_b200_handle *h, const double *const q[9]);
  * Fields) (miso/include/miso/mhd_fields.hpp:83-96).  Synchronises the stream. */
 int miso_b200_download(miso_b200_handle *h, double *const q[9]);
 
+/* miso_b200_download without waiting: the conversion and the copies are
+ * enqueued on the handle's stream and `event` (a cudaEvent_t created by the
+ * caller, or NULL) is recorded after the last copy; q[] must stay valid
+ * (and, for overlap with host work, be pinned) until the event completes.
+ * Steps enqueued afterwards are ordered after the copies, so a snapshot can
+ * drain while the simulation goes on.  No counterpart in the reference,
+ * whose Checkpoint::save copies synchronously (mhd_checkpoint.hpp:35-62). */
+int miso_b200_download_async(miso_b200_handle *h, double *const q[9], void *event);
+
 /* Fill every ghost cell from its periodic or mirror image.  Replaces
  * Integrator::apply_boundary_condition(bc, qq) for the built-in boundaries
  * (miso/include/miso/mhd_integrator_cuda.cuh:396-401). */
@@ -129,8 +138,9 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
 /* Kernel variant of one kernel class on the 3-D FP32-split path:
  * kernel_class 0 = Runge-Kutta stage, 1/2/3 = viscosity sweep x/y/z;
  * variant 0 = tiled (TMA plane tiles / streaming lines / warp-shuffle rows),
- * 1 = flat (one thread per cell), 2 (Runge-Kutta stage only, the default)
- * = pipelined TMA planes with packed FP32x2 differences.  All compute the
+ * 1 = flat (one thread per cell), 2 = pipelined (Runge-Kutta stage: TMA
+ * planes with packed FP32x2 differences, the default; x / y sweeps: lines
+ * streamed on full/empty mbarriers; none for z).  All compute the
  * same step; the autotuner (miso_b200/autotune.py) times them and keeps the
  * fastest.
  * ERR_STATE on grids that use the simple per-cell kernels only. */
@@ -138,7 +148,7 @@ int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant);
 int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant);
 
 /* Planes per work item along the march axis for the Runge-Kutta and the
- * x/y viscosity kernels of the 3-D FP32-split path (defaults 64). */
+ * x/y viscosity kernels of the 3-D FP32-split path (defaults 64 and 128). */
 int miso_b200_set_chunks(miso_b200_handle *h, int rk_chunk, int av_chunk);
 
 /* Enable (1) or disable (0) per-kernel CUDA-event timing on the handle's

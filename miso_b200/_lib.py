@@ -50,6 +50,8 @@ SIGNATURES = {
     "miso_b200_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "miso_b200_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "miso_b200_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_download_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                                ctypes.c_void_p]),
     "miso_b200_fill_ghosts": (ctypes.c_int, [ctypes.c_void_p]),
     "miso_b200_cfl": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "miso_b200_update": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

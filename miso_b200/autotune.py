@@ -19,8 +19,9 @@ import json
 import os
 
 CLASSES = {"rk_stage": 0, "av_x": 1, "av_y": 2, "av_z": 3}
-# variants per class: RK 0 tiled, 1 flat, 2 pipelined planes; AV 0 tiled, 1 flat
-VARIANTS = {"rk_stage": (0, 1, 2), "av_x": (0, 1), "av_y": (0, 1), "av_z": (0, 1)}
+# variants per class: 0 tiled, 1 flat, 2 pipelined (RK: planes with packed
+# differences; x / y sweeps: streamed lines on full/empty mbarriers)
+VARIANTS = {"rk_stage": (0, 1, 2), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1)}
 CHUNKS = (32, 64, 128)
 
 

@@ -36,6 +36,7 @@ EXTRA = {
     "s32_tiled.cu": FAST32,
     "s32_flat.cu": FAST32,
     "s32_rk.cu": FAST32,
+    "s32_av.cu": FAST32,
 }
 
 

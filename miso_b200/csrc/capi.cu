@@ -157,7 +157,8 @@ struct miso_b200_handle {
   alignas(64) unsigned char tm_avc[128];     // AV line map of the characteristic speed
   long long pitch = 0;                       // elements between consecutive field arrays
   int rk_L = 64, rk_tiles_j = 0, rk_tiles_k = 0, rk_items = 0, rk_grid = 0;
-  int av_L = 64, av_grid = 0, z_grid = 0;
+  int av_L = 128, av_grid = 0, z_grid = 0;
+  int avp_grid = 0;  // streamed x / y sweep: 4 resident CTAs per SM
   // The flat kernels run exactly one resident wave (grid = resident blocks)
   // and stride over tiles in order, so the CTAs in flight always cover one
   // contiguous band of planes and stencil neighbours are reused from L2.
@@ -165,8 +166,9 @@ struct miso_b200_handle {
   int z_parts = 0;  // CFL partial minima written by the last z sweep
   bool partials_valid = false;  // `partial` holds CFL minima of the current state
   // kernel variant per class on the 3-D split path: 0 = tiled (TMA plane
-  // tiles / streaming lines), 1 = flat (one thread per cell), 2 (RK only) =
-  // pipelined TMA planes with packed FP32x2 differences
+  // tiles / streaming lines), 1 = flat (one thread per cell); 2: RK =
+  // pipelined TMA planes with packed FP32x2 differences (default), x / y
+  // sweeps = lines streamed on full/empty mbarriers
   int rk_var = 2;
   int av_var[3] = {0, 0, 0};
   double *mon_partial = nullptr;
@@ -491,6 +493,8 @@ struct miso_b200_handle {
       const int t = tb();
       if (av_var[d] == 1)
         launch_s32_av_flat(a, d, flat_grid, stream);
+      else if (av_var[d] == 2 && d < 2)
+        launch_s32_av_pipe(tm_avh[cur], tm_avl[cur], tm_avc, a, d, avp_grid, stream);
       else if (d < 2)
         launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, av_grid, stream);
       else
@@ -668,7 +672,8 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   h->pitch = (long long)(round_up(cells * sizeof(float)) / sizeof(float));
   if (h->split() && s32_tiled_supported(g) && !getenv("MISO_B200_UNTILED")) {
     const size_t pb = round_up(cells * sizeof(float));
-    bool ok = s32_configure() == 0 && s32_rk_pipe_configure() == 0;
+    bool ok = s32_configure() == 0 && s32_rk_pipe_configure() == 0 &&
+              s32_av_pipe_configure() == 0;
     for (int s = 0; s < 2 && ok; ++s) {
       ok = s32_make_tmap(g, h->hi[s][0], pb, 0, h->tm_hi[s]) == 0 &&
            s32_make_tmap(g, h->stg[s][0], pb, 0, h->tm_stg[s]) == 0 &&
@@ -682,11 +687,13 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
       const int per_sm = 2;
       h->rk_grid = h->rk_items < per_sm * h->sms ? h->rk_items : per_sm * h->sms;
       h->av_grid = 3 * h->sms;
+      h->avp_grid = 4 * h->sms;
       h->flat_grid = 3 * h->sms;  // 256 threads x 80 registers: 3 resident CTAs per SM
       if (const char *v = getenv("MISO_B200_RK"))
         h->rk_var = strcmp(v, "flat") == 0 ? 1 : strcmp(v, "tiled") == 0 ? 0 : 2;
       if (const char *v = getenv("MISO_B200_AV"))
-        for (int d = 0; d < 3 && v[d]; ++d) h->av_var[d] = v[d] == 'f' ? 1 : 0;
+        for (int d = 0; d < 3 && v[d]; ++d)
+          h->av_var[d] = v[d] == 'f' ? 1 : (v[d] == 'p' && d < 2) ? 2 : 0;
     }
   }
   e = cudaMemsetAsync(h->block, 0, total, h->stream);
@@ -734,6 +741,32 @@ int miso_b200_upload(miso_b200_handle *h, const double *const q[9]) {
     if ((rc = h->check_launch("to_split"))) return rc;
   }
   return h->cuda(cudaStreamSynchronize(h->stream), "upload synchronize");
+}
+
+// Enqueue the conversion and the copies of miso_b200_download on the
+// handle's stream without waiting; `event` (a cudaEvent_t, may be NULL) is
+// recorded after the last copy.  Later work on the stream is ordered after
+// the copies, so stepping on while a snapshot drains is safe.
+int miso_b200_download_async(miso_b200_handle *h, double *const q[9], void *event) {
+  if (!h || !q) return MISO_B200_ERR_ARG;
+  const size_t bytes = (size_t)h->g.cells * sizeof(double);
+  int rc;
+  for (int f = 0; f < NF; ++f)
+    if (!q[f]) return h->fail(MISO_B200_ERR_ARG, "null field pointer %d", f);
+  if (h->split()) {
+    launch_s32_from_split(h->g.cells, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->IO(), h->sms,
+                          h->stream);
+    h->launches++;
+    if ((rc = h->check_launch("from_split"))) return rc;
+  }
+  for (int f = 0; f < NF; ++f) {
+    const double *src = h->split() ? h->io64[f] : h->q64[0][f];
+    if ((rc = h->cuda(cudaMemcpyAsync(q[f], src, bytes, cudaMemcpyDefault, h->stream),
+                      "download")))
+      return rc;
+  }
+  if (event) return h->cuda(cudaEventRecord((cudaEvent_t)event, h->stream), "record event");
+  return MISO_B200_OK;
 }
 
 int miso_b200_download(miso_b200_handle *h, double *const q[9]) {
@@ -931,7 +964,7 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]) {
 
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
   if (!h || kernel_class < 0 || kernel_class > 3 || variant < 0 ||
-      variant > (kernel_class == 0 ? 2 : 1))
+      variant > (kernel_class == 3 ? 1 : 2))
     return MISO_B200_ERR_ARG;
   if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "kernel variants apply to 3-D split grids");
   if (kernel_class == 0)

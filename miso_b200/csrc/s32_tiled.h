@@ -54,5 +54,10 @@ void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cu
 void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
                         int dir, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);
+// x / y sweep streamed with full/empty mbarriers and no CTA barrier
+// (s32_av.cu); same tensor maps as the line kernel
+int s32_av_pipe_configure();
+void launch_s32_av_pipe(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
+                        int dir, int grid, cudaStream_t st);
 
 }  // namespace miso_b200

@@ -24,10 +24,10 @@ from . import problems as P
 from .integrator import Integrator
 
 PROBLEMS = {
-    "turbulence": lambda n, seed: P.turbulence(n, seed=seed),
-    "blast": lambda n, seed: P.blast(n, seed=seed),
-    "orszag_tang": lambda n, seed: P.orszag_tang(n),
-    "brio_wu": lambda n, seed: P.brio_wu(n),
+    "turbulence": lambda n, seed, smooth=0.0: P.turbulence(n, seed=seed),
+    "blast": lambda n, seed, smooth=0.0: P.blast(n, seed=seed, smooth=smooth),
+    "orszag_tang": lambda n, seed, smooth=0.0: P.orszag_tang(n),
+    "brio_wu": lambda n, seed, smooth=0.0: P.brio_wu(n),
 }
 
 
@@ -95,8 +95,10 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--every", type=int, default=250)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--smooth", type=float, default=0.0,
+                    help="blast: width in cells of the tanh edge of the sphere (0 = step)")
     args = ap.parse_args(argv)
-    prob = PROBLEMS[args.problem](args.n, args.seed)
+    prob = PROBLEMS[args.problem](args.n, args.seed, args.smooth)
     compare(prob, args.steps, args.every, emit=lambda s: print(s, flush=True))
     return 0
 

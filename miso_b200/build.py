@@ -37,6 +37,7 @@ EXTRA = {
     "s32_flat.cu": FAST32,
     "s32_rk.cu": FAST32,
     "s32_av.cu": FAST32,
+    "s32_shell.cu": FAST32,
 }
 
 

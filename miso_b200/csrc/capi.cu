@@ -159,12 +159,14 @@ struct miso_b200_handle {
   int rk_L = 64, rk_tiles_j = 0, rk_tiles_k = 0, rk_items = 0, rk_grid = 0;
   int av_L = 128, av_grid = 0, z_grid = 0;
   int avp_grid = 0;  // streamed x / y sweep: 4 resident CTAs per SM
+  int shell_grid = 0;
   // The flat kernels run exactly one resident wave (grid = resident blocks)
   // and stride over tiles in order, so the CTAs in flight always cover one
   // contiguous band of planes and stencil neighbours are reused from L2.
   int flat_grid = 0;
   int z_parts = 0;  // CFL partial minima written by the last z sweep
   bool partials_valid = false;  // `partial` holds CFL minima of the current state
+  bool lo_shell_stale = false;  // the lo ghost images lag the interior (filled on download)
   // kernel variant per class on the 3-D split path: 0 = tiled (TMA plane
   // tiles / streaming lines), 1 = flat (one thread per cell); 2: RK =
   // pipelined TMA planes with packed FP32x2 differences (default), x / y
@@ -331,6 +333,37 @@ struct miso_b200_handle {
 
   int fill_state() { return split() ? fill_split(cur) : fill64(0); }
 
+  // the lo ghost images catch up with the interior before the state leaves
+  // the device
+  int fresh_lo_shell() {
+    if (!lo_shell_stale) return MISO_B200_OK;
+    lo_shell_stale = false;
+    return shell(lo[cur], nullptr, nullptr);
+  }
+
+  // ghost images of the interior shell of up to two 9-field sets and cc
+  int shell(float *const *set_a, float *const *set_b, float *ccp) {
+    ShellArgs sa;
+    sa.n = 0;
+    for (int f = 0; f < NF; ++f) {
+      sa.p[sa.n] = set_a[f];
+      sa.f[sa.n++] = f;
+    }
+    if (set_b)
+      for (int f = 0; f < NF; ++f) {
+        sa.p[sa.n] = set_b[f];
+        sa.f[sa.n++] = f;
+      }
+    if (ccp) {
+      sa.p[sa.n] = ccp;
+      sa.f[sa.n++] = NF;
+    }
+    const int t = tb();
+    launch_s32_shell(g, sa, shell_grid, stream);
+    te(t, "ghost_shell", ghost_cells() * 8.0 * sa.n);
+    return check_launch("ghost_shell");
+  }
+
   // host-side step scalars exactly as Integrator::divb_parameters_set and
   // runge_kutta_4step form them (host libm exp, as the reference's host path)
   StepScalars host_scalars(double dt) const {
@@ -472,6 +505,13 @@ struct miso_b200_handle {
         launch_s32_rk_tiled(tm, a, st, rk_grid, stream);
       te(t, "rk_stage", interior() * (st == 0 ? 72.0 : st < 3 ? 108.0 : 184.0));
       if ((rc = check_launch("rk_stage"))) return rc;
+      if (rk_var == 2) {  // interior-only writer: fill the images it reads next
+        if (st < 3) {
+          if ((rc = shell(stg[st & 1], nullptr, nullptr))) return rc;
+        } else {
+          if ((rc = shell(hi[c], nullptr, cc32))) return rc;
+        }
+      }
     }
     for (int d = 0; d < 3; ++d) {
       AvArgs a;
@@ -501,6 +541,14 @@ struct miso_b200_handle {
         launch_s32_av_z(a, z_grid, stream);
       te(t, d == 0 ? "av_x" : d == 1 ? "av_y" : "av_z", interior() * 148.0);
       if ((rc = check_launch("av_sweep"))) return rc;
+      // interior-only writers (line and z sweeps): the hi images are read by
+      // the next pass; lo images only by a download (see lo_shell_stale)
+      if (av_var[d] == 0) {
+        if ((rc = shell(hi[cur ^ 1], nullptr, nullptr))) return rc;
+        lo_shell_stale = true;
+      } else {
+        lo_shell_stale = false;
+      }
       cur ^= 1;
     }
     z_parts = av_var[2] == 1 ? flat_grid : z_grid;
@@ -688,6 +736,10 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
       h->rk_grid = h->rk_items < per_sm * h->sms ? h->rk_items : per_sm * h->sms;
       h->av_grid = 3 * h->sms;
       h->avp_grid = 4 * h->sms;
+      {
+        const long long want = (s32_shell_cells(g) + 255) / 256;
+        h->shell_grid = (int)(want < 8LL * h->sms ? want : 8LL * h->sms);
+      }
       h->flat_grid = 3 * h->sms;  // 256 threads x 80 registers: 3 resident CTAs per SM
       if (const char *v = getenv("MISO_B200_RK"))
         h->rk_var = strcmp(v, "flat") == 0 ? 1 : strcmp(v, "tiled") == 0 ? 0 : 2;
@@ -736,6 +788,7 @@ int miso_b200_upload(miso_b200_handle *h, const double *const q[9]) {
     for (int f = 0; f < NF; ++f) src.f[f] = h->io64[f];
     h->cur = 0;
     h->partials_valid = false;
+    h->lo_shell_stale = false;
     launch_s32_to_split(h->g.cells, src, h->H(0), h->L(0), h->sms, h->stream);
     h->launches++;
     if ((rc = h->check_launch("to_split"))) return rc;
@@ -753,6 +806,7 @@ int miso_b200_download_async(miso_b200_handle *h, double *const q[9], void *even
   int rc;
   for (int f = 0; f < NF; ++f)
     if (!q[f]) return h->fail(MISO_B200_ERR_ARG, "null field pointer %d", f);
+  if ((rc = h->fresh_lo_shell())) return rc;
   if (h->split()) {
     launch_s32_from_split(h->g.cells, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->IO(), h->sms,
                           h->stream);
@@ -773,6 +827,7 @@ int miso_b200_download(miso_b200_handle *h, double *const q[9]) {
   if (!h || !q) return MISO_B200_ERR_ARG;
   const size_t bytes = (size_t)h->g.cells * sizeof(double);
   int rc;
+  if ((rc = h->fresh_lo_shell())) return rc;
   if (h->split()) {
     launch_s32_from_split(h->g.cells, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->IO(), h->sms,
                           h->stream);

@@ -11,7 +11,9 @@
 // fluxes in a double-buffered shared array and keeps the x flux in a
 // three-deep register ring.  After the single barrier of the plane it forms
 // the y and z differences of its point and finishes the cell two planes
-// back, whose centre values it pulled into L1 before the wait.
+// back, whose centre values it pulled into L1 before the wait.  Only the
+// interior is written; the ghost images of the outputs are filled by the
+// shell kernel (s32_shell.cu) that follows the stage.
 // The ring is rotated by unrolling the plane loop three times, so no
 // register moves are spent on it.
 //
@@ -274,19 +276,16 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
       D.p[i] = sub2(R2.p[i], mul2(k.wx2, N));
     }
     D.s = __fsub_rn(R2.s, __fmul_rn(k.wx, fmaf(-8.f, F1.s, Fn.s)));
-    const bool nb = near_boundary(g, c, jg, kg);
-    Img im;
-    if (nb) make_img(g, c, jg, kg, im);
     if (STAGE < 3) {
 #pragma unroll
       for (int i = 0; i < NPAIR; ++i) {
         const float2 u0 = f2(__ldg(a.u0.f[2 * i] + cell), __ldg(a.u0.f[2 * i + 1] + cell));
         const float2 v = fma2(k.mdt2, D.p[i], u0);
-        store_cell(a.out.f[2 * i], cell, nb, im, 2 * i, v.x);
-        store_cell(a.out.f[2 * i + 1], cell, nb, im, 2 * i + 1, v.y);
+        a.out.f[2 * i][cell] = v.x;
+        a.out.f[2 * i + 1][cell] = v.y;
       }
       const float u0 = __ldg(a.u0.f[PH] + cell);
-      store_cell(a.out.f[PH], cell, nb, im, PH, fmaf(-k.dt, D.s, u0) * k.decay);
+      a.out.f[PH][cell] = fmaf(-k.dt, D.s, u0) * k.decay;
     } else {
       // U^{n+1} = (hi, lo) - dt * D as a compensated (two-sum) pair, one
       // field pair at a time; the pieces of the characteristic speed are
@@ -301,10 +300,10 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
         const float2 sm2 = add2(h, b);
         const float2 bb = sub2(sm2, h);
         const float2 e = add2(sub2(h, sub2(sm2, bb)), sub2(b, bb));
-        store_cell(h0, cell, nb, im, 2 * i, sm2.x);
-        store_cell(h1, cell, nb, im, 2 * i + 1, sm2.y);
-        store_cell(l0, cell, nb, im, 2 * i, e.x);
-        store_cell(l1, cell, nb, im, 2 * i + 1, e.y);
+        h0[cell] = sm2.x;
+        h1[cell] = sm2.y;
+        l0[cell] = e.x;
+        l1[cell] = e.y;
         // pairs: (ro, mx) (my, mz) (bx, by) (bz, et)
         if (i == 0) {
           s_ro = sm2.x;
@@ -327,8 +326,8 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
         const float pr = sv * k.decay;
         const float pe = fmaf(sv, k.decay, -pr);
         two_sum(pr, pe + t * k.decay, sv, e);
-        store_cell(hp, cell, nb, im, PH, sv);
-        store_cell(lp, cell, nb, im, PH, e);
+        hp[cell] = sv;
+        lp[cell] = e;
       }
       // characteristic speed of the new state (speeds() in s32_common.cuh)
       const float inv = 1.0f / s_ro;
@@ -336,7 +335,7 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
       const float cs = sqrtf(fmaxf(a.gm * a.gm1 * ein, 0.0f));
       const float vv = sqrtf(mm) * inv;
       const float ca = sqrtf(bb2 * inv * FPII4);
-      store_cell(a.cc, cell, nb, im, NF, cs * a.cs_fac + vv * a.vv_fac + ca * a.ca_fac);
+      a.cc[cell] = cs * a.cs_fac + vv * a.vv_fac + ca * a.ca_fac;
     }
   }
 

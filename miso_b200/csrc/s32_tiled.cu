@@ -21,7 +21,8 @@
 //   fluxes, so each face flux and each slope is evaluated once.  The z
 //   sweep (contiguous axis, av_z_kernel) exchanges neighbours with warp
 //   shuffles and folds the CFL candidate of the new state into per-block
-//   minima.
+//   minima.  The sweeps write the interior only; the ghost images follow
+//   from the shell kernel (s32_shell.cu).
 //
 // Physics as in fp32s_kernels.cu (flux form of mhd_integrator_host.hpp:
 // 57-247; limiter.hpp:11-37; mhd_artificial_viscosity_host.hpp:51-348).
@@ -457,16 +458,13 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
           const int x0 = DIR == 0 ? t : li.u;
           const int x1 = DIR == 0 ? li.u : t;
           const int cell = cell_of(g, x0, x1, k);
-          const bool nb = near_boundary(g, x0, x1, k);
-          Img im;
-          if (nb) make_img(g, x0, x1, k, im);
 #pragma unroll
           for (int n = 0; n < NW; ++n) {
             const int f = field_of(n);
             float sv, e;
             two_sum(chi[f * LBOX + tid + 2], clo[f * LBOX + tid + 2] - dF[n] * fac, sv, e);
-            store_cell(a.hi2.f[f], cell, nb, im, f, sv);
-            store_cell(a.lo2.f[f], cell, nb, im, f, e);
+            a.hi2.f[f][cell] = sv;  // interior only: the shell kernel fills the images
+            a.lo2.f[f][cell] = e;
           }
         }
       }
@@ -524,17 +522,14 @@ av_z_kernel(const AvArgs a) {
       dF[n] = Fup - Fdw;
     }
     if (lane >= 2 && lane < 30 && k < nk) {
-      const bool nb = near_boundary(g, i, j, k);
-      Img im;
-      if (nb) make_img(g, i, j, k, im);
       float s[NF];
 #pragma unroll
       for (int n = 0; n < NW; ++n) {
         const int f = field_of(n);
         float e;
         two_sum(u[f], __ldg(a.lo.f[f] + c) - dF[n] * fac, s[f], e);
-        store_cell(a.hi2.f[f], c, nb, im, f, s[f]);
-        store_cell(a.lo2.f[f], c, nb, im, f, e);
+        a.hi2.f[f][c] = s[f];  // interior only: the shell kernel fills the images
+        a.lo2.f[f][c] = e;
       }
       if (a.partial) {
         // CFL candidate of the new state (mhd_integrator_host.hpp:303-334)

@@ -36,6 +36,16 @@ struct AvArgs {
   int L;  // cells per work item along the sweep axis (x, y sweeps)
 };
 
+// Arrays whose interior shell gets its ghost images (s32_shell.cu); f[n] is
+// the field index that selects the mirror sign (NF: never negated).
+struct ShellArgs {
+  float *p[2 * NF + 1];
+  int f[2 * NF + 1];
+  int n;
+};
+void launch_s32_shell(const Geom &g, const ShellArgs &a, int grid, cudaStream_t st);
+long long s32_shell_cells(const Geom &g);  // interior cells within the margin of a face
+
 bool s32_tiled_supported(const Geom &g);
 // 4-D tensor maps (k, j, i, field) over 9 arrays at `pitch_bytes`:
 //   kind 0: RK plane tile (k 36, j 12, i 1, 9 fields)

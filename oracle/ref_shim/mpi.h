@@ -12,10 +12,7 @@
  *   - MPI_Isend copies the payload into a pending-message list keyed by tag;
  *     MPI_Irecv records the destination; MPI_Waitall delivers by tag;
  *   - reductions, broadcasts and gathers copy the local value.
- * None of these calls carries arithmetic.  Compiled by nvcc (the reference's
- * CUDA integrator passes device buffers to MPI, as with a CUDA-aware MPI),
- * every copy goes through cudaMemcpy with cudaMemcpyDefault, which accepts
- * host and device pointers alike.
+ * None of these calls carries arithmetic.
  */
 #ifndef MISO_REF_SHIM_MPI_H
 #define MISO_REF_SHIM_MPI_H
@@ -24,19 +21,6 @@
 #include <cstdlib>
 #include <cstring>
 #include <vector>
-#ifdef __CUDACC__
-#include <cuda_runtime.h>
-#endif
-
-namespace miso_ref_shim {
-inline void copy_bytes(void *dst, const void *src, size_t n) {
-#ifdef __CUDACC__
-  cudaMemcpy(dst, src, n, cudaMemcpyDefault);
-#else
-  std::memcpy(dst, src, n);
-#endif
-}
-}  // namespace miso_ref_shim
 
 typedef int MPI_Comm;
 typedef int MPI_Datatype;
@@ -143,11 +127,11 @@ inline int MPI_Bcast(void *, int, MPI_Datatype, int, MPI_Comm) { return 0; }
 inline int MPI_Barrier(MPI_Comm) { return 0; }
 inline int MPI_Gather(const void *s, int n, MPI_Datatype t, void *r, int, MPI_Datatype,
                       int, MPI_Comm) {
-  miso_ref_shim::copy_bytes(r, s, n * miso_ref_shim::type_size(t));
+  std::memcpy(r, s, n * miso_ref_shim::type_size(t));
   return 0;
 }
 inline int MPI_Allreduce(const void *s, void *r, int n, MPI_Datatype t, MPI_Op, MPI_Comm) {
-  miso_ref_shim::copy_bytes(r, s, n * miso_ref_shim::type_size(t));
+  std::memcpy(r, s, n * miso_ref_shim::type_size(t));
   return 0;
 }
 inline int MPI_Isend(const void *buf, int n, MPI_Datatype t, int, int tag, MPI_Comm,
@@ -156,7 +140,7 @@ inline int MPI_Isend(const void *buf, int n, MPI_Datatype t, int, int tag, MPI_C
   p.tag = tag;
   const size_t b = (size_t)n * miso_ref_shim::type_size(t);
   p.bytes.resize(b);
-  miso_ref_shim::copy_bytes(p.bytes.data(), buf, b);
+  std::memcpy(p.bytes.data(), buf, b);
   miso_ref_shim::sends().push_back(std::move(p));
   *req = 0;
   return 0;
@@ -173,7 +157,7 @@ inline int MPI_Waitall(int, MPI_Request *, MPI_Status *) {
   for (auto &r : R) {
     for (size_t s = 0; s < S.size(); ++s) {
       if (S[s].tag == r.tag) {
-        miso_ref_shim::copy_bytes(r.buf, S[s].bytes.data(), r.bytes);
+        std::memcpy(r.buf, S[s].bytes.data(), r.bytes);
         S.erase(S.begin() + (long)s);
         break;
       }

@@ -76,6 +76,9 @@ void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtr
             int fuse_cfl, int grid, cudaStream_t st);
 void b32_fill(const BatchArgs &a, const FieldPtrs<float> &q, int nfields, int grid,
               cudaStream_t st);
+// ghost images of the near-boundary cells of the listed block tiles
+void b32_edge_fill(const BatchArgs &a, const int *etiles, int ne, const FieldPtrs<float> &q,
+                   int nfields, int ftag, int grid, cudaStream_t st);
 // resident CTAs of the block-tile kernels on `sms` SMs (their persistent grid)
 int b32_block_grid(int sms);
 

@@ -109,7 +109,9 @@ cfl_kernel(BatchArgs a, FieldPtrs<const float> hi) {
 // staged in shared memory once; flux vectors (RK) and limited variables
 // (viscosity) along R and C are formed once per point there, so each cell
 // reads its neighbours from shared memory.  The P axis of 3-D instances
-// keeps per-cell neighbour evaluation from global memory.
+// keeps per-cell neighbour evaluation from global memory.  These kernels
+// write interior cells only; edge_fill_kernel then writes the ghost images
+// of the tiles that touch a boundary.
 // ---------------------------------------------------------------------------
 constexpr int TC = BATCH_TC, TR = BATCH_TR;
 constexpr int U_PTS = (TC + 4) * (TR + 4) > BATCH_TILE + 4 ? (TC + 4) * (TR + 4) : BATCH_TILE + 4;
@@ -274,18 +276,13 @@ rk_block_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float>
           D[f] += wC * ((FC[f][m] - FC[f][m + 4 * S]) + 8.0f * (FC[f][m + 3 * S] - FC[f][m + S]));
       }
       if (P >= 0) diff_p(prev, in.base, c, bg.sP, (float)(g.dsi[P] * INV12), gm1, ch2, D);
-      int xs[3] = {bg.x[0], bg.x[1], bg.x[2]};
-      xs[R] += trl;
-      if (C >= 0) xs[C] += tcl;
-      const bool nb = near_boundary(g, xs[0], xs[1], xs[2]);
-      Img im;
-      if (nb) make_img(g, xs[0], xs[1], xs[2], im);
+      // interior only: the edge-tile fill writes the ghost images
       if (stage < 3) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
           float v = A0[f] - dt * D[f];
           if (f == PH) v *= decay;
-          store_cell(out.f[f] + in.base, c, nb, im, f, v);
+          out.f[f][in.base + c] = v;
         }
       } else {
         float sv[NF];
@@ -304,13 +301,12 @@ rk_block_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float>
           } else {
             two_sum(h, l - dt * D[f], sv[f], e);
           }
-          store_cell(hp, c, nb, im, f, sv[f]);
-          store_cell(lp, c, nb, im, f, e);
+          hp[c] = sv[f];
+          lp[c] = e;
         }
         float cs, vv, ca, ein;
         speeds(sv, (float)in.gm, gm1, cs, vv, ca, ein);
-        store_cell(cc + in.base, c, nb, im, NF,
-                   cs * (float)in.cs_fac + vv * (float)in.vv_fac + ca * (float)in.ca_fac);
+        cc[in.base + c] = cs * (float)in.cs_fac + vv * (float)in.vv_fac + ca * (float)in.ca_fac;
       }
     }
     __syncthreads();
@@ -369,12 +365,6 @@ av_block_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> l
     }
     __syncthreads();
     if (mine) {
-      int xs[3] = {bg.x[0], bg.x[1], bg.x[2]};
-      xs[R] += trl;
-      if (C >= 0) xs[C] += tcl;
-      const bool nb = near_boundary(g, xs[0], xs[1], xs[2]);
-      Img im;
-      if (nb) make_img(g, xs[0], xs[1], xs[2], im);
       const float fac = (float)(g.dsi[dir] * a.sc[bg.idx].dt);
       const float ep = (float)in.ep, fh = (float)in.fh;
       float dF[NW];
@@ -423,8 +413,8 @@ av_block_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> l
         const int f = field_of(n);
         float e;
         two_sum(H0[n], L0[n] - dF[n] * fac, sv[f], e);
-        store_cell(hi2.f[f] + in.base, c, nb, im, f, sv[f]);
-        store_cell(lo2.f[f] + in.base, c, nb, im, f, e);
+        hi2.f[f][in.base + c] = sv[f];  // interior only (edge-tile fill follows)
+        lo2.f[f][in.base + c] = e;
       }
       if (fuse_cfl) {
         // CFL candidate of the new state for the next step (as cfl_kernel)
@@ -447,6 +437,37 @@ av_block_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> l
       // non-negative floats order as their bit patterns
       atomicMin(a.dtmin + bg.idx, __float_as_uint(b));
     }
+  }
+}
+
+// Ghost images of the near-boundary cells of the block tiles that touch an
+// instance's boundary (`etiles`), for `nfields` arrays; ftag >= 0 selects
+// one mirror-sign field for all of them (NF: never negated).
+__global__ void __launch_bounds__(BATCH_TILE)
+edge_fill_kernel(BatchArgs a, const int *etiles, int ne, FieldPtrs<float> q, int nfields,
+                 int ftag) {
+  __shared__ BlockGeo bg;
+  const int tid = threadIdx.x;
+  for (int t = blockIdx.x; t < ne; t += gridDim.x) {
+    load_block(a, etiles[t], bg);
+    const BatchInst &in = bg.in;
+    const Geom &g = in.g;
+    const int tcl = tid / bg.tr, trl = tid % bg.tr;
+    if (tcl < bg.nc && trl < bg.nr) {
+      int xs[3] = {bg.x[0], bg.x[1], bg.x[2]};
+      xs[in.ax_r] += trl;
+      if (in.ax_c >= 0) xs[in.ax_c] += tcl;
+      if (near_boundary(g, xs[0], xs[1], xs[2])) {
+        const long long c = bg.cell0 + (long long)tcl * bg.sC + (long long)trl * bg.sR;
+        Img im;
+        make_img(g, xs[0], xs[1], xs[2], im);
+        for (int f = 0; f < nfields; ++f) {
+          float *p = q.f[f] + in.base;
+          store_img(p, c, im, ftag >= 0 ? ftag : f, p[c]);
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -489,6 +510,10 @@ void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtr
             const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc, int dir,
             int fuse_cfl, int grid, cudaStream_t st) {
   b32::av_block_kernel<<<grid, BATCH_TILE, 0, st>>>(a, hi, lo, hi2, lo2, cc, dir, fuse_cfl);
+}
+void b32_edge_fill(const BatchArgs &a, const int *etiles, int ne, const FieldPtrs<float> &q,
+                   int nfields, int ftag, int grid, cudaStream_t st) {
+  if (ne > 0) b32::edge_fill_kernel<<<grid, BATCH_TILE, 0, st>>>(a, etiles, ne, q, nfields, ftag);
 }
 int b32_block_grid(int sms) {
   int rk = 0, av = 0;

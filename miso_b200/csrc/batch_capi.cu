@@ -44,6 +44,8 @@ struct miso_b200_batch {
   BatchInst *d_insts = nullptr;
   BatchTile *d_tiles = nullptr;
   BlockTile *d_btiles = nullptr;
+  int *d_etiles = nullptr;  // block tiles that touch an instance boundary
+  int netiles = 0;
   StepScalars *d_sc = nullptr;
   unsigned int *d_dtmin = nullptr;
   unsigned int *d_err = nullptr;
@@ -124,6 +126,17 @@ struct miso_b200_batch {
         FieldPtrs<const float> prev = s == 0 ? cst(hi[c]) : cst(stg[(s - 1) & 1]);
         b32_rk(a, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]), mut(stg[s & 1]), cc32, s, bgrid,
                stream);
+        // the block kernels write the interior; images of what the next pass reads
+        if (s < 3) {
+          b32_edge_fill(a, d_etiles, netiles, mut(stg[s & 1]), NF, -1, bgrid, stream);
+        } else {
+          b32_edge_fill(a, d_etiles, netiles, mut(hi[c]), NF, -1, bgrid, stream);
+          FieldPtrs<float> ccf{};
+          ccf.f[0] = cc32;
+          b32_edge_fill(a, d_etiles, netiles, ccf, 1, NF, bgrid, stream);
+          ++launches;
+        }
+        ++launches;
       }
       launches += 1 + 4;
       int last = -1;
@@ -133,8 +146,10 @@ struct miso_b200_batch {
         if (!sweep[d]) continue;  // degenerate for every instance: the state is unchanged
         b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d,
                d == last ? 1 : 0, bgrid, stream);
+        b32_edge_fill(a, d_etiles, netiles, mut(hi[cur ^ 1]), NF, -1, bgrid, stream);
+        b32_edge_fill(a, d_etiles, netiles, mut(lo[cur ^ 1]), NF, -1, bgrid, stream);
         cur ^= 1;
-        ++launches;
+        launches += 3;
       }
       cfl_valid = last >= 0;
     }
@@ -174,6 +189,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   long long off = 0;
   std::vector<BatchTile> tiles;
   std::vector<BlockTile> btiles;
+  std::vector<int> etiles;
   for (int n = 0; n < count; ++n) {
     const miso_b200_grid_desc &gd = grids[n];
     const miso_b200_params &pp = params[n];
@@ -248,9 +264,19 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
       const int np = in.ax_p >= 0 ? g.n[in.ax_p] : 1;
       const int tr = in.ax_c >= 0 ? BATCH_TR : BATCH_TILE;
       const int tc = in.ax_c >= 0 ? BATCH_TC : 1;
+      const int mr = g.m[in.ax_r];
+      const int mc = in.ax_c >= 0 ? g.m[in.ax_c] : 0;
+      const int mp = in.ax_p >= 0 ? g.m[in.ax_p] : 0;
       for (int pp2 = 0; pp2 < np; ++pp2)
         for (int c0 = 0; c0 < nc; c0 += tc)
-          for (int r0 = 0; r0 < nr; r0 += tr) btiles.push_back(BlockTile{n, pp2, c0, r0});
+          for (int r0 = 0; r0 < nr; r0 += tr) {
+            const int r1 = r0 + (tr < nr - r0 ? tr : nr - r0);
+            const int c1 = c0 + (tc < nc - c0 ? tc : nc - c0);
+            const bool edge = r0 < mr || r1 > nr - mr || c0 < mc || c1 > nc - mc ||
+                              pp2 < mp || pp2 >= np - mp;
+            if (edge) etiles.push_back((int)btiles.size());
+            btiles.push_back(BlockTile{n, pp2, c0, r0});
+          }
     }
     off += (g.cells + 63) / 64 * 64;  // instances start on 256-byte (FP32) boundaries
     if (g.cells > b->max_cells) b->max_cells = g.cells;
@@ -258,6 +284,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   b->total = off;
   b->ntiles = (int)tiles.size();
   b->nbtiles = (int)btiles.size();
+  b->netiles = (int)etiles.size();
 
   cudaError_t e = cudaSuccess;
   int dev = 0;
@@ -288,6 +315,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   add((void **)&b->d_insts, sizeof(BatchInst) * count);
   add((void **)&b->d_tiles, sizeof(BatchTile) * tiles.size());
   add((void **)&b->d_btiles, sizeof(BlockTile) * btiles.size());
+  add((void **)&b->d_etiles, sizeof(int) * (etiles.empty() ? 1 : etiles.size()));
   add((void **)&b->d_sc, sizeof(StepScalars) * count);
   add((void **)&b->d_dtmin, sizeof(unsigned int) * count);
   add((void **)&b->d_err, sizeof(unsigned int));
@@ -328,6 +356,9 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
                         cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->d_btiles, btiles.data(), sizeof(BlockTile) * btiles.size(),
+                        cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess && !etiles.empty())
+    e = cudaMemcpyAsync(b->d_etiles, etiles.data(), sizeof(int) * etiles.size(),
                         cudaMemcpyHostToDevice, b->stream);
   std::vector<unsigned int> init(count);
   const float big = 1.e10f;

@@ -39,11 +39,27 @@ struct BlockTile {
   int inst, p, c0, r0;
 };
 
+// Geometry of one block tile, precomputed on the host so every thread of a
+// CTA can pick it up with one parallel copy.
+struct TileGeo {
+  int idx;               // instance
+  int tc, tr;            // tile extent (BATCH_TC x BATCH_TR, or 1 x BATCH_TILE)
+  int nc, nr;            // cells of the tile inside the interior
+  int hc;                // halo width along C (0 when the instance has no C axis)
+  long long cell0;       // element index (instance-relative) of the tile's first cell
+  long long sP, sC, sR;  // strides of the P, C, R axes (0 when absent)
+  int oC, oR;            // total coordinate of the tile origin along C, R
+  int tC, tR;            // total extent along C, R
+  int x[3];              // interior coordinates of the tile origin per array axis
+  int pad;
+};
+TileGeo make_tile_geo(const BatchInst &in, int idx, const BlockTile &bt);
+
 struct BatchArgs {
   const BatchInst *insts;
   const BatchTile *tiles;
   int ntiles;
-  const BlockTile *btiles;  // FP32 block tiles
+  const TileGeo *btiles;  // FP32 block tiles
   int nbtiles;
   int count;
   StepScalars *sc;       // per instance
@@ -76,9 +92,9 @@ void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtr
             int fuse_cfl, int grid, cudaStream_t st);
 void b32_fill(const BatchArgs &a, const FieldPtrs<float> &q, int nfields, int grid,
               cudaStream_t st);
-// ghost images of the near-boundary cells of the listed block tiles
-void b32_edge_fill(const BatchArgs &a, const int *etiles, int ne, const FieldPtrs<float> &q,
-                   int nfields, int ftag, int grid, cudaStream_t st);
+// ghost images of the listed near-boundary cells (instance, x0, x1, x2)
+void b32_shell_fill(const BatchArgs &a, const int4 *cells, int n, const FieldPtrs<float> &q,
+                    int nfields, int ftag, cudaStream_t st);
 // resident CTAs of the block-tile kernels on `sms` SMs (their persistent grid)
 int b32_block_grid(int sms);
 

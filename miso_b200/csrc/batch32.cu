@@ -110,8 +110,8 @@ cfl_kernel(BatchArgs a, FieldPtrs<const float> hi) {
 // (viscosity) along R and C are formed once per point there, so each cell
 // reads its neighbours from shared memory.  The P axis of 3-D instances
 // keeps per-cell neighbour evaluation from global memory.  These kernels
-// write interior cells only; edge_fill_kernel then writes the ghost images
-// of the tiles that touch a boundary.
+// write interior cells only; shell_fill_kernel then writes the ghost images
+// of the near-boundary cells.
 // ---------------------------------------------------------------------------
 constexpr int TC = BATCH_TC, TR = BATCH_TR;
 constexpr int U_PTS = (TC + 4) * (TR + 4) > BATCH_TILE + 4 ? (TC + 4) * (TR + 4) : BATCH_TILE + 4;
@@ -119,44 +119,24 @@ constexpr int FR_PTS = TC * (TR + 4) > BATCH_TILE + 4 ? TC * (TR + 4) : BATCH_TI
 constexpr int FC_PTS = (TC + 4) * TR;
 constexpr int W_PTS = (TC + 4) * TR > U_PTS ? (TC + 4) * TR : U_PTS;
 
-struct BlockGeo {
+struct BlockGeo : TileGeo {
   BatchInst in;
-  int idx;
-  int tc, tr;            // tile extent (TC x TR, or 1 x BATCH_TILE)
-  int nc, nr;            // cells of the tile inside the interior
-  int hc;                // halo width along C (0 when the instance has no C axis)
-  long long cell0;       // element index (instance-relative) of the tile's first cell
-  long long sP, sC, sR;  // strides of the P, C, R axes (0 when absent)
-  int oC, oR;            // total coordinate of the tile origin along C, R
-  int tC, tR;            // total extent along C, R
-  int x[3];              // interior coordinates of the tile origin per array axis
 };
 
+// The tile's geometry and its instance's record, copied into shared memory
+// by the CTA's threads in parallel (one word each).
 __device__ __forceinline__ void load_block(const BatchArgs &a, int t, BlockGeo &bg) {
-  if (threadIdx.x == 0) {
-    const BlockTile bt = a.btiles[t];
-    bg.idx = bt.inst;
-    bg.in = a.insts[bt.inst];
-    const Geom &g = bg.in.g;
-    const int R = bg.in.ax_r, C = bg.in.ax_c, P = bg.in.ax_p;
-    bg.tc = C >= 0 ? TC : 1;
-    bg.tr = C >= 0 ? TR : BATCH_TILE;
-    bg.hc = C >= 0 ? 2 : 0;
-    bg.nr = min(bg.tr, g.n[R] - bt.r0);
-    bg.nc = C >= 0 ? min(bg.tc, g.n[C] - bt.c0) : 1;
-    bg.sR = g.st[R];
-    bg.sC = C >= 0 ? g.st[C] : 0;
-    bg.sP = P >= 0 ? g.st[P] : 0;
-    bg.oR = bt.r0 + g.m[R];
-    bg.oC = C >= 0 ? bt.c0 + g.m[C] : 0;
-    bg.tR = g.t[R];
-    bg.tC = C >= 0 ? g.t[C] : 1;
-    bg.x[0] = bg.x[1] = bg.x[2] = 0;
-    bg.x[R] = bt.r0;
-    if (C >= 0) bg.x[C] = bt.c0;
-    if (P >= 0) bg.x[P] = bt.p;
-    bg.cell0 = (P >= 0 ? (long long)(bt.p + g.m[P]) * bg.sP : 0) + (long long)bg.oC * bg.sC +
-               (long long)bg.oR * bg.sR;
+  constexpr int NT = (int)(sizeof(TileGeo) / 4), NI = (int)(sizeof(BatchInst) / 4);
+  const int inst = __ldg(&a.btiles[t].idx);
+  const int *st = reinterpret_cast<const int *>(a.btiles + t);
+  const int *si = reinterpret_cast<const int *>(a.insts + inst);
+  int *dt = reinterpret_cast<int *>(static_cast<TileGeo *>(&bg));
+  int *di = reinterpret_cast<int *>(&bg.in);
+  for (int w = threadIdx.x; w < NT + NI; w += blockDim.x) {
+    if (w < NT)
+      dt[w] = __ldg(st + w);
+    else
+      di[w - NT] = __ldg(si + w - NT);
   }
   __syncthreads();
 }
@@ -440,34 +420,28 @@ av_block_kernel(BatchArgs a, FieldPtrs<const float> hi, FieldPtrs<const float> l
   }
 }
 
-// Ghost images of the near-boundary cells of the block tiles that touch an
-// instance's boundary (`etiles`), for `nfields` arrays; ftag >= 0 selects
-// one mirror-sign field for all of them (NF: never negated).
+// Ghost images of the listed near-boundary interior cells (instance, x0,
+// x1, x2) of every instance, one cell per thread, for `nfields` arrays;
+// ftag >= 0 selects one mirror-sign field for all of them (NF: never
+// negated).  The cell's values are loaded before any image is stored.
 __global__ void __launch_bounds__(BATCH_TILE)
-edge_fill_kernel(BatchArgs a, const int *etiles, int ne, FieldPtrs<float> q, int nfields,
-                 int ftag) {
-  __shared__ BlockGeo bg;
-  const int tid = threadIdx.x;
-  for (int t = blockIdx.x; t < ne; t += gridDim.x) {
-    load_block(a, etiles[t], bg);
-    const BatchInst &in = bg.in;
+shell_fill_kernel(BatchArgs a, const int4 *cells, int n, FieldPtrs<float> q, int nfields,
+                  int ftag) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int4 w = __ldg(cells + e);
+    const BatchInst &in = a.insts[w.x];
     const Geom &g = in.g;
-    const int tcl = tid / bg.tr, trl = tid % bg.tr;
-    if (tcl < bg.nc && trl < bg.nr) {
-      int xs[3] = {bg.x[0], bg.x[1], bg.x[2]};
-      xs[in.ax_r] += trl;
-      if (in.ax_c >= 0) xs[in.ax_c] += tcl;
-      if (near_boundary(g, xs[0], xs[1], xs[2])) {
-        const long long c = bg.cell0 + (long long)tcl * bg.sC + (long long)trl * bg.sR;
-        Img im;
-        make_img(g, xs[0], xs[1], xs[2], im);
-        for (int f = 0; f < nfields; ++f) {
-          float *p = q.f[f] + in.base;
-          store_img(p, c, im, ftag >= 0 ? ftag : f, p[c]);
-        }
-      }
-    }
-    __syncthreads();
+    const long long base = in.base;
+    const int c = cell_of(g, w.y, w.z, w.w);
+    float v[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+      if (f < nfields) v[f] = q.f[f][base + c];
+    Img im;
+    make_img(g, w.y, w.z, w.w, im);
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+      if (f < nfields) store_img(q.f[f] + base, (long long)c, im, ftag >= 0 ? ftag : f, v[f]);
   }
 }
 
@@ -497,6 +471,32 @@ fill_kernel(BatchArgs a, FieldPtrs<float> q, int nfields) {
 
 }  // namespace b32
 
+TileGeo make_tile_geo(const BatchInst &in, int idx, const BlockTile &bt) {
+  const Geom &g = in.g;
+  const int R = in.ax_r, C = in.ax_c, P = in.ax_p;
+  TileGeo tg{};
+  tg.idx = idx;
+  tg.tc = C >= 0 ? BATCH_TC : 1;
+  tg.tr = C >= 0 ? BATCH_TR : BATCH_TILE;
+  tg.hc = C >= 0 ? 2 : 0;
+  tg.nr = g.n[R] - bt.r0 < tg.tr ? g.n[R] - bt.r0 : tg.tr;
+  tg.nc = C >= 0 ? (g.n[C] - bt.c0 < tg.tc ? g.n[C] - bt.c0 : tg.tc) : 1;
+  tg.sR = g.st[R];
+  tg.sC = C >= 0 ? g.st[C] : 0;
+  tg.sP = P >= 0 ? g.st[P] : 0;
+  tg.oR = bt.r0 + g.m[R];
+  tg.oC = C >= 0 ? bt.c0 + g.m[C] : 0;
+  tg.tR = g.t[R];
+  tg.tC = C >= 0 ? g.t[C] : 1;
+  tg.x[0] = tg.x[1] = tg.x[2] = 0;
+  tg.x[R] = bt.r0;
+  if (C >= 0) tg.x[C] = bt.c0;
+  if (P >= 0) tg.x[P] = bt.p;
+  tg.cell0 = (P >= 0 ? (long long)(bt.p + g.m[P]) * tg.sP : 0) + (long long)tg.oC * tg.sC +
+             (long long)tg.oR * tg.sR;
+  return tg;
+}
+
 void b32_cfl(const BatchArgs &a, const FieldPtrs<const float> &hi, int grid, cudaStream_t st) {
   b32::cfl_kernel<<<grid, BATCH_TILE, 0, st>>>(a, hi);
 }
@@ -511,9 +511,12 @@ void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtr
             int fuse_cfl, int grid, cudaStream_t st) {
   b32::av_block_kernel<<<grid, BATCH_TILE, 0, st>>>(a, hi, lo, hi2, lo2, cc, dir, fuse_cfl);
 }
-void b32_edge_fill(const BatchArgs &a, const int *etiles, int ne, const FieldPtrs<float> &q,
-                   int nfields, int ftag, int grid, cudaStream_t st) {
-  if (ne > 0) b32::edge_fill_kernel<<<grid, BATCH_TILE, 0, st>>>(a, etiles, ne, q, nfields, ftag);
+void b32_shell_fill(const BatchArgs &a, const int4 *cells, int n, const FieldPtrs<float> &q,
+                    int nfields, int ftag, cudaStream_t st) {
+  if (n <= 0) return;
+  int grid = (n + BATCH_TILE - 1) / BATCH_TILE;
+  if (grid > 4096) grid = 4096;
+  b32::shell_fill_kernel<<<grid, BATCH_TILE, 0, st>>>(a, cells, n, q, nfields, ftag);
 }
 int b32_block_grid(int sms) {
   int rk = 0, av = 0;

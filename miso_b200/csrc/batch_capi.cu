@@ -43,9 +43,9 @@ struct miso_b200_batch {
   size_t bytes = 0;
   BatchInst *d_insts = nullptr;
   BatchTile *d_tiles = nullptr;
-  BlockTile *d_btiles = nullptr;
-  int *d_etiles = nullptr;  // block tiles that touch an instance boundary
-  int netiles = 0;
+  TileGeo *d_btiles = nullptr;
+  int4 *d_scells = nullptr;  // near-boundary interior cells (instance, x0, x1, x2)
+  int nscells = 0;
   StepScalars *d_sc = nullptr;
   unsigned int *d_dtmin = nullptr;
   unsigned int *d_err = nullptr;
@@ -128,12 +128,12 @@ struct miso_b200_batch {
                stream);
         // the block kernels write the interior; images of what the next pass reads
         if (s < 3) {
-          b32_edge_fill(a, d_etiles, netiles, mut(stg[s & 1]), NF, -1, bgrid, stream);
+          b32_shell_fill(a, d_scells, nscells, mut(stg[s & 1]), NF, -1, stream);
         } else {
-          b32_edge_fill(a, d_etiles, netiles, mut(hi[c]), NF, -1, bgrid, stream);
+          b32_shell_fill(a, d_scells, nscells, mut(hi[c]), NF, -1, stream);
           FieldPtrs<float> ccf{};
           ccf.f[0] = cc32;
-          b32_edge_fill(a, d_etiles, netiles, ccf, 1, NF, bgrid, stream);
+          b32_shell_fill(a, d_scells, nscells, ccf, 1, NF, stream);
           ++launches;
         }
         ++launches;
@@ -146,8 +146,8 @@ struct miso_b200_batch {
         if (!sweep[d]) continue;  // degenerate for every instance: the state is unchanged
         b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d,
                d == last ? 1 : 0, bgrid, stream);
-        b32_edge_fill(a, d_etiles, netiles, mut(hi[cur ^ 1]), NF, -1, bgrid, stream);
-        b32_edge_fill(a, d_etiles, netiles, mut(lo[cur ^ 1]), NF, -1, bgrid, stream);
+        b32_shell_fill(a, d_scells, nscells, mut(hi[cur ^ 1]), NF, -1, stream);
+        b32_shell_fill(a, d_scells, nscells, mut(lo[cur ^ 1]), NF, -1, stream);
         cur ^= 1;
         launches += 3;
       }
@@ -188,8 +188,8 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   b->split = params[0].precision == MISO_B200_FP32_SPLIT;
   long long off = 0;
   std::vector<BatchTile> tiles;
-  std::vector<BlockTile> btiles;
-  std::vector<int> etiles;
+  std::vector<TileGeo> btiles;
+  std::vector<int4> scells;
   for (int n = 0; n < count; ++n) {
     const miso_b200_grid_desc &gd = grids[n];
     const miso_b200_params &pp = params[n];
@@ -264,19 +264,23 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
       const int np = in.ax_p >= 0 ? g.n[in.ax_p] : 1;
       const int tr = in.ax_c >= 0 ? BATCH_TR : BATCH_TILE;
       const int tc = in.ax_c >= 0 ? BATCH_TC : 1;
-      const int mr = g.m[in.ax_r];
-      const int mc = in.ax_c >= 0 ? g.m[in.ax_c] : 0;
-      const int mp = in.ax_p >= 0 ? g.m[in.ax_p] : 0;
       for (int pp2 = 0; pp2 < np; ++pp2)
         for (int c0 = 0; c0 < nc; c0 += tc)
-          for (int r0 = 0; r0 < nr; r0 += tr) {
-            const int r1 = r0 + (tr < nr - r0 ? tr : nr - r0);
-            const int c1 = c0 + (tc < nc - c0 ? tc : nc - c0);
-            const bool edge = r0 < mr || r1 > nr - mr || c0 < mc || c1 > nc - mc ||
-                              pp2 < mp || pp2 >= np - mp;
-            if (edge) etiles.push_back((int)btiles.size());
-            btiles.push_back(BlockTile{n, pp2, c0, r0});
+          for (int r0 = 0; r0 < nr; r0 += tr)
+            btiles.push_back(make_tile_geo(in, n, BlockTile{n, pp2, c0, r0}));
+      // near-boundary interior cells, whose ghost images the fills write
+      auto nearb = [&](int a2, int x) { return g.s[a2] && (x < g.m[a2] || x >= g.n[a2] - g.m[a2]); };
+      for (int x0 = 0; x0 < g.n[0]; ++x0)
+        for (int x1 = 0; x1 < g.n[1]; ++x1) {
+          const bool row = nearb(0, x0) || nearb(1, x1);
+          for (int x2 = 0; x2 < g.n[2]; ++x2) {
+            if (!row && !nearb(2, x2)) {
+              if (g.n[2] > 2 * g.m[2] && x2 == g.m[2]) x2 = g.n[2] - g.m[2] - 1;  // skip the middle
+              continue;
+            }
+            scells.push_back(make_int4(n, x0, x1, x2));
           }
+        }
     }
     off += (g.cells + 63) / 64 * 64;  // instances start on 256-byte (FP32) boundaries
     if (g.cells > b->max_cells) b->max_cells = g.cells;
@@ -284,7 +288,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   b->total = off;
   b->ntiles = (int)tiles.size();
   b->nbtiles = (int)btiles.size();
-  b->netiles = (int)etiles.size();
+  b->nscells = (int)scells.size();
 
   cudaError_t e = cudaSuccess;
   int dev = 0;
@@ -314,8 +318,8 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   };
   add((void **)&b->d_insts, sizeof(BatchInst) * count);
   add((void **)&b->d_tiles, sizeof(BatchTile) * tiles.size());
-  add((void **)&b->d_btiles, sizeof(BlockTile) * btiles.size());
-  add((void **)&b->d_etiles, sizeof(int) * (etiles.empty() ? 1 : etiles.size()));
+  add((void **)&b->d_btiles, sizeof(TileGeo) * btiles.size());
+  add((void **)&b->d_scells, sizeof(int4) * (scells.empty() ? 1 : scells.size()));
   add((void **)&b->d_sc, sizeof(StepScalars) * count);
   add((void **)&b->d_dtmin, sizeof(unsigned int) * count);
   add((void **)&b->d_err, sizeof(unsigned int));
@@ -355,10 +359,10 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
     e = cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(),
                         cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(b->d_btiles, btiles.data(), sizeof(BlockTile) * btiles.size(),
+    e = cudaMemcpyAsync(b->d_btiles, btiles.data(), sizeof(TileGeo) * btiles.size(),
                         cudaMemcpyHostToDevice, b->stream);
-  if (e == cudaSuccess && !etiles.empty())
-    e = cudaMemcpyAsync(b->d_etiles, etiles.data(), sizeof(int) * etiles.size(),
+  if (e == cudaSuccess && !scells.empty())
+    e = cudaMemcpyAsync(b->d_scells, scells.data(), sizeof(int4) * scells.size(),
                         cudaMemcpyHostToDevice, b->stream);
   std::vector<unsigned int> init(count);
   const float big = 1.e10f;

@@ -342,13 +342,16 @@ struct miso_b200_handle {
   }
 
   // ghost images of the interior shell of up to two 9-field sets and cc
-  int shell(float *const *set_a, float *const *set_b, float *ccp) {
+  // (`imask`: the image masks written, SHELL_ALL by default)
+  int shell(float *const *set_a, float *const *set_b, float *ccp, unsigned imask = SHELL_ALL) {
     ShellArgs sa;
     sa.n = 0;
-    for (int f = 0; f < NF; ++f) {
-      sa.p[sa.n] = set_a[f];
-      sa.f[sa.n++] = f;
-    }
+    sa.imask = imask;
+    if (set_a)
+      for (int f = 0; f < NF; ++f) {
+        sa.p[sa.n] = set_a[f];
+        sa.f[sa.n++] = f;
+      }
     if (set_b)
       for (int f = 0; f < NF; ++f) {
         sa.p[sa.n] = set_b[f];
@@ -505,11 +508,14 @@ struct miso_b200_handle {
         launch_s32_rk_tiled(tm, a, st, rk_grid, stream);
       te(t, "rk_stage", interior() * (st == 0 ? 72.0 : st < 3 ? 108.0 : 184.0));
       if ((rc = check_launch("rk_stage"))) return rc;
-      if (rk_var == 2) {  // interior-only writer: fill the images it reads next
+      if (rk_var == 2) {  // interior-only writer: fill the images read next
         if (st < 3) {
-          if ((rc = shell(stg[st & 1], nullptr, nullptr))) return rc;
+          // the next stage's star stencil reads face ghosts only
+          if ((rc = shell(stg[st & 1], nullptr, nullptr, SHELL_FACES))) return rc;
         } else {
-          if ((rc = shell(hi[c], nullptr, cc32))) return rc;
+          // the x sweep reads hi across the i faces; every sweep reads cc
+          if ((rc = shell(hi[c], nullptr, nullptr, SHELL_FACES_I))) return rc;
+          if ((rc = shell(nullptr, nullptr, cc32, SHELL_FACES))) return rc;
         }
       }
     }
@@ -544,7 +550,10 @@ struct miso_b200_handle {
       // interior-only writers (line and z sweeps): the hi images are read by
       // the next pass; lo images only by a download (see lo_shell_stale)
       if (av_var[d] == 0) {
-        if ((rc = shell(hi[cur ^ 1], nullptr, nullptr))) return rc;
+        // the y sweep reads j-face ghosts, the z sweep k-face ghosts; after
+        // the z sweep the step's final state gets every image
+        const unsigned m = d == 0 ? SHELL_FACES_J : d == 1 ? SHELL_FACES_K : SHELL_ALL;
+        if ((rc = shell(hi[cur ^ 1], nullptr, nullptr, m))) return rc;
         lo_shell_stale = true;
       } else {
         lo_shell_stale = false;

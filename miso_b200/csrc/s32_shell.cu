@@ -12,7 +12,10 @@
 // i-shell planes, (B) the j-shell rows of the remaining planes, (C) the
 // k-ends of the remaining rows, each in k-fastest order so neighbouring
 // threads touch neighbouring cells.  A thread loads the cell's value in
-// every array before it stores any image, so the loads overlap.
+// every array before it stores any image, so the loads overlap.  An image
+// mask limits the work to the images the next pass reads (the faces of one
+// axis for a sweep, the faces of all axes without edges and corners for the
+// Runge-Kutta star stencil, everything for a step's final state).
 #include "common.cuh"
 #include "images.cuh"
 #include "s32_tiled.h"
@@ -60,13 +63,15 @@ shell_kernel(const Geom g, const ShellArgs a, long long total) {
        idx += (long long)gridDim.x * blockDim.x) {
     int x0, x1, x2;
     shell_coords(g, idx, x0, x1, x2);
+    Img im;
+    make_img(g, x0, x1, x2, im);
+    im.valid &= a.imask;  // only the images the next pass reads
+    if (!im.valid) continue;
     const int cell = cell_of(g, x0, x1, x2);
     float v[MAXA];
 #pragma unroll
     for (int n = 0; n < MAXA; ++n)
       if (n < a.n) v[n] = a.p[n][cell];
-    Img im;
-    make_img(g, x0, x1, x2, im);
 #pragma unroll
     for (int n = 0; n < MAXA; ++n) {
       if (n < a.n) {

@@ -42,7 +42,12 @@ struct ShellArgs {
   float *p[2 * NF + 1];
   int f[2 * NF + 1];
   int n;
+  unsigned imask;  // images to write: bit (m-1) for image mask m (1 = i, 2 = j, 4 = k, sums = edges/corners)
 };
+// image masks: the faces of one axis set (no edges or corners), or everything
+constexpr unsigned SHELL_FACES_I = 1u << 0, SHELL_FACES_J = 1u << 1, SHELL_FACES_K = 1u << 3;
+constexpr unsigned SHELL_FACES = SHELL_FACES_I | SHELL_FACES_J | SHELL_FACES_K;
+constexpr unsigned SHELL_ALL = 0x7fu;
 void launch_s32_shell(const Geom &g, const ShellArgs &a, int grid, cudaStream_t st);
 long long s32_shell_cells(const Geom &g);  // interior cells within the margin of a face
 

@@ -424,8 +424,8 @@ def run_batch(args):
     value = world * cells * K / (ms / 1e3) / 1e9
     if rank == 0:
         print(json.dumps({
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": Kg,
-            "warmup": W, "ms_per_step": ms / Kg, "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.precision == "fp32_split" else "f64",
             "data": "synthetic (seeded)",
             "config": {"workload": args.workload, "instances": len(probs),

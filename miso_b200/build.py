@@ -32,6 +32,7 @@ EXTRA = {
     "noalloc.cu": ["--fmad=false"],
     "batch64.cu": ["--fmad=false"],
     "batch32.cu": FAST32,
+    "batch32_rows.cu": FAST32,
     "fp32s_kernels.cu": FAST32,
     "s32_tiled.cu": FAST32,
     "s32_flat.cu": FAST32,

@@ -55,6 +55,14 @@ struct TileGeo {
 };
 TileGeo make_tile_geo(const BatchInst &in, int idx, const BlockTile &bt);
 
+// Row segment of a 1-D or 2-D instance for the warp kernels (batch32_rows.cu):
+// rows [c0, c1) along C (0, 1 for 1-D) and cells from r0 along R.
+struct RowItem {
+  int inst, c0, c1, r0;
+};
+constexpr int ROW_OUT = 28;    // cells a warp finishes along R (shuffle stencils)
+constexpr int ROW_CHUNK = 32;  // rows a warp marches along C
+
 struct BatchArgs {
   const BatchInst *insts;
   const BatchTile *tiles;
@@ -95,6 +103,22 @@ void b32_fill(const BatchArgs &a, const FieldPtrs<float> &q, int nfields, int gr
 // ghost images of the listed near-boundary cells (instance, x0, x1, x2)
 void b32_shell_fill(const BatchArgs &a, const int4 *cells, int n, const FieldPtrs<float> &q,
                     int nfields, int ftag, cudaStream_t st);
+// warp-per-row kernels for 1-D / 2-D instances
+// `combo` (b32_row_combo) selects the axis pair of every item in `items`
+int b32_row_combo(int ax_r, int ax_c);
+constexpr int ROW_COMBOS = 6;
+void b32_rk_rows(const BatchArgs &a, const RowItem *items, int n, int combo,
+                 const FieldPtrs<const float> &prev, const FieldPtrs<const float> &u0,
+                 const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
+                 const FieldPtrs<float> &out, float *cc, int stage, int grid, cudaStream_t st);
+void b32_av_rows_r(const BatchArgs &a, const RowItem *items, int n,
+                   const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
+                   const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc,
+                   int dir, int fuse_cfl, int grid, cudaStream_t st);
+void b32_av_rows_c(const BatchArgs &a, const RowItem *items, int n,
+                   const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
+                   const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc,
+                   int dir, int fuse_cfl, int grid, cudaStream_t st);
 // resident CTAs of the block-tile kernels on `sms` SMs (their persistent grid)
 int b32_block_grid(int sms);
 

@@ -37,7 +37,15 @@ struct miso_b200_batch {
   int ntiles = 0;
   int nbtiles = 0;
   int bgrid = 0;  // persistent grid of the FP32 block-tile kernels
+  // FP32 warp-per-row items of the 1-D / 2-D instances: per axis pair for
+  // the Runge-Kutta stage (28 cells along R), all of them for the sweep
+  // along R, and 32-cell items for the sweep along C
+  RowItem *d_rows = nullptr, *d_rows_c = nullptr;
+  int row_off[ROW_COMBOS + 1] = {};
+  int nrows = 0, nrows_c = 0;
+  int rgrid = 0;
   bool sweep[3] = {false, false, false};  // some instance is non-degenerate along d
+  bool sweep_c[3] = {false, false, false};  // d is the C axis of some 2-D instance
 
   void *block = nullptr;
   size_t bytes = 0;
@@ -124,8 +132,18 @@ struct miso_b200_batch {
       const int c = cur;
       for (int s = 0; s < 4; ++s) {
         FieldPtrs<const float> prev = s == 0 ? cst(hi[c]) : cst(stg[(s - 1) & 1]);
-        b32_rk(a, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]), mut(stg[s & 1]), cc32, s, bgrid,
-               stream);
+        if (nbtiles) {
+          b32_rk(a, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]), mut(stg[s & 1]), cc32, s, bgrid,
+                 stream);
+          ++launches;
+        }
+        for (int cb = 0; cb < ROW_COMBOS; ++cb) {
+          const int n = row_off[cb + 1] - row_off[cb];
+          if (!n) continue;
+          b32_rk_rows(a, d_rows + row_off[cb], n, cb, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]),
+                      mut(stg[s & 1]), cc32, s, rgrid, stream);
+          ++launches;
+        }
         // the block kernels write the interior; images of what the next pass reads
         if (s < 3) {
           b32_shell_fill(a, d_scells, nscells, mut(stg[s & 1]), NF, -1, stream);
@@ -138,18 +156,32 @@ struct miso_b200_batch {
         }
         ++launches;
       }
-      launches += 1 + 4;
+      launches += 1;
       int last = -1;
       for (int d = 0; d < 3; ++d)
         if (sweep[d]) last = d;
       for (int d = 0; d < 3; ++d) {
         if (!sweep[d]) continue;  // degenerate for every instance: the state is unchanged
-        b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d,
-               d == last ? 1 : 0, bgrid, stream);
+        const int fuse = d == last ? 1 : 0;
+        if (nbtiles) {
+          b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d, fuse,
+                 bgrid, stream);
+          ++launches;
+        }
+        if (nrows) {  // sweeps along R and degenerate ones of the 1-D / 2-D instances
+          b32_av_rows_r(a, d_rows, nrows, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]),
+                        mut(lo[cur ^ 1]), cc32, d, fuse, rgrid, stream);
+          ++launches;
+        }
+        if (nrows_c && sweep_c[d]) {  // sweeps along C of the 2-D instances
+          b32_av_rows_c(a, d_rows_c, nrows_c, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]),
+                        mut(lo[cur ^ 1]), cc32, d, fuse, rgrid, stream);
+          ++launches;
+        }
         b32_shell_fill(a, d_scells, nscells, mut(hi[cur ^ 1]), NF, -1, stream);
         b32_shell_fill(a, d_scells, nscells, mut(lo[cur ^ 1]), NF, -1, stream);
         cur ^= 1;
-        launches += 3;
+        launches += 2;
       }
       cfl_valid = last >= 0;
     }
@@ -189,6 +221,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   long long off = 0;
   std::vector<BatchTile> tiles;
   std::vector<TileGeo> btiles;
+  std::vector<RowItem> rows[ROW_COMBOS], rows_c;
   std::vector<int4> scells;
   for (int n = 0; n < count; ++n) {
     const miso_b200_grid_desc &gd = grids[n];
@@ -262,12 +295,26 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
       const int nr = g.n[in.ax_r];
       const int nc = in.ax_c >= 0 ? g.n[in.ax_c] : 1;
       const int np = in.ax_p >= 0 ? g.n[in.ax_p] : 1;
-      const int tr = in.ax_c >= 0 ? BATCH_TR : BATCH_TILE;
-      const int tc = in.ax_c >= 0 ? BATCH_TC : 1;
-      for (int pp2 = 0; pp2 < np; ++pp2)
-        for (int c0 = 0; c0 < nc; c0 += tc)
-          for (int r0 = 0; r0 < nr; r0 += tr)
-            btiles.push_back(make_tile_geo(in, n, BlockTile{n, pp2, c0, r0}));
+      if (in.ax_p >= 0) {
+        // 3-D: block tiles
+        for (int pp2 = 0; pp2 < np; ++pp2)
+          for (int c0 = 0; c0 < nc; c0 += BATCH_TC)
+            for (int r0 = 0; r0 < nr; r0 += BATCH_TR)
+              btiles.push_back(make_tile_geo(in, n, BlockTile{n, pp2, c0, r0}));
+      } else {
+        // 1-D / 2-D: warp-per-row items
+        const int cb = b32_row_combo(in.ax_r, in.ax_c);
+        const int ch = in.ax_c >= 0 ? ROW_CHUNK : 1;
+        for (int c0 = 0; c0 < nc; c0 += ch)
+          for (int r0 = 0; r0 < nr; r0 += ROW_OUT)
+            rows[cb].push_back(RowItem{n, c0, c0 + ch < nc ? c0 + ch : nc, r0});
+        if (in.ax_c >= 0) {
+          b->sweep_c[in.ax_c] = true;
+          for (int c0 = 0; c0 < nc; c0 += ROW_CHUNK)
+            for (int r0 = 0; r0 < nr; r0 += 32)
+              rows_c.push_back(RowItem{n, c0, c0 + ROW_CHUNK < nc ? c0 + ROW_CHUNK : nc, r0});
+        }
+      }
       // near-boundary interior cells, whose ghost images the fills write
       auto nearb = [&](int a2, int x) { return g.s[a2] && (x < g.m[a2] || x >= g.n[a2] - g.m[a2]); };
       for (int x0 = 0; x0 < g.n[0]; ++x0)
@@ -288,6 +335,14 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   b->total = off;
   b->ntiles = (int)tiles.size();
   b->nbtiles = (int)btiles.size();
+  std::vector<RowItem> rows_all;
+  for (int cb = 0; cb < ROW_COMBOS; ++cb) {
+    b->row_off[cb] = (int)rows_all.size();
+    rows_all.insert(rows_all.end(), rows[cb].begin(), rows[cb].end());
+  }
+  b->row_off[ROW_COMBOS] = (int)rows_all.size();
+  b->nrows = (int)rows_all.size();
+  b->nrows_c = (int)rows_c.size();
   b->nscells = (int)scells.size();
 
   cudaError_t e = cudaSuccess;
@@ -300,6 +355,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   }
   b->grid = b->sms * 8;
   b->bgrid = b32_block_grid(b->sms);
+  b->rgrid = 8 * b->sms;  // 8 warps per CTA, one row item per warp at a time
   if (stream) {
     b->stream = (cudaStream_t)stream;
   } else {
@@ -318,7 +374,9 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   };
   add((void **)&b->d_insts, sizeof(BatchInst) * count);
   add((void **)&b->d_tiles, sizeof(BatchTile) * tiles.size());
-  add((void **)&b->d_btiles, sizeof(TileGeo) * btiles.size());
+  add((void **)&b->d_btiles, sizeof(TileGeo) * (btiles.empty() ? 1 : btiles.size()));
+  add((void **)&b->d_rows, sizeof(RowItem) * (rows_all.empty() ? 1 : rows_all.size()));
+  add((void **)&b->d_rows_c, sizeof(RowItem) * (rows_c.empty() ? 1 : rows_c.size()));
   add((void **)&b->d_scells, sizeof(int4) * (scells.empty() ? 1 : scells.size()));
   add((void **)&b->d_sc, sizeof(StepScalars) * count);
   add((void **)&b->d_dtmin, sizeof(unsigned int) * count);
@@ -358,8 +416,14 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(),
                         cudaMemcpyHostToDevice, b->stream);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && !btiles.empty())
     e = cudaMemcpyAsync(b->d_btiles, btiles.data(), sizeof(TileGeo) * btiles.size(),
+                        cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess && !rows_all.empty())
+    e = cudaMemcpyAsync(b->d_rows, rows_all.data(), sizeof(RowItem) * rows_all.size(),
+                        cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess && !rows_c.empty())
+    e = cudaMemcpyAsync(b->d_rows_c, rows_c.data(), sizeof(RowItem) * rows_c.size(),
                         cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess && !scells.empty())
     e = cudaMemcpyAsync(b->d_scells, scells.data(), sizeof(int4) * scells.size(),

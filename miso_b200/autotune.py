@@ -20,7 +20,7 @@ import os
 
 CLASSES = {"rk_stage": 0, "av_x": 1, "av_y": 2, "av_z": 3}
 # variants per class: 0 tiled, 1 flat, 2 pipelined (RK: planes with packed
-# differences; x / y sweeps: streamed lines on full/empty mbarriers)
+# differences; x / y sweeps: one warp per line segment marching along the axis)
 VARIANTS = {"rk_stage": (0, 1, 2), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1)}
 CHUNKS = (32, 64, 128)
 

@@ -158,7 +158,7 @@ struct miso_b200_handle {
   long long pitch = 0;                       // elements between consecutive field arrays
   int rk_L = 64, rk_tiles_j = 0, rk_tiles_k = 0, rk_items = 0, rk_grid = 0;
   int av_L = 128, av_grid = 0, z_grid = 0;
-  int avp_grid = 0;  // streamed x / y sweep: 4 resident CTAs per SM
+  int avp_grid = 0;  // warp-march x / y sweep: 2 resident CTAs of 8 warps per SM
   int shell_grid = 0;
   // The flat kernels run exactly one resident wave (grid = resident blocks)
   // and stride over tiles in order, so the CTAs in flight always cover one
@@ -170,7 +170,7 @@ struct miso_b200_handle {
   // kernel variant per class on the 3-D split path: 0 = tiled (TMA plane
   // tiles / streaming lines), 1 = flat (one thread per cell); 2: RK =
   // pipelined TMA planes with packed FP32x2 differences (default), x / y
-  // sweeps = lines streamed on full/empty mbarriers
+  // sweeps = one warp per line segment marching along the sweep axis
   int rk_var = 2;
   int av_var[3] = {0, 0, 0};
   double *mon_partial = nullptr;
@@ -338,32 +338,34 @@ struct miso_b200_handle {
   int fresh_lo_shell() {
     if (!lo_shell_stale) return MISO_B200_OK;
     lo_shell_stale = false;
-    return shell(lo[cur], nullptr, nullptr);
+    return shell(lo[cur], SHELL_ALL);
   }
 
-  // ghost images of the interior shell of up to two 9-field sets and cc
-  // (`imask`: the image masks written, SHELL_ALL by default)
-  int shell(float *const *set_a, float *const *set_b, float *ccp, unsigned imask = SHELL_ALL) {
+  // ghost images of the interior shell: the 9 arrays of `set` with image
+  // mask `mset`, and (when given) cc with mask `mcc`
+  int shell(float *const *set, unsigned mset, float *ccp = nullptr, unsigned mcc = 0) {
     ShellArgs sa;
     sa.n = 0;
-    sa.imask = imask;
-    if (set_a)
+    if (set)
       for (int f = 0; f < NF; ++f) {
-        sa.p[sa.n] = set_a[f];
-        sa.f[sa.n++] = f;
-      }
-    if (set_b)
-      for (int f = 0; f < NF; ++f) {
-        sa.p[sa.n] = set_b[f];
-        sa.f[sa.n++] = f;
+        sa.p[sa.n] = set[f];
+        sa.f[sa.n] = f;
+        sa.m[sa.n++] = mset;
       }
     if (ccp) {
       sa.p[sa.n] = ccp;
-      sa.f[sa.n++] = NF;
+      sa.f[sa.n] = NF;
+      sa.m[sa.n++] = mcc;
     }
+    unsigned any = 0;
+    for (int n = 0; n < sa.n; ++n) any |= sa.m[n];
+    sa.slab = any == SHELL_FACES_I ? 0 : any == SHELL_FACES_J ? 1 : any == SHELL_FACES_K ? 2 : -1;
+    const long long cells = s32_shell_count(g, sa.slab);
+    long long grid = (cells + 255) / 256;
+    if (grid > 8LL * sms) grid = 8LL * sms;
     const int t = tb();
-    launch_s32_shell(g, sa, shell_grid, stream);
-    te(t, "ghost_shell", ghost_cells() * 8.0 * sa.n);
+    launch_s32_shell(g, sa, (int)grid, stream);
+    te(t, "ghost_shell", (double)cells * 8.0 * sa.n);
     return check_launch("ghost_shell");
   }
 
@@ -511,11 +513,10 @@ struct miso_b200_handle {
       if (rk_var == 2) {  // interior-only writer: fill the images read next
         if (st < 3) {
           // the next stage's star stencil reads face ghosts only
-          if ((rc = shell(stg[st & 1], nullptr, nullptr, SHELL_FACES))) return rc;
+          if ((rc = shell(stg[st & 1], SHELL_FACES))) return rc;
         } else {
           // the x sweep reads hi across the i faces; every sweep reads cc
-          if ((rc = shell(hi[c], nullptr, nullptr, SHELL_FACES_I))) return rc;
-          if ((rc = shell(nullptr, nullptr, cc32, SHELL_FACES))) return rc;
+          if ((rc = shell(hi[c], SHELL_FACES_I, cc32, SHELL_FACES))) return rc;
         }
       }
     }
@@ -540,7 +541,7 @@ struct miso_b200_handle {
       if (av_var[d] == 1)
         launch_s32_av_flat(a, d, flat_grid, stream);
       else if (av_var[d] == 2 && d < 2)
-        launch_s32_av_pipe(tm_avh[cur], tm_avl[cur], tm_avc, a, d, avp_grid, stream);
+        launch_s32_av_march(a, d, avp_grid, stream);
       else if (d < 2)
         launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, av_grid, stream);
       else
@@ -549,11 +550,11 @@ struct miso_b200_handle {
       if ((rc = check_launch("av_sweep"))) return rc;
       // interior-only writers (line and z sweeps): the hi images are read by
       // the next pass; lo images only by a download (see lo_shell_stale)
-      if (av_var[d] == 0) {
+      if (av_var[d] == 0 || (av_var[d] == 2 && d < 2)) {
         // the y sweep reads j-face ghosts, the z sweep k-face ghosts; after
         // the z sweep the step's final state gets every image
         const unsigned m = d == 0 ? SHELL_FACES_J : d == 1 ? SHELL_FACES_K : SHELL_ALL;
-        if ((rc = shell(hi[cur ^ 1], nullptr, nullptr, m))) return rc;
+        if ((rc = shell(hi[cur ^ 1], m))) return rc;
         lo_shell_stale = true;
       } else {
         lo_shell_stale = false;
@@ -729,8 +730,7 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   h->pitch = (long long)(round_up(cells * sizeof(float)) / sizeof(float));
   if (h->split() && s32_tiled_supported(g) && !getenv("MISO_B200_UNTILED")) {
     const size_t pb = round_up(cells * sizeof(float));
-    bool ok = s32_configure() == 0 && s32_rk_pipe_configure() == 0 &&
-              s32_av_pipe_configure() == 0;
+    bool ok = s32_configure() == 0 && s32_rk_pipe_configure() == 0;
     for (int s = 0; s < 2 && ok; ++s) {
       ok = s32_make_tmap(g, h->hi[s][0], pb, 0, h->tm_hi[s]) == 0 &&
            s32_make_tmap(g, h->stg[s][0], pb, 0, h->tm_stg[s]) == 0 &&
@@ -743,8 +743,8 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
       s32_rk_items(g, h->rk_L, h->rk_tiles_j, h->rk_tiles_k, h->rk_items);
       const int per_sm = 2;
       h->rk_grid = h->rk_items < per_sm * h->sms ? h->rk_items : per_sm * h->sms;
-      h->av_grid = 3 * h->sms;
-      h->avp_grid = 4 * h->sms;
+      h->av_grid = 2 * h->sms;  // line sweeps: two CTAs per SM
+      h->avp_grid = 2 * h->sms;
       {
         const long long want = (s32_shell_cells(g) + 255) / 256;
         h->shell_grid = (int)(want < 8LL * h->sms ? want : 8LL * h->sms);

@@ -56,10 +56,63 @@ __device__ __forceinline__ void flux_dir(const float u[NF], const PrimF &p, floa
   F[PH] = ch2 * bd;
 }
 
-__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
-  s = a + b;
-  const float bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
+// ---------------------------------------------------------------------------
+// One arithmetic for a single field (float) and for a pair of fields
+// (float2, the packed FP32x2 add / mul / fma of sm_100: component-wise,
+// round to nearest, so each component gets the bits the scalar operation
+// gives).  Products are never contracted behind the caller's back: every
+// fma is written out.
+// ---------------------------------------------------------------------------
+template <class V>
+__device__ __forceinline__ V vs(float x);
+template <>
+__device__ __forceinline__ float vs<float>(float x) { return x; }
+template <>
+__device__ __forceinline__ float2 vs<float2>(float x) { return make_float2(x, x); }
+
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float vmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b, rounded once ((-1) * b is exact)
+__device__ __forceinline__ float vsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(-1.f, -1.f), b, a);
+}
+__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ float2 vmax(float2 a, float2 b) {
+  return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y));
+}
+__device__ __forceinline__ float vmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ float2 vmin(float2 a, float2 b) {
+  return make_float2(fminf(a.x, b.x), fminf(a.y, b.y));
+}
+// approximate reciprocal (PTX rcp.approx.ftz.f32) of d held at |d| >= 1e-20
+// with its sign: the divisor of the limiter ratio
+__device__ __forceinline__ float guard_rcp(float d) {
+  const float g = copysignf(fmaxf(fabsf(d), 1e-20f), d);
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(g));
+  return r;
+}
+__device__ __forceinline__ float2 guard_rcp(float2 d) {
+  return make_float2(guard_rcp(d.x), guard_rcp(d.y));
+}
+// H(ra) * max(0, t), H the step (0 where ra carries a sign bit, else 1)
+__device__ __forceinline__ float hstep(float ra, float t) {
+  return signbit(ra) ? 0.0f : fmaxf(0.0f, t);
+}
+__device__ __forceinline__ float2 hstep(float2 ra, float2 t) {
+  return make_float2(hstep(ra.x, t.x), hstep(ra.y, t.y));
+}
+
+template <class V>
+__device__ __forceinline__ void two_sum(V a, V b, V &s, V &e) {
+  s = vadd(a, b);
+  const V bb = vsub(s, a);
+  e = vadd(vsub(a, vsub(s, bb)), vsub(b, bb));
 }
 
 // characteristic-speed pieces of a conserved state
@@ -77,24 +130,37 @@ __device__ __forceinline__ void speeds(const float s[NF], float gm, float gm1, f
 // ---------------------------------------------------------------------------
 // Artificial viscosity helpers (limiter.hpp:11-37)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float dqq_eval(float qq_dw, float qq_cn, float qq_up, float ep) {
-  const float d_dw = qq_cn - qq_dw;
-  const float d_up = qq_up - qq_cn;
-  const float d_cn = (qq_up - qq_dw) * 0.5f;
-  const float mx = fmaxf(fmaxf(ep * d_dw, ep * d_up), d_cn);
-  const float mn = fminf(fminf(ep * d_dw, ep * d_up), d_cn);
-  return fminf(0.0f, mx) + fmaxf(0.0f, mn);
+// generalized minmod slope of the centre point (limiter.hpp:11-20)
+template <class V>
+__device__ __forceinline__ V dqq_t(V qq_dw, V qq_cn, V qq_up, V ep) {
+  const V d_dw = vsub(qq_cn, qq_dw);
+  const V d_up = vsub(qq_up, qq_cn);
+  const V d_cn = vmul(vsub(qq_up, qq_dw), vs<V>(0.5f));
+  const V a = vmul(ep, d_dw), b = vmul(ep, d_up);
+  const V mx = vmax(vmax(a, b), d_cn);
+  const V mn = vmin(vmin(a, b), d_cn);
+  return vadd(vmin(vs<V>(0.0f), mx), vmax(vs<V>(0.0f), mn));
 }
 
+// limited face flux (limiter.hpp:22-37); hcc = -1/2 of the face speed
+template <class V>
+__device__ __forceinline__ V flux_t(V qq_dw, V qq_up, V dqq_dw, V dqq_up, V hcc, V fh) {
+  const V qql = vfma(vs<V>(0.5f), dqq_dw, qq_dw);
+  const V qqr = vfma(vs<V>(-0.5f), dqq_up, qq_up);
+  const V diff = vsub(qqr, qql);
+  const V ra = vmin(vs<V>(1.0f), vmul(diff, guard_rcp(vsub(qq_up, qq_dw))));
+  const V pp = hstep(ra, vfma(fh, vadd(ra, vs<V>(-1.0f)), vs<V>(1.0f)));
+  return vmul(vmul(hcc, pp), diff);
+}
+
+__device__ __forceinline__ float dqq_eval(float qq_dw, float qq_cn, float qq_up, float ep) {
+  return dqq_t<float>(qq_dw, qq_cn, qq_up, ep);
+}
+
+// cc: the face speed
 __device__ __forceinline__ float flux_core(float qq_dw, float qq_up, float dqq_dw, float dqq_up,
                                            float cc, float fh) {
-  const float qql = qq_dw + 0.5f * dqq_dw;
-  const float qqr = qq_up - 0.5f * dqq_up;
-  float dqq = qq_up - qq_dw;
-  dqq = copysignf(fmaxf(fabsf(dqq), 1e-20f), dqq);
-  const float ra = fminf(1.0f, __fdividef(qqr - qql, dqq));
-  const float pp = (0.5f + copysignf(0.5f, ra)) * fmaxf(0.0f, 1.0f + fh * (ra - 1.0f));
-  return -0.5f * cc * pp * (qqr - qql);
+  return flux_t<float>(qq_dw, qq_up, dqq_dw, dqq_up, -0.5f * cc, fh);
 }
 
 // limited quantities of a point: ro, mx, my, mz, bx, by, bz, ph, ro*e
@@ -109,6 +175,20 @@ __device__ __forceinline__ void limited_vars(const float u[NF], float w[NW]) {
   const float inv = 1.0f / u[RO];
   w[8] = u[ET] - 0.5f * (u[MX] * u[MX] + u[MY] * u[MY] + u[MZ] * u[MZ]) * inv -
          (u[BX] * u[BX] + u[BY] * u[BY] + u[BZ] * u[BZ]) * FPII8;
+}
+
+// the limited quantities as pairs (ro, mx) (my, mz) (bx, by) (bz, ph) and
+// ro*e alone; pair i component c is limited quantity 2i + c
+struct W9 {
+  float2 p[4];
+  float s;
+};
+__device__ __forceinline__ void limited_w9(const float u[NF], W9 &w) {
+  float t[NW];
+  limited_vars(u, t);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w.p[i] = make_float2(t[2 * i], t[2 * i + 1]);
+  w.s = t[8];
 }
 
 }  // namespace s32t

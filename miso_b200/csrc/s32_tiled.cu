@@ -14,14 +14,17 @@
 //   runs; the last stage also writes the characteristic speed.
 //
 // Artificial viscosity:
-//   x and y sweeps (av_line_kernel) stream along their axis: a CTA of 128
-//   threads owns 128 consecutive k cells of one line; per plane one TMA
-//   copy each brings hi, lo and the characteristic speed (k box of 132
-//   cells), and a register queue carries the limiter slopes and face
-//   fluxes, so each face flux and each slope is evaluated once.  The z
-//   sweep (contiguous axis, av_z_kernel) exchanges neighbours with warp
-//   shuffles and folds the CFL candidate of the new state into per-block
-//   minima.  The sweeps write the interior only; the ghost images follow
+//   x and y sweeps (av_line_kernel) stream along their axis: four consumer
+//   warps own 128 consecutive k cells of one line; per plane one TMA copy
+//   each brings hi, lo and the characteristic speed (k box of 132 cells)
+//   into a ring of slots that a fifth warp fills.  Full / empty mbarriers
+//   order the ring, so no CTA barrier runs in the loop (a CTA barrier per
+//   plane, with the first thread waiting for the copy, measured 1.1x
+//   slower).  A register queue carries the limiter slopes and face fluxes,
+//   so each face flux and each slope is evaluated once, on packed field
+//   pairs.  The z sweep (contiguous axis, av_z_kernel) exchanges
+//   neighbours with warp shuffles and folds the CFL candidate of the new
+//   state into per-block minima.  The sweeps write the interior only; the ghost images follow
 //   from the shell kernel (s32_shell.cu).
 //
 // Physics as in fp32s_kernels.cu (flux form of mhd_integrator_host.hpp:
@@ -298,10 +301,12 @@ constexpr int L_CC = L_LO + L_LO;
 constexpr int L_SLOT = L_CC + (LBOX * 4 + 127) / 128 * 128;
 constexpr unsigned L_TX = 2 * NF * LBOX * 4 + LBOX * 4;  // bytes per slot fill
 
+constexpr int LCW = LK / 32;  // consumer warps; one more warp issues the copies
+
 struct __align__(128) LineSmem {
   unsigned char slot[LNB][L_SLOT];
-  unsigned long long bar[LNB];
-  int abort;
+  unsigned long long full[LNB];   // copy of the slot landed (1 arrival + bytes)
+  unsigned long long empty[LNB];  // slot read by every consumer warp (LCW arrivals)
 };
 
 struct LineItem {
@@ -351,45 +356,65 @@ __device__ __forceinline__ void line_issue(const CUtensorMap *thi, const CUtenso
   const int k0 = it.kb * LK;
   const int cj = DIR == 0 ? it.u + g.m[1] : p + g.m[1];
   const int ci = DIR == 0 ? p + g.m[0] : it.u + g.m[0];
-  mbar_expect_tx(&sm.bar[s], L_TX);
-  tma4(thi, sl + L_HI, &sm.bar[s], k0, cj, ci, 0);
-  tma4(tlo, sl + L_LO, &sm.bar[s], k0, cj, ci, 0);
-  tma3(tcc, sl + L_CC, &sm.bar[s], k0, cj, ci);
+  mbar_expect_tx(&sm.full[s], L_TX);
+  tma4(thi, sl + L_HI, &sm.full[s], k0, cj, ci, 0);
+  tma4(tlo, sl + L_LO, &sm.full[s], k0, cj, ci, 0);
+  tma3(tcc, sl + L_CC, &sm.full[s], k0, cj, ci);
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(LK, 3)
+__global__ void __launch_bounds__(LK + 32, 2)
 av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CUtensorMap tlo,
                const __grid_constant__ CUtensorMap tcc, const AvArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   LineSmem &sm = *reinterpret_cast<LineSmem *>(smem_raw);
   const Geom &g = a.g;
   constexpr int OTH = DIR == 0 ? 1 : 0;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31;
   const int nk = g.n[2], nu = g.n[OTH];
   const int kblocks = (nk + LK - 1) / LK;
   const int chunks = (g.n[DIR] + a.L - 1) / a.L;
   const int items = kblocks * nu * chunks;
   if (tid == 0) {
-    for (int b = 0; b < LNB; ++b) mbar_init(&sm.bar[b], 1);
-    sm.abort = 0;
+    for (int b = 0; b < LNB; ++b) {
+      mbar_init(&sm.full[b], 1);
+      mbar_init(&sm.empty[b], LCW);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
+  __syncthreads();  // the only CTA barrier
   if ((int)blockIdx.x >= items) return;
-  const float fac = (float)(g.dsi[DIR] * a.sc->dt);
-  LineCursor<DIR> prod;
-  int issued = 0;
-  if (tid == 0) {
-    prod.begin(a, kblocks, nu, items);
-    for (int s = 0; s < LNB && prod.valid(items); ++s) {
-      line_issue<DIR>(&thi, &tlo, &tcc, sm, s, g, prod.cur, prod.p);
-      prod.next(a, kblocks, nu, items);
-      ++issued;
+
+  if (tid >= LK) {
+    // producer warp: one lane fills the slots in plane order, each once the
+    // consumer warps have released its previous plane
+    if (tid == LK) {
+      LineCursor<DIR> prod;
+      prod.begin(a, kblocks, nu, items);
+      int s = 0;
+      for (; prod.valid(items); ++s) {
+        const int b = s % LNB;
+        if (s >= LNB && !mbar_wait(&sm.empty[b], (unsigned)(((s / LNB) - 1) & 1))) {
+          atomicOr(a.err, ERRBIT_TIMEOUT);
+          break;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        line_issue<DIR>(&thi, &tlo, &tcc, sm, b, g, prod.cur, prod.p);
+        prod.next(a, kblocks, nu, items);
+      }
+      // the last copies land before the CTA exits (bounded)
+      for (int s2 = s > LNB ? s - LNB : 0; s2 < s; ++s2)
+        mbar_wait(&sm.full[s2 % LNB], (unsigned)((s2 / LNB) & 1));
     }
+    return;
   }
+
+  const float fac = (float)(g.dsi[DIR] * a.sc->dt);
   int seq = 0;
-  float wm2[NW], wm1[NW], w0[NW], w1[NW], dq0[NW], F0[NW];
+  // limiter state on field pairs: W9 holds (ro, mx) (my, mz) (bx, by) (bz, ph)
+  // as packed pairs and ro*e alone
+  const float2 ep2 = vs<float2>(a.ep), fh2 = vs<float2>(a.fh), mfac2 = vs<float2>(-fac);
+  W9 wm2, wm1, w0, w1, dq0, F0;
   float ccm1 = 0.f, cc0 = 0.f, cc1 = 0.f;
   for (int it = blockIdx.x; it < items; it += gridDim.x) {
     const LineItem li = line_item<DIR>(a, it, kblocks, nu);
@@ -397,43 +422,43 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
     const bool active = k < nk;
     for (int p = li.t0 - 2; p <= li.t1 + 1; ++p, ++seq) {
       const int s = (int)(seq % LNB);
-      if (tid == 0 && !mbar_wait(&sm.bar[s], (unsigned)((seq / LNB) & 1))) sm.abort = 1;
-      __syncthreads();
-      if (sm.abort) {
-        if (tid == 0) {
-          atomicOr(a.err, ERRBIT_TIMEOUT);
-          for (int s2 = seq + 1; s2 < issued; ++s2)
-            mbar_wait(&sm.bar[s2 % LNB], (unsigned)((s2 / LNB) & 1));
-        }
+      if (!mbar_wait(&sm.full[s], (unsigned)((seq / LNB) & 1))) {
+        atomicOr(a.err, ERRBIT_TIMEOUT);
         return;
       }
       const float *shi = reinterpret_cast<const float *>(sm.slot[s] + L_HI);
       const float *scc = reinterpret_cast<const float *>(sm.slot[s] + L_CC);
-      float u[NF], wp[NW];
+      W9 wp;
+      {
+        float u[NF];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) u[f] = shi[f * LBOX + tid + 2];
-      limited_vars(u, wp);
+        for (int f = 0; f < NF; ++f) u[f] = shi[f * LBOX + tid + 2];
+        limited_w9(u, wp);
+      }
       const float ccp = scc[tid + 2];
       const int r = p - li.t0;  // -2 .. t1-t0+1
       if (r == -2) {
-#pragma unroll
-        for (int n = 0; n < NW; ++n) wm2[n] = wp[n];
+        wm2 = wp;
       } else if (r == -1) {
-#pragma unroll
-        for (int n = 0; n < NW; ++n) wm1[n] = wp[n];
+        wm1 = wp;
         ccm1 = ccp;
       } else if (r == 0) {
-#pragma unroll
-        for (int n = 0; n < NW; ++n) w0[n] = wp[n];
+        w0 = wp;
         cc0 = ccp;
       } else if (r == 1) {
+        w1 = wp;
+        // -1/2 of the face speed 0.5 (cc[t-1] + cc[t])
+        const float hcc = -0.25f * (ccm1 + cc0);
+        const float2 hcc2 = vs<float2>(hcc);
 #pragma unroll
-        for (int n = 0; n < NW; ++n) {
-          w1[n] = wp[n];
-          const float dqm = dqq_eval(wm2[n], wm1[n], w0[n], a.ep);
-          dq0[n] = dqq_eval(wm1[n], w0[n], w1[n], a.ep);
-          F0[n] = flux_core(wm1[n], w0[n], dqm, dq0[n], 0.5f * (ccm1 + cc0), a.fh);
+        for (int i = 0; i < 4; ++i) {
+          const float2 dqm = dqq_t(wm2.p[i], wm1.p[i], w0.p[i], ep2);
+          dq0.p[i] = dqq_t(wm1.p[i], w0.p[i], w1.p[i], ep2);
+          F0.p[i] = flux_t(wm1.p[i], w0.p[i], dqm, dq0.p[i], hcc2, fh2);
         }
+        const float dqm = dqq_t(wm2.s, wm1.s, w0.s, a.ep);
+        dq0.s = dqq_t(wm1.s, w0.s, w1.s, a.ep);
+        F0.s = flux_t(wm1.s, w0.s, dqm, dq0.s, hcc, a.fh);
         cc1 = ccp;
       } else {
         // centre cell t = p - 2; its plane sits two slots back
@@ -441,17 +466,26 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
         const int sc_ = (int)((seq - 2) % LNB);
         const float *chi = reinterpret_cast<const float *>(sm.slot[sc_] + L_HI);
         const float *clo = reinterpret_cast<const float *>(sm.slot[sc_] + L_LO);
-        float dF[NW];
+        const float hcc = -0.25f * (cc0 + cc1);
+        const float2 hcc2 = vs<float2>(hcc);
+        W9 dF;
 #pragma unroll
-        for (int n = 0; n < NW; ++n) {
-          const float dq1 = dqq_eval(w0[n], w1[n], wp[n], a.ep);
-          const float F1 = flux_core(w0[n], w1[n], dq0[n], dq1, 0.5f * (cc0 + cc1), a.fh);
-          dF[n] = F1 - F0[n];
-          F0[n] = F1;
-          dq0[n] = dq1;
-          w0[n] = w1[n];
-          w1[n] = wp[n];
+        for (int i = 0; i < 4; ++i) {
+          const float2 dq1 = dqq_t(w0.p[i], w1.p[i], wp.p[i], ep2);
+          const float2 F1 = flux_t(w0.p[i], w1.p[i], dq0.p[i], dq1, hcc2, fh2);
+          dF.p[i] = vsub(F1, F0.p[i]);
+          F0.p[i] = F1;
+          dq0.p[i] = dq1;
         }
+        {
+          const float dq1 = dqq_t(w0.s, w1.s, wp.s, a.ep);
+          const float F1 = flux_t(w0.s, w1.s, dq0.s, dq1, hcc, a.fh);
+          dF.s = vsub(F1, F0.s);
+          F0.s = F1;
+          dq0.s = dq1;
+        }
+        w0 = w1;
+        w1 = wp;
         cc0 = cc1;
         cc1 = ccp;
         if (active) {
@@ -459,31 +493,69 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
           const int x1 = DIR == 0 ? li.u : t;
           const int cell = cell_of(g, x0, x1, k);
 #pragma unroll
-          for (int n = 0; n < NW; ++n) {
-            const int f = field_of(n);
+          for (int i = 0; i < 4; ++i) {
+            const int f0 = field_of(2 * i), f1 = field_of(2 * i + 1);
+            const float2 h = make_float2(chi[f0 * LBOX + tid + 2], chi[f1 * LBOX + tid + 2]);
+            const float2 l = make_float2(clo[f0 * LBOX + tid + 2], clo[f1 * LBOX + tid + 2]);
+            float2 sv, e;
+            two_sum(h, vfma(dF.p[i], mfac2, l), sv, e);
+            // interior only: the shell kernel fills the images
+            a.hi2.f[f0][cell] = sv.x;
+            a.hi2.f[f1][cell] = sv.y;
+            a.lo2.f[f0][cell] = e.x;
+            a.lo2.f[f1][cell] = e.y;
+          }
+          {
             float sv, e;
-            two_sum(chi[f * LBOX + tid + 2], clo[f * LBOX + tid + 2] - dF[n] * fac, sv, e);
-            a.hi2.f[f][cell] = sv;  // interior only: the shell kernel fills the images
-            a.lo2.f[f][cell] = e;
+            two_sum(chi[ET * LBOX + tid + 2], vfma(dF.s, -fac, clo[ET * LBOX + tid + 2]), sv, e);
+            a.hi2.f[ET][cell] = sv;
+            a.lo2.f[ET][cell] = e;
           }
         }
       }
-      __syncthreads();  // every thread is done with the slot of plane p-2
-      if (tid == 0 && seq >= 2 && prod.valid(items)) {
-        const int fs = (int)((seq - 2) % LNB);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        line_issue<DIR>(&thi, &tlo, &tcc, sm, fs, g, prod.cur, prod.p);
-        prod.next(a, kblocks, nu, items);
-        ++issued;
+      // release the slots this warp is done with: plane p-2 (read for the
+      // cell just finished, or a leading halo plane), and at the item's last
+      // plane the two trailing halo planes
+      __syncwarp();
+      if (lane == 0) {
+        if (r >= 0) mbar_arrive(&sm.empty[(seq - 2) % LNB]);
+        if (p == li.t1 + 1) {
+          mbar_arrive(&sm.empty[(seq - 1) % LNB]);
+          mbar_arrive(&sm.empty[seq % LNB]);
+        }
       }
     }
   }
 }
 
 // ---- z sweep (contiguous axis) ----
-// Each warp loads 32 consecutive cells of a row and updates the inner 28;
-// neighbours come from warp shuffles.  The CFL candidate of the new state
-// is folded into a per-block minimum.
+// Each warp loads 32 consecutive cells of a row (hi and lo words and the
+// characteristic speed, all at once) and updates the inner 28; neighbours
+// come from warp shuffles, the limiter runs on packed field pairs.  (Loading
+// the next segment before working on the current one measured 1.2x slower:
+// the registers it holds cut the warps in flight.)  The CFL candidate of the
+// new state is folded into a per-block minimum.
+struct ZSeg {
+  float u[NF], l[NF], cc;
+};
+
+__device__ __forceinline__ void z_load(const AvArgs &a, int wi, int segs, int lane, ZSeg &z,
+                                       int &c, int &k) {
+  const Geom &g = a.g;
+  const int sg = wi % segs;
+  const int row = wi / segs;
+  const int j = row % g.n[1];
+  const int i = row / g.n[1];
+  k = sg * 28 + lane - 2;               // interior k of this lane
+  const int kc = min(k, g.n[2] + 1);  // stay inside the array (ghosts reach nk+1)
+  c = cell_of(g, i, j, kc);
+#pragma unroll
+  for (int f = 0; f < NF; ++f) z.u[f] = __ldg(a.hi.f[f] + c);
+#pragma unroll
+  for (int f = 0; f < NF; ++f) z.l[f] = __ldg(a.lo.f[f] + c);
+  z.cc = __ldg(a.cc + c);
+}
+
 __global__ void __launch_bounds__(128)
 av_z_kernel(const AvArgs a) {
   const Geom &g = a.g;
@@ -493,43 +565,63 @@ av_z_kernel(const AvArgs a) {
   const int rows = g.n[0] * g.n[1];
   const int work = rows * segs;
   const float fac = (float)(g.dsi[2] * a.sc->dt);
+  const float2 ep2 = vs<float2>(a.ep), fh2 = vs<float2>(a.fh), mfac2 = vs<float2>(-fac);
   const int warps = gridDim.x * (blockDim.x >> 5);
   float best = 1.e10f;
   bool bad = false;
   for (int wi = blockIdx.x * (blockDim.x >> 5) + wid; wi < work; wi += warps) {
-    const int sg = wi % segs;
-    const int row = wi / segs;
-    const int j = row % g.n[1];
-    const int i = row / g.n[1];
-    const int k = sg * 28 + lane - 2;  // interior k of this lane
-    const int kc = min(k, nk + 1);     // stay inside the array (ghosts reach nk+1)
-    const int c = cell_of(g, i, j, kc);
-    float u[NF], w[NW];
+    ZSeg cur;
+    int c, k;
+    z_load(a, wi, segs, lane, cur, c, k);
+    W9 w;
+    limited_w9(cur.u, w);
+    const float cc_up = __shfl_down_sync(0xffffffffu, cur.cc, 1);
+    const float hcc = -0.25f * (cur.cc + cc_up);  // -1/2 of the face speed
+    const float2 hcc2 = vs<float2>(hcc);
+    W9 dF;
 #pragma unroll
-    for (int f = 0; f < NF; ++f) u[f] = __ldg(a.hi.f[f] + c);
-    limited_vars(u, w);
-    const float cc = __ldg(a.cc + c);
-    const float cc_up = __shfl_down_sync(0xffffffffu, cc, 1);
-    float dF[NW];
-#pragma unroll
-    for (int n = 0; n < NW; ++n) {
-      const float wm = __shfl_up_sync(0xffffffffu, w[n], 1);
-      const float wp = __shfl_down_sync(0xffffffffu, w[n], 1);
-      const float dq = dqq_eval(wm, w[n], wp, a.ep);
+    for (int n = 0; n < 4; ++n) {
+      const float2 wm = make_float2(__shfl_up_sync(0xffffffffu, w.p[n].x, 1),
+                                    __shfl_up_sync(0xffffffffu, w.p[n].y, 1));
+      const float2 wp = make_float2(__shfl_down_sync(0xffffffffu, w.p[n].x, 1),
+                                    __shfl_down_sync(0xffffffffu, w.p[n].y, 1));
+      const float2 dq = dqq_t(wm, w.p[n], wp, ep2);
+      const float2 dq_up = make_float2(__shfl_down_sync(0xffffffffu, dq.x, 1),
+                                       __shfl_down_sync(0xffffffffu, dq.y, 1));
+      const float2 Fup = flux_t(w.p[n], wp, dq, dq_up, hcc2, fh2);
+      const float2 Fdw = make_float2(__shfl_up_sync(0xffffffffu, Fup.x, 1),
+                                     __shfl_up_sync(0xffffffffu, Fup.y, 1));
+      dF.p[n] = vsub(Fup, Fdw);
+    }
+    {
+      const float wm = __shfl_up_sync(0xffffffffu, w.s, 1);
+      const float wp = __shfl_down_sync(0xffffffffu, w.s, 1);
+      const float dq = dqq_t(wm, w.s, wp, a.ep);
       const float dq_up = __shfl_down_sync(0xffffffffu, dq, 1);
-      const float Fup = flux_core(w[n], wp, dq, dq_up, 0.5f * (cc + cc_up), a.fh);
+      const float Fup = flux_t(w.s, wp, dq, dq_up, hcc, a.fh);
       const float Fdw = __shfl_up_sync(0xffffffffu, Fup, 1);
-      dF[n] = Fup - Fdw;
+      dF.s = vsub(Fup, Fdw);
     }
     if (lane >= 2 && lane < 30 && k < nk) {
       float s[NF];
 #pragma unroll
-      for (int n = 0; n < NW; ++n) {
-        const int f = field_of(n);
+      for (int n = 0; n < 4; ++n) {
+        const int f0 = field_of(2 * n), f1 = field_of(2 * n + 1);
+        float2 sv, e;
+        two_sum(make_float2(cur.u[f0], cur.u[f1]),
+                vfma(dF.p[n], mfac2, make_float2(cur.l[f0], cur.l[f1])), sv, e);
+        s[f0] = sv.x;
+        s[f1] = sv.y;
+        a.hi2.f[f0][c] = sv.x;  // interior only: the shell kernel fills the images
+        a.hi2.f[f1][c] = sv.y;
+        a.lo2.f[f0][c] = e.x;
+        a.lo2.f[f1][c] = e.y;
+      }
+      {
         float e;
-        two_sum(u[f], __ldg(a.lo.f[f] + c) - dF[n] * fac, s[f], e);
-        a.hi2.f[f][c] = s[f];  // interior only: the shell kernel fills the images
-        a.lo2.f[f][c] = e;
+        two_sum(cur.u[ET], vfma(dF.s, -fac, cur.l[ET]), s[ET], e);
+        a.hi2.f[ET][c] = s[ET];
+        a.lo2.f[ET][c] = e;
       }
       if (a.partial) {
         // CFL candidate of the new state (mhd_integrator_host.hpp:303-334)
@@ -662,9 +754,9 @@ void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc,
   const CUtensorMap &c = *(const CUtensorMap *)tm_cc;
   const size_t smem = sizeof(s32t::LineSmem);
   if (dir == 0)
-    s32t::av_line_kernel<0><<<grid, s32t::LK, smem, st>>>(h, l, c, a);
+    s32t::av_line_kernel<0><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, a);
   else
-    s32t::av_line_kernel<1><<<grid, s32t::LK, smem, st>>>(h, l, c, a);
+    s32t::av_line_kernel<1><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, a);
 }
 
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st) {

@@ -41,8 +41,10 @@ struct AvArgs {
 struct ShellArgs {
   float *p[2 * NF + 1];
   int f[2 * NF + 1];
+  unsigned m[2 * NF + 1];  // per array: images to write, bit (m-1) for image mask m
+                           // (1 = i, 2 = j, 4 = k, sums = edges and corners)
   int n;
-  unsigned imask;  // images to write: bit (m-1) for image mask m (1 = i, 2 = j, 4 = k, sums = edges/corners)
+  int slab;  // >= 0: every mask lies on the faces of this axis (enumerate its slabs only)
 };
 // image masks: the faces of one axis set (no edges or corners), or everything
 constexpr unsigned SHELL_FACES_I = 1u << 0, SHELL_FACES_J = 1u << 1, SHELL_FACES_K = 1u << 3;
@@ -50,6 +52,7 @@ constexpr unsigned SHELL_FACES = SHELL_FACES_I | SHELL_FACES_J | SHELL_FACES_K;
 constexpr unsigned SHELL_ALL = 0x7fu;
 void launch_s32_shell(const Geom &g, const ShellArgs &a, int grid, cudaStream_t st);
 long long s32_shell_cells(const Geom &g);  // interior cells within the margin of a face
+long long s32_shell_count(const Geom &g, int slab);  // cells a shell launch visits
 
 bool s32_tiled_supported(const Geom &g);
 // 4-D tensor maps (k, j, i, field) over 9 arrays at `pitch_bytes`:
@@ -69,10 +72,8 @@ void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cu
 void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
                         int dir, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);
-// x / y sweep streamed with full/empty mbarriers and no CTA barrier
-// (s32_av.cu); same tensor maps as the line kernel
-int s32_av_pipe_configure();
-void launch_s32_av_pipe(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
-                        int dir, int grid, cudaStream_t st);
+// x / y sweep, one warp per 32-cell line segment marching along the sweep
+// axis (s32_av.cu): no shared memory, no CTA barrier; interior-only writes
+void launch_s32_av_march(const AvArgs &a, int dir, int grid, cudaStream_t st);
 
 }  // namespace miso_b200

@@ -22,6 +22,9 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned
                "r"(bytes)
                : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 // Bounded wait for phase `parity`; false on timeout.
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
   const unsigned a = smem_u32(bar);

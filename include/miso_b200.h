@@ -137,13 +137,12 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
 
 /* Kernel variant of one kernel class on the 3-D FP32-split path:
  * kernel_class 0 = Runge-Kutta stage, 1/2/3 = viscosity sweep x/y/z;
- * variant 0 = tiled (TMA plane tiles / streaming lines / warp-shuffle rows),
- * 1 = flat (one thread per cell), 2 = pipelined (Runge-Kutta stage: TMA
- * planes with packed FP32x2 differences, the default; x / y sweeps: one
- * warp per line segment marching along the sweep axis; none for z).  All
- * compute the
- * same step; the autotuner (miso_b200/autotune.py) times them and keeps the
- * fastest.
+ * variant 0 = tiled (TMA plane tiles / streaming lines fed by a producer
+ * warp / warp-shuffle rows), 1 = flat (one thread per cell), 2 = pipelined
+ * (Runge-Kutta stage: TMA planes with packed FP32x2 differences, the
+ * default; x / y sweeps: one warp per line segment marching along the sweep
+ * axis; none for z).  All compute the same step; the autotuner
+ * (miso_b200/autotune.py) times them and keeps the fastest.
  * ERR_STATE on grids that use the simple per-cell kernels only. */
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant);
 int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant);

@@ -191,5 +191,56 @@ __device__ __forceinline__ void limited_w9(const float u[NF], W9 &w) {
   w.s = t[8];
 }
 
+// Flux difference F(k+1/2) - F(k-1/2) of the z sweep for the cells of a
+// warp that holds 32 consecutive cells of a row, one per lane (hi words u
+// and characteristic speed cc of the lane's cell); neighbours come from
+// warp shuffles, so lanes 2..29 get a complete difference.
+__device__ __forceinline__ void z_flux_diff(const float u[NF], float cc, float ep, float fh,
+                                            W9 &dF) {
+  W9 w;
+  limited_w9(u, w);
+  const float cc_up = __shfl_down_sync(0xffffffffu, cc, 1);
+  const float hcc = -0.25f * (cc + cc_up);  // -1/2 of the face speed
+  const float2 hcc2 = vs<float2>(hcc), ep2 = vs<float2>(ep), fh2 = vs<float2>(fh);
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    const float2 wm = make_float2(__shfl_up_sync(0xffffffffu, w.p[n].x, 1),
+                                  __shfl_up_sync(0xffffffffu, w.p[n].y, 1));
+    const float2 wp = make_float2(__shfl_down_sync(0xffffffffu, w.p[n].x, 1),
+                                  __shfl_down_sync(0xffffffffu, w.p[n].y, 1));
+    const float2 dq = dqq_t(wm, w.p[n], wp, ep2);
+    const float2 dq_up = make_float2(__shfl_down_sync(0xffffffffu, dq.x, 1),
+                                     __shfl_down_sync(0xffffffffu, dq.y, 1));
+    const float2 Fup = flux_t(w.p[n], wp, dq, dq_up, hcc2, fh2);
+    const float2 Fdw = make_float2(__shfl_up_sync(0xffffffffu, Fup.x, 1),
+                                   __shfl_up_sync(0xffffffffu, Fup.y, 1));
+    dF.p[n] = vsub(Fup, Fdw);
+  }
+  const float wm = __shfl_up_sync(0xffffffffu, w.s, 1);
+  const float wp = __shfl_down_sync(0xffffffffu, w.s, 1);
+  const float dq = dqq_t(wm, w.s, wp, ep);
+  const float dq_up = __shfl_down_sync(0xffffffffu, dq, 1);
+  const float Fup = flux_t(w.s, wp, dq, dq_up, hcc, fh);
+  const float Fdw = __shfl_up_sync(0xffffffffu, Fup, 1);
+  dF.s = vsub(Fup, Fdw);
+}
+
+// (hi, lo) - fac * dF as compensated pairs into s (hi words) and e (lo words)
+__device__ __forceinline__ void av_update(const float u[NF], const float l[NF], const W9 &dF,
+                                          float fac, float s[NF], float e[NF]) {
+  const float2 mfac2 = vs<float2>(-fac);
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    const int f0 = field_of(2 * n), f1 = field_of(2 * n + 1);
+    float2 sv, ev;
+    two_sum(make_float2(u[f0], u[f1]), vfma(dF.p[n], mfac2, make_float2(l[f0], l[f1])), sv, ev);
+    s[f0] = sv.x;
+    s[f1] = sv.y;
+    e[f0] = ev.x;
+    e[f1] = ev.y;
+  }
+  two_sum(u[ET], vfma(dF.s, -fac, l[ET]), s[ET], e[ET]);
+}
+
 }  // namespace s32t
 }  // namespace miso_b200

@@ -533,8 +533,10 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
 // characteristic speed, all at once) and updates the inner 28; neighbours
 // come from warp shuffles, the limiter runs on packed field pairs.  (Loading
 // the next segment before working on the current one measured 1.2x slower:
-// the registers it holds cut the warps in flight.)  The CFL candidate of the
-// new state is folded into a per-block minimum.
+// the registers it holds cut the warps in flight.  Staging the segments in
+// shared memory by TMA, a slot ring per warp, measured 2x slower: copies of
+// 128-byte boxes keep the TMA unit busy for little data.)  The CFL candidate
+// of the new state is folded into a per-block minimum.
 struct ZSeg {
   float u[NF], l[NF], cc;
 };
@@ -565,7 +567,6 @@ av_z_kernel(const AvArgs a) {
   const int rows = g.n[0] * g.n[1];
   const int work = rows * segs;
   const float fac = (float)(g.dsi[2] * a.sc->dt);
-  const float2 ep2 = vs<float2>(a.ep), fh2 = vs<float2>(a.fh), mfac2 = vs<float2>(-fac);
   const int warps = gridDim.x * (blockDim.x >> 5);
   float best = 1.e10f;
   bool bad = false;
@@ -573,55 +574,15 @@ av_z_kernel(const AvArgs a) {
     ZSeg cur;
     int c, k;
     z_load(a, wi, segs, lane, cur, c, k);
-    W9 w;
-    limited_w9(cur.u, w);
-    const float cc_up = __shfl_down_sync(0xffffffffu, cur.cc, 1);
-    const float hcc = -0.25f * (cur.cc + cc_up);  // -1/2 of the face speed
-    const float2 hcc2 = vs<float2>(hcc);
     W9 dF;
-#pragma unroll
-    for (int n = 0; n < 4; ++n) {
-      const float2 wm = make_float2(__shfl_up_sync(0xffffffffu, w.p[n].x, 1),
-                                    __shfl_up_sync(0xffffffffu, w.p[n].y, 1));
-      const float2 wp = make_float2(__shfl_down_sync(0xffffffffu, w.p[n].x, 1),
-                                    __shfl_down_sync(0xffffffffu, w.p[n].y, 1));
-      const float2 dq = dqq_t(wm, w.p[n], wp, ep2);
-      const float2 dq_up = make_float2(__shfl_down_sync(0xffffffffu, dq.x, 1),
-                                       __shfl_down_sync(0xffffffffu, dq.y, 1));
-      const float2 Fup = flux_t(w.p[n], wp, dq, dq_up, hcc2, fh2);
-      const float2 Fdw = make_float2(__shfl_up_sync(0xffffffffu, Fup.x, 1),
-                                     __shfl_up_sync(0xffffffffu, Fup.y, 1));
-      dF.p[n] = vsub(Fup, Fdw);
-    }
-    {
-      const float wm = __shfl_up_sync(0xffffffffu, w.s, 1);
-      const float wp = __shfl_down_sync(0xffffffffu, w.s, 1);
-      const float dq = dqq_t(wm, w.s, wp, a.ep);
-      const float dq_up = __shfl_down_sync(0xffffffffu, dq, 1);
-      const float Fup = flux_t(w.s, wp, dq, dq_up, hcc, a.fh);
-      const float Fdw = __shfl_up_sync(0xffffffffu, Fup, 1);
-      dF.s = vsub(Fup, Fdw);
-    }
+    z_flux_diff(cur.u, cur.cc, a.ep, a.fh, dF);
     if (lane >= 2 && lane < 30 && k < nk) {
-      float s[NF];
+      float s[NF], e[NF];
+      av_update(cur.u, cur.l, dF, fac, s, e);
 #pragma unroll
-      for (int n = 0; n < 4; ++n) {
-        const int f0 = field_of(2 * n), f1 = field_of(2 * n + 1);
-        float2 sv, e;
-        two_sum(make_float2(cur.u[f0], cur.u[f1]),
-                vfma(dF.p[n], mfac2, make_float2(cur.l[f0], cur.l[f1])), sv, e);
-        s[f0] = sv.x;
-        s[f1] = sv.y;
-        a.hi2.f[f0][c] = sv.x;  // interior only: the shell kernel fills the images
-        a.hi2.f[f1][c] = sv.y;
-        a.lo2.f[f0][c] = e.x;
-        a.lo2.f[f1][c] = e.y;
-      }
-      {
-        float e;
-        two_sum(cur.u[ET], vfma(dF.s, -fac, cur.l[ET]), s[ET], e);
-        a.hi2.f[ET][c] = s[ET];
-        a.lo2.f[ET][c] = e;
+      for (int f = 0; f < NF; ++f) {
+        a.hi2.f[f][c] = s[f];  // interior only: the shell kernel fills the images
+        a.lo2.f[f][c] = e[f];
       }
       if (a.partial) {
         // CFL candidate of the new state (mhd_integrator_host.hpp:303-334)

@@ -514,8 +514,9 @@ struct miso_b200_handle {
         if (st < 3) {
           // the next stage's star stencil reads face ghosts only
           if ((rc = shell(stg[st & 1], SHELL_FACES))) return rc;
-        } else {
-          // the x sweep reads hi across the i faces; every sweep reads cc
+        } else if (av_var[0] == 1 || av_var[1] == 1 || av_var[2] == 1) {
+          // a flat sweep reads hi across the i faces and cc across its own
+          // faces (the line, march and z sweeps read the imaged interior)
           if ((rc = shell(hi[c], SHELL_FACES_I, cc32, SHELL_FACES))) return rc;
         }
       }
@@ -548,13 +549,15 @@ struct miso_b200_handle {
         launch_s32_av_z(a, z_grid, stream);
       te(t, d == 0 ? "av_x" : d == 1 ? "av_y" : "av_z", interior() * 148.0);
       if ((rc = check_launch("av_sweep"))) return rc;
-      // interior-only writers (line and z sweeps): the hi images are read by
-      // the next pass; lo images only by a download (see lo_shell_stale)
-      if (av_var[d] == 0 || (av_var[d] == 2 && d < 2)) {
-        // the y sweep reads j-face ghosts, the z sweep k-face ghosts; after
-        // the z sweep the step's final state gets every image
-        const unsigned m = d == 0 ? SHELL_FACES_J : d == 1 ? SHELL_FACES_K : SHELL_ALL;
-        if ((rc = shell(hi[cur ^ 1], m))) return rc;
+      // interior-only writers (line, march and z sweeps): the step's final
+      // state gets every hi image; within the step only a flat sweep reads
+      // ghosts (the others read the imaged interior across a face); lo
+      // images are read by a download only (see lo_shell_stale)
+      if (av_var[d] != 1) {
+        if (d == 2 || av_var[d + 1] == 1) {
+          const unsigned m = d == 0 ? SHELL_FACES_J : d == 1 ? SHELL_FACES_K : SHELL_ALL;
+          if ((rc = shell(hi[cur ^ 1], m))) return rc;
+        }
         lo_shell_stale = true;
       } else {
         lo_shell_stale = false;

@@ -75,6 +75,26 @@ __device__ __forceinline__ void store_cell(T *p, long long cell, bool nb, const 
     p[cell] = v;
 }
 
+// Interior coordinate whose value the coordinate t of axis a holds, for t
+// in [-m, n + m): t itself inside, else the periodic wrap or the mirror
+// (the inverse of the image map above).  side = 0 / 1 on the low / high
+// ghost layer (the mirror sign of the value is g.negmask[a][side]), -1
+// inside.  Lets a pass read a neighbour across a face without the ghost
+// layer being filled.
+__device__ __forceinline__ int ghost_src(const Geom &g, int a, int t, int &side) {
+  const int n = g.n[a];
+  if (t < 0) {
+    side = 0;
+    return g.periodic[a] ? t + n : -1 - t;
+  }
+  if (t >= n) {
+    side = 1;
+    return g.periodic[a] ? t - n : 2 * n - 1 - t;
+  }
+  side = -1;
+  return t;
+}
+
 __device__ __forceinline__ int cell_of(const Geom &g, int x0, int x1, int x2) {
   return (x0 + g.m[0]) * (int)g.st[0] + (x1 + g.m[1]) * (int)g.st[1] + (x2 + g.m[2]);
 }

@@ -52,10 +52,19 @@ av_march_kernel(const AvArgs a) {
     const int x0b = DIR == 0 ? 0 : u, x1b = DIR == 0 ? u : 0;
     const int cell0 = cell_of(g, x0b, x1b, kc);  // t = 0
     auto load_w = [&](int t, float wv[NW], float &ccv) {
-      const int cell = cell0 + t * S;
+      // a plane across a face: the interior plane it images, with the
+      // mirror signs of that face
+      int side;
+      const int cell = cell0 + ghost_src(g, DIR, t, side) * S;
       float uu[NF];
 #pragma unroll
       for (int f = 0; f < NF; ++f) uu[f] = __ldg(a.hi.f[f] + cell);
+      if (side >= 0) {
+        const unsigned neg = g.negmask[DIR][side];
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+          if ((neg >> f) & 1u) uu[f] = -uu[f];
+      }
       limited_vars(uu, wv);
       ccv = __ldg(a.cc + cell);
     };

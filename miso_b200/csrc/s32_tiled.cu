@@ -354,8 +354,11 @@ __device__ __forceinline__ void line_issue(const CUtensorMap *thi, const CUtenso
                                            const Geom &g, const LineItem &it, int p) {
   unsigned char *sl = sm.slot[s];
   const int k0 = it.kb * LK;
-  const int cj = DIR == 0 ? it.u + g.m[1] : p + g.m[1];
-  const int ci = DIR == 0 ? p + g.m[0] : it.u + g.m[0];
+  // a plane across a face comes from the interior plane it images
+  int side;
+  const int ps = ghost_src(g, DIR, p, side);
+  const int cj = DIR == 0 ? it.u + g.m[1] : ps + g.m[1];
+  const int ci = DIR == 0 ? ps + g.m[0] : it.u + g.m[0];
   mbar_expect_tx(&sm.full[s], L_TX);
   tma4(thi, sl + L_HI, &sm.full[s], k0, cj, ci, 0);
   tma4(tlo, sl + L_LO, &sm.full[s], k0, cj, ci, 0);
@@ -433,6 +436,14 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
         float u[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) u[f] = shi[f * LBOX + tid + 2];
+        if (p < 0 || p >= g.n[DIR]) {
+          // the plane was copied from the interior plane it images: apply
+          // the mirror signs of that face (none on a periodic axis)
+          const unsigned neg = g.negmask[DIR][p < 0 ? 0 : 1];
+#pragma unroll
+          for (int f = 0; f < NF; ++f)
+            if ((neg >> f) & 1u) u[f] = -u[f];
+        }
         limited_w9(u, wp);
       }
       const float ccp = scc[tid + 2];
@@ -529,14 +540,18 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
 }
 
 // ---- z sweep (contiguous axis) ----
-// Each warp loads 32 consecutive cells of a row (hi and lo words and the
-// characteristic speed, all at once) and updates the inner 28; neighbours
-// come from warp shuffles, the limiter runs on packed field pairs.  (Loading
-// the next segment before working on the current one measured 1.2x slower:
-// the registers it holds cut the warps in flight.  Staging the segments in
-// shared memory by TMA, a slot ring per warp, measured 2x slower: copies of
-// 128-byte boxes keep the TMA unit busy for little data.)  The CFL candidate
-// of the new state is folded into a per-block minimum.
+// Each warp loads 32 consecutive cells of a row (hi words and the
+// characteristic speed; lanes across a face read the interior cell they
+// image) and updates the inner 28, loading their lo words for the update;
+// neighbours come from warp shuffles, the limiter runs on packed field
+// pairs.  The kernel is latency-bound and lives on warps in flight: 56
+// registers give nine 128-thread CTAs per SM, and every variant that held
+// more registers measured slower (the next segment's loads issued early:
+// 1.2x; lo loaded with hi: 1.3x; a register cap with spills: 2.3x).
+// Staging the segments in shared memory by TMA, a slot ring per warp,
+// measured 2x slower: copies of 128-byte boxes keep the TMA unit busy for
+// little data.  The CFL candidate of the new state is folded into a
+// per-block minimum.
 struct ZSeg {
   float u[NF], l[NF], cc;
 };
@@ -548,13 +563,20 @@ __device__ __forceinline__ void z_load(const AvArgs &a, int wi, int segs, int la
   const int row = wi / segs;
   const int j = row % g.n[1];
   const int i = row / g.n[1];
-  k = sg * 28 + lane - 2;               // interior k of this lane
-  const int kc = min(k, g.n[2] + 1);  // stay inside the array (ghosts reach nk+1)
-  c = cell_of(g, i, j, kc);
+  k = sg * 28 + lane - 2;  // interior k of this lane
+  // a lane across a face reads the interior cell it images (lanes past the
+  // ghost layer, whose values no output uses, stay on its last cell)
+  int side;
+  const int ks = ghost_src(g, 2, min(k, g.n[2] + 1), side);
+  c = cell_of(g, i, j, ks);
 #pragma unroll
   for (int f = 0; f < NF; ++f) z.u[f] = __ldg(a.hi.f[f] + c);
+  if (side >= 0) {
+    const unsigned neg = g.negmask[2][side];
 #pragma unroll
-  for (int f = 0; f < NF; ++f) z.l[f] = __ldg(a.lo.f[f] + c);
+    for (int f = 0; f < NF; ++f)
+      if ((neg >> f) & 1u) z.u[f] = -z.u[f];
+  }
   z.cc = __ldg(a.cc + c);
 }
 
@@ -578,6 +600,8 @@ av_z_kernel(const AvArgs a) {
     z_flux_diff(cur.u, cur.cc, a.ep, a.fh, dF);
     if (lane >= 2 && lane < 30 && k < nk) {
       float s[NF], e[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) cur.l[f] = __ldg(a.lo.f[f] + c);
       av_update(cur.u, cur.l, dF, fac, s, e);
 #pragma unroll
       for (int f = 0; f < NF; ++f) {

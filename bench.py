@@ -158,7 +158,10 @@ def cpu_reference(n: int, steps: int, warm: int, procs: int):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
-def dist_init():
+def dist_init(backend: str = "nccl", timeout_s: float = 300.0):
+    """Rank, world size and local rank from the torchrun environment; joins
+    the process group when there is more than one rank (NCCL on the GPU
+    box; the multi-rank host logic is tested with gloo on CPU)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -166,16 +169,18 @@ def dist_init():
         import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return rank, world, local
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """The maximum of a per-rank time over all ranks (every rank gets it)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -29,6 +29,7 @@ extern "C" {
 #define MISO_B200_ERR_STATE (-4)    /* call not valid in the handle's current state */
 #define MISO_B200_ERR_NOMEM (-5)    /* device allocation failed */
 #define MISO_B200_ERR_TIMEOUT (-6)  /* a bounded device-side wait (TMA copy) ran out */
+#define MISO_B200_ERR_HALO (-7)     /* the halo exchange callback reported an error */
 
 #define MISO_B200_FP64 0        /* primitive FP64 state, bit-faithful to the reference */
 #define MISO_B200_FP32_SPLIT 1  /* conserved FP32 hi/lo state, FP32 RHS and viscosity */
@@ -134,6 +135,45 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]);
  * the reference's FieldsView for custom boundary work
  * (miso/include/miso/mhd_fields.hpp:17-34). */
 int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
+
+/* Halo exchange of a grid decomposed into shards along i (the slowest
+ * axis).  Replaces the reference's HaloExchanger for the neighbour faces of
+ * a Cartesian decomposition (miso/include/miso/mhd_halo_exchange.hpp:
+ * 451-621) and the MPI_Allreduce of dt in Integrator::cfl
+ * (miso/include/miso/mhd_integrator_cuda.cuh:476).  A face's ghost layer
+ * along i is `margin` whole planes of each array, contiguous in memory, so
+ * nothing is packed: the callback moves `bytes` contiguous bytes per array
+ * and face.
+ *
+ * exchange: called on the host whenever a pass has written arrays whose i
+ *   ghosts the next pass reads.  It must make `stream` (the handle's
+ *   cudaStream_t) wait until, for every array a and every face marked
+ *   external, send_lo[a] has reached the low neighbour's recv_hi[a] and the
+ *   low neighbour's send_hi[a] has reached recv_lo[a] (high face alike:
+ *   send_hi[a] -> high neighbour's recv_lo[a], its send_lo[a] ->
+ *   recv_hi[a]).  Typically: a group of ncclSend/ncclRecv on `stream`, or
+ *   cudaMemcpyAsync between shards of one process.  Nonzero return =
+ *   MISO_B200_ERR_HALO.  Arrays are double (FP64) or float (FP32 split).
+ * min_all: minimum of *value over all shards, written back (host value);
+ *   NULL = this shard alone.  miso_b200_cfl() returns the global dt with it.
+ *
+ * ext_lo / ext_hi mark the low / high i face as shared with a neighbour
+ * (its ghosts come from the exchange, never from a periodic or mirror
+ * image); a face not marked keeps the grid descriptor's boundary.  With
+ * ops == NULL the handle returns to a single grid.  While halo exchange is
+ * on, steps are taken with miso_b200_cfl + miso_b200_update (host dt, the
+ * reference's own sequence); miso_b200_run and miso_b200_update_device
+ * return MISO_B200_ERR_STATE.  miso_b200_monitors covers this shard only. */
+typedef struct miso_b200_halo_ops {
+  int (*exchange)(void *user, int narrays, size_t bytes, int ext_lo, int ext_hi,
+                  void *const *send_lo, void *const *send_hi, void *const *recv_lo,
+                  void *const *recv_hi, void *stream);
+  int (*min_all)(void *user, double *value);
+  void *user;
+} miso_b200_halo_ops;
+
+int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
+                       const miso_b200_halo_ops *ops);
 
 /* Kernel variant of one kernel class on the 3-D FP32-split path:
  * kernel_class 0 = Runge-Kutta stage, 1/2/3 = viscosity sweep x/y/z;

@@ -19,6 +19,7 @@ ERR_NONFINITE = -3
 ERR_STATE = -4
 ERR_NOMEM = -5
 ERR_TIMEOUT = -6
+ERR_HALO = -7
 
 FP64 = 0
 FP32_SPLIT = 1
@@ -43,6 +44,20 @@ class Params(ctypes.Structure):
                 ("vv_fac", ctypes.c_double), ("precision", ctypes.c_int)]
 
 
+_vpp = ctypes.POINTER(ctypes.c_void_p)
+# int exchange(user, narrays, bytes, ext_lo, ext_hi, send_lo, send_hi, recv_lo, recv_hi, stream)
+HALO_EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t,
+                                    ctypes.c_int, ctypes.c_int, _vpp, _vpp, _vpp, _vpp,
+                                    ctypes.c_void_p)
+# int min_all(user, double *value)
+HALO_MIN_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, _dp)
+
+
+class HaloOps(ctypes.Structure):
+    _fields_ = [("exchange", HALO_EXCHANGE_FN), ("min_all", HALO_MIN_FN),
+                ("user", ctypes.c_void_p)]
+
+
 # name -> (restype, argtypes); the exported set must match include/miso_b200.h
 SIGNATURES = {
     "miso_b200_create": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(Params),
@@ -64,6 +79,8 @@ SIGNATURES = {
     "miso_b200_device_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
     "miso_b200_launch_count": (ctypes.c_int, [ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_longlong)]),
+    "miso_b200_set_halo": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(HaloOps)]),
     "miso_b200_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_get_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,

@@ -150,6 +150,9 @@ struct miso_b200_handle {
 
   // tiled FP32-split path (3-D grids)
   bool tiled = false;
+  // halo exchange with neighbouring shards along i (miso_b200_set_halo)
+  miso_b200_halo_ops halo_ops{};
+  bool halo_on = false;
   alignas(64) unsigned char tm_hi[2][128];   // RK plane-tile maps of hi[set] (4-D: k, j, i, field)
   alignas(64) unsigned char tm_stg[2][128];  // RK plane-tile maps of stg[set]
   alignas(64) unsigned char tm_avh[2][128];  // AV line maps of hi[set]
@@ -331,7 +334,46 @@ struct miso_b200_handle {
     return check_launch("fill_ghosts");
   }
 
-  int fill_state() { return split() ? fill_split(cur) : fill64(0); }
+  int fill_state() {
+    int rc = split() ? fill_split(cur) : fill64(0);
+    if (rc) return rc;
+    return split() ? halo_f(hi[cur], lo[cur]) : halo_d(q64[0]);
+  }
+
+  // Exchange of the i ghost planes of `n` arrays (element size `elem`) with
+  // the neighbouring shards, through the caller's callback; a no-op for a
+  // single grid.
+  int halo_exchange(void *const *arr, int n, size_t elem) {
+    if (!halo_on) return MISO_B200_OK;
+    const long long plane = (long long)g.t[1] * g.t[2];
+    const int m = g.m[0], ni = g.n[0];
+    void *slo[2 * NF + 1], *shi[2 * NF + 1], *rlo[2 * NF + 1], *rhi[2 * NF + 1];
+    for (int a = 0; a < n; ++a) {
+      char *b = (char *)arr[a];
+      slo[a] = b + (size_t)m * plane * elem;           // interior planes 0 .. m-1
+      shi[a] = b + (size_t)ni * plane * elem;          // interior planes n-m .. n-1
+      rlo[a] = b;                                       // low ghost planes
+      rhi[a] = b + (size_t)(ni + m) * plane * elem;    // high ghost planes
+    }
+    const int r = halo_ops.exchange(halo_ops.user, n, (size_t)m * plane * elem, g.ext[0][0],
+                                    g.ext[0][1], slo, shi, rlo, rhi, (void *)stream);
+    if (r) return fail(MISO_B200_ERR_HALO, "halo exchange callback returned %d", r);
+    return MISO_B200_OK;
+  }
+  int halo_d(double *const *set) {
+    void *arr[NF];
+    for (int f = 0; f < NF; ++f) arr[f] = set[f];
+    return halo_exchange(arr, NF, sizeof(double));
+  }
+  int halo_f(float *const *a, float *const *b = nullptr, float *c = nullptr) {
+    void *arr[2 * NF + 1];
+    int n = 0;
+    for (int f = 0; f < NF; ++f) arr[n++] = a[f];
+    if (b)
+      for (int f = 0; f < NF; ++f) arr[n++] = b[f];
+    if (c) arr[n++] = c;
+    return halo_exchange(arr, n, sizeof(float));
+  }
 
   // the lo ghost images catch up with the interior before the state leaves
   // the device
@@ -424,6 +466,7 @@ struct miso_b200_handle {
         te(t, "rk_stage", interior() * (s == 0 ? 144.0 : 216.0));
         if ((rc = check_launch("rhs_stage"))) return rc;
         if ((rc = fill64(seq_r[s]))) return rc;
+        if ((rc = halo_d(q64[seq_r[s]]))) return rc;
       }
       // AV on B(2): x: B -> qq, y: qq -> A, z: A -> qq
       int t = tb();
@@ -437,6 +480,7 @@ struct miso_b200_handle {
         te(t, "av_sweep", interior() * 152.0);
         if ((rc = check_launch("av_sweep"))) return rc;
         if ((rc = fill64(dst[d]))) return rc;
+        if ((rc = halo_d(q64[dst[d]]))) return rc;
       }
       return MISO_B200_OK;
     }
@@ -453,8 +497,10 @@ struct miso_b200_handle {
       if ((rc = check_launch("rk_stage"))) return rc;
       if (s < 3) {
         if ((rc = fill_stage(s & 1))) return rc;
+        if ((rc = halo_f(stg[s & 1]))) return rc;
       } else {
         if ((rc = fill_split(c))) return rc;
+        if ((rc = halo_f(hi[c], lo[c]))) return rc;
       }
     }
     int t = tb();
@@ -469,6 +515,7 @@ struct miso_b200_handle {
       if ((rc = check_launch("av_sweep"))) return rc;
       cur ^= 1;
       if ((rc = fill_split(cur))) return rc;
+      if ((rc = halo_f(hi[cur], lo[cur]))) return rc;
     }
     return MISO_B200_OK;
   }
@@ -520,6 +567,9 @@ struct miso_b200_handle {
           if ((rc = shell(hi[c], SHELL_FACES_I, cc32, SHELL_FACES))) return rc;
         }
       }
+      // a shard's i ghosts of the stage output (and of hi and cc after the
+      // last stage, read by the x sweep) come from the neighbours
+      if ((rc = st < 3 ? halo_f(stg[st & 1]) : halo_f(hi[c], nullptr, cc32))) return rc;
     }
     for (int d = 0; d < 3; ++d) {
       AvArgs a;
@@ -563,6 +613,12 @@ struct miso_b200_handle {
         lo_shell_stale = false;
       }
       cur ^= 1;
+    }
+    // a shard: the step's final state (hi and lo, so that a download needs
+    // no exchange) takes its i ghosts from the neighbouring shards
+    if (halo_on) {
+      if ((rc = fresh_lo_shell())) return rc;
+      if ((rc = halo_f(hi[cur], lo[cur]))) return rc;
     }
     z_parts = av_var[2] == 1 ? flat_grid : z_grid;
     partials_valid = true;
@@ -871,7 +927,40 @@ int miso_b200_cfl(miso_b200_handle *h, double *dt_out) {
     return rc;
   if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cfl synchronize"))) return rc;
   if (v.err & (ERRBIT_NONFINITE | ERRBIT_TIMEOUT)) return h->read_err();
-  *dt_out = v.dt;
+  double dt = v.dt;
+  // a shard: the minimum over all shards, as the reference's MPI_Allreduce
+  if (h->halo_on && h->halo_ops.min_all) {
+    const int r = h->halo_ops.min_all(h->halo_ops.user, &dt);
+    if (r) return h->fail(MISO_B200_ERR_HALO, "min_all callback returned %d", r);
+  }
+  *dt_out = dt;
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
+                       const miso_b200_halo_ops *ops) {
+  if (!h) return MISO_B200_ERR_ARG;
+  Geom &g = h->g;
+  if (ops && !ops->exchange) return h->fail(MISO_B200_ERR_ARG, "halo ops without exchange");
+  if (ops && !g.s[0]) return h->fail(MISO_B200_ERR_ARG, "halo exchange needs an i axis of size > 1");
+  h->halo_on = ops != nullptr && (ext_lo || ext_hi);
+  h->halo_ops = ops ? *ops : miso_b200_halo_ops{};
+  for (int side = 0; side < 2; ++side) {
+    const bool ext = h->halo_on && (side == 0 ? ext_lo : ext_hi);
+    g.ext[0][side] = ext ? 1 : 0;
+    // no image across a shared face; elsewhere the descriptor's mirror signs
+    g.negmask[0][side] = 0;
+    if (!ext && !g.periodic[0])
+      for (int f = 0; f < NF; ++f)
+        if (g.sign[0][side][f] < 0) g.negmask[0][side] |= (unsigned short)(1u << f);
+  }
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
+  h->partials_valid = false;
   return MISO_B200_OK;
 }
 
@@ -887,11 +976,15 @@ int miso_b200_update(miso_b200_handle *h, double dt) {
 
 int miso_b200_update_device(miso_b200_handle *h) {
   if (!h) return MISO_B200_ERR_ARG;
+  if (h->halo_on)
+    return h->fail(MISO_B200_ERR_STATE, "a shard steps with cfl() and update(dt)");
   return h->enqueue_update();
 }
 
 int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
   if (!h || nsteps < 0) return MISO_B200_ERR_ARG;
+  if (h->halo_on)
+    return h->fail(MISO_B200_ERR_STATE, "a shard steps with cfl() and update(dt)");
   int rc;
   if (!use_graph) {
     for (int n = 0; n < nsteps; ++n) {

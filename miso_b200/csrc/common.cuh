@@ -35,6 +35,9 @@ struct Geom {
   int periodic[3];
   float sign[3][2][NF];  // mirror sign on non-periodic faces
   unsigned short negmask[3][2];  // bit f set where sign[a][side][f] < 0 (0 on periodic axes)
+  // 1 where the face is shared with a neighbouring shard of a decomposed
+  // grid: its ghost layer is filled by the halo exchange, never by an image
+  unsigned char ext[3][2];
 };
 
 // Per-step scalars, resident in device memory so a whole step can run

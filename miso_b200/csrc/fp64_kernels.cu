@@ -181,6 +181,7 @@ fill_axis_kernel(Geom g, FieldPtrs<T> q, int a, int nfields) {
     const long long uv = lin % plane;
     const int layer = (int)(lin / plane);  // 0..2m-1
     const int side = layer / m, gi = layer % m;
+    if (g.ext[a][side]) continue;  // a face shared with a neighbouring shard
     const int u = (int)(uv / g.t[c]), v = (int)(uv % g.t[c]);
     int dst, src;
     const bool per = g.periodic[a] != 0;

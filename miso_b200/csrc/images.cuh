@@ -36,11 +36,11 @@ __device__ __forceinline__ void make_img(const Geom &g, int x0, int x1, int x2, 
     h[a] = false;
     d[a] = 0;
     nm[a] = 0;
-    if (xs[a] < m) {
+    if (xs[a] < m && !g.ext[a][0]) {
       h[a] = true;
       d[a] = ((g.periodic[a] ? X + n : 2 * m - 1 - X) - X) * (int)g.st[a];
       nm[a] = g.negmask[a][0];
-    } else if (xs[a] >= n - m) {
+    } else if (xs[a] >= n - m && !g.ext[a][1]) {
       h[a] = true;
       d[a] = ((g.periodic[a] ? X - n : 2 * (m + n) - 1 - X) - X) * (int)g.st[a];
       nm[a] = g.negmask[a][1];
@@ -79,10 +79,15 @@ __device__ __forceinline__ void store_cell(T *p, long long cell, bool nb, const 
 // in [-m, n + m): t itself inside, else the periodic wrap or the mirror
 // (the inverse of the image map above).  side = 0 / 1 on the low / high
 // ghost layer (the mirror sign of the value is g.negmask[a][side]), -1
-// inside.  Lets a pass read a neighbour across a face without the ghost
+// inside and on a face shared with a neighbouring shard (whose ghost layer
+// the halo exchange fills: t is returned as it is).  Lets a pass read a neighbour across a face without the ghost
 // layer being filled.
 __device__ __forceinline__ int ghost_src(const Geom &g, int a, int t, int &side) {
   const int n = g.n[a];
+  if ((t < 0 && g.ext[a][0]) || (t >= n && g.ext[a][1])) {
+    side = -1;  // a face shared with a neighbouring shard: its ghosts hold the neighbour's cells
+    return t;
+  }
   if (t < 0) {
     side = 0;
     return g.periodic[a] ? t + n : -1 - t;

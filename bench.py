@@ -55,6 +55,10 @@ def parse():
                     help="turbulence: one 3-D grid (the headline); the batch workloads run "
                          "many instances through the batched solver")
     ap.add_argument("--count", type=int, default=0, help="instances of a batch workload")
+    ap.add_argument("--decomp", choices=["replicas", "slab"], default="replicas",
+                    help="turbulence under torchrun: independent n^3 grids per rank "
+                         "(replicas), or one (n*N) x n x n periodic grid cut into N slabs "
+                         "along x with the face halos exchanged over NCCL after every pass")
     return ap.parse_args()
 
 
@@ -337,23 +341,7 @@ def run_b200(args):
                 "l1_B": l1(a[P.BX:P.BZ + 1], b[P.BX:P.BZ + 1])}
 
     # ---- roofline of the dominant kernel
-    peak, peak_src = hbm_peak()
-    dom = max(report.items(), key=lambda kv: kv[1]["ms"])
-    dname, d = dom
-    achieved = (d["bytes"] / d["launches"]) / (d["ms"] / d["launches"] / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                traffic = json.load(f).get(f"{args.precision}:{dname}")
-        except Exception:
-            traffic = None
-    roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-                "traffic": traffic,
-                "step_frac": value / world * ALG_BYTES[args.precision] / peak,
-                "alg_bytes_per_cell_step": ALG_BYTES[args.precision]}
+    roofline = roofline_of(report, args.precision, value / world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -383,6 +371,124 @@ def run_b200(args):
                         for k, v in report.items()},
             "roofline": roofline, "e2e": e2e, "e2e_host_fields": host_fields, "fp64": fp64, "cpu_baseline": cpu,
             "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def roofline_of(report: dict, precision: str, value_per_gpu: float) -> dict:
+    """Roofline of the dominant kernel of a per-kernel timing report."""
+    peak, peak_src = hbm_peak()
+    dname, d = max(report.items(), key=lambda kv: kv[1]["ms"])
+    achieved = (d["bytes"] / d["launches"]) / (d["ms"] / d["launches"] / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(f"{precision}:{dname}")
+        except Exception:
+            traffic = None
+    return {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+            "traffic": traffic, "step_frac": value_per_gpu * ALG_BYTES[precision] / peak,
+            "alg_bytes_per_cell_step": ALG_BYTES[precision]}
+
+
+def run_slab(args):
+    """One periodic grid of (n * N) x n x n cells over N GPUs, cut into N
+    slabs along x (miso_b200.shard): every pass's i ghost planes travel to
+    the neighbouring ranks by NCCL point-to-point copies, dt is reduced by
+    an all-reduce of the minimum, and a step is the reference's host-dt
+    sequence cfl() -> update(dt).  Every slab holds the unit cube's
+    turbulence field (its Fourier modes have period 1 in x, so the stacked
+    field is the periodic field of the long box).  Weak scaling: n^3 cells
+    per GPU."""
+    import torch
+
+    from miso_b200 import problems as P
+    from miso_b200.integrator import Integrator
+    from miso_b200.shard import DistHalo, ShardSpec
+
+    rank, world, local = dist_init()
+    torch.cuda.set_device(local)
+    n, K, W = args.n, args.steps, args.warmup
+    prob = P.turbulence(n, seed=0)
+    cells = prob.grid.n_interior
+    stream = torch.cuda.Stream()
+    integ = Integrator(prob.config, prob.grid, precision=args.precision,
+                       stream=stream.cuda_stream)
+    integ.upload(prob.q)
+    integ.apply_boundary_condition()
+    tuning = {}
+    if args.precision == "fp32_split":
+        from miso_b200.autotune import autotune
+        tuning = autotune(integ)  # the tuner steps with run(): before the halo is attached
+        integ.upload(prob.q)
+    if world > 1:
+        DistHalo(periodic_x=True, device="cuda").attach(
+            integ, ShardSpec(rank, world, 0, n, prob.grid, True, True))
+    integ.apply_boundary_condition()
+
+    def steps(k):
+        for _ in range(k):
+            integ.update(integ.cfl())
+
+    steps(W)
+    integ.sync()
+    integ.set_timing(True)
+    steps(2)
+    integ.sync()
+    report = integ.timing_report()
+    integ.set_timing(False)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    l0 = integ.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    sampler.start()
+    e0.record(stream)
+    steps(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = integ.launch_count() - l0
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    value = world * cells * K / (ms / 1e3) / 1e9
+    # e2e: the same host-dt steps with the step's monitors read back
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        integ.update(integ.cfl())
+        integ.monitors()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    e2e = {"value": world * cells * K / e2e_s / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": 96, "d2h_bytes_per_step": 8 + 8 * 8 * 2 * sms,
+           "path": "Integrator.cfl() (dt all-reduced) -> update(dt) -> monitors() per step"}
+    integ.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32_split" else "f64",
+            "data": "synthetic (seeded solenoidal Fourier modes)",
+            "config": {"workload": f"3D decaying MHD turbulence ({n}*{world})x{n}x{n} periodic, "
+                                   f"one grid in {world} slabs along x, {args.precision}",
+                       "precision": args.precision, "cells_per_gpu": cells,
+                       "l2": "inputs larger than L2 (state > 1 GB)",
+                       "parallelism": f"slab x{world} (NCCL halo exchange)"},
+            "timed_path": "Integrator.cfl() -> update(dt) per step, dt all-reduced over ranks",
+            "tuning": tuning, "gpu_launches": launches,
+            "kernels": {k: {"launches": v["launches"], "ms_per_step": v["ms"] / 2}
+                        for k, v in report.items()},
+            "roofline": roofline_of(report, args.precision, value / world), "e2e": e2e,
+            "cpu_baseline": None, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -469,6 +575,8 @@ def main():
         run_reference(args)
     elif args.workload != "turbulence":
         run_batch(args)
+    elif args.decomp == "slab":
+        run_slab(args)
     else:
         run_b200(args)
 

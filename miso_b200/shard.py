@@ -179,8 +179,10 @@ class LocalHalo(_Halo):
 
     def exchange(self, r, slo, shi, rlo, rhi, nbytes, ext_lo, ext_hi, stream):
         import torch
-        self._planes[r] = (slo, shi)
+        self._planes[r] = (slo, shi, stream)
         self._bar.wait()
+        if any(p[2] != stream for p in self._planes):
+            raise RuntimeError("in-process shards must share one CUDA stream")
         with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
             for a in range(len(rlo)):
                 if ext_lo:
@@ -277,13 +279,22 @@ class _nullcontext:
 def run_local_shards(prob, count: int, steps: int, precision: str = "fp64", variants=None,
                      stream=None) -> tuple[np.ndarray, list[float]]:
     """Advance ``prob`` by ``steps`` host-dt steps (cfl, then update) as
-    ``count`` shards on the current GPU, one host thread per shard; return
-    the gathered global interior and the time steps taken."""
+    ``count`` shards on the current GPU, one host thread per shard, all on
+    one CUDA stream (``stream``, or a new one); return the gathered global
+    interior and the time steps taken."""
     import torch
     periodic_x = bool(prob.config["domain"]["periodic"]["x"])
     specs = split_grid(prob.grid, count, periodic_x)
     halo = LocalHalo(count, periodic_x)
-    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    # one stream for every shard (a null stream would give each handle its
+    # own, and the halo copies would then race with the neighbours' passes)
+    keep = None
+    if stream is None:
+        keep = torch.cuda.Stream()
+        stream = keep.cuda_stream
+    if not stream:
+        raise ValueError("the shards need one explicit (non-null) CUDA stream")
+    st = stream
     integs = []
     for s in specs:
         integ = Integrator(prob.config, s.grid, sign=prob.sign, precision=precision, stream=st)

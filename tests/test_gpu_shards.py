@@ -70,3 +70,40 @@ def test_shard_refuses_device_dt_steps():
         integ.run(1, graph=False)
     assert e.value.code == _lib.ERR_STATE
     integ.close()
+
+
+def test_dist_halo_one_rank_nccl_equals_single_grid():
+    """The torch.distributed transport on the GPU: one NCCL rank whose two
+    i faces are shared with itself (the periodic wrap through the exchange
+    callback, dt through an NCCL all-reduce) steps like the single grid."""
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+
+    from miso_b200.shard import DistHalo, ShardSpec
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        prob = P.turbulence(32, seed=4)
+        ref, dts = single(prob, 3, "fp32_split")
+        integ = Integrator(prob.config, prob.grid, precision="fp32_split")
+        DistHalo(periodic_x=True, device="cuda").attach(
+            integ, ShardSpec(0, 1, 0, 32, prob.grid, True, True))
+        integ.upload(prob.q)
+        integ.apply_boundary_condition()
+        got_dts = []
+        for _ in range(3):
+            dt = integ.cfl()
+            integ.update(dt)
+            got_dts.append(dt)
+        got = integ.download()[(slice(None),) + prob.grid.interior]
+        integ.close()
+        assert got_dts == dts
+        assert np.array_equal(got, ref)
+    finally:
+        dist.destroy_process_group()

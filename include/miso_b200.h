@@ -136,6 +136,18 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]);
  * (miso/include/miso/mhd_fields.hpp:17-34). */
 int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
 
+/* Built-in source term of the momentum and energy equations: the Source
+ * argument of Integrator::update (miso/include/miso/mhd_integrator_host.hpp:
+ * 134-168 and 241; concept mhd_model_base.hpp:131-155), default
+ * EmptySourceTerm.  MISO_B200_SOURCE_POINT_GRAVITY is the magnetosphere
+ * demo's gravity (demo/mhd3d_magnetosphere/src/src.hpp:17-44): force per
+ * volume -ro g x / |x|^3 about the coordinate origin, params[0] = g, no
+ * heating.  FP64 form only (MISO_B200_ERR_STATE in the split form); every
+ * cell centre must lie off the origin. */
+#define MISO_B200_SOURCE_NONE 0
+#define MISO_B200_SOURCE_POINT_GRAVITY 1
+int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, int nparams);
+
 /* Halo exchange of a grid decomposed into shards along i (the slowest
  * axis).  Replaces the reference's HaloExchanger for the neighbour faces of
  * a Cartesian decomposition (miso/include/miso/mhd_halo_exchange.hpp:

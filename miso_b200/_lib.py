@@ -79,6 +79,7 @@ SIGNATURES = {
     "miso_b200_device_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
     "miso_b200_launch_count": (ctypes.c_int, [ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_longlong)]),
+    "miso_b200_set_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int]),
     "miso_b200_set_halo": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(HaloOps)]),
     "miso_b200_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),

@@ -150,6 +150,10 @@ struct miso_b200_handle {
 
   // tiled FP32-split path (3-D grids)
   bool tiled = false;
+  // built-in source term (miso_b200_set_source) and the cell centres it
+  // reads, one array per axis (ghosts included)
+  Source src{};
+  double *axc[3] = {};
   // halo exchange with neighbouring shards along i (miso_b200_set_halo)
   miso_b200_halo_ops halo_ops{};
   bool halo_on = false;
@@ -462,7 +466,8 @@ struct miso_b200_handle {
       const int seq_r[4] = {1, 2, 1, 2};
       for (int s = 0; s < 4; ++s) {
         const int t = tb();
-        launch_fp64_rhs_stage(g, c64(0), c64(seq_a[s]), f64(seq_r[s]), sc, s, p.gm, sms, stream);
+        launch_fp64_rhs_stage(g, c64(0), c64(seq_a[s]), f64(seq_r[s]), sc, s, p.gm, src, sms,
+                              stream);
         te(t, "rk_stage", interior() * (s == 0 ? 144.0 : 216.0));
         if ((rc = check_launch("rhs_stage"))) return rc;
         if ((rc = fill64(seq_r[s]))) return rc;
@@ -767,6 +772,7 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   add((void **)&h->partial, sizeof(float) * h->nparts_alloc);
   add((void **)&h->mon_partial, sizeof(double) * 8 * h->mon_blocks);
   add((void **)&h->sc, sizeof(StepScalars));
+  for (int a = 0; a < 3; ++a) add((void **)&h->axc[a], sizeof(double) * g.t[a]);
   e = cudaMalloc(&h->block, total);
   if (e != cudaSuccess) {
     if (h->own_stream) cudaStreamDestroy(h->stream);
@@ -824,6 +830,31 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
     delete h;
     return create_fail(MISO_B200_ERR_CUDA, "device memset failed");
   }
+  // cell centres per axis, placed as UniformAxisProvider::loc places them
+  // (grid.hpp:22-31): x_min + (i_global + 0.5) * (x_max - x_min) / size
+  for (int a = 0; a < 3; ++a) {
+    std::vector<double> xs(g.t[a]);
+    for (int i = 0; i < g.t[a]; ++i) {
+      const int ig = i - g.m[a];
+      const double sp = (hi[a] - lo[a]) / (double)sz[a];
+      xs[i] = lo[a] + ((double)ig + 0.5) * sp;
+    }
+    // after the block's memset: the copy is ordered behind it on the stream
+    e = cudaMemcpyAsync(h->axc[a], xs.data(), sizeof(double) * g.t[a], cudaMemcpyHostToDevice,
+                        h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      cudaFree(h->block);
+      if (h->own_stream) cudaStreamDestroy(h->stream);
+      delete h;
+      return create_fail(MISO_B200_ERR_CUDA, "copy of the cell centres failed");
+    }
+  }
+  h->src.kind = 0;
+  h->src.g = 0.0;
+  h->src.x = h->axc[0];
+  h->src.y = h->axc[1];
+  h->src.z = h->axc[2];
   *out = h;
   return MISO_B200_OK;
 }
@@ -934,6 +965,30 @@ int miso_b200_cfl(miso_b200_handle *h, double *dt_out) {
     if (r) return h->fail(MISO_B200_ERR_HALO, "min_all callback returned %d", r);
   }
   *dt_out = dt;
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, int nparams) {
+  if (!h) return MISO_B200_ERR_ARG;
+  if (kind == MISO_B200_SOURCE_NONE) {
+    h->src.kind = 0;
+    h->src.g = 0.0;
+  } else if (kind == MISO_B200_SOURCE_POINT_GRAVITY) {
+    if (!params || nparams < 1 || !std::isfinite(params[0]))
+      return h->fail(MISO_B200_ERR_ARG, "point gravity needs its constant g in params[0]");
+    if (h->split())
+      return h->fail(MISO_B200_ERR_STATE, "source terms run in the FP64 form");
+    h->src.kind = 1;
+    h->src.g = params[0];
+  } else {
+    return h->fail(MISO_B200_ERR_ARG, "unknown source kind %d", kind);
+  }
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
   return MISO_B200_OK;
 }
 

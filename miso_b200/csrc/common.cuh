@@ -40,6 +40,18 @@ struct Geom {
   unsigned char ext[3][2];
 };
 
+// Built-in source term of the momentum and energy equations (the Source
+// concept of mhd_model_base.hpp:131-155): none (EmptySourceTerm), or the
+// point gravity at the coordinate origin of the magnetosphere demo
+// (demo/mhd3d_magnetosphere/src/src.hpp:17-44).  x / y / z are the cell
+// centres per axis (total cells, ghosts included), as grid.hpp:22-31 places
+// them.
+struct Source {
+  int kind;  // 0 none, 1 point gravity
+  double g;  // gravitational constant: force per volume -ro g x / |x|^3
+  const double *x, *y, *z;
+};
+
 // Per-step scalars, resident in device memory so a whole step can run
 // without a host round trip.  Written by the CFL finalisation kernel (device
 // dt) or uploaded by the host (host dt, as Integrator::update(dt) receives

@@ -154,11 +154,31 @@ __device__ __forceinline__ double av_dflux(const double w[5], double ccl, double
 
 // One Runge-Kutta stage for interior cell c: out = orgn + dt * R(argm)
 // (mhd_integrator_host.hpp:106-244, expression by expression).
+// The source's force per volume at cell (i, j, k) (array indices) from the
+// stage's argument state (src.vx/vy/vz of the reference, evaluated on c_qq).
+__device__ __forceinline__ void source_force(const Source &s, const FieldPtrs<const double> &a,
+                                             long long c, int i, int j, int k, double &sx,
+                                             double &sy, double &sz) {
+  sx = sy = sz = 0.0;
+  if (s.kind == 1) {
+    const double X = s.x[i], Y = s.y[j], Z = s.z[k];
+    const double rr = sqrt(X * X + Y * Y + Z * Z);
+    const double r3 = rr * rr * rr;  // util::pow3
+    const double ro = a.f[RO][c];
+    sx = -ro * s.g * X / r3;
+    sy = -ro * s.g * Y / r3;
+    sz = -ro * s.g * Z / r3;
+  }
+}
+
 __device__ __forceinline__ void rhs_cell(const Geom &g, const FieldPtrs<const double> &o,
                                          const FieldPtrs<const double> &a, long long c,
                                          double dt, double ch2, double decay, double gm,
-                                         double out[NF]) {
-  const double src = 0.0;  // EmptySourceTerm (mhd_model_base.hpp:131-155)
+                                         double out[NF], double sx = 0.0, double sy = 0.0,
+                                         double sz = 0.0) {
+  // sx, sy, sz: the source's force per volume (0 for EmptySourceTerm,
+  // mhd_model_base.hpp:131-155); src.ei adds 0 for every built-in source
+  const double src = 0.0;
     DirTerms X, Y, Z;
     dir_terms(a, c, g.st[0] * g.s[0], 0, g.dsi[0], gm, X);
     dir_terms(a, c, g.st[1] * g.s[1], 1, g.dsi[1], gm, Y);
@@ -171,11 +191,11 @@ __device__ __forceinline__ void rhs_cell(const Geom &g, const FieldPtrs<const do
     const double ro = oro + dt * (-X.ro_v - Y.ro_v - Z.ro_v);
 
     const double vx = (oro * ovx + dt * (-X.mx_v - Y.mx_v - Z.mx_v - X.pr - X.bb * PII8 +
-                                        PII4 * (+X.bx_b + Y.bx_b + Z.bx_b) + src)) / ro;
+                                        PII4 * (+X.bx_b + Y.bx_b + Z.bx_b) + sx)) / ro;
     const double vy = (oro * ovy + dt * (-X.my_v - Y.my_v - Z.my_v - Y.pr - Y.bb * PII8 +
-                                        PII4 * (+X.by_b + Y.by_b + Z.by_b) + src)) / ro;
+                                        PII4 * (+X.by_b + Y.by_b + Z.by_b) + sy)) / ro;
     const double vz = (oro * ovz + dt * (-X.mz_v - Y.mz_v - Z.mz_v - Z.pr - Z.bb * PII8 +
-                                        PII4 * (+X.bz_b + Y.bz_b + Z.bz_b) + src)) / ro;
+                                        PII4 * (+X.bz_b + Y.bz_b + Z.bz_b) + sz)) / ro;
 
     const double bx = obx + dt * (-Y.vd_be[0] - Z.vd_be[0] + Y.ve_bd[0] + Z.ve_bd[0] - X.ph);
     const double by = oby + dt * (-X.vd_be[1] - Z.vd_be[1] + X.ve_bd[1] + Z.ve_bd[1] - Y.ph);

@@ -25,7 +25,8 @@ namespace fp64 {
 // mhd_integrator_host.hpp:106-244 expression by expression.
 __global__ void __launch_bounds__(128)
 rhs_stage_kernel(Geom g, FieldPtrs<const double> o, FieldPtrs<const double> a,
-                 FieldPtrs<double> r, const StepScalars *__restrict__ sc, int stage, double gm) {
+                 FieldPtrs<double> r, const StepScalars *__restrict__ sc, int stage, double gm,
+                 Source src) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
   const double dt = sc->dts[stage];
   const double ch2 = sc->ch2;
@@ -38,8 +39,9 @@ rhs_stage_kernel(Geom g, FieldPtrs<const double> o, FieldPtrs<const double> a,
     const int i = (int)(r1 / g.n[1]) + g.m[0];
     const long long c = i * g.st[0] + j * g.st[1] + k;
 
-    double out[NF];
-    rhs_cell(g, o, a, c, dt, ch2, decay, gm, out);
+    double out[NF], sx, sy, sz;
+    source_force(src, a, c, i, j, k, sx, sy, sz);
+    rhs_cell(g, o, a, c, dt, ch2, decay, gm, out, sx, sy, sz);
 #pragma unroll
     for (int f = 0; f < NF; ++f) r.f[f][c] = out[f];
   }
@@ -222,11 +224,11 @@ static int grid_blocks(long long work, int threads, int sms, int per_sm) {
 
 void launch_fp64_rhs_stage(const Geom &g, const FieldPtrs<const double> &o,
                            const FieldPtrs<const double> &a, const FieldPtrs<double> &r,
-                           const StepScalars *sc, int stage, double gm, int sms,
-                           cudaStream_t st) {
+                           const StepScalars *sc, int stage, double gm, const Source &src,
+                           int sms, cudaStream_t st) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
   fp64::rhs_stage_kernel<<<grid_blocks(nint, 128, sms, 16), 128, 0, st>>>(g, o, a, r, sc, stage,
-                                                                            gm);
+                                                                            gm, src);
 }
 
 void launch_fp64_char_velocity(const Geom &g, const FieldPtrs<const double> &q, double *cc,

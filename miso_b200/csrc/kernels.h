@@ -9,8 +9,8 @@ namespace miso_b200 {
 // ---- FP64 form (bit-faithful to the reference's double host path) ----
 void launch_fp64_rhs_stage(const Geom &g, const FieldPtrs<const double> &o,
                            const FieldPtrs<const double> &a, const FieldPtrs<double> &r,
-                           const StepScalars *sc, int stage, double gm, int sms,
-                           cudaStream_t st);
+                           const StepScalars *sc, int stage, double gm, const Source &src,
+                           int sms, cudaStream_t st);
 void launch_fp64_char_velocity(const Geom &g, const FieldPtrs<const double> &q, double *cc,
                                double gm, double cs_fac, double vv_fac, double ca_fac, int sms,
                                cudaStream_t st);

@@ -139,6 +139,15 @@ class Integrator:
                                         ctypes.c_void_p(stream or 0), ctypes.byref(h)), None)
         self._h = h
         self._lib = lib
+        src = cfg.get("source") or {}
+        kind = src.get("kind", "none")
+        if kind != "none":
+            kinds = {"point_gravity": 1}
+            if kind not in kinds:
+                self.close()
+                raise ValueError(f"unknown source kind {kind!r}")
+            par = (ctypes.c_double * 1)(float(src["g"]))
+            self._check(lib.miso_b200_set_source(h, kinds[kind], par, 1))
 
     # -- lifetime -----------------------------------------------------------
     def close(self):

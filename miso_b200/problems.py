@@ -159,6 +159,16 @@ def _modes_on_grid(g: Grid, k, vec, phase, L=(1.0, 1.0, 1.0), lo=(0.0, 0.0, 0.0)
     return out
 
 
+def with_point_gravity(prob: Problem, g: float) -> Problem:
+    """``prob`` with the magnetosphere demo's point gravity at the origin
+    (demo/mhd3d_magnetosphere/src/src.hpp:17-44): force per volume
+    -ro g x / |x|^3 in the momentum equations, no heating.  Sizes must keep
+    every cell centre off the origin (even sizes on a centred box)."""
+    cfg = dict(prob.config)
+    cfg["source"] = {"kind": "point_gravity", "g": float(g)}
+    return Problem(prob.name + "_grav", prob.grid, cfg, prob.q, prob.sign)
+
+
 def turbulence(n: int = 256, seed: int = 0, mach: float = 0.5, beta: float = 1.0,
                gm: float = 5.0 / 3.0, cfl: float = 0.4) -> Problem:
     """3-D decaying MHD turbulence on the periodic unit cube.

@@ -180,7 +180,11 @@ static inline double D3(const double *a, const double *b, const double *e, long 
 }
 
 /* mhd_integrator_host.hpp:57-247 with the derived arrays of eos.hpp:25-31
- * and lines 64-89; the source term is the empty one (adds 0.0). */
+ * and lines 64-89.  The source term (src.vx/vy/vz inside dt * (...), src.ei
+ * added to the new total energy, lines 134-168 and 241) is the empty one
+ * (adds 0.0) or the point gravity of the magnetosphere demo
+ * (demo/mhd3d_magnetosphere/src/src.hpp:17-44): force per volume
+ * -ro g x / |x|^3 on the stage's argument state, no heating. */
 static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
                   double *const a[NF], double *const r[NF], double dt, double ch2,
                   double tau, double *pr, double *bb, double *ht, double *vb) {
@@ -195,7 +199,7 @@ static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
   const long si = g->st[0] * g->s[0], sj = g->st[1] * g->s[1], sk = g->st[2] * g->s[2];
   const double *ro = a[RO], *vx = a[VX], *vy = a[VY], *vz = a[VZ];
   const double *bx = a[BX], *by = a[BY], *bz = a[BZ], *ph = a[PH];
-  const double src = 0.0; /* EmptySourceTerm (mhd_model_base.hpp:131-155) */
+  const double src = 0.0; /* EmptySourceTerm (mhd_model_base.hpp:131-155), and src.ei */
   for (int i = g->m[0]; i < g->t[0] - g->m[0]; ++i) {
     const double dxi = g->daxi[0][i];
     for (int j = g->m[1]; j < g->t[1] - g->m[1]; ++j) {
@@ -203,6 +207,15 @@ static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
       for (int k = g->m[2]; k < g->t[2] - g->m[2]; ++k) {
         const double dzi = g->daxi[2][k];
         const long c = IDX(g, i, j, k);
+        double sx = src, sy = src, sz = src;
+        if (d->source == 1) {
+          const double X = g->ax[0][i], Y = g->ax[1][j], Z = g->ax[2][k];
+          const double rr = sqrt(X * X + Y * Y + Z * Z);
+          const double r3 = rr * rr * rr; /* util::pow3 */
+          sx = -a[RO][c] * d->g_grav * X / r3;
+          sy = -a[RO][c] * d->g_grav * Y / r3;
+          sz = -a[RO][c] * d->g_grav * Z / r3;
+        }
 
         r[RO][c] = o[RO][c] + dt * (-D2(ro, vx, c, si, dxi) - D2(ro, vy, c, sj, dyi) -
                                     D2(ro, vz, c, sk, dzi));
@@ -213,7 +226,7 @@ static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
                           D1(bb, c, si, dxi) * PII8 +
                           PII4 * (+D2(bx, bx, c, si, dxi) + D2(bx, by, c, sj, dyi) +
                                   D2(bx, bz, c, sk, dzi)) +
-                          src)) / r[RO][c];
+                          sx)) / r[RO][c];
 
         r[VY][c] = (o[RO][c] * o[VY][c] +
                     dt * (-D3(ro, vy, vx, c, si, dxi) - D3(ro, vy, vy, c, sj, dyi) -
@@ -221,7 +234,7 @@ static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
                           D1(bb, c, sj, dyi) * PII8 +
                           PII4 * (+D2(by, bx, c, si, dxi) + D2(by, by, c, sj, dyi) +
                                   D2(by, bz, c, sk, dzi)) +
-                          src)) / r[RO][c];
+                          sy)) / r[RO][c];
 
         r[VZ][c] = (o[RO][c] * o[VZ][c] +
                     dt * (-D3(ro, vz, vx, c, si, dxi) - D3(ro, vz, vy, c, sj, dyi) -
@@ -229,7 +242,7 @@ static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
                           D1(bb, c, sk, dzi) * PII8 +
                           PII4 * (+D2(bz, bx, c, si, dxi) + D2(bz, by, c, sj, dyi) +
                                   D2(bz, bz, c, sk, dzi)) +
-                          src)) / r[RO][c];
+                          sz)) / r[RO][c];
 
         r[BX][c] = o[BX][c] + dt * (-D2(vy, bx, c, sj, dyi) - D2(vz, bx, c, sk, dzi) +
                                     D2(vx, by, c, sj, dyi) + D2(vx, bz, c, sk, dzi) -

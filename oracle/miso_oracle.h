@@ -34,6 +34,8 @@ typedef struct miso_oracle_desc {
   double cfl_number;
   double ep, fh;              /* limiter parameters (config_defaults.hpp:24-27) */
   double cs_fac, ca_fac, vv_fac;
+  int source;                 /* 0 EmptySourceTerm, 1 point gravity at the origin */
+  double g_grav;              /* its gravitational constant (force -ro g x / |x|^3) */
 } miso_oracle_desc;
 
 /* Fill every ghost cell of q (9 arrays) from its periodic or mirror image. */

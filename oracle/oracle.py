@@ -36,7 +36,8 @@ class Desc(ctypes.Structure):
                 ("gm", ctypes.c_double), ("cfl_number", ctypes.c_double),
                 ("ep", ctypes.c_double), ("fh", ctypes.c_double),
                 ("cs_fac", ctypes.c_double), ("ca_fac", ctypes.c_double),
-                ("vv_fac", ctypes.c_double)]
+                ("vv_fac", ctypes.c_double),
+                ("source", ctypes.c_int), ("g_grav", ctypes.c_double)]
 
 
 def make_desc(grid, config, sign=None) -> Desc:
@@ -55,6 +56,9 @@ def make_desc(grid, config, sign=None) -> Desc:
     av = config["mhd"]["artificial_viscosity"]
     d.ep, d.fh = av["ep"], av["fh"]
     d.cs_fac, d.ca_fac, d.vv_fac = av["cs_fac"], av["ca_fac"], av["vv_fac"]
+    src = config.get("source") or {}
+    d.source = {"none": 0, "point_gravity": 1}[src.get("kind", "none")]
+    d.g_grav = float(src.get("g", 0.0))
     return d
 
 

@@ -56,6 +56,31 @@ struct DescBC {
   }
 };
 
+// The point gravity of the magnetosphere demo
+// (demo/mhd3d_magnetosphere/src/src.hpp:17-44), restated as a source
+// functor of the reference's Source concept (mhd_model_base.hpp:131-155):
+// force per volume -ro g x / |x|^3 from the stage's argument state, no
+// heating.
+struct PointGravity {
+  GridView<const Real> grid;
+  Real g_grav;
+  PointGravity(Grid<Real, B> &g, Real gg) : grid(g.const_view()), g_grav(gg) {}
+  Real r3(int i, int j, int k) const {
+    return util::pow3(util::sqrt(grid.x[i] * grid.x[i] + grid.y[j] * grid.y[j] +
+                                 grid.z[k] * grid.z[k]));
+  }
+  Real vx(mhd::FieldsView<const Real> qq, int i, int j, int k) const {
+    return -qq.ro(i, j, k) * g_grav * grid.x[i] / r3(i, j, k);
+  }
+  Real vy(mhd::FieldsView<const Real> qq, int i, int j, int k) const {
+    return -qq.ro(i, j, k) * g_grav * grid.y[j] / r3(i, j, k);
+  }
+  Real vz(mhd::FieldsView<const Real> qq, int i, int j, int k) const {
+    return -qq.ro(i, j, k) * g_grav * grid.z[k] / r3(i, j, k);
+  }
+  Real ei(mhd::FieldsView<const Real>, int, int, int) const { return 0.0; }
+};
+
 struct Session {
   std::unique_ptr<Env> env;
   std::string path;
@@ -132,10 +157,14 @@ int miso_ref_run(const miso_oracle_desc *d, double *const q[9], int nsteps, int 
     mhd::Fields<Real, B> qq(*s.grid);
     to_fields(qq, q);
     if (fill_first) s.integ->apply_boundary_condition(*s.bc, qq);
+    PointGravity grav(*s.grid, d->g_grav);
     for (int n = 0; n < nsteps; ++n) {
       const Real dt = s.integ->cfl(qq, *s.eos);
       if (dt_out) dt_out[n] = dt;
-      s.integ->update(dt, *s.eos, *s.bc, s.src, qq);
+      if (d->source == 1)
+        s.integ->update(dt, *s.eos, *s.bc, grav, qq);
+      else
+        s.integ->update(dt, *s.eos, *s.bc, s.src, qq);
     }
     from_fields(qq, q);
     return 0;
@@ -168,7 +197,10 @@ int miso_ref_stage(const miso_oracle_desc *d, double *const orgn[9], double *con
     to_fields(r, rslt);
     s.integ->ch_divb_square = ch_divb_square;
     s.integ->tau_divb = tau_divb;
-    s.integ->update_sc4(dt, *s.eos, s.src, o, a, r);
+    if (d->source == 1)
+      s.integ->update_sc4(dt, *s.eos, PointGravity(*s.grid, d->g_grav), o, a, r);
+    else
+      s.integ->update_sc4(dt, *s.eos, s.src, o, a, r);
     from_fields(r, rslt);
     return 0;
   } catch (const std::exception &e) {

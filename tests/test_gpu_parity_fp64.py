@@ -40,6 +40,9 @@ CASES = [
     ("turb12", lambda: P.turbulence(12, seed=3), 6),
     ("blast12", lambda: P.blast(12, seed=5), 6),
     ("turb_aniso", lambda: _aniso(), 4),
+    # the magnetosphere demo's point-gravity source term
+    ("blast12_grav", lambda: P.with_point_gravity(P.blast(12, seed=5), 0.3), 6),
+    ("ot32_grav", lambda: P.with_point_gravity(P.orszag_tang(32), 2.0), 10),
 ]
 
 
@@ -155,3 +158,11 @@ def test_bad_dt_is_rejected():
         with pytest.raises(_lib.MisoError) as exc:
             integ.update(-1.0)
         assert exc.value.code == _lib.ERR_ARG
+
+
+def test_point_gravity_needs_fp64():
+    from miso_b200 import _lib
+    prob = P.with_point_gravity(P.blast(8, seed=1), 0.3)
+    with pytest.raises(_lib.MisoError) as e:
+        Integrator(prob.config, prob.grid, precision="fp32_split")
+    assert e.value.code == _lib.ERR_STATE

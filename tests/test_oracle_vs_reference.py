@@ -19,6 +19,9 @@ CASES = [
     ("sod_x", lambda: P.sod(64), 20),
     ("turb10", lambda: P.turbulence(10, seed=4), 3),
     ("blast10", lambda: P.blast(10, seed=6), 3),
+    # the magnetosphere demo's point-gravity source term
+    ("blast10_grav", lambda: P.with_point_gravity(P.blast(10, seed=6), 0.3), 3),
+    ("ot24_grav", lambda: P.with_point_gravity(P.orszag_tang(24), 2.0), 6),
 ]
 
 
@@ -32,9 +35,13 @@ def test_run_bit_exact(name, make, nsteps, oracle, reference):
     assert np.array_equal(interior(prob, a), interior(prob, b))
 
 
-def test_stage_bit_exact(oracle, reference):
-    """One RHS stage (update_sc4) with arbitrary divergence-cleaning scalars."""
-    prob = P.turbulence(9, seed=8)
+@pytest.mark.parametrize("grav", [False, True])
+def test_stage_bit_exact(oracle, reference, grav):
+    """One RHS stage (update_sc4) with arbitrary divergence-cleaning scalars,
+    with and without the point-gravity source."""
+    prob = P.turbulence(10, seed=8)
+    if grav:
+        prob = P.with_point_gravity(prob, 0.7)
     q = prob.q.copy()
     oracle.fill_ghosts(prob, q)
     r1 = np.zeros_like(q)

@@ -1,0 +1,101 @@
+"""The reference's run loop for one grid: ModelBase (mhd_model_base.hpp:41-116).
+
+``Model.run()`` is ModelBase::run: apply the initial condition, resume from
+the last snapshot when ``io.continue`` is set and one exists, write the run's
+set-up files, then step (cfl, update, time += dt: ModelBase::update and
+Time::update, time.hpp:64-67) until ``time.tend``, writing a snapshot after
+every step at which ``time >= time.dt_output * n_output`` (save_if_needed,
+mhd_model_base.hpp:81-87).  Snapshots go to the reference's run-directory
+layout through :class:`miso_b200.checkpoint.Output`; they are taken with
+``save_async``, so the device-to-host copy of a snapshot overlaps the steps
+that follow it.
+
+Configuration keys, as the reference reads them: ``time.tend``,
+``time.dt_output``, ``io.enabled``, ``io.continue``, ``io.save_dir``.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+from .checkpoint import Output
+from .grid import Grid
+from .integrator import MHD
+
+
+class Model:
+    """One grid's model: fields, integrator, time and output."""
+
+    def __init__(self, config: dict, grid: Grid, initial_state: np.ndarray, sign=None,
+                 precision: str = "fp64"):
+        t = config.get("time") or {}
+        if "tend" not in t or "dt_output" not in t:
+            raise KeyError("config needs time.tend and time.dt_output")
+        self.tend = float(t["tend"])
+        self.dt_output = float(t["dt_output"])
+        if not (self.tend > 0 and self.dt_output > 0):
+            raise ValueError("time.tend and time.dt_output must be > 0")
+        io = config.get("io") or {}
+        self.io_enabled = bool(io.get("enabled", True))
+        self.resume = bool(io.get("continue", False))
+        self.config = config
+        self.grid = grid
+        self.q0 = initial_state
+        self.mhd = MHD(config, grid, sign=sign, precision=precision)
+        self.output = (Output(io.get("save_dir", "data/"), config, grid)
+                       if self.io_enabled else None)
+        # Time::initialize (time.hpp:37-41)
+        self.time = 0.0
+        self.n_step = 0
+        self.n_output = 0
+
+    # -- ModelBase -------------------------------------------------------------
+    def update(self) -> float:
+        """ModelBase::update: cfl, update, time += dt."""
+        dt = self.mhd.cfl()
+        self.mhd.update(dt)
+        self.time += dt
+        self.n_step += 1
+        return dt
+
+    def save_state(self):
+        if self.output is not None:
+            self.output.save_async(self.mhd.integrator, self.time, self.n_output, self.n_step)
+
+    def load_state(self):
+        """Time::load and Checkpoint::load of the snapshot named in
+        time/n_output.txt (the state is uploaded with its ghost cells, as
+        the reference reads them back)."""
+        with open(os.path.join(self.output.time_dir, "n_output.txt")) as f:
+            n = int(f.readline())
+        self.time, self.n_output, self.n_step = self.output.load_time(n)
+        self.mhd.integrator.upload(self.output.load(self.n_output))
+
+    def save_if_needed(self):
+        if self.time >= self.dt_output * self.n_output:
+            self.save_state()
+            self.n_output += 1
+
+    def run(self):
+        """ModelBase::run (mhd_model_base.hpp:88-116)."""
+        self.mhd.apply_initial_condition(self.q0)
+        if (self.resume and self.output is not None and
+                os.path.exists(os.path.join(self.output.time_dir, "n_output.txt"))):
+            self.load_state()
+        if self.output is not None:
+            self.output.write_setup()
+        self.save_if_needed()
+        while self.time < self.tend:
+            self.update()
+            self.save_if_needed()
+        if self.output is not None:
+            self.output.wait()
+
+    def state(self) -> np.ndarray:
+        return self.mhd.integrator.download()
+
+    def close(self):
+        if self.output is not None:
+            self.output.wait()
+        self.mhd.integrator.close()

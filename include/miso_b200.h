@@ -142,8 +142,10 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
  * EmptySourceTerm.  MISO_B200_SOURCE_POINT_GRAVITY is the magnetosphere
  * demo's gravity (demo/mhd3d_magnetosphere/src/src.hpp:17-44): force per
  * volume -ro g x / |x|^3 about the coordinate origin, params[0] = g, no
- * heating.  FP64 form only (MISO_B200_ERR_STATE in the split form); every
- * cell centre must lie off the origin. */
+ * heating.  Both forms: FP64 bit for bit as the reference adds it; in the
+ * FP32 split form the force is formed in FP32 and the 3-D RK stage runs
+ * variant 2 (set_variant of another RK variant is refused while a source
+ * is on).  Every cell centre must lie off the origin. */
 #define MISO_B200_SOURCE_NONE 0
 #define MISO_B200_SOURCE_POINT_GRAVITY 1
 int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, int nparams);

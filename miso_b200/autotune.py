@@ -35,7 +35,9 @@ def _key(integ) -> str:
     import torch
     g = integ.grid
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-    return f"{integ.precision}:{g.i_size}x{g.j_size}x{g.k_size}:sm{sms}"
+    src = (integ.config.get("source") or {}).get("kind", "none")
+    tag = "" if src == "none" else f":{src}"
+    return f"{integ.precision}:{g.i_size}x{g.j_size}x{g.k_size}:sm{sms}{tag}"
 
 
 def _load():
@@ -66,6 +68,19 @@ def _times(integ, steps):
     return {k: v["ms"] / v["launches"] for k, v in rep.items()}
 
 
+def _try_variant(integ, kc: int, var: int) -> bool:
+    """Set a variant; False where the handle refuses it (a source term
+    pins the RK stage to variant 2)."""
+    from . import _lib
+    try:
+        integ.set_variant(kc, var)
+        return True
+    except _lib.MisoError as exc:
+        if exc.code == _lib.ERR_STATE:
+            return False
+        raise
+
+
 def apply(integ, choice: dict):
     for name, kc in CLASSES.items():
         integ.set_variant(kc, int(choice[name]))
@@ -84,12 +99,10 @@ def autotune(integ, steps: int = 2, use_cache: bool = True) -> dict:
         return dict(cache[key], cached=True)
     best = {}
     for var in range(max(len(v) for v in VARIANTS.values())):
-        for name, kc in CLASSES.items():
-            if var in VARIANTS[name]:
-                integ.set_variant(kc, var)
+        live = {name for name, kc in CLASSES.items()
+                if var in VARIANTS[name] and _try_variant(integ, kc, var)}
         for name, ms in _times(integ, steps).items():
-            if name in CLASSES and var in VARIANTS[name] and \
-                    (name not in best or ms < best[name][1]):
+            if name in live and (name not in best or ms < best[name][1]):
                 best[name] = (var, ms)
     choice = {name: v for name, (v, _) in best.items()}
     for name, kc in CLASSES.items():

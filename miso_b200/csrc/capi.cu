@@ -497,7 +497,7 @@ struct miso_b200_handle {
       FieldPtrs<const float> prev = s == 0 ? cst(H(c)) : cst(S((s - 1) & 1));
       FieldPtrs<float> out = s < 3 ? S(s & 1) : S(0);
       const int t = tb();
-      launch_s32_rk_stage(g, prev, H(c), L(c), out, sc, s, p.gm, sms, stream);
+      launch_s32_rk_stage(g, prev, H(c), L(c), out, sc, s, p.gm, src, sms, stream);
       te(t, "rk_stage", interior() * (s == 0 ? 72.0 : s < 3 ? 108.0 : 180.0));
       if ((rc = check_launch("rk_stage"))) return rc;
       if (s < 3) {
@@ -550,6 +550,8 @@ struct miso_b200_handle {
       a.tiles_j = rk_tiles_j;
       a.tiles_k = rk_tiles_k;
       a.items = rk_items;
+      a.src = src;
+      a.src_ro = st == 0 ? hi[c][RO] : stg[(st - 1) & 1][RO];
       const void *tm = st == 0 ? (const void *)tm_hi[c] : (const void *)tm_stg[(st - 1) & 1];
       const int t = tb();
       if (rk_var == 1)
@@ -976,10 +978,9 @@ int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, in
   } else if (kind == MISO_B200_SOURCE_POINT_GRAVITY) {
     if (!params || nparams < 1 || !std::isfinite(params[0]))
       return h->fail(MISO_B200_ERR_ARG, "point gravity needs its constant g in params[0]");
-    if (h->split())
-      return h->fail(MISO_B200_ERR_STATE, "source terms run in the FP64 form");
     h->src.kind = 1;
     h->src.g = params[0];
+    if (h->tiled) h->rk_var = 2;  // the pipelined RK stage carries the source on 3-D grids
   } else {
     return h->fail(MISO_B200_ERR_ARG, "unknown source kind %d", kind);
   }
@@ -1182,6 +1183,8 @@ int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
       variant > (kernel_class == 3 ? 1 : 2))
     return MISO_B200_ERR_ARG;
   if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "kernel variants apply to 3-D split grids");
+  if (kernel_class == 0 && variant != 2 && h->src.kind != 0)
+    return h->fail(MISO_B200_ERR_STATE, "with a source term the RK stage runs variant 2");
   if (kernel_class == 0)
     h->rk_var = variant;
   else

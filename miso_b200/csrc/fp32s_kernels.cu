@@ -90,7 +90,8 @@ __device__ __forceinline__ void decode_index(const Geom &g, long long lin, int &
 // hi/lo state in place (each cell reads only its own hi/lo).
 __global__ void __launch_bounds__(128)
 rk_stage_kernel(Geom g, FieldPtrs<const float> prev, FieldPtrs<float> hi, FieldPtrs<float> lo,
-                FieldPtrs<float> out, const StepScalars *__restrict__ sc, int stage, float gm1) {
+                FieldPtrs<float> out, const StepScalars *__restrict__ sc, int stage, float gm1,
+                Source src) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
   const float dt = (float)sc->dts[stage];
   const float ch2 = (float)sc->ch2;
@@ -115,6 +116,14 @@ rk_stage_kernel(Geom g, FieldPtrs<const float> prev, FieldPtrs<float> hi, FieldP
       flux(load_cons(prev, c - 2 * s), d, gm1, ch2, M2);
 #pragma unroll
       for (int f = 0; f < NF; ++f) R[f] -= ((M2[f] - P2[f]) + 8.0f * (P1[f] - M1[f])) * w;
+    }
+    if (src.kind == 1) {  // point gravity on the argument state's density
+      const float X = (float)src.x[i], Y = (float)src.y[j], Z = (float)src.z[k];
+      const float rr = sqrtf(X * X + Y * Y + Z * Z);
+      const float a = -prev.f[RO][c] * (float)src.g / (rr * rr * rr);
+      R[MX] += a * X;
+      R[MY] += a * Y;
+      R[MZ] += a * Z;
     }
     if (stage < 3) {
 #pragma unroll
@@ -346,10 +355,10 @@ static int blocks_for(long long work, int threads, int sms, int per_sm) {
 void launch_s32_rk_stage(const Geom &g, const FieldPtrs<const float> &prev,
                          const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
                          const FieldPtrs<float> &out, const StepScalars *sc, int stage, double gm,
-                         int sms, cudaStream_t st) {
+                         const Source &src, int sms, cudaStream_t st) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
   s32::rk_stage_kernel<<<blocks_for(nint, 128, sms, 16), 128, 0, st>>>(
-      g, prev, hi, lo, out, sc, stage, (float)(gm - 1.0));
+      g, prev, hi, lo, out, sc, stage, (float)(gm - 1.0), src);
 }
 
 void launch_s32_char_velocity(const Geom &g, const FieldPtrs<const float> &u, float *cc,

@@ -9,7 +9,7 @@ namespace miso_b200 {
 void launch_s32_rk_stage(const Geom &g, const FieldPtrs<const float> &prev,
                          const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
                          const FieldPtrs<float> &out, const StepScalars *sc, int stage, double gm,
-                         int sms, cudaStream_t st);
+                         const Source &src, int sms, cudaStream_t st);
 void launch_s32_char_velocity(const Geom &g, const FieldPtrs<const float> &u, float *cc,
                               double gm, double cs_fac, double vv_fac, double ca_fac, int sms,
                               cudaStream_t st);

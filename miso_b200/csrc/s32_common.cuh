@@ -130,6 +130,19 @@ __device__ __forceinline__ void speeds(const float s[NF], float gm, float gm1, f
 // ---------------------------------------------------------------------------
 // Artificial viscosity helpers (limiter.hpp:11-37)
 // ---------------------------------------------------------------------------
+// The point-gravity force per volume -ro g x / |x|^3 in FP32 at array
+// indices (i, j, k) (Source, common.cuh; demo/mhd3d_magnetosphere/src/
+// src.hpp:17-44).
+__device__ __forceinline__ void gravity_force(const Source &s, float ro, int i, int j, int k,
+                                              float &fx, float &fy, float &fz) {
+  const float X = (float)s.x[i], Y = (float)s.y[j], Z = (float)s.z[k];
+  const float rr = sqrtf(X * X + Y * Y + Z * Z);
+  const float a = -ro * (float)s.g / (rr * rr * rr);
+  fx = a * X;
+  fy = a * Y;
+  fz = a * Z;
+}
+
 // generalized minmod slope of the centre point (limiter.hpp:11-20)
 template <class V>
 __device__ __forceinline__ V dqq_t(V qq_dw, V qq_cn, V qq_up, V ep) {

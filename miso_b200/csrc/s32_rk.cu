@@ -149,7 +149,7 @@ struct Pipe {
   unsigned par;  // (seq / NBUF) & 1
 };
 
-template <int STAGE>
+template <int STAGE, bool SRC>
 __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const CUtensorMap *tm,
                                            const Item &itm, int q, V9 &Fn, const V9 &F1,
                                            const V9 &F2, V9 &Rn, const V9 &R2, Pipe &pp) {
@@ -278,6 +278,15 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
       D.p[i] = sub2(R2.p[i], mul2(k.wx2, N));
     }
     D.s = __fsub_rn(R2.s, __fmul_rn(k.wx, fmaf(-8.f, F1.s, Fn.s)));
+    if (SRC) {
+      // the source's force enters the momentum RHS: D -= force
+      const float ro = STAGE == 0 ? A0[RO] : __ldg(a.src_ro + cell);
+      float fx, fy, fz;
+      gravity_force(a.src, ro, c + g.m[0], jg + g.m[1], kg + g.m[2], fx, fy, fz);
+      D.p[0].y -= fx;  // (ro, mx)
+      D.p[1].x -= fy;  // (my, mz)
+      D.p[1].y -= fz;
+    }
     if (STAGE < 3) {
 #pragma unroll
       for (int i = 0; i < NPAIR; ++i) {
@@ -349,7 +358,7 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
   return true;
 }
 
-template <int STAGE>
+template <int STAGE, bool SRC>
 __global__ void __launch_bounds__(NTHR, 2)
 rk_pipe_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -390,11 +399,11 @@ rk_pipe_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
     const int qe = itm.i_end + 1;
     // ring slots: F(q) -> Fn, F(q-1) -> F1, F(q-2) -> F2 (R likewise)
     for (int q = itm.i_start - 2; q <= qe; q += 3) {
-      if (!plane_step<STAGE>(a, sm, &tm, itm, q, FA, FC, FB, RA, RB, pp)) return;
+      if (!plane_step<STAGE, SRC>(a, sm, &tm, itm, q, FA, FC, FB, RA, RB, pp)) return;
       if (q + 1 > qe) break;
-      if (!plane_step<STAGE>(a, sm, &tm, itm, q + 1, FB, FA, FC, RB, RC, pp)) return;
+      if (!plane_step<STAGE, SRC>(a, sm, &tm, itm, q + 1, FB, FA, FC, RB, RC, pp)) return;
       if (q + 2 > qe) break;
-      if (!plane_step<STAGE>(a, sm, &tm, itm, q + 2, FC, FB, FA, RC, RA, pp)) return;
+      if (!plane_step<STAGE, SRC>(a, sm, &tm, itm, q + 2, FC, FB, FA, RC, RA, pp)) return;
     }
   }
 }
@@ -406,23 +415,36 @@ int s32_rk_pipe_configure() {
   cudaError_t e = cudaSuccess;
 #define MISO_SET(kern) \
   if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
-  MISO_SET(s32p::rk_pipe_kernel<0>);
-  MISO_SET(s32p::rk_pipe_kernel<1>);
-  MISO_SET(s32p::rk_pipe_kernel<2>);
-  MISO_SET(s32p::rk_pipe_kernel<3>);
+  MISO_SET((s32p::rk_pipe_kernel<0, false>));
+  MISO_SET((s32p::rk_pipe_kernel<1, false>));
+  MISO_SET((s32p::rk_pipe_kernel<2, false>));
+  MISO_SET((s32p::rk_pipe_kernel<3, false>));
+  MISO_SET((s32p::rk_pipe_kernel<0, true>));
+  MISO_SET((s32p::rk_pipe_kernel<1, true>));
+  MISO_SET((s32p::rk_pipe_kernel<2, true>));
+  MISO_SET((s32p::rk_pipe_kernel<3, true>));
 #undef MISO_SET
   return e == cudaSuccess ? 0 : -1;
 }
 
-void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st) {
-  const CUtensorMap &m = *(const CUtensorMap *)tm;
+template <bool SRC>
+static void launch_pipe(const CUtensorMap &m, const RkArgs &a, int stage, int grid,
+                        cudaStream_t st) {
   const size_t smem = sizeof(s32p::PipeSmem);
   switch (stage) {
-    case 0: s32p::rk_pipe_kernel<0><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
-    case 1: s32p::rk_pipe_kernel<1><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
-    case 2: s32p::rk_pipe_kernel<2><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
-    default: s32p::rk_pipe_kernel<3><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
+    case 0: s32p::rk_pipe_kernel<0, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
+    case 1: s32p::rk_pipe_kernel<1, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
+    case 2: s32p::rk_pipe_kernel<2, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
+    default: s32p::rk_pipe_kernel<3, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
   }
+}
+
+void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st) {
+  const CUtensorMap &m = *(const CUtensorMap *)tm;
+  if (a.src.kind != 0)
+    launch_pipe<true>(m, a, stage, grid, st);
+  else
+    launch_pipe<false>(m, a, stage, grid, st);
 }
 
 }  // namespace miso_b200

@@ -21,6 +21,8 @@ struct RkArgs {
   float gm, gm1, cs_fac, vv_fac, ca_fac;
   int L;  // planes per work item along i
   int tiles_j, tiles_k, items;
+  Source src;           // built-in source term (kind 0: none)
+  const float *src_ro;  // density of the stage's argument state (the source's ro)
 };
 
 // Arguments of one artificial-viscosity sweep launch.

@@ -21,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libmiso_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmiso_ref.so")
+REF_F32_SO = os.path.join(HERE, "_ref", "libmiso_ref_f32.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -156,12 +157,27 @@ class Reference(_Lib):
     prefix = "miso_ref_"
     path = REF_SO
 
+    def update(self, prob, q, dt):
+        """One step of ``q`` in place with the given dt (Integrator::update)."""
+        f = self.lib.miso_ref_update
+        f.argtypes = [ctypes.POINTER(Desc), ctypes.c_void_p, ctypes.c_double]
+        f.restype = ctypes.c_int
+        d = make_desc(prob.grid, prob.config, prob.sign)
+        rc = f(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p), float(dt))
+        if rc:
+            raise RuntimeError(f"{self.prefix}update failed: {rc}")
+
     def symmetric_index(self, i, i_total, i_margin, outer):
         f = self.lib.miso_ref_symmetric_index
         f.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(ctypes.c_int)] * 2
         g, t = ctypes.c_int(), ctypes.c_int()
         f(i, i_total, i_margin, int(outer), ctypes.byref(g), ctypes.byref(t))
         return g.value, t.value
+
+
+class ReferenceF32(Reference):
+    """The reference's integrator built with Real = float, as its demos are."""
+    path = REF_F32_SO
 
 
 def reference_available() -> bool:

@@ -28,7 +28,15 @@
 #include "miso_oracle.h"
 
 using namespace miso;
+// The reference is templated on Real: double by default, float for the
+// build that mirrors its demos (compiled with -DMISO_REF_FLOAT).  The C
+// entry points always exchange double arrays; a float build converts on the
+// way in and out (float -> double -> float is exact).
+#ifdef MISO_REF_FLOAT
+using Real = float;
+#else
 using Real = double;
+#endif
 using B = backend::Host;
 
 namespace {
@@ -136,14 +144,14 @@ void to_fields(mhd::Fields<Real, B> &qq, double *const q[9]) {
   Array3D<Real, B> *f[9] = {&qq.ro, &qq.vx, &qq.vy, &qq.vz, &qq.bx,
                             &qq.by, &qq.bz, &qq.ei, &qq.ph};
   for (int v = 0; v < 9; ++v)
-    std::memcpy(f[v]->data(), q[v], sizeof(double) * f[v]->size());
+    for (size_t n = 0; n < f[v]->size(); ++n) f[v]->data()[n] = (Real)q[v][n];
 }
 
 void from_fields(const mhd::Fields<Real, B> &qq, double *const q[9]) {
   const Array3D<Real, B> *f[9] = {&qq.ro, &qq.vx, &qq.vy, &qq.vz, &qq.bx,
                                   &qq.by, &qq.bz, &qq.ei, &qq.ph};
   for (int v = 0; v < 9; ++v)
-    std::memcpy(q[v], f[v]->data(), sizeof(double) * f[v]->size());
+    for (size_t n = 0; n < f[v]->size(); ++n) q[v][n] = (double)f[v]->data()[n];
 }
 
 } // namespace
@@ -170,6 +178,25 @@ int miso_ref_run(const miso_oracle_desc *d, double *const q[9], int nsteps, int 
     return 0;
   } catch (const std::exception &e) {
     std::fprintf(stderr, "miso_ref_run: %s\n", e.what());
+    return -1;
+  }
+}
+
+/* One step (update) with a given dt, as ModelBase::update does after cfl. */
+int miso_ref_update(const miso_oracle_desc *d, double *const q[9], double dt) {
+  try {
+    Session s(*d);
+    mhd::Fields<Real, B> qq(*s.grid);
+    to_fields(qq, q);
+    PointGravity grav(*s.grid, (Real)d->g_grav);
+    if (d->source == 1)
+      s.integ->update((Real)dt, *s.eos, *s.bc, grav, qq);
+    else
+      s.integ->update((Real)dt, *s.eos, *s.bc, s.src, qq);
+    from_fields(qq, q);
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "miso_ref_update: %s\n", e.what());
     return -1;
   }
 }

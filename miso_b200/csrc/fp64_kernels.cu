@@ -87,6 +87,189 @@ av_sweep_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<double> r,
   }
 }
 
+// A viscosity sweep marching along the sweep axis: a warp owns 32
+// neighbouring lines (along `lane_ax`) and walks a chunk of L cells of them
+// along `dir`, carrying the limited variables, their slopes and the face
+// fluxes of the previous cells in registers, so each slope and each face
+// flux is formed once instead of three and two times.  The arguments of
+// every dqq_eval and flux_core call are the per-cell sweep's (av_cell), so
+// every output is bit for bit the same.  Interior cells only; ghost cells
+// along `dir` are read as neighbours.
+__device__ __forceinline__ void av_load_w(const FieldPtrs<const double> &q, const double *cc,
+                                          long long c, double w[NF], double &ccv) {
+  const double ro = __ldg(q.f[RO] + c);
+  w[0] = ro;
+  w[1] = ro * __ldg(q.f[VX] + c);
+  w[2] = ro * __ldg(q.f[VY] + c);
+  w[3] = ro * __ldg(q.f[VZ] + c);
+  w[4] = __ldg(q.f[BX] + c);
+  w[5] = __ldg(q.f[BY] + c);
+  w[6] = __ldg(q.f[BZ] + c);
+  w[7] = __ldg(q.f[PH] + c);
+  w[8] = ro * __ldg(q.f[EI] + c);
+  ccv = __ldg(cc + c);
+}
+
+__global__ void __launch_bounds__(128)
+av_march_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<double> r,
+                const double *__restrict__ cc, const StepScalars *__restrict__ sc, int dir,
+                int lane_ax, int line_ax, double ep, double fh, int L) {
+  const long long sD = g.st[dir], sL = g.st[lane_ax], sU = g.st[line_ax];
+  const int nD = g.n[dir], nL = g.n[lane_ax], nU = g.n[line_ax];
+  const int lane = threadIdx.x & 31;
+  const int lblocks = (nL + 31) / 32;
+  const int chunks = (nD + L - 1) / L;
+  const long long items = (long long)lblocks * nU * chunks;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const double dt = sc->dt, dsi = g.dsi[dir];
+  for (long long wi = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < items;
+       wi += nw) {
+    const int lb = (int)(wi % lblocks);
+    const long long r1 = wi / lblocks;
+    const int u = (int)(r1 % nU);
+    const int t0 = (int)(r1 / nU) * L;
+    const int t1 = min(nD, t0 + L);
+    const int l = lb * 32 + lane;
+    const bool active = l < nL;
+    const int lc = min(l, nL - 1);  // idle lanes shadow the last line; their values go unused
+    const long long base = (long long)(lc + g.m[lane_ax]) * sL +
+                           (long long)(u + g.m[line_ax]) * sU + (long long)g.m[dir] * sD;
+    // prologue: cells t0-2 .. t0+1 give the slopes at t0-1, t0 and the flux
+    // through the face between t0-1 and t0
+    double w0[NF], w1[NF], dq0[NF], F0[NF], cc0, cc1;
+    {
+      double wa[NF], wb[NF], cca, ccb;
+      av_load_w(q, cc, base + (long long)(t0 - 2) * sD, wa, cca);
+      av_load_w(q, cc, base + (long long)(t0 - 1) * sD, wb, ccb);
+      av_load_w(q, cc, base + (long long)t0 * sD, w0, cc0);
+      av_load_w(q, cc, base + (long long)(t0 + 1) * sD, w1, cc1);
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
+        const double dqm = dqq_eval(wa[n], wb[n], w0[n], ep);
+        dq0[n] = dqq_eval(wb[n], w0[n], w1[n], ep);
+        F0[n] = flux_core(wb[n], w0[n], dqm, dq0[n], 0.5 * (ccb + cc0), fh);
+      }
+    }
+    for (int t = t0; t < t1; ++t) {
+      const long long c = base + (long long)t * sD;
+      double wp[NF], ccp;
+      av_load_w(q, cc, c + 2 * sD, wp, ccp);
+      double dF[NF];
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
+        const double dq1 = dqq_eval(w0[n], w1[n], wp[n], ep);
+        const double F1 = flux_core(w0[n], w1[n], dq0[n], dq1, 0.5 * (cc0 + cc1), fh);
+        dF[n] = F1 - F0[n];
+        F0[n] = F1;
+        dq0[n] = dq1;
+      }
+      if (active) {
+        // the per-cell sweep's update (av_cell), cell t holding w0
+        const double ro_c = w0[0];
+        const double ro = ro_c - dF[0] * dsi * dt;
+        double v[3], b[3];
+#pragma unroll
+        for (int e = 0; e < 3; ++e) v[e] = (w0[1 + e] - dF[1 + e] * dsi * dt) / ro;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) b[e] = w0[4 + e] - dF[4 + e] * dsi * dt;
+        const double ph = w0[7] - dF[7] * dsi * dt;
+        const double ei_c = __ldg(q.f[EI] + c);
+        const double vx_c = __ldg(q.f[VX] + c), vy_c = __ldg(q.f[VY] + c),
+                     vz_c = __ldg(q.f[VZ] + c);
+        const double Et = ro_c * ei_c + 0.5 * ro_c * (vx_c * vx_c + vy_c * vy_c + vz_c * vz_c) +
+                          PII8 * (w0[4] * w0[4] + w0[5] * w0[5] + w0[6] * w0[6]);
+        const double ei = (Et - dF[8] * dsi * dt -
+                           0.5 * ro * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) -
+                           PII8 * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2])) / ro;
+        r.f[RO][c] = ro;
+        r.f[VX][c] = v[0];
+        r.f[VY][c] = v[1];
+        r.f[VZ][c] = v[2];
+        r.f[BX][c] = b[0];
+        r.f[BY][c] = b[1];
+        r.f[BZ][c] = b[2];
+        r.f[EI][c] = ei;
+        r.f[PH][c] = ph;
+      }
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
+        w0[n] = w1[n];
+        w1[n] = wp[n];
+      }
+      cc0 = cc1;
+      cc1 = ccp;
+    }
+  }
+}
+
+// The z sweep (the contiguous axis): a warp loads 32 consecutive cells of a
+// row and updates the inner 28; each lane forms the slope and the upper
+// face flux of its own cell once and takes its neighbours' by warp
+// shuffles -- the same dqq_eval and flux_core arguments as the per-cell
+// sweep, so every output is bit for bit the same.
+__global__ void __launch_bounds__(128)
+av_z_shfl_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<double> r,
+                 const double *__restrict__ cc, const StepScalars *__restrict__ sc, double ep,
+                 double fh) {
+  const int lane = threadIdx.x & 31;
+  const int nk = g.n[2];
+  const int segs = (nk + 27) / 28;
+  const long long work = (long long)g.n[0] * g.n[1] * segs;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const double dt = sc->dt, dsi = g.dsi[2];
+  for (long long wi = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < work;
+       wi += nw) {
+    const int sg = (int)(wi % segs);
+    const long long row = wi / segs;
+    const int j = (int)(row % g.n[1]) + g.m[1];
+    const int i = (int)(row / g.n[1]) + g.m[0];
+    const int k = sg * 28 + lane - 2;  // interior k of this lane (-2 .. nk+1 read)
+    const int kc = min(k, nk + 1);
+    const long long c = i * g.st[0] + j * g.st[1] + kc + g.m[2];
+    double w[NF], ccv;
+    av_load_w(q, cc, c, w, ccv);
+    const double cc_up = __shfl_down_sync(0xffffffffu, ccv, 1);
+    double dF[NF];
+#pragma unroll
+    for (int n = 0; n < NF; ++n) {
+      const double wm = __shfl_up_sync(0xffffffffu, w[n], 1);
+      const double wp = __shfl_down_sync(0xffffffffu, w[n], 1);
+      const double dq = dqq_eval(wm, w[n], wp, ep);
+      const double dq_up = __shfl_down_sync(0xffffffffu, dq, 1);
+      const double Fup = flux_core(w[n], wp, dq, dq_up, 0.5 * (ccv + cc_up), fh);
+      const double Fdw = __shfl_up_sync(0xffffffffu, Fup, 1);
+      dF[n] = Fup - Fdw;
+    }
+    if (lane >= 2 && lane < 30 && k < nk) {
+      const double ro_c = w[0];
+      const double ro = ro_c - dF[0] * dsi * dt;
+      double v[3], b[3];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) v[e] = (w[1 + e] - dF[1 + e] * dsi * dt) / ro;
+#pragma unroll
+      for (int e = 0; e < 3; ++e) b[e] = w[4 + e] - dF[4 + e] * dsi * dt;
+      const double ph = w[7] - dF[7] * dsi * dt;
+      const double ei_c = __ldg(q.f[EI] + c);
+      const double vx_c = __ldg(q.f[VX] + c), vy_c = __ldg(q.f[VY] + c),
+                   vz_c = __ldg(q.f[VZ] + c);
+      const double Et = ro_c * ei_c + 0.5 * ro_c * (vx_c * vx_c + vy_c * vy_c + vz_c * vz_c) +
+                        PII8 * (w[4] * w[4] + w[5] * w[5] + w[6] * w[6]);
+      const double ei = (Et - dF[8] * dsi * dt -
+                         0.5 * ro * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) -
+                         PII8 * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2])) / ro;
+      r.f[RO][c] = ro;
+      r.f[VX][c] = v[0];
+      r.f[VY][c] = v[1];
+      r.f[VZ][c] = v[2];
+      r.f[BX][c] = b[0];
+      r.f[BY][c] = b[1];
+      r.f[BZ][c] = b[2];
+      r.f[EI][c] = ei;
+      r.f[PH][c] = ph;
+    }
+  }
+}
+
 // ----------------------------------------------------------------------
 // CFL (mhd_integrator_host.hpp:303-334): per-block float-rounded minimum of
 // cfl * min3(dx,dy,dz) / (cs + |v| + ca) over the interior, then one block
@@ -242,6 +425,21 @@ void launch_fp64_av_sweep(const Geom &g, const FieldPtrs<const double> &q,
                           const FieldPtrs<double> &r, const double *cc, const StepScalars *sc,
                           int dir, double ep, double fh, int sms, cudaStream_t st) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
+  // the marching sweep wherever the sweep axis and a lane axis are real;
+  // the per-cell sweep elsewhere (a degenerate sweep still rounds: v =
+  // (ro v) / ro)
+  const int lane_ax = dir == 2 ? -1 : (g.s[2] ? 2 : (dir == 0 ? 1 : 0));
+  if (dir == 2 && g.s[2] && g.n[2] >= 4) {
+    fp64::av_z_shfl_kernel<<<sms * 8, 128, 0, st>>>(g, q, r, cc, sc, ep, fh);
+    return;
+  }
+  if (dir < 2 && g.s[dir] && lane_ax >= 0 && g.s[lane_ax] && g.n[dir] >= 4) {
+    const int line_ax = 3 - dir - lane_ax;
+    const int L = 64;
+    fp64::av_march_kernel<<<sms * 8, 128, 0, st>>>(g, q, r, cc, sc, dir, lane_ax, line_ax, ep,
+                                                   fh, L);
+    return;
+  }
   fp64::av_sweep_kernel<<<grid_blocks(nint, 128, sms, 16), 128, 0, st>>>(g, q, r, cc, sc, dir,
                                                                            ep, fh);
 }

@@ -10,7 +10,6 @@ GPU: the demo's FP64 result equals the oracle bit for bit, in the default
 import os
 import shutil
 import subprocess
-import sys
 
 import numpy as np
 import pytest

@@ -1,7 +1,6 @@
 """The split form against the reference's own Real = float build (the type
 its demos use), both measured against the Real = double build stepped with
 the same dt sequence: the split form's error must be the smaller one."""
-import numpy as np
 import pytest
 
 from conftest import interior, rel_l1

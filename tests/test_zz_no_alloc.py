@@ -12,7 +12,6 @@ already run every other test; it passes alone in a fresh process as well.
 """
 import ctypes
 
-import numpy as np
 import pytest
 
 from miso_b200 import _lib

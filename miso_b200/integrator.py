@@ -13,8 +13,10 @@ the fields and forwards ``cfl``/``update``.  The equation of state, the
 boundary condition and the source term are the built-in ones the reference's
 MHD demos use: ideal gas with ``eos.gm``; periodic faces where
 ``domain.periodic`` says so and the symmetric mirror (per-field sign) on the
-other faces; no source.  Every call goes through ``libmiso_b200.so``;
-nothing here computes on the CPU.
+other faces; no source, or the magnetosphere demo's point gravity when
+``source.kind`` is ``"point_gravity"`` (``source.g`` its acceleration).
+Every call goes through ``libmiso_b200.so``; nothing here computes on the
+CPU.
 """
 from __future__ import annotations
 
@@ -117,23 +119,7 @@ class Integrator:
         self.bc = BuiltinBoundary(sign)
         self.src = EmptySourceTerm()
         lib = _lib.load()
-        gd = _lib.GridDesc()
-        gd.i_size, gd.j_size, gd.k_size, gd.margin = (grid.i_size, grid.j_size, grid.k_size,
-                                                      grid.margin)
-        gd.x_min, gd.x_max, gd.y_min, gd.y_max = grid.x_min, grid.x_max, grid.y_min, grid.y_max
-        gd.z_min, gd.z_max = grid.z_min, grid.z_max
-        per = cfg["domain"]["periodic"]
-        gd.periodic[0], gd.periodic[1], gd.periodic[2] = (int(per["x"]), int(per["y"]),
-                                                          int(per["z"]))
-        for n, v in enumerate(self.bc.sign.reshape(-1)):
-            gd.sign[n] = float(v)
-        pp = _lib.Params()
-        av = cfg["mhd"]["artificial_viscosity"]
-        pp.gm = cfg["eos"]["gm"]
-        pp.cfl_number = cfg["mhd"]["cfl_number"]
-        pp.ep, pp.fh = av["ep"], av["fh"]
-        pp.cs_fac, pp.ca_fac, pp.vv_fac = av["cs_fac"], av["ca_fac"], av["vv_fac"]
-        pp.precision = PRECISIONS[precision]
+        gd, pp = make_descs(cfg, grid, sign=self.bc.sign, precision=precision)
         h = ctypes.c_void_p()
         _lib.check(lib.miso_b200_create(ctypes.byref(gd), ctypes.byref(pp),
                                         ctypes.c_void_p(stream or 0), ctypes.byref(h)), None)

@@ -144,8 +144,8 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
  * volume -ro g x / |x|^3 about the coordinate origin, params[0] = g, no
  * heating.  Both forms: FP64 bit for bit as the reference adds it; in the
  * FP32 split form the force is formed in FP32 and the 3-D RK stage runs
- * variant 2 (set_variant of another RK variant is refused while a source
- * is on).  Every cell centre must lie off the origin. */
+ * variant 2 or 3 (set_variant of another RK variant is refused while a
+ * source is on).  Every cell centre must lie off the origin. */
 #define MISO_B200_SOURCE_NONE 0
 #define MISO_B200_SOURCE_POINT_GRAVITY 1
 int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, int nparams);
@@ -193,10 +193,15 @@ int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
  * kernel_class 0 = Runge-Kutta stage, 1/2/3 = viscosity sweep x/y/z;
  * variant 0 = tiled (TMA plane tiles / streaming lines fed by a producer
  * warp / warp-shuffle rows), 1 = flat (one thread per cell), 2 = pipelined
- * (Runge-Kutta stage: TMA planes with packed FP32x2 differences, the
- * default; x / y sweeps: one warp per line segment marching along the sweep
- * axis; none for z).  All compute the same step; the autotuner
- * (miso_b200/autotune.py) times them and keeps the fastest.
+ * (Runge-Kutta stage: TMA planes with packed FP32x2 differences; x / y
+ * sweeps: one warp per line segment marching along the sweep axis; none
+ * for z), 3 (Runge-Kutta stage only, the default) = variant 2 with the last
+ * stage's update deferred into the x sweep: that stage writes its
+ * right-hand side and the x sweep forms the new state from it as it streams
+ * the state in (this needs x sweep variant 0 and no flat sweep; otherwise
+ * it runs as variant 2).  All compute the same step up to FP32 rounding
+ * order; the autotuner (miso_b200/autotune.py) times them and keeps the
+ * fastest.
  * ERR_STATE on grids that use the simple per-cell kernels only. */
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant);
 int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant);

@@ -6,6 +6,9 @@ and z viscosity sweeps, each as a tiled kernel (TMA plane tiles, streaming
 lines, warp-shuffle rows) or a flat one (one thread per cell), and for the
 Runge-Kutta stage also the pipelined plane kernel -- and a few
 work-item lengths along the march axis, and keeps the fastest of each.
+Where the pipelined RK stage and the line x sweep win, it also times the
+pipelined stage with its last update deferred into the x sweep (RK variant
+3), which moves work from one class to the other, on the whole step.
 Results are cached in a JSON file keyed by precision, grid shape and SM
 count ($MISO_B200_TUNE_CACHE, default ~/.cache/miso_b200/tune.json), so a
 later run of the same shape skips the search.
@@ -20,8 +23,11 @@ import os
 
 CLASSES = {"rk_stage": 0, "av_x": 1, "av_y": 2, "av_z": 3}
 # variants per class: 0 tiled, 1 flat, 2 pipelined (RK: planes with packed
-# differences; x / y sweeps: one warp per line segment marching along the axis)
-VARIANTS = {"rk_stage": (0, 1, 2), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1)}
+# differences; x / y sweeps: one warp per line segment marching along the
+# axis); RK 3: variant 2 with the last stage's update deferred into the x
+# sweep (compared on the whole step, not per class)
+VARIANTS = {"rk_stage": (0, 1, 2, 3), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1)}
+PER_CLASS = {"rk_stage": (0, 1, 2), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1)}
 CHUNKS = (32, 64, 128)
 
 
@@ -68,6 +74,11 @@ def _times(integ, steps):
     return {k: v["ms"] / v["launches"] for k, v in rep.items()}
 
 
+def _step_ms(t: dict) -> float:
+    return (t.get("rk_stage", 0) * 4 + t.get("av_x", 0) + t.get("av_y", 0) +
+            t.get("av_z", 0))
+
+
 def _try_variant(integ, kc: int, var: int) -> bool:
     """Set a variant; False where the handle refuses it (a source term
     pins the RK stage to variant 2)."""
@@ -98,23 +109,34 @@ def autotune(integ, steps: int = 2, use_cache: bool = True) -> dict:
         apply(integ, cache[key])
         return dict(cache[key], cached=True)
     best = {}
-    for var in range(max(len(v) for v in VARIANTS.values())):
+    for var in range(max(len(v) for v in PER_CLASS.values())):
         live = {name for name, kc in CLASSES.items()
-                if var in VARIANTS[name] and _try_variant(integ, kc, var)}
+                if var in PER_CLASS[name] and _try_variant(integ, kc, var)}
         for name, ms in _times(integ, steps).items():
             if name in live and (name not in best or ms < best[name][1]):
                 best[name] = (var, ms)
     choice = {name: v for name, (v, _) in best.items()}
     for name, kc in CLASSES.items():
         integ.set_variant(kc, choice[name])
+    if choice["rk_stage"] == 2 and choice["av_x"] == 0 and 1 not in (choice["av_y"],
+                                                                      choice["av_z"]):
+        # the deferred last stage: cheaper RK stages, a dearer x sweep
+        t2 = _times(integ, steps)
+        integ.set_variant(0, 3)
+        t3 = _times(integ, steps)
+        if _step_ms(t3) < _step_ms(t2):
+            choice["rk_stage"] = 3
+            best["rk_stage"] = (3, t3["rk_stage"])
+            best["av_x"] = (0, t3["av_x"])
+        else:
+            integ.set_variant(0, 2)
     # work-item lengths for the winning variants
     chunk_best = None
     for rk_chunk in CHUNKS:
         for av_chunk in CHUNKS:
             integ.set_chunks(rk_chunk, av_chunk)
             t = _times(integ, 1)
-            total = t.get("rk_stage", 0) * 4 + t.get("av_x", 0) + t.get("av_y", 0) + \
-                t.get("av_z", 0)
+            total = _step_ms(t)
             if chunk_best is None or total < chunk_best[0]:
                 chunk_best = (total, rk_chunk, av_chunk)
     choice["rk_chunk"], choice["av_chunk"] = chunk_best[1], chunk_best[2]

@@ -162,6 +162,7 @@ struct miso_b200_handle {
   alignas(64) unsigned char tm_avh[2][128];  // AV line maps of hi[set]
   alignas(64) unsigned char tm_avl[2][128];  // AV line maps of lo[set]
   alignas(64) unsigned char tm_avc[128];     // AV line map of the characteristic speed
+  alignas(64) unsigned char tm_avd[128];     // AV line map of stg[1] (deferred last-stage D)
   long long pitch = 0;                       // elements between consecutive field arrays
   int rk_L = 64, rk_tiles_j = 0, rk_tiles_k = 0, rk_items = 0, rk_grid = 0;
   int av_L = 128, av_grid = 0, z_grid = 0;
@@ -178,7 +179,7 @@ struct miso_b200_handle {
   // tiles / streaming lines), 1 = flat (one thread per cell); 2: RK =
   // pipelined TMA planes with packed FP32x2 differences (default), x / y
   // sweeps = one warp per line segment marching along the sweep axis
-  int rk_var = 2;
+  int rk_var = 3;  // pipelined stages, the last update deferred into the x sweep
   int av_var[3] = {0, 0, 0};
   double *mon_partial = nullptr;
   int mon_blocks = 0;
@@ -528,16 +529,26 @@ struct miso_b200_handle {
   // Tiled FP32-split step: 4 RK stage launches and 3 viscosity sweeps; ghost
   // images, the characteristic speed and the next step's CFL minima are
   // written by those kernels themselves.
+  // RK variant 3: the pipelined stages with the last stage's update deferred
+  // into the x line sweep (rk_pipe_kernel<4> writes its right-hand side D to
+  // stg[1]; av_line_kernel<0, true> forms U^{n+1} from hi, lo and D as it
+  // streams them).  Needs the line x sweep and no flat sweep, which would
+  // read the images of U^{n+1} and its speed.
+  bool defer_last() const {
+    return rk_var == 3 && av_var[0] == 0 && av_var[1] != 1 && av_var[2] != 1;
+  }
+
   int enqueue_update_tiled() {
     int rc;
     const int c = cur;
+    const bool defer = defer_last();
     for (int st = 0; st < 4; ++st) {
       RkArgs a;
       a.g = g;
       a.u0 = cfs(hi[c]);
       a.hi = fs(hi[c]);
       a.lo = fs(lo[c]);
-      a.out = fs(stg[st & 1]);
+      a.out = fs(defer && st == 3 ? stg[1] : stg[st & 1]);
       a.cc = cc32;
       a.sc = sc;
       a.err = &sc->err;
@@ -557,14 +568,15 @@ struct miso_b200_handle {
       if (rk_var == 1)
         launch_s32_rk_flat(st == 0 ? cfs(hi[c]) : cfs(stg[(st - 1) & 1]), a, st, flat_grid,
                            stream);
-      else if (rk_var == 2)
-        launch_s32_rk_pipe(tm, a, st, rk_grid, stream);
+      else if (rk_var >= 2)
+        launch_s32_rk_pipe(tm, a, defer && st == 3 ? 4 : st, rk_grid, stream);
 
       else
         launch_s32_rk_tiled(tm, a, st, rk_grid, stream);
-      te(t, "rk_stage", interior() * (st == 0 ? 72.0 : st < 3 ? 108.0 : 184.0));
+      te(t, "rk_stage",
+         interior() * (st == 0 || (defer && st == 3) ? 72.0 : st < 3 ? 108.0 : 184.0));
       if ((rc = check_launch("rk_stage"))) return rc;
-      if (rk_var == 2) {  // interior-only writer: fill the images read next
+      if (rk_var >= 2) {  // interior-only writer: fill the images read next
         if (st < 3) {
           // the next stage's star stencil reads face ghosts only
           if ((rc = shell(stg[st & 1], SHELL_FACES))) return rc;
@@ -575,8 +587,12 @@ struct miso_b200_handle {
         }
       }
       // a shard's i ghosts of the stage output (and of hi and cc after the
-      // last stage, read by the x sweep) come from the neighbours
-      if ((rc = st < 3 ? halo_f(stg[st & 1]) : halo_f(hi[c], nullptr, cc32))) return rc;
+      // last stage, read by the x sweep; of D when the update is deferred:
+      // the U^n ghosts are current since the last step's exchange) come from
+      // the neighbours
+      if ((rc = st < 3 || defer ? halo_f(stg[defer && st == 3 ? 1 : st & 1])
+                                : halo_f(hi[c], nullptr, cc32)))
+        return rc;
     }
     for (int d = 0; d < 3; ++d) {
       AvArgs a;
@@ -595,16 +611,23 @@ struct miso_b200_handle {
       a.gm1 = (float)(p.gm - 1.0);
       a.cfl_dx = (float)cfl_dx;
       a.L = av_L;
+      a.cc_out = cc32;
+      a.cs_fac = (float)p.cs_fac;
+      a.vv_fac = (float)p.vv_fac;
+      a.ca_fac = (float)p.ca_fac;
       const int t = tb();
       if (av_var[d] == 1)
         launch_s32_av_flat(a, d, flat_grid, stream);
       else if (av_var[d] == 2 && d < 2)
         launch_s32_av_march(a, d, avp_grid, stream);
+      else if (d == 0 && defer)
+        launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avd, a, 0, true, av_grid, stream);
       else if (d < 2)
-        launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, av_grid, stream);
+        launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, false, av_grid, stream);
       else
         launch_s32_av_z(a, z_grid, stream);
-      te(t, d == 0 ? "av_x" : d == 1 ? "av_y" : "av_z", interior() * 148.0);
+      te(t, d == 0 ? "av_x" : d == 1 ? "av_y" : "av_z",
+         interior() * (d == 0 && defer ? 184.0 : 148.0));
       if ((rc = check_launch("av_sweep"))) return rc;
       // interior-only writers (line, march and z sweeps): the step's final
       // state gets every hi image; within the step only a flat sweep reads
@@ -805,6 +828,7 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
            s32_make_tmap(g, h->lo[s][0], pb, 1, h->tm_avl[s]) == 0;
     }
     if (ok) ok = s32_make_tmap_cc(g, h->cc32, h->tm_avc) == 0;
+    if (ok) ok = s32_make_tmap(g, h->stg[1][0], pb, 1, h->tm_avd) == 0;
     if (ok) {
       h->tiled = true;
       s32_rk_items(g, h->rk_L, h->rk_tiles_j, h->rk_tiles_k, h->rk_items);
@@ -818,7 +842,10 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
       }
       h->flat_grid = 3 * h->sms;  // 256 threads x 80 registers: 3 resident CTAs per SM
       if (const char *v = getenv("MISO_B200_RK"))
-        h->rk_var = strcmp(v, "flat") == 0 ? 1 : strcmp(v, "tiled") == 0 ? 0 : 2;
+        h->rk_var = strcmp(v, "flat") == 0    ? 1
+                    : strcmp(v, "tiled") == 0 ? 0
+                    : strcmp(v, "pipe") == 0  ? 2
+                                              : 3;
       if (const char *v = getenv("MISO_B200_AV"))
         for (int d = 0; d < 3 && v[d]; ++d)
           h->av_var[d] = v[d] == 'f' ? 1 : (v[d] == 'p' && d < 2) ? 2 : 0;
@@ -980,7 +1007,8 @@ int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, in
       return h->fail(MISO_B200_ERR_ARG, "point gravity needs its constant g in params[0]");
     h->src.kind = 1;
     h->src.g = params[0];
-    if (h->tiled) h->rk_var = 2;  // the pipelined RK stage carries the source on 3-D grids
+    // the pipelined RK stage carries the source on 3-D grids
+    if (h->tiled && h->rk_var < 2) h->rk_var = 2;
   } else {
     return h->fail(MISO_B200_ERR_ARG, "unknown source kind %d", kind);
   }
@@ -1180,11 +1208,11 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]) {
 
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
   if (!h || kernel_class < 0 || kernel_class > 3 || variant < 0 ||
-      variant > (kernel_class == 3 ? 1 : 2))
+      variant > (kernel_class == 0 ? 3 : kernel_class == 3 ? 1 : 2))
     return MISO_B200_ERR_ARG;
   if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "kernel variants apply to 3-D split grids");
-  if (kernel_class == 0 && variant != 2 && h->src.kind != 0)
-    return h->fail(MISO_B200_ERR_STATE, "with a source term the RK stage runs variant 2");
+  if (kernel_class == 0 && variant < 2 && h->src.kind != 0)
+    return h->fail(MISO_B200_ERR_STATE, "with a source term the RK stage runs variant 2 or 3");
   if (kernel_class == 0)
     h->rk_var = variant;
   else

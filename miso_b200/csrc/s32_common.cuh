@@ -115,6 +115,31 @@ __device__ __forceinline__ void two_sum(V a, V b, V &s, V &e) {
   e = vadd(vsub(a, vsub(s, bb)), vsub(b, bb));
 }
 
+// The last Runge-Kutta stage's closing pieces, written with explicitly
+// rounded operations so that every kernel that forms them (the stage
+// itself, or the x sweep it is deferred into) gets the same bits.
+//   ph: (sv, t) = two_sum(hi, lo - dt D) is damped by `decay` into the pair
+//   (sv, e) = two_sum(sv * decay, fma(sv, decay, -sv * decay) + t * decay)
+__device__ __forceinline__ void ph_damp(float sv, float t, float decay, float &s, float &e) {
+  const float pr = __fmul_rn(sv, decay);
+  const float pe = __fmaf_rn(sv, decay, -pr);
+  two_sum(pr, __fmaf_rn(t, decay, pe), s, e);
+}
+// characteristic speed cs_fac cs + vv_fac |v| + ca_fac ca of a state with
+// density ro, |m|^2 = mm, |B|^2 = bb and total energy et
+__device__ __forceinline__ float char_speed(float ro, float mm, float bb, float et, float gm,
+                                            float gm1, float cs_fac, float vv_fac,
+                                            float ca_fac) {
+  const float inv = 1.0f / ro;
+  const float kin = __fmul_rn(__fmul_rn(0.5f, mm), inv);
+  const float mag = __fmul_rn(bb, FPII8);
+  const float ein = __fmul_rn(__fsub_rn(__fsub_rn(et, kin), mag), inv);
+  const float cs = sqrtf(fmaxf(__fmul_rn(__fmul_rn(gm, gm1), ein), 0.0f));
+  const float vv = __fmul_rn(sqrtf(mm), inv);
+  const float ca = sqrtf(__fmul_rn(__fmul_rn(bb, inv), FPII4));
+  return __fmaf_rn(ca, ca_fac, __fmaf_rn(vv, vv_fac, __fmul_rn(cs, cs_fac)));
+}
+
 // characteristic-speed pieces of a conserved state
 __device__ __forceinline__ void speeds(const float s[NF], float gm, float gm1, float &cs,
                                        float &vv, float &ca, float &ein) {

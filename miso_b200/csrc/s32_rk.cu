@@ -33,6 +33,13 @@
 // Physics: flux form of mhd_integrator_host.hpp:57-247 (Integrator::
 // update_sc4) with the stage factors of runge_kutta_4step
 // (mhd_integrator_host.hpp:258-277) and the GLM damping of ph.
+//
+// STAGE 0-3 are the four stages.  STAGE 4 is the last stage with its update
+// deferred: it writes the stage's right-hand side D (source included) to
+// `out` and reads no centre values; the x viscosity sweep then forms
+// U^{n+1} = (hi, lo) - dt_4 D plane by plane as it streams the state in
+// (av_line_kernel<0, true>), which saves the step one write and one read of
+// the full split state.
 #include <cuda.h>
 
 #include "common.cuh"
@@ -168,7 +175,7 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
   // 1.3x slower: the lines do not survive in L1 next to 190 KB of shared
   // memory per SM)
   float A0[NF], A1[NF];
-  if (out_ok) {
+  if (STAGE < 4 && out_ok) {
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
       if (STAGE < 3) {
@@ -287,7 +294,15 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
       D.p[1].x -= fy;  // (my, mz)
       D.p[1].y -= fz;
     }
-    if (STAGE < 3) {
+    if (STAGE == 4) {
+      // deferred update: the right-hand side itself
+#pragma unroll
+      for (int i = 0; i < NPAIR; ++i) {
+        a.out.f[2 * i][cell] = D.p[i].x;
+        a.out.f[2 * i + 1][cell] = D.p[i].y;
+      }
+      a.out.f[PH][cell] = D.s;
+    } else if (STAGE < 3) {
 #pragma unroll
       for (int i = 0; i < NPAIR; ++i) {
         const float2 u0 = f2(A0[2 * i], A0[2 * i + 1]);
@@ -334,19 +349,12 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
         float *hp = a.hi.f[PH], *lp = a.lo.f[PH];
         float sv, t, e;
         two_sum(A0[PH], fmaf(-k.dt, D.s, A1[PH]), sv, t);
-        const float pr = sv * k.decay;
-        const float pe = fmaf(sv, k.decay, -pr);
-        two_sum(pr, pe + t * k.decay, sv, e);
+        ph_damp(sv, t, k.decay, sv, e);
         hp[cell] = sv;
         lp[cell] = e;
       }
-      // characteristic speed of the new state (speeds() in s32_common.cuh)
-      const float inv = 1.0f / s_ro;
-      const float ein = (s_et - 0.5f * mm * inv - bb2 * FPII8) * inv;
-      const float cs = sqrtf(fmaxf(a.gm * a.gm1 * ein, 0.0f));
-      const float vv = sqrtf(mm) * inv;
-      const float ca = sqrtf(bb2 * inv * FPII4);
-      a.cc[cell] = cs * a.cs_fac + vv * a.vv_fac + ca * a.ca_fac;
+      // characteristic speed of the new state
+      a.cc[cell] = char_speed(s_ro, mm, bb2, s_et, a.gm, a.gm1, a.cs_fac, a.vv_fac, a.ca_fac);
     }
   }
 
@@ -372,8 +380,8 @@ rk_pipe_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
     k.wx = (float)(g.dsi[0] * INV12);
     k.wy = (float)(g.dsi[1] * INV12);
     k.wz = (float)(g.dsi[2] * INV12);
-    k.dt = (float)a.sc->dts[STAGE];
-    k.decay = (float)a.sc->ph_decay[STAGE];
+    k.dt = (float)a.sc->dts[STAGE < 4 ? STAGE : 3];
+    k.decay = (float)a.sc->ph_decay[STAGE < 4 ? STAGE : 3];
     k.ch2 = (float)a.sc->ch2;
     k.wx2 = f2(k.wx, k.wx);
     k.wy2 = f2(k.wy, k.wy);
@@ -419,10 +427,12 @@ int s32_rk_pipe_configure() {
   MISO_SET((s32p::rk_pipe_kernel<1, false>));
   MISO_SET((s32p::rk_pipe_kernel<2, false>));
   MISO_SET((s32p::rk_pipe_kernel<3, false>));
+  MISO_SET((s32p::rk_pipe_kernel<4, false>));
   MISO_SET((s32p::rk_pipe_kernel<0, true>));
   MISO_SET((s32p::rk_pipe_kernel<1, true>));
   MISO_SET((s32p::rk_pipe_kernel<2, true>));
   MISO_SET((s32p::rk_pipe_kernel<3, true>));
+  MISO_SET((s32p::rk_pipe_kernel<4, true>));
 #undef MISO_SET
   return e == cudaSuccess ? 0 : -1;
 }
@@ -435,7 +445,8 @@ static void launch_pipe(const CUtensorMap &m, const RkArgs &a, int stage, int gr
     case 0: s32p::rk_pipe_kernel<0, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
     case 1: s32p::rk_pipe_kernel<1, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
     case 2: s32p::rk_pipe_kernel<2, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
-    default: s32p::rk_pipe_kernel<3, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
+    case 3: s32p::rk_pipe_kernel<3, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
+    default: s32p::rk_pipe_kernel<4, SRC><<<grid, s32p::NTHR, smem, st>>>(m, a); break;
   }
 }
 

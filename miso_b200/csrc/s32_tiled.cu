@@ -300,14 +300,49 @@ constexpr int L_LO = (NF * LBOX * 4 + 127) / 128 * 128;
 constexpr int L_CC = L_LO + L_LO;
 constexpr int L_SLOT = L_CC + (LBOX * 4 + 127) / 128 * 128;
 constexpr unsigned L_TX = 2 * NF * LBOX * 4 + LBOX * 4;  // bytes per slot fill
+// x sweep with the last Runge-Kutta update deferred into it: the third
+// block of a slot holds the stage's right-hand side D (9 fields) in place
+// of the characteristic speed
+constexpr int L_D = L_CC;
+constexpr int L_SLOT_D = L_D + L_LO;
+constexpr unsigned L_TX_D = 3 * NF * LBOX * 4;
 
 constexpr int LCW = LK / 32;  // consumer warps; one more warp issues the copies
 
-struct __align__(128) LineSmem {
-  unsigned char slot[LNB][L_SLOT];
+template <bool DEFER>
+struct __align__(128) LineSmemT {
+  unsigned char slot[LNB][DEFER ? L_SLOT_D : L_SLOT];
   unsigned long long full[LNB];   // copy of the slot landed (1 arrival + bytes)
   unsigned long long empty[LNB];  // slot read by every consumer warp (LCW arrivals)
 };
+using LineSmem = LineSmemT<false>;
+
+// One field of U^{n+1} = (h, l) - dt D as a compensated pair (s, e), with
+// the GLM damping of ph: the last Runge-Kutta stage's update, operation for
+// operation as rk_pipe_kernel<3> forms it (s32_rk.cu).
+template <int F>
+__device__ __forceinline__ void last_stage_field(float h, float l, float d, float dt,
+                                                 float decay, float &sv, float &e) {
+  if (F == PH) {
+    float t;
+    two_sum(h, fmaf(-dt, d, l), sv, t);
+    ph_damp(sv, t, decay, sv, e);
+  } else {
+    two_sum(h, fmaf(-dt, d, l), sv, e);
+  }
+}
+
+// Characteristic speed of a state's hi words, with the sums of squares
+// gathered in rk_pipe_kernel<3>'s order.
+__device__ __forceinline__ float last_stage_cc(const float u[NF], const AvArgs &a) {
+  float mm = u[MX] * u[MX];
+  mm = fmaf(u[MY], u[MY], mm);
+  mm = fmaf(u[MZ], u[MZ], mm);
+  float bb2 = u[BX] * u[BX];
+  bb2 = fmaf(u[BY], u[BY], bb2);
+  bb2 = fmaf(u[BZ], u[BZ], bb2);
+  return char_speed(u[RO], mm, bb2, u[ET], a.gm, a.gm1, a.cs_fac, a.vv_fac, a.ca_fac);
+}
 
 struct LineItem {
   int kb, u, t0, t1;
@@ -348,9 +383,9 @@ struct LineCursor {
   }
 };
 
-template <int DIR>
+template <int DIR, bool DEFER>
 __device__ __forceinline__ void line_issue(const CUtensorMap *thi, const CUtensorMap *tlo,
-                                           const CUtensorMap *tcc, LineSmem &sm, int s,
+                                           const CUtensorMap *t3, LineSmemT<DEFER> &sm, int s,
                                            const Geom &g, const LineItem &it, int p) {
   unsigned char *sl = sm.slot[s];
   const int k0 = it.kb * LK;
@@ -359,18 +394,27 @@ __device__ __forceinline__ void line_issue(const CUtensorMap *thi, const CUtenso
   const int ps = ghost_src(g, DIR, p, side);
   const int cj = DIR == 0 ? it.u + g.m[1] : ps + g.m[1];
   const int ci = DIR == 0 ? ps + g.m[0] : it.u + g.m[0];
-  mbar_expect_tx(&sm.full[s], L_TX);
+  mbar_expect_tx(&sm.full[s], DEFER ? L_TX_D : L_TX);
   tma4(thi, sl + L_HI, &sm.full[s], k0, cj, ci, 0);
   tma4(tlo, sl + L_LO, &sm.full[s], k0, cj, ci, 0);
-  tma3(tcc, sl + L_CC, &sm.full[s], k0, cj, ci);
+  if (DEFER)
+    tma4(t3, sl + L_D, &sm.full[s], k0, cj, ci, 0);
+  else
+    tma3(t3, sl + L_CC, &sm.full[s], k0, cj, ci);
 }
 
-template <int DIR>
+// DEFER (x sweep only): the state is U^{n+1} = (hi, lo) - dt_4 D of the
+// deferred last Runge-Kutta stage (rk_pipe_kernel<4>); t3 maps D in place of
+// the characteristic speed.  Each plane's state and speed are formed as the
+// plane arrives, and the sweep writes the speed of the cells it finishes
+// for the y and z sweeps.
+template <int DIR, bool DEFER>
 __global__ void __launch_bounds__(LK + 32, 2)
 av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CUtensorMap tlo,
-               const __grid_constant__ CUtensorMap tcc, const AvArgs a) {
+               const __grid_constant__ CUtensorMap t3, const AvArgs a) {
+  static_assert(!DEFER || DIR == 0, "the deferred update rides on the x sweep");
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  LineSmem &sm = *reinterpret_cast<LineSmem *>(smem_raw);
+  LineSmemT<DEFER> &sm = *reinterpret_cast<LineSmemT<DEFER> *>(smem_raw);
   const Geom &g = a.g;
   constexpr int OTH = DIR == 0 ? 1 : 0;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -402,7 +446,7 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
           break;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        line_issue<DIR>(&thi, &tlo, &tcc, sm, b, g, prod.cur, prod.p);
+        line_issue<DIR, DEFER>(&thi, &tlo, &t3, sm, b, g, prod.cur, prod.p);
         prod.next(a, kblocks, nu, items);
       }
       // the last copies land before the CTA exits (bounded)
@@ -413,6 +457,8 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
   }
 
   const float fac = (float)(g.dsi[DIR] * a.sc->dt);
+  const float dt4 = DEFER ? (float)a.sc->dts[3] : 0.f;
+  const float decay4 = DEFER ? (float)a.sc->ph_decay[3] : 0.f;
   int seq = 0;
   // limiter state on field pairs: W9 holds (ro, mx) (my, mz) (bx, by) (bz, ph)
   // as packed pairs and ro*e alone
@@ -430,12 +476,30 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
         return;
       }
       const float *shi = reinterpret_cast<const float *>(sm.slot[s] + L_HI);
-      const float *scc = reinterpret_cast<const float *>(sm.slot[s] + L_CC);
       W9 wp;
+      float ccp;
       {
         float u[NF];
+        if (DEFER) {
+          const float *slo = reinterpret_cast<const float *>(sm.slot[s] + L_LO);
+          const float *sd = reinterpret_cast<const float *>(sm.slot[s] + L_D);
+          const int o = tid + 2;
+          float e;
+          last_stage_field<RO>(shi[RO * LBOX + o], slo[RO * LBOX + o], sd[RO * LBOX + o], dt4, decay4, u[RO], e);
+          last_stage_field<MX>(shi[MX * LBOX + o], slo[MX * LBOX + o], sd[MX * LBOX + o], dt4, decay4, u[MX], e);
+          last_stage_field<MY>(shi[MY * LBOX + o], slo[MY * LBOX + o], sd[MY * LBOX + o], dt4, decay4, u[MY], e);
+          last_stage_field<MZ>(shi[MZ * LBOX + o], slo[MZ * LBOX + o], sd[MZ * LBOX + o], dt4, decay4, u[MZ], e);
+          last_stage_field<BX>(shi[BX * LBOX + o], slo[BX * LBOX + o], sd[BX * LBOX + o], dt4, decay4, u[BX], e);
+          last_stage_field<BY>(shi[BY * LBOX + o], slo[BY * LBOX + o], sd[BY * LBOX + o], dt4, decay4, u[BY], e);
+          last_stage_field<BZ>(shi[BZ * LBOX + o], slo[BZ * LBOX + o], sd[BZ * LBOX + o], dt4, decay4, u[BZ], e);
+          last_stage_field<ET>(shi[ET * LBOX + o], slo[ET * LBOX + o], sd[ET * LBOX + o], dt4, decay4, u[ET], e);
+          last_stage_field<PH>(shi[PH * LBOX + o], slo[PH * LBOX + o], sd[PH * LBOX + o], dt4, decay4, u[PH], e);
+          ccp = last_stage_cc(u, a);
+        } else {
 #pragma unroll
-        for (int f = 0; f < NF; ++f) u[f] = shi[f * LBOX + tid + 2];
+          for (int f = 0; f < NF; ++f) u[f] = shi[f * LBOX + tid + 2];
+          ccp = reinterpret_cast<const float *>(sm.slot[s] + L_CC)[tid + 2];
+        }
         if (p < 0 || p >= g.n[DIR]) {
           // the plane was copied from the interior plane it images: apply
           // the mirror signs of that face (none on a periodic axis)
@@ -446,7 +510,6 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
         }
         limited_w9(u, wp);
       }
-      const float ccp = scc[tid + 2];
       const int r = p - li.t0;  // -2 .. t1-t0+1
       if (r == -2) {
         wm2 = wp;
@@ -477,6 +540,8 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
         const int sc_ = (int)((seq - 2) % LNB);
         const float *chi = reinterpret_cast<const float *>(sm.slot[sc_] + L_HI);
         const float *clo = reinterpret_cast<const float *>(sm.slot[sc_] + L_LO);
+        const float *cd = reinterpret_cast<const float *>(sm.slot[sc_] + (DEFER ? L_D : L_LO));
+        const float cct = cc0;  // speed of the centre cell
         const float hcc = -0.25f * (cc0 + cc1);
         const float2 hcc2 = vs<float2>(hcc);
         W9 dF;
@@ -503,11 +568,28 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
           const int x0 = DIR == 0 ? t : li.u;
           const int x1 = DIR == 0 ? li.u : t;
           const int cell = cell_of(g, x0, x1, k);
+          const int o = tid + 2;
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int f0 = field_of(2 * i), f1 = field_of(2 * i + 1);
-            const float2 h = make_float2(chi[f0 * LBOX + tid + 2], chi[f1 * LBOX + tid + 2]);
-            const float2 l = make_float2(clo[f0 * LBOX + tid + 2], clo[f1 * LBOX + tid + 2]);
+            float2 h = make_float2(chi[f0 * LBOX + o], chi[f1 * LBOX + o]);
+            float2 l = make_float2(clo[f0 * LBOX + o], clo[f1 * LBOX + o]);
+            if (DEFER) {
+              // the centre's U^{n+1} pair, formed again from its slot
+              if (i == 0) {
+                last_stage_field<RO>(h.x, l.x, cd[RO * LBOX + o], dt4, decay4, h.x, l.x);
+                last_stage_field<MX>(h.y, l.y, cd[MX * LBOX + o], dt4, decay4, h.y, l.y);
+              } else if (i == 1) {
+                last_stage_field<MY>(h.x, l.x, cd[MY * LBOX + o], dt4, decay4, h.x, l.x);
+                last_stage_field<MZ>(h.y, l.y, cd[MZ * LBOX + o], dt4, decay4, h.y, l.y);
+              } else if (i == 2) {
+                last_stage_field<BX>(h.x, l.x, cd[BX * LBOX + o], dt4, decay4, h.x, l.x);
+                last_stage_field<BY>(h.y, l.y, cd[BY * LBOX + o], dt4, decay4, h.y, l.y);
+              } else {
+                last_stage_field<BZ>(h.x, l.x, cd[BZ * LBOX + o], dt4, decay4, h.x, l.x);
+                last_stage_field<PH>(h.y, l.y, cd[PH * LBOX + o], dt4, decay4, h.y, l.y);
+              }
+            }
             float2 sv, e;
             two_sum(h, vfma(dF.p[i], mfac2, l), sv, e);
             // interior only: the shell kernel fills the images
@@ -517,11 +599,14 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
             a.lo2.f[f1][cell] = e.y;
           }
           {
+            float h = chi[ET * LBOX + o], l = clo[ET * LBOX + o];
+            if (DEFER) last_stage_field<ET>(h, l, cd[ET * LBOX + o], dt4, decay4, h, l);
             float sv, e;
-            two_sum(chi[ET * LBOX + tid + 2], vfma(dF.s, -fac, clo[ET * LBOX + tid + 2]), sv, e);
+            two_sum(h, vfma(dF.s, -fac, l), sv, e);
             a.hi2.f[ET][cell] = sv;
             a.lo2.f[ET][cell] = e;
           }
+          if (DEFER) a.cc_out[cell] = cct;  // read by the y and z sweeps
         }
       }
       // release the slots this warp is done with: plane p-2 (read for the
@@ -701,6 +786,7 @@ int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out) {
 int s32_configure() {
   const int rk = (int)sizeof(s32t::RkSmem);
   const int ln = (int)sizeof(s32t::LineSmem);
+  const int lnd = (int)sizeof(s32t::LineSmemT<true>);
   cudaError_t e = cudaSuccess;
 #define MISO_SET(k, b) \
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b)
@@ -708,8 +794,9 @@ int s32_configure() {
   MISO_SET(s32t::rk_tiled_kernel<1>, rk);
   MISO_SET(s32t::rk_tiled_kernel<2>, rk);
   MISO_SET(s32t::rk_tiled_kernel<3>, rk);
-  MISO_SET(s32t::av_line_kernel<0>, ln);
-  MISO_SET(s32t::av_line_kernel<1>, ln);
+  MISO_SET((s32t::av_line_kernel<0, false>), ln);
+  MISO_SET((s32t::av_line_kernel<1, false>), ln);
+  MISO_SET((s32t::av_line_kernel<0, true>), lnd);
 #undef MISO_SET
   return e == cudaSuccess ? 0 : -1;
 }
@@ -732,16 +819,19 @@ void launch_s32_rk_tiled(const void *tm, const RkArgs &a, int stage, int grid, c
   }
 }
 
-void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
-                        int dir, int grid, cudaStream_t st) {
+void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, const AvArgs &a,
+                        int dir, bool defer, int grid, cudaStream_t st) {
   const CUtensorMap &h = *(const CUtensorMap *)tm_hi;
   const CUtensorMap &l = *(const CUtensorMap *)tm_lo;
-  const CUtensorMap &c = *(const CUtensorMap *)tm_cc;
+  const CUtensorMap &c = *(const CUtensorMap *)tm3;
   const size_t smem = sizeof(s32t::LineSmem);
-  if (dir == 0)
-    s32t::av_line_kernel<0><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, a);
+  if (dir == 0 && defer)
+    s32t::av_line_kernel<0, true>
+        <<<grid, s32t::LK + 32, sizeof(s32t::LineSmemT<true>), st>>>(h, l, c, a);
+  else if (dir == 0)
+    s32t::av_line_kernel<0, false><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, a);
   else
-    s32t::av_line_kernel<1><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, a);
+    s32t::av_line_kernel<1, false><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, a);
 }
 
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st) {

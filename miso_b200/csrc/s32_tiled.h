@@ -36,6 +36,10 @@ struct AvArgs {
   float *partial;  // z sweep: per-block CFL minima of the new state (nullable)
   float ep, fh, gm, gm1, cfl_dx;
   int L;  // cells per work item along the sweep axis (x, y sweeps)
+  // x sweep with the last RK update deferred into it: hi / lo hold U^n, and
+  // the speed of U^{n+1} = (hi, lo) - dt_4 D goes to cc_out
+  float *cc_out;
+  float cs_fac, vv_fac, ca_fac;
 };
 
 // Arrays whose interior shell gets its ghost images (s32_shell.cu); f[n] is
@@ -71,8 +75,10 @@ void launch_s32_rk_tiled(const void *tm, const RkArgs &a, int stage, int grid, c
 int s32_rk_pipe_configure();
 void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st);
 
-void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm_cc, const AvArgs &a,
-                        int dir, int grid, cudaStream_t st);
+// tm3: the characteristic speed (3-D map), or with `defer` (x sweep only)
+// the deferred last RK stage's right-hand side D (4-D map, kind 1)
+void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, const AvArgs &a,
+                        int dir, bool defer, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);
 // x / y sweep, one warp per 32-cell line segment marching along the sweep
 // axis (s32_av.cu): no shared memory, no CTA barrier; interior-only writes

@@ -19,6 +19,7 @@ sources) on the host cores instead.  Rank 0 prints one JSON line.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import multiprocessing as mp
 import os
@@ -76,29 +77,41 @@ def hbm_peak():
 
 
 class ClockSampler:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling around the timed region: samples every 100 ms,
+    each with its timestamp, and keeps those taken between ``mark()`` and
+    ``stop()`` (all of them if none falls inside, as for a region shorter
+    than the interval)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.t0 = self.t1 = None
         self.tmp = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.tmp, stderr=subprocess.DEVNULL)
+            time.sleep(0.5)  # nvidia-smi's start-up, outside the timed region
         except Exception:
             self.proc = None
+        self.mark()
+
+    def mark(self):
+        """The timed region starts now."""
+        self.t0 = datetime.datetime.now()
 
     def stop(self):
+        self.t1 = datetime.datetime.now()
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)  # the sample that closes the region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -106,23 +119,31 @@ class ClockSampler:
             self.proc.kill()
         self.tmp.flush()
         with open(self.tmp.name) as f:
-            rows = [r.strip().split(",") for r in f if r.strip()]
+            rows = [[x.strip() for x in r.strip().split(",")] for r in f if r.strip()]
         os.unlink(self.tmp.name)
+
+        def when(r):
+            try:
+                return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f")
+            except (ValueError, IndexError):
+                return None
+
+        inside = [r for r in rows if when(r) and self.t0 <= when(r) <= self.t1]
+        use = inside or rows
         sm, smax, reasons = [], [], set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for r in rows:
-            r = [x.strip() for x in r]
+        for r in use:
             try:
-                sm.append(float(r[1]))
-                smax.append(float(r[2]))
+                sm.append(float(r[2]))
+                smax.append(float(r[3]))
             except (ValueError, IndexError):
                 continue
-            for nm, val in zip(names, r[5:9]):
+            for nm, val in zip(names, r[6:10]):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "samples": len(sm), "samples_in_region": len(inside), "reasons": sorted(reasons)}
 
 
 # ---------------------------------------------------------------------------
@@ -170,7 +191,6 @@ def dist_init(backend: str = "nccl", timeout_s: float = 300.0):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
@@ -383,18 +403,27 @@ def roofline_of(report: dict, precision: str, value_per_gpu: float) -> dict:
     peak, peak_src = hbm_peak()
     dname, d = max(report.items(), key=lambda kv: kv[1]["ms"])
     achieved = (d["bytes"] / d["launches"]) / (d["ms"] / d["launches"] / 1e3) / 1e9
-    traffic = None
+    traffic = step_dram = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
-                traffic = json.load(f).get(f"{precision}:{dname}")
+                tj = json.load(f)
+            traffic = tj.get(f"{precision}:{dname}")
+            step_dram = tj.get(f"{precision}:step_per_cell")
         except Exception:
-            traffic = None
-    return {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
-            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-            "traffic": traffic, "step_frac": value_per_gpu * ALG_BYTES[precision] / peak,
-            "alg_bytes_per_cell_step": ALG_BYTES[precision]}
+            traffic = step_dram = None
+    out = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
+           "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+           "traffic": traffic, "step_frac": value_per_gpu * ALG_BYTES[precision] / peak,
+           "alg_bytes_per_cell_step": ALG_BYTES[precision]}
+    if step_dram:
+        # the step fuses passes of the canonical structure (the last RK
+        # update rides on the x sweep), so its DRAM bytes per cell, measured
+        # by ncu, go beside the canonical fraction
+        out["step_dram_bytes_per_cell"] = step_dram
+        out["step_dram_frac"] = value_per_gpu * step_dram / peak
+    return out
 
 
 def run_slab(args):

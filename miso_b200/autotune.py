@@ -81,7 +81,7 @@ def _step_ms(t: dict) -> float:
 
 def _try_variant(integ, kc: int, var: int) -> bool:
     """Set a variant; False where the handle refuses it (a source term
-    pins the RK stage to variant 2)."""
+    pins the RK stage to variants 2 and 3)."""
     from . import _lib
     try:
         integ.set_variant(kc, var)

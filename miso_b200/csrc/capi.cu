@@ -19,6 +19,7 @@
 
 #include "../../include/miso_b200.h"
 #include "common.cuh"
+#include "images.cuh"
 #include "kernels.h"
 #include "kernels_s32.h"
 #include "s32_tiled.h"
@@ -36,64 +37,92 @@ constexpr size_t ALIGN = 256;
 size_t round_up(size_t x) { return (x + ALIGN - 1) / ALIGN * ALIGN; }
 
 // FP64 monitors: per-block partial sums of 8 quantities (interior cells).
+// The conserved state and |div B| (4th-order central differences) of cell c
+// at interior coordinates x[3], folded into the accumulators.  The split
+// form takes a neighbour across a face from the interior cell it images (the
+// lo ghost words lag the interior between a step and a download); the FP64
+// form's ghosts are filled after every step.
 template <bool SPLIT>
-__global__ void __launch_bounds__(256)
-monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
-               FieldPtrs<const float> lo, double *__restrict__ partial) {
-  const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
-  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (long long lin = blockIdx.x * (long long)blockDim.x + threadIdx.x; lin < nint;
-       lin += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(lin % g.n[2]) + g.m[2];
-    const long long r1 = lin / g.n[2];
-    const int j = (int)(r1 % g.n[1]) + g.m[1];
-    const int i = (int)(r1 / g.n[1]) + g.m[0];
-    const long long c = i * g.st[0] + j * g.st[1] + k;
-    double u[NF];
+__device__ __forceinline__ void monitor_cell(const Geom &g, const FieldPtrs<const double> &q,
+                                             const FieldPtrs<const float> &hi,
+                                             const FieldPtrs<const float> &lo, long long c,
+                                             const int x[3], double acc[8]) {
+  double u[NF];
+  if (SPLIT) {
+    for (int f = 0; f < NF; ++f) u[f] = (double)hi.f[f][c] + (double)lo.f[f][c];
+  } else {
+    const double ro = q.f[RO][c], vx = q.f[VX][c], vy = q.f[VY][c], vz = q.f[VZ][c];
+    const double bx = q.f[BX][c], by = q.f[BY][c], bz = q.f[BZ][c];
+    u[RO] = ro;
+    u[MX] = ro * vx;
+    u[MY] = ro * vy;
+    u[MZ] = ro * vz;
+    u[BX] = bx;
+    u[BY] = by;
+    u[BZ] = bz;
+    u[ET] = ro * q.f[EI][c] + 0.5 * ro * (vx * vx + vy * vy + vz * vz) +
+            PII8 * (bx * bx + by * by + bz * bz);
+    u[PH] = q.f[PH][c];
+  }
+  double divb = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    if (!g.s[d]) continue;
+    const long long s = g.st[d];
+    double p2, p1, m1, m2;
     if (SPLIT) {
-      for (int f = 0; f < NF; ++f) u[f] = (double)hi.f[f][c] + (double)lo.f[f][c];
-    } else {
-      const double ro = q.f[RO][c], vx = q.f[VX][c], vy = q.f[VY][c], vz = q.f[VZ][c];
-      const double bx = q.f[BX][c], by = q.f[BY][c], bz = q.f[BZ][c];
-      u[RO] = ro;
-      u[MX] = ro * vx;
-      u[MY] = ro * vy;
-      u[MZ] = ro * vz;
-      u[BX] = bx;
-      u[BY] = by;
-      u[BZ] = bz;
-      u[ET] = ro * q.f[EI][c] + 0.5 * ro * (vx * vx + vy * vy + vz * vz) +
-              PII8 * (bx * bx + by * by + bz * bz);
-      u[PH] = q.f[PH][c];
-    }
-    double divb = 0.0;
-    for (int d = 0; d < 3; ++d) {
-      if (!g.s[d]) continue;
-      const long long s = g.st[d];
-      double p2, p1, m1, m2;
-      if (SPLIT) {
-        const float *h = hi.f[BX + d], *l = lo.f[BX + d];
+      const float *h = hi.f[BX + d], *l = lo.f[BX + d];
+      if (x[d] >= 2 && x[d] < g.n[d] - 2) {
         p2 = (double)h[c + 2 * s] + l[c + 2 * s];
         p1 = (double)h[c + s] + l[c + s];
         m1 = (double)h[c - s] + l[c - s];
         m2 = (double)h[c - 2 * s] + l[c - 2 * s];
       } else {
-        const double *b = q.f[BX + d];
-        p2 = b[c + 2 * s];
-        p1 = b[c + s];
-        m1 = b[c - s];
-        m2 = b[c - 2 * s];
+        auto at = [&](int o) {
+          int side;
+          const int t = ghost_src(g, d, x[d] + o, side);
+          const long long cc = c + (long long)(t - x[d]) * s;
+          const double v = (double)h[cc] + l[cc];
+          return (side >= 0 && ((g.negmask[d][side] >> (BX + d)) & 1u)) ? -v : v;
+        };
+        p2 = at(2);
+        p1 = at(1);
+        m1 = at(-1);
+        m2 = at(-2);
       }
-      divb += (-p2 + 8.0 * p1 - 8.0 * m1 + m2) * INV12 * g.dsi[d];
+    } else {
+      const double *b = q.f[BX + d];
+      p2 = b[c + 2 * s];
+      p1 = b[c + s];
+      m1 = b[c - s];
+      m2 = b[c - 2 * s];
     }
-    acc[0] += u[RO];
-    acc[1] += u[MX];
-    acc[2] += u[MY];
-    acc[3] += u[MZ];
-    acc[4] += u[ET];
-    acc[5] += fabs(divb);
-    acc[6] = fmax(acc[6], fabs(divb));
-    acc[7] += u[PH] * u[PH];
+    divb += (-p2 + 8.0 * p1 - 8.0 * m1 + m2) * INV12 * g.dsi[d];
+  }
+  acc[0] += u[RO];
+  acc[1] += u[MX];
+  acc[2] += u[MY];
+  acc[3] += u[MZ];
+  acc[4] += u[ET];
+  acc[5] += fabs(divb);
+  acc[6] = fmax(acc[6], fabs(divb));
+  acc[7] += u[PH] * u[PH];
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(256, 4)
+monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
+               FieldPtrs<const float> lo, double *__restrict__ partial) {
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
+  for (long long lin = blockIdx.x * (long long)blockDim.x + threadIdx.x; lin < nint;
+       lin += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(lin % g.n[2]);
+    const long long r1 = lin / g.n[2];
+    const int j = (int)(r1 % g.n[1]);
+    const int i = (int)(r1 / g.n[1]);
+    const int x[3] = {i, j, k};
+    monitor_cell<SPLIT>(g, q, hi, lo,
+                        (i + g.m[0]) * g.st[0] + (j + g.m[1]) * g.st[1] + k + g.m[2], x, acc);
   }
   __shared__ double red[8][256];
   for (int q8 = 0; q8 < 8; ++q8) red[q8][threadIdx.x] = acc[q8];

@@ -81,13 +81,15 @@ struct StageK {
   float dt, decay, ch2, gm, gm1, cs_fac, vv_fac, ca_fac;
 };
 
-// write the finished cell `cell` of stage `stage` (centre values A0 / A1)
-__device__ __forceinline__ void rk_finish(int stage, const StageK &k, long long base, int cell,
+// write the finished cell `cell` of a stage (centre values A0 / A1; LAST: the
+// fourth stage, which updates hi / lo and writes the speed)
+template <bool LAST>
+__device__ __forceinline__ void rk_finish(const StageK &k, long long base, int cell,
                                           const float D[NF], const float A0[NF],
                                           const float A1[NF], const FieldPtrs<float> &hi,
                                           const FieldPtrs<float> &lo, const FieldPtrs<float> &out,
                                           float *cc) {
-  if (stage < 3) {
+  if (!LAST) {
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
       float v = A0[f] - k.dt * D[f];
@@ -117,13 +119,14 @@ __device__ __forceinline__ void rk_finish(int stage, const StageK &k, long long 
   }
 }
 
-__device__ __forceinline__ void load_centre(int stage, long long base, int cell,
+template <bool LAST>
+__device__ __forceinline__ void load_centre(long long base, int cell,
                                             const FieldPtrs<const float> &u0,
                                             const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
                                             float A0[NF], float A1[NF]) {
 #pragma unroll
   for (int f = 0; f < NF; ++f) {
-    if (stage < 3) {
+    if (!LAST) {
       A0[f] = __ldg(u0.f[f] + base + cell);
     } else {
       A0[f] = hi.f[f][base + cell];
@@ -134,8 +137,8 @@ __device__ __forceinline__ void load_centre(int stage, long long base, int cell,
 
 // One row q of a 2-D march: F(q) -> Fn, F(q-1) in F1, F(q-2) in F2;
 // R(q) -> Rn, R(q-2) in R2 (see the file comment for P, N and R).
-template <int AR, int AC>
-__device__ __forceinline__ void rk_row(int stage, const StageK &k, const RowGeo &q,
+template <int AR, int AC, bool LAST>
+__device__ __forceinline__ void rk_row(const StageK &k, const RowGeo &q,
                                        const RowItem &it, int qrow, int rt, bool lane_out,
                                        const FieldPtrs<const float> &prev,
                                        const FieldPtrs<const float> &u0,
@@ -166,18 +169,18 @@ __device__ __forceinline__ void rk_row(int stage, const StageK &k, const RowGeo 
   }
   if (fin) {
     float A0[NF], A1[NF], D[NF];
-    load_centre(stage, q.base, ccell, u0, hi, lo, A0, A1);
+    load_centre<LAST>(q.base, ccell, u0, hi, lo, A0, A1);
 #pragma unroll
     for (int f = 0; f < NF; ++f)
       D[f] = __fsub_rn(R2[f], __fmul_rn(q.wC, fmaf(-8.f, F1[f], Fn[f])));
-    rk_finish(stage, k, q.base, ccell, D, A0, A1, hi, lo, out, cc);
+    rk_finish<LAST>(k, q.base, ccell, D, A0, A1, hi, lo, out, cc);
   }
 }
 
 // One item of the Runge-Kutta stage: axes AR (unit stride) and AC (-1: 1-D)
-template <int AR, int AC>
+template <int AR, int AC, bool LAST>
 __device__ __forceinline__ void rk_item(const RowItem &it, const RowGeo &q, const StageK &k,
-                                        int stage, const FieldPtrs<const float> &prev,
+                                        const FieldPtrs<const float> &prev,
                                         const FieldPtrs<const float> &u0,
                                         const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
                                         const FieldPtrs<float> &out, float *cc) {
@@ -189,14 +192,14 @@ __device__ __forceinline__ void rk_item(const RowItem &it, const RowGeo &q, cons
     // 1-D: one row
     const int cell = rt * q.sR;
     float A0[NF], A1[NF];
-    if (lane_out) load_centre(stage, q.base, cell, u0, hi, lo, A0, A1);
+    if (lane_out) load_centre<LAST>(q.base, cell, u0, hi, lo, A0, A1);
     float u[NF], F[NF], D[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) u[f] = __ldg(prev.f[f] + q.base + cell);
     flux_of<AR < 0 ? 0 : AR>(u, k.gm1, k.ch2, F);
 #pragma unroll
     for (int f = 0; f < NF; ++f) D[f] = q.wR * dR(F[f]);
-    if (lane_out) rk_finish(stage, k, q.base, cell, D, A0, A1, hi, lo, out, cc);
+    if (lane_out) rk_finish<LAST>(k, q.base, cell, D, A0, A1, hi, lo, out, cc);
     return;
   }
   constexpr int CC = AC < 0 ? 0 : AC;
@@ -205,20 +208,20 @@ __device__ __forceinline__ void rk_item(const RowItem &it, const RowGeo &q, cons
   for (int f = 0; f < NF; ++f) FA[f] = FB[f] = FC[f] = RA[f] = RB[f] = RC[f] = 0.f;
   const int qe = it.c1 + 1;
   for (int qr = it.c0 - 2; qr <= qe; qr += 3) {
-    rk_row<AR, CC>(stage, k, q, it, qr, rt, lane_out, prev, u0, hi, lo, out, cc, FA, FC, FB, RA,
-                   RB);
+    rk_row<AR, CC, LAST>(k, q, it, qr, rt, lane_out, prev, u0, hi, lo, out, cc, FA, FC, FB, RA,
+                         RB);
     if (qr + 1 > qe) break;
-    rk_row<AR, CC>(stage, k, q, it, qr + 1, rt, lane_out, prev, u0, hi, lo, out, cc, FB, FA, FC,
-                   RB, RC);
+    rk_row<AR, CC, LAST>(k, q, it, qr + 1, rt, lane_out, prev, u0, hi, lo, out, cc, FB, FA, FC,
+                         RB, RC);
     if (qr + 2 > qe) break;
-    rk_row<AR, CC>(stage, k, q, it, qr + 2, rt, lane_out, prev, u0, hi, lo, out, cc, FC, FB, FA,
-                   RC, RA);
+    rk_row<AR, CC, LAST>(k, q, it, qr + 2, rt, lane_out, prev, u0, hi, lo, out, cc, FC, FB, FA,
+                         RC, RA);
   }
 }
 
 // Runge-Kutta stage over the items of one axis pair (AR unit-stride axis,
 // AC the other one, -1 for 1-D instances)
-template <int AR, int AC>
+template <int AR, int AC, bool LAST>
 __global__ void __launch_bounds__(256, 2)
 rk_rows_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const float> prev,
                FieldPtrs<const float> u0, FieldPtrs<float> hi, FieldPtrs<float> lo,
@@ -238,7 +241,7 @@ rk_rows_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const fl
     k.cs_fac = (float)in.cs_fac;
     k.vv_fac = (float)in.vv_fac;
     k.ca_fac = (float)in.ca_fac;
-    rk_item<AR, AC>(it, q, k, stage, prev, u0, hi, lo, out, cc);
+    rk_item<AR, AC, LAST>(it, q, k, prev, u0, hi, lo, out, cc);
   }
 }
 
@@ -419,8 +422,13 @@ void b32_rk_rows(const BatchArgs &a, const RowItem *items, int n, int combo,
                  const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
                  const FieldPtrs<float> &out, float *cc, int stage, int grid, cudaStream_t st) {
   if (n <= 0) return;
-#define MISO_RK_ROWS(R, C) \
-  b32r::rk_rows_kernel<R, C><<<grid, 256, 0, st>>>(a, items, n, prev, u0, hi, lo, out, cc, stage)
+#define MISO_RK_ROWS(R, C)                                                                   \
+  if (stage == 3)                                                                          \
+    b32r::rk_rows_kernel<R, C, true><<<grid, 256, 0, st>>>(a, items, n, prev, u0, hi, lo, out, \
+                                                           cc, stage);                     \
+  else                                                                                     \
+    b32r::rk_rows_kernel<R, C, false><<<grid, 256, 0, st>>>(a, items, n, prev, u0, hi, lo,     \
+                                                            out, cc, stage)
   switch (combo) {
     case 0: MISO_RK_ROWS(0, -1); break;
     case 1: MISO_RK_ROWS(1, -1); break;

@@ -179,6 +179,9 @@ __device__ __forceinline__ void diff_p(const FieldPtrs<const float> &s, long lon
 }
 
 // Runge-Kutta stage `stage` for every instance (flux form; see rk_flat_kernel).
+// LAST: the fourth stage (updates hi / lo and writes the speed), an
+// instantiation of its own so the first three carry no lo words.
+template <bool LAST>
 __global__ void __launch_bounds__(BATCH_TILE, 3)
 rk_block_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float> u0,
                 FieldPtrs<float> hi, FieldPtrs<float> lo, FieldPtrs<float> out, float *cc,
@@ -206,7 +209,7 @@ rk_block_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float>
     if (mine) {
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
-        if (stage < 3) {
+        if (!LAST) {
           A0[f] = __ldg(u0.f[f] + in.base + c);
         } else {
           A0[f] = hi.f[f][in.base + c];
@@ -257,7 +260,7 @@ rk_block_kernel(BatchArgs a, FieldPtrs<const float> prev, FieldPtrs<const float>
       }
       if (P >= 0) diff_p(prev, in.base, c, bg.sP, (float)(g.dsi[P] * INV12), gm1, ch2, D);
       // interior only: the edge-tile fill writes the ghost images
-      if (stage < 3) {
+      if (!LAST) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
           float v = A0[f] - dt * D[f];
@@ -504,7 +507,10 @@ void b32_rk(const BatchArgs &a, const FieldPtrs<const float> &prev,
             const FieldPtrs<const float> &u0, const FieldPtrs<float> &hi,
             const FieldPtrs<float> &lo, const FieldPtrs<float> &out, float *cc, int stage,
             int grid, cudaStream_t st) {
-  b32::rk_block_kernel<<<grid, BATCH_TILE, 0, st>>>(a, prev, u0, hi, lo, out, cc, stage);
+  if (stage == 3)
+    b32::rk_block_kernel<true><<<grid, BATCH_TILE, 0, st>>>(a, prev, u0, hi, lo, out, cc, stage);
+  else
+    b32::rk_block_kernel<false><<<grid, BATCH_TILE, 0, st>>>(a, prev, u0, hi, lo, out, cc, stage);
 }
 void b32_av(const BatchArgs &a, const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
             const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc, int dir,
@@ -520,8 +526,8 @@ void b32_shell_fill(const BatchArgs &a, const int4 *cells, int n, const FieldPtr
 }
 int b32_block_grid(int sms) {
   int rk = 0, av = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rk, b32::rk_block_kernel, BATCH_TILE, 0) !=
-          cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rk, b32::rk_block_kernel<true>, BATCH_TILE,
+                                                    0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&av, b32::av_block_kernel, BATCH_TILE, 0) !=
           cudaSuccess)
     return 2 * sms;

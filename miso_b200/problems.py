@@ -37,6 +37,7 @@ class Problem:
     config: dict
     q: np.ndarray                      # (9, I, J, K) float64, reference layout
     sign: np.ndarray = None            # (3, 2, 9) mirror signs on symmetric faces
+    blend: np.ndarray = None           # state the magnetosphere boundary blends toward
 
     def __post_init__(self):
         if self.sign is None:
@@ -167,6 +168,51 @@ def with_point_gravity(prob: Problem, g: float) -> Problem:
     cfg = dict(prob.config)
     cfg["source"] = {"kind": "point_gravity", "g": float(g)}
     return Problem(prob.name + "_grav", prob.grid, cfg, prob.q, prob.sign)
+
+
+def magnetosphere(n: int = 128, extent: float = 44.8, radius: float = 3.5,
+                  blend_to_initial: bool = True) -> Problem:
+    """The magnetosphere demo (demo/mhd3d_magnetosphere: config.yaml and
+    src/ic.hpp): a dipole planet at the origin of [-extent, extent]^3 in the
+    solar wind, with the demo's boundary (mirror faces, the solar wind held
+    in the x-inner ghosts, a blend toward a reference state near the sphere
+    r = radius, floors), its CFL with that sphere masked and its point
+    gravity.  ro = max(r^-3, 0.2 ro_sw), B the dipole r^-5 (-3xz, -3yz,
+    x^2 + y^2 - 2z^2), p = max(p_earth r^-2, p_sw), v = 0, and the solar
+    wind on x < x_min + 0.8.  The demo blends toward a field state that it
+    allocates and never writes; here ``blend`` is the initial condition
+    (zeros with ``blend_to_initial=False``).  Even n keeps cell centres off
+    the origin."""
+    g = Grid(n, n, n, 2, -extent, extent, -extent, extent, -extent, extent)
+    gm = 5.0 / 3.0
+    cfg = make_config(gm, periodic=(False, False, False), cfl_number=0.3, ep=1.2, fh=1.0,
+                      cs_fac=1.0, ca_fac=0.8, vv_fac=1.0)
+    sw = {"mass_density": 5.0e-4, "gas_pressure": 3.56e-8, "x_velocity_field": 0.05,
+          "z_magnetic_field": -1.5e-4}
+    ms = {"gas_pressure": 5.4e-7, "radius": float(radius), "a0": 100.0,
+          "gravitational_acceleration": 1.35e-6}
+    cfg["boundary"] = {"kind": "magnetosphere", "cfl_mask": True}
+    cfg["solar_wind"] = sw
+    cfg["magnetosphere"] = ms
+    cfg["floor"] = {"ro_floor": 1.0e-8, "pr_floor": 1.0e-10}
+    cfg["source"] = {"kind": "point_gravity", "g": ms["gravitational_acceleration"]}
+    X, Y, Z = np.meshgrid(g.x, g.y, g.z, indexing="ij")
+    rr = np.sqrt(X * X + Y * Y + Z * Z)
+    q = _alloc(g)
+    q[RO] = np.maximum(rr ** -3, 0.2 * sw["mass_density"])
+    r5 = rr ** -5
+    q[BX] = -r5 * 3.0 * X * Z
+    q[BY] = -r5 * 3.0 * Y * Z
+    q[BZ] = r5 * (X * X + Y * Y - 2.0 * Z * Z)
+    pr = np.maximum(ms["gas_pressure"] * rr ** -2, sw["gas_pressure"])
+    q[EI] = pr / (gm - 1.0) / q[RO]
+    wind = X < g.x_min + 0.8
+    q[RO][wind] = sw["mass_density"]
+    q[EI][wind] = sw["gas_pressure"] / (gm - 1.0) / sw["mass_density"]
+    q[VX][wind] = sw["x_velocity_field"]
+    q[BZ][wind] = sw["z_magnetic_field"]
+    blend = q.copy() if blend_to_initial else np.zeros_like(q)
+    return Problem(f"magnetosphere_{n}", g, cfg, q, None, blend)
 
 
 def turbulence(n: int = 256, seed: int = 0, mach: float = 0.5, beta: float = 1.0,

@@ -126,38 +126,95 @@ static inline long IDX(const geom *g, int i, int j, int k) {
 /* update reads them (all stencils are axis-aligned), so interior results  */
 /* are unaffected.                                                          */
 /* ---------------------------------------------------------------------- */
-static void fill_axis(const geom *g, const miso_oracle_desc *d, double *const q[NF], int a) {
+/* One face (axis a, side 0 inner / 1 outer) for the fields in `mask`. */
+static void fill_face(const geom *g, const miso_oracle_desc *d, double *const q[NF], int a,
+                      int side, unsigned mask) {
   if (!g->s[a]) return;
   const int m = g->m[a], t = g->t[a];
   const int b = (a + 1) % 3, c = (a + 2) % 3;
-  for (int side = 0; side < 2; ++side) {
-    for (int gi = 0; gi < m; ++gi) {
-      int dst, src;
-      double sgn[NF];
-      if (d->periodic[a]) {
-        dst = side == 0 ? gi : t - m + gi;
-        src = side == 0 ? t - 2 * m + gi : m + gi;
-        for (int f = 0; f < NF; ++f) sgn[f] = 1.0;
-      } else {
-        dst = side == 0 ? gi : t - m + gi;
-        src = side == 0 ? 2 * m - gi - 1 : t - m - gi - 1;
-        for (int f = 0; f < NF; ++f) sgn[f] = d->sign[a][side][f];
-      }
-      for (int u = 0; u < g->t[b]; ++u) {
-        for (int v = 0; v < g->t[c]; ++v) {
-          int id[3], is_[3];
-          id[a] = dst; id[b] = u; id[c] = v;
-          is_[a] = src; is_[b] = u; is_[c] = v;
-          long ld = IDX(g, id[0], id[1], id[2]);
-          long ls = IDX(g, is_[0], is_[1], is_[2]);
-          for (int f = 0; f < NF; ++f) q[f][ld] = sgn[f] * q[f][ls];
-        }
+  for (int gi = 0; gi < m; ++gi) {
+    int dst, src;
+    double sgn[NF];
+    if (d->periodic[a]) {
+      dst = side == 0 ? gi : t - m + gi;
+      src = side == 0 ? t - 2 * m + gi : m + gi;
+      for (int f = 0; f < NF; ++f) sgn[f] = 1.0;
+    } else {
+      dst = side == 0 ? gi : t - m + gi;
+      src = side == 0 ? 2 * m - gi - 1 : t - m - gi - 1;
+      for (int f = 0; f < NF; ++f) sgn[f] = d->sign[a][side][f];
+    }
+    for (int u = 0; u < g->t[b]; ++u) {
+      for (int v = 0; v < g->t[c]; ++v) {
+        int id[3], is_[3];
+        id[a] = dst; id[b] = u; id[c] = v;
+        is_[a] = src; is_[b] = u; is_[c] = v;
+        long ld = IDX(g, id[0], id[1], id[2]);
+        long ls = IDX(g, is_[0], is_[1], is_[2]);
+        for (int f = 0; f < NF; ++f)
+          if ((mask >> f) & 1u) q[f][ld] = sgn[f] * q[f][ls];
       }
     }
   }
 }
 
+static void fill_axis(const geom *g, const miso_oracle_desc *d, double *const q[NF], int a) {
+  fill_face(g, d, q, a, 0, 0x1ffu);
+  fill_face(g, d, q, a, 1, 0x1ffu);
+}
+
+/* ---------------------------------------------------------------------- */
+/* The magnetosphere demo's boundary (demo/mhd3d_magnetosphere/src/bc.hpp: */
+/* 39-158), in its order: mirror on x outer, y inner / outer, z inner /     */
+/* outer (all fields), x inner (vy, vz, bx, by, ph); the x-inner ghosts of   */
+/* ro, vx, ei, bz set to the solar wind; then on every cell, ghosts         */
+/* included, ro..ph blended toward the `blend` state with weight f = a0 h / */
+/* (a0 h + 1), h = max2(0, (r / r_inner)^2 - 1), and the floors             */
+/* ro = max2(ro, ro_floor), ei = max2(ei, pr_floor / (gm - 1) / ro).  max2  */
+/* is the reference's float-rounded util::max2.                             */
+/* ---------------------------------------------------------------------- */
+static void magnetosphere_bc(const geom *g, const miso_oracle_desc *d, double *const q[NF]) {
+  fill_face(g, d, q, 0, 1, 0x1ffu);
+  fill_face(g, d, q, 1, 0, 0x1ffu);
+  fill_face(g, d, q, 1, 1, 0x1ffu);
+  fill_face(g, d, q, 2, 0, 0x1ffu);
+  fill_face(g, d, q, 2, 1, 0x1ffu);
+  fill_face(g, d, q, 0, 0, (1u << VY) | (1u << VZ) | (1u << BX) | (1u << BY) | (1u << PH));
+  if (g->s[0])
+    for (int i = 0; i < g->m[0]; ++i)
+      for (int j = 0; j < g->t[1]; ++j)
+        for (int k = 0; k < g->t[2]; ++k) {
+          const long c = IDX(g, i, j, k); /* the inner ghosts i < m (symmetric_index) */
+          q[RO][c] = d->sw_ro;
+          q[VX][c] = d->sw_vx;
+          q[EI][c] = d->sw_pr / (d->gm - 1.0) / q[RO][c];
+          q[BZ][c] = d->sw_bz;
+        }
+  for (int i = 0; i < g->t[0]; ++i)
+    for (int j = 0; j < g->t[1]; ++j)
+      for (int k = 0; k < g->t[2]; ++k) {
+        const long c = IDX(g, i, j, k);
+        const double x = g->ax[0][i], y = g->ax[1][j], z = g->ax[2][k];
+        const double rr = sqrt(x * x + y * y + z * z);
+        const double r1 = rr / d->r_inner;
+        const double hh = fmax2(0.0, r1 * r1 - 1.0);
+        const double f = d->a0 * hh / (d->a0 * hh + 1.0);
+        for (int v = 0; v < NF; ++v) {
+          const double b = d->blend[v] ? d->blend[v][c] : 0.0;
+          q[v][c] = q[v][c] * f + b * (1.0 - f);
+        }
+        q[RO][c] = fmax2(q[RO][c], d->ro_floor);
+        q[EI][c] = fmax2(q[EI][c], d->pr_floor / (d->gm - 1.0) / q[RO][c]);
+      }
+}
+
+/* Integrator::apply_boundary_condition: the boundary functor, then the halo
+ * exchange (periodic faces of one rank). */
 static void fill_ghosts(const geom *g, const miso_oracle_desc *d, double *const q[NF]) {
+  if (d->boundary == 1) {
+    magnetosphere_bc(g, d, q);
+    return;
+  }
   for (int a = 0; a < 3; ++a) fill_axis(g, d, q, a);
 }
 
@@ -409,6 +466,14 @@ static double cfl(const geom *g, const miso_oracle_desc *d, double *const q[NF])
         double ca = sqrt((+q[BX][c] * q[BX][c] + q[BY][c] * q[BY][c] + q[BZ][c] * q[BZ][c]) /
                          q[RO][c] * PII4);
         double total_vel = cs + vv + ca;
+        if (d->cfl_masked) {
+          /* demo/mhd3d_magnetosphere/src/timestep.hpp:15-49: the sphere
+           * r <= r_inner moves at slow_speed 1e-10 */
+          const double x = g->ax[0][i], y = g->ax[1][j], z = g->ax[2][k];
+          const double rr = sqrt(x * x + y * y + z * z);
+          const double mask = rr > d->r_inner ? 1.0 : 0.0;
+          total_vel = total_vel * mask + 1.e-10 * (1.0 - mask);
+        }
         dt = fmin2(dt, d->cfl_number * fmin3(g->dax[0][i], g->dax[1][j], g->dax[2][k]) /
                            total_vel);
       }

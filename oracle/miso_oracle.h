@@ -36,6 +36,17 @@ typedef struct miso_oracle_desc {
   double cs_fac, ca_fac, vv_fac;
   int source;                 /* 0 EmptySourceTerm, 1 point gravity at the origin */
   double g_grav;              /* its gravitational constant (force -ro g x / |x|^3) */
+  /* Boundary: 0 = the mirror / periodic faces above; 1 = the magnetosphere
+   * demo's boundary (demo/mhd3d_magnetosphere/src/bc.hpp:39-158): mirror
+   * faces, the solar-wind ro, vx, ei, bz fixed in the x-inner ghosts, then on
+   * every cell a blend toward `blend` near the sphere r = r_inner and floors
+   * on ro and ei.  Non-periodic axes only. */
+  int boundary;
+  double sw_ro, sw_pr, sw_vx, sw_bz; /* solar_wind: mass_density, gas_pressure, x_velocity_field, z_magnetic_field */
+  double r_inner, a0;                /* magnetosphere: radius, a0 */
+  double ro_floor, pr_floor;         /* floor: ro_floor, pr_floor */
+  const double *blend[9];            /* primitive state with ghosts; NULL: zeros */
+  int cfl_masked;                    /* 1: the demo's CFL with r <= r_inner masked (timestep.hpp:15-49) */
 } miso_oracle_desc;
 
 /* Fill every ghost cell of q (9 arrays) from its periodic or mirror image. */

@@ -38,10 +38,18 @@ class Desc(ctypes.Structure):
                 ("ep", ctypes.c_double), ("fh", ctypes.c_double),
                 ("cs_fac", ctypes.c_double), ("ca_fac", ctypes.c_double),
                 ("vv_fac", ctypes.c_double),
-                ("source", ctypes.c_int), ("g_grav", ctypes.c_double)]
+                ("source", ctypes.c_int), ("g_grav", ctypes.c_double),
+                ("boundary", ctypes.c_int),
+                ("sw_ro", ctypes.c_double), ("sw_pr", ctypes.c_double),
+                ("sw_vx", ctypes.c_double), ("sw_bz", ctypes.c_double),
+                ("r_inner", ctypes.c_double), ("a0", ctypes.c_double),
+                ("ro_floor", ctypes.c_double), ("pr_floor", ctypes.c_double),
+                ("blend", ctypes.c_void_p * 9), ("cfl_masked", ctypes.c_int)]
 
 
-def make_desc(grid, config, sign=None) -> Desc:
+def make_desc(grid, config, sign=None, blend=None) -> Desc:
+    """The descriptor of a run; ``blend`` (a (9, I, J, K) float64 array) is
+    the state the magnetosphere boundary blends toward (zeros if None)."""
     d = Desc()
     d.i_size, d.j_size, d.k_size, d.margin = grid.i_size, grid.j_size, grid.k_size, grid.margin
     d.x_min, d.x_max = grid.x_min, grid.x_max
@@ -60,6 +68,20 @@ def make_desc(grid, config, sign=None) -> Desc:
     src = config.get("source") or {}
     d.source = {"none": 0, "point_gravity": 1}[src.get("kind", "none")]
     d.g_grav = float(src.get("g", 0.0))
+    bnd = config.get("boundary") or {}
+    if bnd.get("kind", "faces") == "magnetosphere":
+        sw, ms, fl = config["solar_wind"], config["magnetosphere"], config["floor"]
+        d.boundary = 1
+        d.sw_ro, d.sw_pr = sw["mass_density"], sw["gas_pressure"]
+        d.sw_vx, d.sw_bz = sw["x_velocity_field"], sw["z_magnetic_field"]
+        d.r_inner, d.a0 = ms["radius"], ms["a0"]
+        d.ro_floor, d.pr_floor = fl["ro_floor"], fl["pr_floor"]
+        d.cfl_masked = int(bool(bnd.get("cfl_mask", True)))
+        if blend is not None:
+            assert blend.dtype == np.float64 and blend.flags.c_contiguous and blend.shape[0] == 9
+            for f in range(9):
+                d.blend[f] = blend[f].ctypes.data
+            d._keep = blend  # the arrays outlive the call
     return d
 
 
@@ -111,7 +133,7 @@ class _Lib:
 
     def run(self, prob, q: np.ndarray, nsteps: int, fill_first: bool = True):
         """Advance ``q`` in place by ``nsteps`` (cfl + update); returns the dts."""
-        d = make_desc(prob.grid, prob.config, prob.sign)
+        d = make_desc(prob.grid, prob.config, prob.sign, getattr(prob, "blend", None))
         dts = np.zeros(max(nsteps, 1))
         rc = self._run(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p), nsteps,
                        int(fill_first), dts.ctypes.data_as(_dp))
@@ -120,11 +142,11 @@ class _Lib:
         return dts[:nsteps]
 
     def cfl(self, prob, q):
-        d = make_desc(prob.grid, prob.config, prob.sign)
+        d = make_desc(prob.grid, prob.config, prob.sign, getattr(prob, "blend", None))
         return self._cfl(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p))
 
     def stage(self, prob, orgn, argm, rslt, dt, ch2, tau):
-        d = make_desc(prob.grid, prob.config, prob.sign)
+        d = make_desc(prob.grid, prob.config, prob.sign, getattr(prob, "blend", None))
         rc = self._stage(ctypes.byref(d), ctypes.cast(_ptrs(orgn), ctypes.c_void_p),
                          ctypes.cast(_ptrs(argm), ctypes.c_void_p),
                          ctypes.cast(_ptrs(rslt), ctypes.c_void_p), dt, ch2, tau)
@@ -132,19 +154,19 @@ class _Lib:
             raise RuntimeError(f"{self.prefix}stage failed: {rc}")
 
     def av(self, prob, q, dt):
-        d = make_desc(prob.grid, prob.config, prob.sign)
+        d = make_desc(prob.grid, prob.config, prob.sign, getattr(prob, "blend", None))
         rc = self._av(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p), dt)
         if rc:
             raise RuntimeError(f"{self.prefix}av failed: {rc}")
 
     def fill_ghosts(self, prob, q):
-        d = make_desc(prob.grid, prob.config, prob.sign)
+        d = make_desc(prob.grid, prob.config, prob.sign, getattr(prob, "blend", None))
         rc = self._fill(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p))
         if rc:
             raise RuntimeError(f"{self.prefix}fill_ghosts failed: {rc}")
 
     def min_dxyz(self, prob):
-        d = make_desc(prob.grid, prob.config, prob.sign)
+        d = make_desc(prob.grid, prob.config, prob.sign, getattr(prob, "blend", None))
         return self._mind(ctypes.byref(d))
 
 
@@ -162,7 +184,7 @@ class Reference(_Lib):
         f = self.lib.miso_ref_update
         f.argtypes = [ctypes.POINTER(Desc), ctypes.c_void_p, ctypes.c_double]
         f.restype = ctypes.c_int
-        d = make_desc(prob.grid, prob.config, prob.sign)
+        d = make_desc(prob.grid, prob.config, prob.sign, getattr(prob, "blend", None))
         rc = f(ctypes.byref(d), ctypes.cast(_ptrs(q), ctypes.c_void_p), float(dt))
         if rc:
             raise RuntimeError(f"{self.prefix}update failed: {rc}")

@@ -64,6 +64,122 @@ struct DescBC {
   }
 };
 
+// The magnetosphere demo's boundary (demo/mhd3d_magnetosphere/src/bc.hpp:
+// 39-158), restated as a boundary functor of the reference's concept on the
+// reference's own boundary_condition helpers and util::max2: mirror faces
+// (x outer, y inner / outer, z inner / outer for all fields; x inner for vy,
+// vz, bx, by, ph), the solar wind fixed in the x-inner ghosts of ro, vx, ei,
+// bz, then on every cell a blend toward the state qq_init and floors on ro
+// and ei.  The demo allocates qq_init and never writes it; here it holds the
+// descriptor's blend state (zeros where none is given).
+struct MagnetoBC {
+  mpi::Shape &shape;
+  double sign[3][2][9];
+  Real gm, ro_sw, pr_sw, vx_sw, bz_imf, rra, a0, ro_floor, pr_floor;
+  mhd::Fields<Real, B> qq_init;
+
+  MagnetoBC(mpi::Shape &s, const miso_oracle_desc &d, Grid<Real, B> &g)
+      : shape(s), gm(d.gm), ro_sw(d.sw_ro), pr_sw(d.sw_pr), vx_sw(d.sw_vx), bz_imf(d.sw_bz),
+        rra(d.r_inner), a0(d.a0), ro_floor(d.ro_floor), pr_floor(d.pr_floor),
+        qq_init(g.i_total, g.j_total, g.k_total) {
+    std::memcpy(sign, d.sign, sizeof(sign));
+    Array3D<Real, B> *f[9] = {&qq_init.ro, &qq_init.vx, &qq_init.vy, &qq_init.vz, &qq_init.bx,
+                              &qq_init.by, &qq_init.bz, &qq_init.ei, &qq_init.ph};
+    for (int v = 0; v < 9; ++v)
+      for (size_t n = 0; n < f[v]->size(); ++n)
+        f[v]->data()[n] = d.blend[v] ? (Real)d.blend[v][n] : Real(0);
+  }
+
+  void mirror(mhd::FieldsView<Real> &qq, GridView<const Real> grid, int a, int s,
+              unsigned mask) const {
+    namespace bc = miso::boundary_condition;
+    Array3DView<Real> *f[9] = {&qq.ro, &qq.vx, &qq.vy, &qq.vz, &qq.bx,
+                               &qq.by, &qq.bz, &qq.ei, &qq.ph};
+    const Direction dirs[3] = {Direction::X, Direction::Y, Direction::Z};
+    const Side sides[2] = {Side::INNER, Side::OUTER};
+    if (!bc::is_physical_boundary(dirs[a], sides[s], shape)) return;
+    for (int v = 0; v < 9; ++v)
+      if ((mask >> v) & 1u)
+        bc::symmetric(B{}, *f[v], grid, sign[a][s][v] < 0 ? Sign::Neg : Sign::Pos, dirs[a],
+                      sides[s]);
+  }
+
+  void apply(mhd::FieldsView<Real> qq, GridView<const Real> grid) const {
+    namespace bc = miso::boundary_condition;
+    mirror(qq, grid, 0, 1, 0x1ffu);
+    mirror(qq, grid, 1, 0, 0x1ffu);
+    mirror(qq, grid, 1, 1, 0x1ffu);
+    mirror(qq, grid, 2, 0, 0x1ffu);
+    mirror(qq, grid, 2, 1, 0x1ffu);
+    if (bc::is_physical_boundary(Direction::X, Side::INNER, shape)) {
+      mirror(qq, grid, 0, 0, (1u << 2) | (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8));
+      int i0, i1, j0, j1, k0, k1;
+      bc::range_set(i0, i1, j0, j1, k0, k1, Direction::X, grid);
+      for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+          for (int k = k0; k < k1; ++k) {
+            int ig, it;
+            bc::symmetric_index(i, grid.i_total, grid.i_margin, ig, it, Side::INNER);
+            qq.ro(ig, j, k) = ro_sw;
+            qq.vx(ig, j, k) = vx_sw;
+            qq.ei(ig, j, k) = pr_sw / (gm - 1.0) / qq.ro(ig, j, k);
+            qq.bz(ig, j, k) = bz_imf;
+          }
+    }
+    auto qi = qq_init.const_view();
+    for (int i = 0; i < grid.i_total; ++i)
+      for (int j = 0; j < grid.j_total; ++j)
+        for (int k = 0; k < grid.k_total; ++k) {
+          const Real rr = util::sqrt(grid.x[i] * grid.x[i] + grid.y[j] * grid.y[j] +
+                                     grid.z[k] * grid.z[k]);
+          const Real hh = util::max2<Real>(0.0, util::pow2(rr / rra) - 1.0);
+          const Real f = a0 * hh / (a0 * hh + 1.0);
+          auto lerp = [f](Real a, Real b) { return a * f + b * (1.0 - f); };
+          qq.ro(i, j, k) = lerp(qq.ro(i, j, k), qi.ro(i, j, k));
+          qq.vx(i, j, k) = lerp(qq.vx(i, j, k), qi.vx(i, j, k));
+          qq.vy(i, j, k) = lerp(qq.vy(i, j, k), qi.vy(i, j, k));
+          qq.vz(i, j, k) = lerp(qq.vz(i, j, k), qi.vz(i, j, k));
+          qq.bx(i, j, k) = lerp(qq.bx(i, j, k), qi.bx(i, j, k));
+          qq.by(i, j, k) = lerp(qq.by(i, j, k), qi.by(i, j, k));
+          qq.bz(i, j, k) = lerp(qq.bz(i, j, k), qi.bz(i, j, k));
+          qq.ei(i, j, k) = lerp(qq.ei(i, j, k), qi.ei(i, j, k));
+          qq.ph(i, j, k) = lerp(qq.ph(i, j, k), qi.ph(i, j, k));
+          qq.ro(i, j, k) = util::max2<Real>(qq.ro(i, j, k), ro_floor);
+          qq.ei(i, j, k) = util::max2<Real>(qq.ei(i, j, k), pr_floor / (gm - 1.0) / qq.ro(i, j, k));
+        }
+  }
+};
+
+// The demo's CFL with the sphere r <= radius masked
+// (demo/mhd3d_magnetosphere/src/timestep.hpp:15-49), on the reference's own
+// reduce and util::min2 / min3.
+Real masked_cfl(const mhd::Fields<Real, B> &qq, const Grid<Real, B> &grid, Real gm,
+                Real cfl_number, Real rra) {
+  const Real slow_speed = 1.e-10;
+  const Real dt_max = 1.e10;
+  auto qq_v = qq.const_view();
+  auto grid_v = grid.const_view();
+  Range3D range{{grid.i_margin, grid.i_total - grid.i_margin},
+                {grid.j_margin, grid.j_total - grid.j_margin},
+                {grid.k_margin, grid.k_total - grid.k_margin}};
+  const auto f = [=](int i, int j, int k) {
+    Real cs = util::sqrt(gm * (gm - 1.0) * qq_v.ei(i, j, k));
+    Real vv = util::sqrt(qq_v.vx(i, j, k) * qq_v.vx(i, j, k) + qq_v.vy(i, j, k) * qq_v.vy(i, j, k) +
+                         qq_v.vz(i, j, k) * qq_v.vz(i, j, k));
+    Real ca = util::sqrt((qq_v.bx(i, j, k) * qq_v.bx(i, j, k) + qq_v.by(i, j, k) * qq_v.by(i, j, k) +
+                          qq_v.bz(i, j, k) * qq_v.bz(i, j, k)) /
+                         qq_v.ro(i, j, k) * pii4<Real>);
+    Real total_vel = (cs + vv + ca);
+    Real rr = util::sqrt(util::pow2(grid_v.x[i]) + util::pow2(grid_v.y[j]) + util::pow2(grid_v.z[k]));
+    Real mask = rr > rra ? 1.0 : 0.0;
+    Real masked_vel = total_vel * mask + slow_speed * (1.0 - mask);
+    Real dxyz = util::min3(grid_v.dx[i], grid_v.dy[j], grid_v.dz[k]);
+    return cfl_number * dxyz / masked_vel;
+  };
+  const auto op = [](Real a, Real b) { return util::min2(a, b); };
+  return reduce(B{}, range, dt_max, f, op);
+}
+
 // The point gravity of the magnetosphere demo
 // (demo/mhd3d_magnetosphere/src/src.hpp:17-44), restated as a source
 // functor of the reference's Source concept (mhd_model_base.hpp:131-155):
@@ -99,9 +215,33 @@ struct Session {
   std::unique_ptr<mhd::Integrator<Real, B>> integ;
   std::unique_ptr<eos::IdealEOS<Real>> eos;
   std::unique_ptr<DescBC> bc;
+  std::unique_ptr<MagnetoBC> mbc;
   mhd::EmptySourceTerm<Real> src;
+  const miso_oracle_desc &desc;
 
-  explicit Session(const miso_oracle_desc &d) {
+  // f(boundary functor) with the descriptor's boundary
+  template <class F> void with_bc(F &&f) {
+    if (desc.boundary == 1)
+      f(*mbc);
+    else
+      f(*bc);
+  }
+  // Integrator::update with the descriptor's boundary and source
+  void update(Real dt, mhd::Fields<Real, B> &qq) {
+    with_bc([&](auto &b) {
+      if (desc.source == 1)
+        integ->update(dt, *eos, b, PointGravity(*grid, (Real)desc.g_grav), qq);
+      else
+        integ->update(dt, *eos, b, src, qq);
+    });
+  }
+  Real cfl(const mhd::Fields<Real, B> &qq) {
+    if (desc.cfl_masked)
+      return masked_cfl(qq, *grid, eos->gm, (Real)desc.cfl_number, (Real)desc.r_inner);
+    return integ->cfl(qq, *eos);
+  }
+
+  explicit Session(const miso_oracle_desc &d) : desc(d) {
     static Env *global_env = new Env();
     (void)global_env;
     char tmpl[] = "/tmp/miso_ref_cfgXXXXXX";
@@ -136,6 +276,7 @@ struct Session {
     integ.reset(new mhd::Integrator<Real, B>(*config, *grid, *ctx));
     eos.reset(new eos::IdealEOS<Real>(d.gm));
     bc.reset(new DescBC(*shape, d));
+    if (d.boundary == 1) mbc.reset(new MagnetoBC(*shape, d, *grid));
   }
   ~Session() { std::remove(path.c_str()); }
 };
@@ -164,15 +305,11 @@ int miso_ref_run(const miso_oracle_desc *d, double *const q[9], int nsteps, int 
     Session s(*d);
     mhd::Fields<Real, B> qq(*s.grid);
     to_fields(qq, q);
-    if (fill_first) s.integ->apply_boundary_condition(*s.bc, qq);
-    PointGravity grav(*s.grid, d->g_grav);
+    if (fill_first) s.with_bc([&](auto &b) { s.integ->apply_boundary_condition(b, qq); });
     for (int n = 0; n < nsteps; ++n) {
-      const Real dt = s.integ->cfl(qq, *s.eos);
+      const Real dt = s.cfl(qq);
       if (dt_out) dt_out[n] = dt;
-      if (d->source == 1)
-        s.integ->update(dt, *s.eos, *s.bc, grav, qq);
-      else
-        s.integ->update(dt, *s.eos, *s.bc, s.src, qq);
+      s.update(dt, qq);
     }
     from_fields(qq, q);
     return 0;
@@ -188,11 +325,7 @@ int miso_ref_update(const miso_oracle_desc *d, double *const q[9], double dt) {
     Session s(*d);
     mhd::Fields<Real, B> qq(*s.grid);
     to_fields(qq, q);
-    PointGravity grav(*s.grid, (Real)d->g_grav);
-    if (d->source == 1)
-      s.integ->update((Real)dt, *s.eos, *s.bc, grav, qq);
-    else
-      s.integ->update((Real)dt, *s.eos, *s.bc, s.src, qq);
+    s.update((Real)dt, qq);
     from_fields(qq, q);
     return 0;
   } catch (const std::exception &e) {
@@ -206,7 +339,7 @@ double miso_ref_cfl(const miso_oracle_desc *d, double *const q[9]) {
     Session s(*d);
     mhd::Fields<Real, B> qq(*s.grid);
     to_fields(qq, q);
-    return s.integ->cfl(qq, *s.eos);
+    return s.cfl(qq);
   } catch (const std::exception &e) {
     std::fprintf(stderr, "miso_ref_cfl: %s\n", e.what());
     return -1.0;
@@ -241,7 +374,7 @@ int miso_ref_av(const miso_oracle_desc *d, double *const q[9], double dt) {
     Session s(*d);
     mhd::Fields<Real, B> qq(*s.grid);
     to_fields(qq, q);
-    s.integ->apply_artificial_viscosity(dt, *s.eos, *s.bc, qq);
+    s.with_bc([&](auto &b) { s.integ->apply_artificial_viscosity(dt, *s.eos, b, qq); });
     from_fields(qq, q);
     return 0;
   } catch (const std::exception &e) {
@@ -255,7 +388,7 @@ int miso_ref_fill_ghosts(const miso_oracle_desc *d, double *const q[9]) {
     Session s(*d);
     mhd::Fields<Real, B> qq(*s.grid);
     to_fields(qq, q);
-    s.integ->apply_boundary_condition(*s.bc, qq);
+    s.with_bc([&](auto &b) { s.integ->apply_boundary_condition(b, qq); });
     from_fields(qq, q);
     return 0;
   } catch (const std::exception &e) {

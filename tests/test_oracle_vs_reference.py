@@ -22,6 +22,10 @@ CASES = [
     # the magnetosphere demo's point-gravity source term
     ("blast10_grav", lambda: P.with_point_gravity(P.blast(10, seed=6), 0.3), 3),
     ("ot24_grav", lambda: P.with_point_gravity(P.orszag_tang(24), 2.0), 6),
+    # the magnetosphere demo: its boundary (solar-wind inflow, blend toward a
+    # state near the sphere, floors), masked CFL and gravity
+    ("magneto16", lambda: P.magnetosphere(16, extent=12.0), 4),
+    ("magneto16_zero_blend", lambda: P.magnetosphere(16, extent=12.0, blend_to_initial=False), 3),
 ]
 
 
@@ -67,3 +71,25 @@ def test_cfl_and_min_dxyz(oracle, reference):
         oracle.fill_ghosts(prob, q)
         assert oracle.cfl(prob, q) == reference.cfl(prob, q)
         assert oracle.min_dxyz(prob) == reference.min_dxyz(prob)
+
+
+@pytest.mark.parametrize("blend", [True, False])
+def test_magnetosphere_boundary_bit_exact(oracle, reference, blend):
+    """The magnetosphere demo's boundary on every cell, ghosts included (the
+    oracle applies its faces in the demo's order), and its masked CFL."""
+    prob = P.magnetosphere(16, extent=12.0, blend_to_initial=blend)
+    rng = np.random.default_rng(7)
+    q = prob.q * (1.0 + 0.05 * rng.standard_normal(prob.q.shape))
+    q[P.EI] = np.abs(q[P.EI])
+    q[P.RO] = np.abs(q[P.RO])
+    a, b = q.copy(), q.copy()
+    oracle.fill_ghosts(prob, a)
+    reference.fill_ghosts(prob, b)
+    assert np.array_equal(a, b)
+    assert not np.array_equal(a, q)
+    assert oracle.cfl(prob, a) == reference.cfl(prob, b)
+    # the mask matters: without it the sphere's cells set a different step
+    nomask = P.magnetosphere(16, extent=12.0, blend_to_initial=blend)
+    nomask.config["boundary"]["cfl_mask"] = False
+    assert oracle.cfl(nomask, a) == reference.cfl(nomask, b)
+    assert oracle.cfl(nomask, a) != oracle.cfl(prob, a)

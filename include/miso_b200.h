@@ -150,6 +150,36 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]);
 #define MISO_B200_SOURCE_POINT_GRAVITY 1
 int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, int nparams);
 
+/* Boundary functor.  Replaces the `bc` argument of Integrator::update /
+ * apply_boundary_condition (miso/include/miso/mhd_integrator_host.hpp:
+ * 250-255) for a boundary other than the descriptor's per-face mirror /
+ * periodic one.  MISO_B200_BOUNDARY_FACES (the default) is that one.
+ * MISO_B200_BOUNDARY_MAGNETOSPHERE is the magnetosphere demo's boundary
+ * (demo/mhd3d_magnetosphere/src/bc.hpp:39-158), applied after every pass as
+ * the reference applies its functor:
+ *   - the descriptor's mirror faces;
+ *   - in the x-inner ghosts, ro, vx, ei and bz set to the solar wind
+ *     (ei = pr_sw / (gm - 1) / ro_sw);
+ *   - on every cell, ghosts included, each field blended toward the state
+ *     of miso_b200_set_blend_state (zeros until set) with weight
+ *     f = a0 h / (a0 h + 1), h = max(0, (r / radius)^2 - 1), r the distance
+ *     from the coordinate origin;
+ *   - floors ro >= ro_floor and ei >= pr_floor / (gm - 1) / ro.
+ * The maxima are rounded through float, as the reference's util::max2 is.
+ * params: [0] ro_sw, [1] pr_sw, [2] vx_sw, [3] bz_imf, [4] radius, [5] a0,
+ * [6] ro_floor, [7] pr_floor, [8] nonzero: miso_b200_cfl masks the sphere
+ * r <= radius as the demo's TimeStep::cfl does (timestep.hpp:15-49).
+ * FP64 form and non-periodic axes only (ERR_STATE / ERR_ARG otherwise).
+ * The FP64 form stays bit for bit the reference's. */
+#define MISO_B200_BOUNDARY_FACES 0
+#define MISO_B200_BOUNDARY_MAGNETOSPHERE 1
+int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, int nparams);
+/* The state the magnetosphere boundary blends toward: 9 primitive arrays
+ * with ghosts, host or device pointers, copied.  The demo allocates this
+ * state and never writes it; a caller passes the initial condition, or
+ * zeros for the demo as it runs on zero-filled memory. */
+int miso_b200_set_blend_state(miso_b200_handle *h, const double *const q[9]);
+
 /* Halo exchange of a grid decomposed into shards along i (the slowest
  * axis).  Replaces the reference's HaloExchanger for the neighbour faces of
  * a Cartesian decomposition (miso/include/miso/mhd_halo_exchange.hpp:

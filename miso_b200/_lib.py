@@ -80,6 +80,8 @@ SIGNATURES = {
     "miso_b200_launch_count": (ctypes.c_int, [ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_longlong)]),
     "miso_b200_set_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int]),
+    "miso_b200_set_boundary": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int]),
+    "miso_b200_set_blend_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "miso_b200_set_halo": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(HaloOps)]),
     "miso_b200_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),

@@ -182,6 +182,8 @@ struct miso_b200_handle {
   // built-in source term (miso_b200_set_source) and the cell centres it
   // reads, one array per axis (ghosts included)
   Source src{};
+  Magneto mag{};               // the magnetosphere demo's boundary (FP64 form)
+  double *blend_block = nullptr;  // its reference state (9 arrays), once set
   double *axc[3] = {};
   // halo exchange with neighbouring shards along i (miso_b200_set_halo)
   miso_b200_halo_ops halo_ops{};
@@ -352,6 +354,19 @@ struct miso_b200_handle {
     launches += g.s[0] + g.s[1] + g.s[2] - 1;
     return check_launch("fill_ghosts");
   }
+  // Integrator::apply_boundary_condition of the FP64 state: the mirror /
+  // periodic fill, then the magnetosphere boundary where it is on (the
+  // caller exchanges shared faces after both, as the reference's halo
+  // exchange follows its boundary functor)
+  int bc64(int set) {
+    int rc = fill64(set);
+    if (rc || !mag.on) return rc;
+    const int t = tb();
+    launch_magneto_bc(g, f64(set), mag, p.gm, sms, stream);
+    te(t, "magnetosphere_bc", (double)g.cells * 144.0);
+    launches += 1;
+    return check_launch("magnetosphere boundary");
+  }
   int fill_split(int s) {
     const int t = tb();
     launch_fill_ghosts<float>(g, H(s), NF, sms, stream);
@@ -369,7 +384,7 @@ struct miso_b200_handle {
   }
 
   int fill_state() {
-    int rc = split() ? fill_split(cur) : fill64(0);
+    int rc = split() ? fill_split(cur) : bc64(0);
     if (rc) return rc;
     return split() ? halo_f(hi[cur], lo[cur]) : halo_d(q64[0]);
   }
@@ -481,7 +496,8 @@ struct miso_b200_handle {
       launch_cfl_finalize(partial, nparts, sc, p.cfl_number, min_dxyz, stream);
       te(t, "cfl", interior() * 32.0);
     } else {
-      launch_fp64_cfl(g, c64(0), partial, sc, p.gm, p.cfl_number, cfl_dx, min_dxyz, sms, stream);
+      launch_fp64_cfl(g, c64(0), partial, sc, p.gm, p.cfl_number, cfl_dx, min_dxyz, mag, sms,
+                      stream);
       te(t, "cfl", interior() * 64.0);
     }
     launches += 1;
@@ -500,7 +516,7 @@ struct miso_b200_handle {
                               stream);
         te(t, "rk_stage", interior() * (s == 0 ? 144.0 : 216.0));
         if ((rc = check_launch("rhs_stage"))) return rc;
-        if ((rc = fill64(seq_r[s]))) return rc;
+        if ((rc = bc64(seq_r[s]))) return rc;
         if ((rc = halo_d(q64[seq_r[s]]))) return rc;
       }
       // AV on B(2): x: B -> qq, y: qq -> A, z: A -> qq
@@ -514,7 +530,7 @@ struct miso_b200_handle {
         launch_fp64_av_sweep(g, c64(src[d]), f64(dst[d]), cc64, sc, d, p.ep, p.fh, sms, stream);
         te(t, "av_sweep", interior() * 152.0);
         if ((rc = check_launch("av_sweep"))) return rc;
-        if ((rc = fill64(dst[d]))) return rc;
+        if ((rc = bc64(dst[d]))) return rc;
         if ((rc = halo_d(q64[dst[d]]))) return rc;
       }
       return MISO_B200_OK;
@@ -925,6 +941,7 @@ int miso_b200_destroy(miso_b200_handle *h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->block) cudaFree(h->block);
+  if (h->blend_block) cudaFree(h->blend_block);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
   return MISO_B200_OK;
@@ -1048,6 +1065,71 @@ int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, in
     h->graph = nullptr;
   }
   return MISO_B200_OK;
+}
+
+int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, int nparams) {
+  if (!h) return MISO_B200_ERR_ARG;
+  if (kind == MISO_B200_BOUNDARY_FACES) {
+    h->mag.on = 0;
+    h->mag.mask_cfl = 0;
+  } else if (kind == MISO_B200_BOUNDARY_MAGNETOSPHERE) {
+    if (h->split())
+      return h->fail(MISO_B200_ERR_STATE, "the magnetosphere boundary runs on the FP64 form");
+    if (!params || nparams < 9)
+      return h->fail(MISO_B200_ERR_ARG, "the magnetosphere boundary takes 9 parameters");
+    for (int n = 0; n < 8; ++n)
+      if (!std::isfinite(params[n]))
+        return h->fail(MISO_B200_ERR_ARG, "non-finite boundary parameter %d", n);
+    if (!(params[4] > 0.0) || !(params[0] > 0.0))
+      return h->fail(MISO_B200_ERR_ARG, "radius and solar-wind density must be > 0");
+    for (int a = 0; a < 3; ++a)
+      if (h->g.s[a] && h->g.periodic[a])
+        return h->fail(MISO_B200_ERR_ARG, "the magnetosphere boundary needs non-periodic axes");
+    Magneto &m = h->mag;
+    m.ro_sw = params[0];
+    m.pr_sw = params[1];
+    m.vx_sw = params[2];
+    m.bz_sw = params[3];
+    m.r_inner = params[4];
+    m.a0 = params[5];
+    m.ro_floor = params[6];
+    m.pr_floor = params[7];
+    m.mask_cfl = params[8] != 0.0;
+    m.x = h->axc[0];
+    m.y = h->axc[1];
+    m.z = h->axc[2];
+    m.on = 1;
+  } else {
+    return h->fail(MISO_B200_ERR_ARG, "unknown boundary kind %d", kind);
+  }
+  h->partials_valid = false;
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_blend_state(miso_b200_handle *h, const double *const q[9]) {
+  if (!h || !q) return MISO_B200_ERR_ARG;
+  if (h->split())
+    return h->fail(MISO_B200_ERR_STATE, "the magnetosphere boundary runs on the FP64 form");
+  const size_t bytes = (size_t)h->g.cells * sizeof(double);
+  int rc;
+  if (!h->blend_block &&
+      (rc = h->cuda(cudaMalloc((void **)&h->blend_block, bytes * NF), "allocate blend state")))
+    return rc;
+  for (int f = 0; f < NF; ++f) {
+    if (!q[f]) return h->fail(MISO_B200_ERR_ARG, "null field pointer %d", f);
+    double *dst = h->blend_block + (size_t)f * h->g.cells;
+    if ((rc = h->cuda(cudaMemcpyAsync(dst, q[f], bytes, cudaMemcpyDefault, h->stream),
+                      "upload blend state")))
+      return rc;
+    h->mag.blend[f] = dst;
+  }
+  return h->cuda(cudaStreamSynchronize(h->stream), "upload blend state");
 }
 
 int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,

@@ -46,6 +46,18 @@ struct Geom {
 // (demo/mhd3d_magnetosphere/src/src.hpp:17-44).  x / y / z are the cell
 // centres per axis (total cells, ghosts included), as grid.hpp:22-31 places
 // them.
+// The magnetosphere demo's boundary (demo/mhd3d_magnetosphere/src/bc.hpp:
+// 39-158) and its masked CFL (timestep.hpp:15-49), for the FP64 form.
+struct Magneto {
+  int on;        // the boundary runs after every ghost fill
+  int mask_cfl;  // the CFL gives the sphere r <= r_inner the speed 1e-10
+  double ro_sw, pr_sw, vx_sw, bz_sw;  // solar wind held in the x-inner ghosts
+  double r_inner, a0;                 // blend toward `blend` near the sphere
+  double ro_floor, pr_floor;
+  const double *blend[9];  // primitive state with ghosts (null: zeros)
+  const double *x, *y, *z; // cell centres per axis, ghosts included
+};
+
 struct Source {
   int kind;  // 0 none, 1 point gravity
   double g;  // gravitational constant: force per volume -ro g x / |x|^3

@@ -277,7 +277,7 @@ av_z_shfl_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<double> r,
 // ----------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 cfl_partial_kernel(Geom g, FieldPtrs<const double> q, float *__restrict__ partial,
-                   unsigned int *__restrict__ err, double gm, double cfl_dx) {
+                   unsigned int *__restrict__ err, double gm, double cfl_dx, Magneto mg) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
   float best = 1.e10f;
   bool bad = false;
@@ -293,10 +293,19 @@ cfl_partial_kernel(Geom g, FieldPtrs<const double> q, float *__restrict__ partia
     const double cs = sqrt(gm * (gm - 1.0) * ei);
     const double vv = sqrt(+vx * vx + vy * vy + vz * vz);
     const double ca = sqrt((+bx * bx + by * by + bz * bz) / ro * PII4);
-    const double total_vel = cs + vv + ca;
+    double total_vel = cs + vv + ca;
+    bad |= !isfinite(total_vel);
+    if (mg.mask_cfl) {
+      // the magnetosphere demo's CFL (timestep.hpp:15-49): the sphere
+      // r <= r_inner moves at slow_speed 1e-10
+      const double x = mg.x[i], y = mg.y[j], z = mg.z[k];
+      const double rr = sqrt(x * x + y * y + z * z);
+      const double mask = rr > mg.r_inner ? 1.0 : 0.0;
+      total_vel = total_vel * mask + 1.e-10 * (1.0 - mask);
+    }
     // util::min2(dt, x): both sides through float; fminf ignores a NaN side.
     best = fminf(best, __double2float_rn(cfl_dx / total_vel));
-    bad |= !(ro > 0.0) || !(ei >= 0.0) || !isfinite(total_vel);
+    bad |= !(ro > 0.0) || !(ei >= 0.0);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
@@ -387,6 +396,50 @@ fill_axis_kernel(Geom g, FieldPtrs<T> q, int a, int nfields) {
   }
 }
 
+// The magnetosphere demo's boundary after the mirror fill (bc.hpp:39-158):
+// the x-inner ghosts of ro, vx, ei, bz take the solar wind (a physical face
+// only), then every cell, ghosts included, is blended toward the reference
+// state with weight f = a0 h / (a0 h + 1), h = max2(0, (r / r_inner)^2 - 1),
+// and floored: ro = max2(ro, ro_floor), ei = max2(ei, pr_floor / (gm - 1) /
+// ro).  max2 is the float-rounded util::max2 (utility.hpp:91-124).  The
+// mirror faces come first in a different face order than the demo's; that
+// changes edge and corner ghosts only, which no stencil reads.
+__global__ void __launch_bounds__(256)
+magneto_bc_kernel(Geom g, FieldPtrs<double> q, Magneto mg, double gm) {
+  const long long cells = g.cells;
+  const bool inflow = g.s[0] && !g.periodic[0] && !g.ext[0][0];
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cells;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(c % g.t[2]);
+    const long long r1 = c / g.t[2];
+    const int j = (int)(r1 % g.t[1]);
+    const int i = (int)(r1 / g.t[1]);
+    double u[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) u[f] = q.f[f][c];
+    if (inflow && i < g.m[0]) {
+      u[RO] = mg.ro_sw;
+      u[VX] = mg.vx_sw;
+      u[EI] = mg.pr_sw / (gm - 1.0) / u[RO];
+      u[BZ] = mg.bz_sw;
+    }
+    const double x = mg.x[i], y = mg.y[j], z = mg.z[k];
+    const double rr = sqrt(x * x + y * y + z * z);
+    const double r1n = rr / mg.r_inner;
+    const double hh = fmax2f(0.0, r1n * r1n - 1.0);
+    const double w = mg.a0 * hh / (mg.a0 * hh + 1.0);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const double b = mg.blend[f] ? mg.blend[f][c] : 0.0;
+      u[f] = u[f] * w + b * (1.0 - w);
+    }
+    u[RO] = fmax2f(u[RO], mg.ro_floor);
+    u[EI] = fmax2f(u[EI], mg.pr_floor / (gm - 1.0) / u[RO]);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) q.f[f][c] = u[f];
+  }
+}
+
 template __global__ void fill_axis_kernel<double>(Geom, FieldPtrs<double>, int, int);
 template __global__ void fill_axis_kernel<float>(Geom, FieldPtrs<float>, int, int);
 
@@ -448,9 +501,9 @@ int cfl_partial_blocks(int sms) { return sms * 4; }
 
 void launch_fp64_cfl(const Geom &g, const FieldPtrs<const double> &q, float *partial,
                      StepScalars *sc, double gm, double cfl_number, double cfl_dx,
-                     double min_dxyz, int sms, cudaStream_t st) {
+                     double min_dxyz, const Magneto &mg, int sms, cudaStream_t st) {
   const int nb = cfl_partial_blocks(sms);
-  fp64::cfl_partial_kernel<<<nb, 256, 0, st>>>(g, q, partial, &sc->err, gm, cfl_dx);
+  fp64::cfl_partial_kernel<<<nb, 256, 0, st>>>(g, q, partial, &sc->err, gm, cfl_dx, mg);
   cfl_finalize_kernel<<<1, 1024, 0, st>>>(partial, nb, sc, cfl_number, min_dxyz);
 }
 
@@ -468,6 +521,11 @@ void launch_fill_ghosts(const Geom &g, const FieldPtrs<T> &q, int nfields, int s
     const long long work = 2LL * g.m[a] * g.t[b] * g.t[c];
     fill_axis_kernel<T><<<grid_blocks(work, 256, sms, 8), 256, 0, st>>>(g, q, a, nfields);
   }
+}
+
+void launch_magneto_bc(const Geom &g, const FieldPtrs<double> &q, const Magneto &mg, double gm,
+                       int sms, cudaStream_t st) {
+  magneto_bc_kernel<<<grid_blocks(g.cells, 256, sms, 8), 256, 0, st>>>(g, q, mg, gm);
 }
 
 template void launch_fill_ghosts<double>(const Geom &, const FieldPtrs<double> &, int, int,

@@ -20,9 +20,12 @@ void launch_fp64_av_sweep(const Geom &g, const FieldPtrs<const double> &q,
 int cfl_partial_blocks(int sms);
 void launch_fp64_cfl(const Geom &g, const FieldPtrs<const double> &q, float *partial,
                      StepScalars *sc, double gm, double cfl_number, double cfl_dx,
-                     double min_dxyz, int sms, cudaStream_t st);
+                     double min_dxyz, const Magneto &mg, int sms, cudaStream_t st);
 void launch_cfl_finalize(const float *partial, int nparts, StepScalars *sc, double cfl_number,
                          double min_dxyz, cudaStream_t st);
+// the magnetosphere demo's boundary after a mirror fill (FP64 state)
+void launch_magneto_bc(const Geom &g, const FieldPtrs<double> &q, const Magneto &mg, double gm,
+                       int sms, cudaStream_t st);
 template <typename T>
 void launch_fill_ghosts(const Geom &g, const FieldPtrs<T> &q, int nfields, int sms,
                         cudaStream_t st);

@@ -15,6 +15,10 @@ MHD demos use: ideal gas with ``eos.gm``; periodic faces where
 ``domain.periodic`` says so and the symmetric mirror (per-field sign) on the
 other faces; no source, or the magnetosphere demo's point gravity when
 ``source.kind`` is ``"point_gravity"`` (``source.g`` its acceleration).
+With ``boundary.kind == "magnetosphere"`` (FP64 form) the magnetosphere
+demo's boundary and masked CFL replace the plain faces, configured from the
+demo's own ``solar_wind``, ``magnetosphere`` and ``floor`` sections; the
+state it blends toward is the ``blend`` argument (zeros if None).
 Every call goes through ``libmiso_b200.so``; nothing here computes on the
 CPU.
 """
@@ -108,7 +112,7 @@ class Integrator:
     """One grid advanced on the current CUDA device."""
 
     def __init__(self, config: dict, grid: Grid, sign=None, precision: str = "fp64",
-                 stream: int | None = None):
+                 stream: int | None = None, blend=None):
         cfg = merge_defaults(config)
         self.config = cfg
         self.grid = grid
@@ -125,15 +129,36 @@ class Integrator:
                                         ctypes.c_void_p(stream or 0), ctypes.byref(h)), None)
         self._h = h
         self._lib = lib
+        try:
+            self._configure(cfg, blend)
+        except Exception:
+            self.close()
+            raise
+
+    def _configure(self, cfg: dict, blend):
+        """The source and boundary descriptors of the configuration."""
+        lib, h = self._lib, self._h
         src = cfg.get("source") or {}
         kind = src.get("kind", "none")
         if kind != "none":
             kinds = {"point_gravity": 1}
             if kind not in kinds:
-                self.close()
                 raise ValueError(f"unknown source kind {kind!r}")
             par = (ctypes.c_double * 1)(float(src["g"]))
             self._check(lib.miso_b200_set_source(h, kinds[kind], par, 1))
+        bnd = cfg.get("boundary") or {}
+        bkind = bnd.get("kind", "faces")
+        if bkind == "magnetosphere":
+            sw, ms, fl = cfg["solar_wind"], cfg["magnetosphere"], cfg["floor"]
+            par = (ctypes.c_double * 9)(
+                sw["mass_density"], sw["gas_pressure"], sw["x_velocity_field"],
+                sw["z_magnetic_field"], ms["radius"], ms["a0"], fl["ro_floor"], fl["pr_floor"],
+                1.0 if bnd.get("cfl_mask", True) else 0.0)
+            self._check(lib.miso_b200_set_boundary(h, 1, par, 9))
+            if blend is not None:
+                self._check(lib.miso_b200_set_blend_state(h, _field_ptrs(blend)))
+        elif bkind != "faces":
+            raise ValueError(f"unknown boundary kind {bkind!r}")
 
     # -- lifetime -----------------------------------------------------------
     def close(self):
@@ -237,9 +262,10 @@ class Integrator:
 class MHD:
     """Fields + integrator for one grid (miso/include/miso/mhd.hpp:15-50)."""
 
-    def __init__(self, config: dict, grid: Grid, sign=None, precision: str = "fp64"):
+    def __init__(self, config: dict, grid: Grid, sign=None, precision: str = "fp64",
+                 blend=None):
         self.grid = grid
-        self.integrator = Integrator(config, grid, sign=sign, precision=precision)
+        self.integrator = Integrator(config, grid, sign=sign, precision=precision, blend=blend)
 
     def apply_initial_condition(self, q):
         """Upload initial fields and fill the ghosts (mhd.hpp:28-35)."""

@@ -28,7 +28,7 @@ class Model:
     """One grid's model: fields, integrator, time and output."""
 
     def __init__(self, config: dict, grid: Grid, initial_state: np.ndarray, sign=None,
-                 precision: str = "fp64"):
+                 precision: str = "fp64", blend=None):
         t = config.get("time") or {}
         if "tend" not in t or "dt_output" not in t:
             raise KeyError("config needs time.tend and time.dt_output")
@@ -42,7 +42,7 @@ class Model:
         self.config = config
         self.grid = grid
         self.q0 = initial_state
-        self.mhd = MHD(config, grid, sign=sign, precision=precision)
+        self.mhd = MHD(config, grid, sign=sign, precision=precision, blend=blend)
         self.output = (Output(io.get("save_dir", "data/"), config, grid)
                        if self.io_enabled else None)
         # Time::initialize (time.hpp:37-41)

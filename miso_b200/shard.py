@@ -297,7 +297,9 @@ def run_local_shards(prob, count: int, steps: int, precision: str = "fp64", vari
     st = stream
     integs = []
     for s in specs:
-        integ = Integrator(prob.config, s.grid, sign=prob.sign, precision=precision, stream=st)
+        blend = getattr(prob, "blend", None)
+        integ = Integrator(prob.config, s.grid, sign=prob.sign, precision=precision, stream=st,
+                           blend=None if blend is None else split_state(blend, prob.grid, s))
         for cls, var in (variants or {}).items():
             integ.set_variant(cls, var)
         halo.attach(integ, s)

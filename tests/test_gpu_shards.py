@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 
 
 def single(prob, steps, precision, variants=None):
-    integ = Integrator(prob.config, prob.grid, sign=prob.sign, precision=precision)
+    integ = Integrator(prob.config, prob.grid, sign=prob.sign, precision=precision,
+                       blend=prob.blend)
     for cls, var in (variants or {}).items():
         integ.set_variant(cls, var)
     integ.upload(prob.q)
@@ -43,6 +44,9 @@ CASES = [
      {0: 1, 1: 1, 2: 1, 3: 1}),
     ("blast32_split_march_x2", lambda: P.blast(32, seed=1), "fp32_split", 2,
      {0: 0, 1: 2, 2: 2}),
+    # the magnetosphere demo's boundary: inflow on the first shard only, the
+    # blend on every shard's cells before the exchange
+    ("magneto16_fp64_x2", lambda: P.magnetosphere(16, extent=12.0), "fp64", 2, None),
 ]
 
 

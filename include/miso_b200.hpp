@@ -182,6 +182,39 @@ class Integrator {
     stage_out(dst);
   }
 
+  // -- source and boundary descriptors ---------------------------------------
+  // the magnetosphere demo's point gravity (demo/mhd3d_magnetosphere/src/
+  // src.hpp:17-44): force per volume -ro g x / |x|^3, both forms
+  void set_point_gravity(double g) {
+    check(miso_b200_set_source(h_, MISO_B200_SOURCE_POINT_GRAVITY, &g, 1), h_,
+          "miso_b200_set_source");
+  }
+  // the magnetosphere demo's boundary and masked CFL (bc.hpp:39-158,
+  // timestep.hpp:15-49), FP64 form: the config's solar_wind, magnetosphere
+  // and floor entries
+  struct Magnetosphere {
+    double ro_sw, pr_sw, vx_sw, bz_imf;
+    double radius, a0;
+    double ro_floor, pr_floor;
+    bool mask_cfl = true;
+  };
+  void set_magnetosphere_boundary(const Magnetosphere &m) {
+    const double p[9] = {m.ro_sw,  m.pr_sw,    m.vx_sw,    m.bz_imf,         m.radius,
+                         m.a0,     m.ro_floor, m.pr_floor, m.mask_cfl ? 1.0 : 0.0};
+    check(miso_b200_set_boundary(h_, MISO_B200_BOUNDARY_MAGNETOSPHERE, p, 9), h_,
+          "miso_b200_set_boundary");
+  }
+  // the state the boundary blends toward near the sphere (the initial
+  // condition, typically)
+  template <class Fields>
+  void set_blend_state(const Fields &qq) {
+    const Real *src[9] = {qq.ro.data(), qq.vx.data(), qq.vy.data(), qq.vz.data(), qq.bx.data(),
+                          qq.by.data(), qq.bz.data(), qq.ei.data(), qq.ph.data()};
+    const double *q[9];
+    stage_in(src, q);
+    check(miso_b200_set_blend_state(h_, q), h_, "miso_b200_set_blend_state");
+  }
+
   // nsteps of ModelBase::update() with dt kept on the device (resident state)
   void run(int nsteps, bool graph = true) {
     check(miso_b200_run(h_, nsteps, graph ? 1 : 0), h_, "miso_b200_run");

@@ -18,6 +18,8 @@
  *   miso/include/miso/eos.hpp:25-42                       gas_pressure, sound_speed
  *   miso/include/miso/boundary_condition.hpp:77-136       symmetric mirror
  *   miso/include/miso/mhd_halo_exchange.hpp:51-265        periodic wrap (1 rank)
+ *   demo/mhd3d_magnetosphere/src/bc.hpp:39-158            magnetosphere boundary
+ *   demo/mhd3d_magnetosphere/src/timestep.hpp:15-49       masked CFL
  *   miso/include/miso/grid.hpp:22-99,241                  axes, min_dxyz
  *   miso/include/miso/constants.hpp:8-16                  inv12, pii4, pii8
  */

@@ -24,10 +24,10 @@ import os
 CLASSES = {"rk_stage": 0, "av_x": 1, "av_y": 2, "av_z": 3}
 # variants per class: 0 tiled, 1 flat, 2 pipelined (RK: planes with packed
 # differences; x / y sweeps: one warp per line segment marching along the
-# axis); RK 3: variant 2 with the last stage's update deferred into the x
+# axis; z sweep: rows streamed by TMA); RK 3: variant 2 with the last stage's update deferred into the x
 # sweep (compared on the whole step, not per class)
-VARIANTS = {"rk_stage": (0, 1, 2, 3), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1)}
-PER_CLASS = {"rk_stage": (0, 1, 2), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1)}
+VARIANTS = {"rk_stage": (0, 1, 2, 3), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1, 2)}
+PER_CLASS = {"rk_stage": (0, 1, 2), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1, 2)}
 CHUNKS = (32, 64, 128)
 
 

@@ -194,10 +194,13 @@ struct miso_b200_handle {
   alignas(64) unsigned char tm_avl[2][128];  // AV line maps of lo[set]
   alignas(64) unsigned char tm_avc[128];     // AV line map of the characteristic speed
   alignas(64) unsigned char tm_avd[128];     // AV line map of stg[1] (deferred last-stage D)
+  alignas(64) unsigned char tm_zwh[2][128];  // z line sweep: 8-wide wrap maps of hi[set]
+  alignas(64) unsigned char tm_zwc[128];     // and of the characteristic speed
   long long pitch = 0;                       // elements between consecutive field arrays
   int rk_L = 64, rk_tiles_j = 0, rk_tiles_k = 0, rk_items = 0, rk_grid = 0;
   int av_L = 128, av_grid = 0, z_grid = 0;
   int avp_grid = 0;  // warp-march x / y sweep: 2 resident CTAs of 8 warps per SM
+  int zl_grid = 0;   // z line sweep: resident CTAs per SM x SMs
   int shell_grid = 0;
   // The flat kernels run exactly one resident wave (grid = resident blocks)
   // and stride over tiles in order, so the CTAs in flight always cover one
@@ -669,6 +672,9 @@ struct miso_b200_handle {
         launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avd, a, 0, true, av_grid, stream);
       else if (d < 2)
         launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, false, av_grid, stream);
+      else if (av_var[2] == 2)
+        launch_s32_av_zline(tm_avh[cur], tm_avl[cur], tm_avc, tm_zwh[cur], tm_zwc, a, zl_grid,
+                            stream);
       else
         launch_s32_av_z(a, z_grid, stream);
       te(t, d == 0 ? "av_x" : d == 1 ? "av_y" : "av_z",
@@ -695,7 +701,7 @@ struct miso_b200_handle {
       if ((rc = fresh_lo_shell())) return rc;
       if ((rc = halo_f(hi[cur], lo[cur]))) return rc;
     }
-    z_parts = av_var[2] == 1 ? flat_grid : z_grid;
+    z_parts = av_var[2] == 1 ? flat_grid : av_var[2] == 2 ? zl_grid : z_grid;
     partials_valid = true;
     return MISO_B200_OK;
   }
@@ -874,6 +880,8 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
     }
     if (ok) ok = s32_make_tmap_cc(g, h->cc32, h->tm_avc) == 0;
     if (ok) ok = s32_make_tmap(g, h->stg[1][0], pb, 1, h->tm_avd) == 0;
+    for (int s = 0; s < 2 && ok; ++s) ok = s32_make_tmap(g, h->hi[s][0], pb, 2, h->tm_zwh[s]) == 0;
+    if (ok) ok = s32_make_tmap_cc(g, h->cc32, h->tm_zwc, 8) == 0;
     if (ok) {
       h->tiled = true;
       s32_rk_items(g, h->rk_L, h->rk_tiles_j, h->rk_tiles_k, h->rk_items);
@@ -881,6 +889,7 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
       h->rk_grid = h->rk_items < per_sm * h->sms ? h->rk_items : per_sm * h->sms;
       h->av_grid = 2 * h->sms;  // line sweeps: two CTAs per SM
       h->avp_grid = 2 * h->sms;
+      h->zl_grid = s32_zline_per_sm() * h->sms;
       {
         const long long want = (s32_shell_cells(g) + 255) / 256;
         h->shell_grid = (int)(want < 8LL * h->sms ? want : 8LL * h->sms);
@@ -893,7 +902,7 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
                                               : 3;
       if (const char *v = getenv("MISO_B200_AV"))
         for (int d = 0; d < 3 && v[d]; ++d)
-          h->av_var[d] = v[d] == 'f' ? 1 : (v[d] == 'p' && d < 2) ? 2 : 0;
+          h->av_var[d] = v[d] == 'f' ? 1 : v[d] == 'p' ? 2 : 0;
     }
   }
   e = cudaMemsetAsync(h->block, 0, total, h->stream);
@@ -1319,7 +1328,7 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]) {
 
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
   if (!h || kernel_class < 0 || kernel_class > 3 || variant < 0 ||
-      variant > (kernel_class == 0 ? 3 : kernel_class == 3 ? 1 : 2))
+      variant > (kernel_class == 0 ? 3 : 2))
     return MISO_B200_ERR_ARG;
   if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "kernel variants apply to 3-D split grids");
   if (kernel_class == 0 && variant < 2 && h->src.kind != 0)

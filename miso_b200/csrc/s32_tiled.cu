@@ -718,6 +718,201 @@ av_z_kernel(const AvArgs a) {
   }
 }
 
+// ---- z sweep as a streaming line (sweep variant 2) ----
+// The x / y line structure applied to the contiguous axis: a CTA owns ZK
+// consecutive k cells of one i plane and walks a chunk of j rows; per row a
+// producer warp copies hi, lo and the characteristic speed of the segment
+// (k box of 132 from 2 cells before it) into a ring slot by TMA, and four
+// consumer warps, each on 32 consecutive cells of which it updates the
+// inner 28, take their neighbours by shuffles (z_flux_diff, as
+// av_z_kernel).  A lane across a k face reads the interior cell it images:
+// in the segment's own box for a mirror face, or, for a periodic face, in
+// an 8-word box copied from the far end of the row.  Rows are independent,
+// so the ring only keeps copies in flight; the CFL candidate of the new
+// state is folded into a per-CTA minimum.
+constexpr int ZK = 112;  // k cells a CTA updates per row (4 warps x 28)
+constexpr int ZWB = 8;   // k box of the wrap copies
+constexpr int ZNB = 6;   // ring slots
+constexpr int ZL_HI = 0;
+constexpr int ZL_LO = L_LO;
+constexpr int ZL_CC = 2 * L_LO;
+constexpr int ZL_WL = ZL_CC + (LBOX * 4 + 127) / 128 * 128;
+constexpr int ZL_WLC = ZL_WL + (NF * ZWB * 4 + 127) / 128 * 128;
+constexpr int ZL_WR = ZL_WLC + 128;
+constexpr int ZL_WRC = ZL_WR + (NF * ZWB * 4 + 127) / 128 * 128;
+constexpr int ZL_SLOT = ZL_WRC + 128;
+constexpr unsigned ZL_TX = 2 * NF * LBOX * 4 + LBOX * 4;
+constexpr unsigned ZL_TXW = (NF + 1) * ZWB * 4;
+
+struct __align__(128) ZLineSmem {
+  unsigned char slot[ZNB][ZL_SLOT];
+  unsigned long long full[ZNB];
+  unsigned long long empty[ZNB];
+};
+
+struct ZItem {
+  int kb, i, t0, t1;
+};
+
+__device__ __forceinline__ ZItem z_item(const AvArgs &a, int it, int kblocks) {
+  ZItem r;
+  r.kb = it % kblocks;
+  const int r1 = it / kblocks;
+  r.i = r1 % a.g.n[0];
+  const int ch = r1 / a.g.n[0];
+  r.t0 = ch * a.L;
+  r.t1 = min(a.g.n[1], r.t0 + a.L);
+  return r;
+}
+
+__global__ void __launch_bounds__(LK + 32, 2)
+av_zline_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CUtensorMap tlo,
+                const __grid_constant__ CUtensorMap tcc, const __grid_constant__ CUtensorMap twh,
+                const __grid_constant__ CUtensorMap twc, const AvArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  ZLineSmem &sm = *reinterpret_cast<ZLineSmem *>(smem_raw);
+  const Geom &g = a.g;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int nk = g.n[2];
+  const int kblocks = (nk + ZK - 1) / ZK;
+  const int chunks = (g.n[1] + a.L - 1) / a.L;
+  const int items = kblocks * g.n[0] * chunks;
+  const int xl = nk - nk % 4;  // first array column of the left wrap copy
+  if (tid == 0) {
+    for (int b = 0; b < ZNB; ++b) {
+      mbar_init(&sm.full[b], 1);
+      mbar_init(&sm.empty[b], LCW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();  // the only CTA-wide barrier
+  if (tid >= LK) {
+    // producer warp: one lane fills the slots row by row
+    if (tid == LK) {
+      int s = 0;
+      bool stop = false;
+      for (int it = blockIdx.x; it < items && !stop; it += gridDim.x) {
+        const ZItem z = z_item(a, it, kblocks);
+        // wrap copies for the blocks with lanes across a k face (the last
+        // lane of block kb sits at k = kb * ZK + 113)
+        const bool wl = g.periodic[2] && z.kb == 0;
+        const bool wr = g.periodic[2] && z.kb * ZK + 4 * 28 + 1 >= nk;
+        const unsigned tx = ZL_TX + (wl ? ZL_TXW : 0u) + (wr ? ZL_TXW : 0u);
+        for (int j = z.t0; j < z.t1; ++j, ++s) {
+          const int b = s % ZNB;
+          if (s >= ZNB && !mbar_wait(&sm.empty[b], (unsigned)(((s / ZNB) - 1) & 1))) {
+            atomicOr(a.err, ERRBIT_TIMEOUT);
+            stop = true;
+            break;
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          unsigned char *sl = sm.slot[b];
+          const int x = z.kb * ZK, y = j + g.m[1], zc = z.i + g.m[0];
+          mbar_expect_tx(&sm.full[b], tx);
+          tma4(&thi, sl + ZL_HI, &sm.full[b], x, y, zc, 0);
+          tma4(&tlo, sl + ZL_LO, &sm.full[b], x, y, zc, 0);
+          tma3(&tcc, sl + ZL_CC, &sm.full[b], x, y, zc);
+          if (wl) {
+            tma4(&twh, sl + ZL_WL, &sm.full[b], xl, y, zc, 0);
+            tma3(&twc, sl + ZL_WLC, &sm.full[b], xl, y, zc);
+          }
+          if (wr) {
+            tma4(&twh, sl + ZL_WR, &sm.full[b], 0, y, zc, 0);
+            tma3(&twc, sl + ZL_WRC, &sm.full[b], 0, y, zc);
+          }
+        }
+      }
+      // the last copies land before the CTA exits (bounded)
+      for (int s2 = s > ZNB ? s - ZNB : 0; s2 < s; ++s2)
+        mbar_wait(&sm.full[s2 % ZNB], (unsigned)((s2 / ZNB) & 1));
+    }
+    return;
+  }
+
+  const float fac = (float)(g.dsi[2] * a.sc->dt);
+  float best = 1.e10f;
+  bool bad = false, stop = false;
+  int seq = 0;
+  for (int it = blockIdx.x; it < items && !stop; it += gridDim.x) {
+    const ZItem z = z_item(a, it, kblocks);
+    const int k = z.kb * ZK + 28 * w + lane - 2;
+    const int kk = min(k, nk + 1);
+    // where this lane's words sit in a slot, and the mirror signs they take
+    int region = 0, off = 28 * w + lane;
+    unsigned neg = 0;
+    if (kk < 0 || kk >= nk) {
+      int side;
+      const int img = ghost_src(g, 2, kk, side);
+      if (g.periodic[2]) {
+        region = kk < 0 ? 1 : 2;
+        off = img + 2 - (kk < 0 ? xl : 0);
+      } else {
+        off = img - (z.kb * ZK - 2);
+        neg = g.negmask[2][side];
+      }
+    }
+    const bool out = lane >= 2 && lane < 30 && k < nk;
+    for (int j = z.t0; j < z.t1; ++j, ++seq) {
+      const int s = seq % ZNB;
+      if (!mbar_wait(&sm.full[s], (unsigned)((seq / ZNB) & 1))) {
+        // leave the loops (every consumer warp still meets the barrier below)
+        atomicOr(a.err, ERRBIT_TIMEOUT);
+        stop = true;
+        break;
+      }
+      const unsigned char *sl = sm.slot[s];
+      const float *h = reinterpret_cast<const float *>(
+          sl + (region == 0 ? ZL_HI : region == 1 ? ZL_WL : ZL_WR));
+      const float *cp = reinterpret_cast<const float *>(
+          sl + (region == 0 ? ZL_CC : region == 1 ? ZL_WLC : ZL_WRC));
+      const int stride = region == 0 ? LBOX : ZWB;
+      float u[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        u[f] = h[f * stride + off];
+        if ((neg >> f) & 1u) u[f] = -u[f];
+      }
+      W9 dF;
+      z_flux_diff(u, cp[off], a.ep, a.fh, dF);
+      if (out) {
+        const float *lo = reinterpret_cast<const float *>(sl + ZL_LO);
+        float l[NF], sv[NF], e[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) l[f] = lo[f * LBOX + 28 * w + lane];
+        av_update(u, l, dF, fac, sv, e);
+        const int c = cell_of(g, z.i, j, k);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          a.hi2.f[f][c] = sv[f];  // interior only: the shell kernel fills the images
+          a.lo2.f[f][c] = e[f];
+        }
+        if (a.partial) {
+          float cs, vv, ca, ein;
+          speeds(sv, a.gm, a.gm1, cs, vv, ca, ein);
+          const float tv = cs + vv + ca;
+          best = fminf(best, a.cfl_dx / tv);
+          bad |= !(sv[RO] > 0.0f) || !(ein >= 0.0f) || !isfinite(tv);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.empty[s]);
+    }
+  }
+  if (a.partial) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    __shared__ float red[LCW];
+    if (lane == 0) red[w] = best;
+    if (bad) atomicOr(a.err, ERRBIT_NONFINITE);
+    asm volatile("bar.sync 1, %0;" ::"r"(LK) : "memory");  // the consumer warps only
+    if (tid == 0) {
+      float b = red[0];
+      for (int w2 = 1; w2 < LCW; ++w2) b = fminf(b, red[w2]);
+      a.partial[blockIdx.x] = b;
+    }
+  }
+}
+
 }  // namespace s32t
 
 // ---------------------------------------------------------------------------
@@ -761,7 +956,7 @@ int s32_make_tmap(const Geom &g, const float *field0, size_t pitch_bytes, int ki
   cuuint64_t strides[3] = {(cuuint64_t)g.t[2] * 4, (cuuint64_t)g.t[2] * g.t[1] * 4,
                            (cuuint64_t)pitch_bytes};
   cuuint32_t box_rk[4] = {s32t::HK, s32t::HJ, 1, NF};
-  cuuint32_t box_av[4] = {s32t::LBOX, 1, 1, NF};
+  cuuint32_t box_av[4] = {kind == 2 ? (cuuint32_t)s32t::ZWB : (cuuint32_t)s32t::LBOX, 1, 1, NF};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = fn((CUtensorMap *)tm_out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)field0,
                   dims, strides, kind == 0 ? box_rk : box_av, estr,
@@ -770,12 +965,12 @@ int s32_make_tmap(const Geom &g, const float *field0, size_t pitch_bytes, int ki
   return r == CUDA_SUCCESS ? 0 : -2;
 }
 
-int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out) {
+int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out, int kbox) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return -1;
   cuuint64_t dims[3] = {(cuuint64_t)g.t[2], (cuuint64_t)g.t[1], (cuuint64_t)g.t[0]};
   cuuint64_t strides[2] = {(cuuint64_t)g.t[2] * 4, (cuuint64_t)g.t[2] * g.t[1] * 4};
-  cuuint32_t box[3] = {s32t::LBOX, 1, 1};
+  cuuint32_t box[3] = {(cuuint32_t)kbox, 1, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn((CUtensorMap *)tm_out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)cc, dims,
                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -787,6 +982,7 @@ int s32_configure() {
   const int rk = (int)sizeof(s32t::RkSmem);
   const int ln = (int)sizeof(s32t::LineSmem);
   const int lnd = (int)sizeof(s32t::LineSmemT<true>);
+  const int zl = (int)sizeof(s32t::ZLineSmem);
   cudaError_t e = cudaSuccess;
 #define MISO_SET(k, b) \
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b)
@@ -797,6 +993,7 @@ int s32_configure() {
   MISO_SET((s32t::av_line_kernel<0, false>), ln);
   MISO_SET((s32t::av_line_kernel<1, false>), ln);
   MISO_SET((s32t::av_line_kernel<0, true>), lnd);
+  MISO_SET(s32t::av_zline_kernel, zl);
 #undef MISO_SET
   return e == cudaSuccess ? 0 : -1;
 }
@@ -836,6 +1033,23 @@ void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, c
 
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st) {
   s32t::av_z_kernel<<<grid, 128, 0, st>>>(a);
+}
+
+int s32_zline_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, s32t::av_zline_kernel, s32t::LK + 32,
+                                                    sizeof(s32t::ZLineSmem)) != cudaSuccess ||
+      n < 1)
+    n = 1;
+  return n;
+}
+
+void launch_s32_av_zline(const void *tm_hi, const void *tm_lo, const void *tm_cc,
+                         const void *tm_wh, const void *tm_wc, const AvArgs &a, int grid,
+                         cudaStream_t st) {
+  s32t::av_zline_kernel<<<grid, s32t::LK + 32, sizeof(s32t::ZLineSmem), st>>>(
+      *(const CUtensorMap *)tm_hi, *(const CUtensorMap *)tm_lo, *(const CUtensorMap *)tm_cc,
+      *(const CUtensorMap *)tm_wh, *(const CUtensorMap *)tm_wc, a);
 }
 
 }  // namespace miso_b200

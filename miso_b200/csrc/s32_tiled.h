@@ -65,8 +65,9 @@ bool s32_tiled_supported(const Geom &g);
 //   kind 0: RK plane tile (k 36, j 12, i 1, 9 fields)
 //   kind 1: AV line (k 132, j 1, i 1, 9 fields)
 int s32_make_tmap(const Geom &g, const float *field0, size_t pitch_bytes, int kind, void *tm_out);
-// 3-D tensor map of one array for the AV line (k 132, j 1, i 1)
-int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out);
+//   kind 2: the z line sweep's wrap copies (k 8, j 1, i 1, 9 fields)
+// 3-D tensor map of one array for the AV line (k kbox, j 1, i 1)
+int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out, int kbox = 132);
 int s32_configure();
 void s32_rk_items(const Geom &g, int L, int &tiles_j, int &tiles_k, int &items);
 void launch_s32_rk_tiled(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st);
@@ -80,6 +81,12 @@ void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cu
 void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, const AvArgs &a,
                         int dir, bool defer, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);
+// z sweep as a streaming line (TMA rows of 132 k cells, wrap copies of 8 for
+// periodic k faces); writes a.partial[blockIdx.x]
+int s32_zline_per_sm();  // resident z line CTAs per SM (after s32_configure)
+void launch_s32_av_zline(const void *tm_hi, const void *tm_lo, const void *tm_cc,
+                         const void *tm_wh, const void *tm_wc, const AvArgs &a, int grid,
+                         cudaStream_t st);
 // x / y sweep, one warp per 32-cell line segment marching along the sweep
 // axis (s32_av.cu): no shared memory, no CTA barrier; interior-only writes
 void launch_s32_av_march(const AvArgs &a, int dir, int grid, cudaStream_t st);

@@ -114,15 +114,32 @@ monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
                FieldPtrs<const float> lo, double *__restrict__ partial) {
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
-  for (long long lin = blockIdx.x * (long long)blockDim.x + threadIdx.x; lin < nint;
-       lin += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(lin % g.n[2]);
-    const long long r1 = lin / g.n[2];
-    const int j = (int)(r1 % g.n[1]);
-    const int i = (int)(r1 / g.n[1]);
-    const int x[3] = {i, j, k};
-    monitor_cell<SPLIT>(g, q, hi, lo,
-                        (i + g.m[0]) * g.st[0] + (j + g.m[1]) * g.st[1] + k + g.m[2], x, acc);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long lin = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (lin < nint) {
+    // decode the interior index once, then step it by the grid stride with
+    // carries (no 64-bit division per cell)
+    const int n1 = g.n[1], n2 = g.n[2];
+    int k = (int)(lin % n2);
+    const long long r1 = lin / n2;
+    int j = (int)(r1 % n1);
+    int i = (int)(r1 / n1);
+    const int dk = (int)(stride % n2);
+    const long long s1 = stride / n2;
+    const int dj = (int)(s1 % n1);
+    const int di = (int)(s1 / n1);
+    for (; lin < nint; lin += stride) {
+      const int x[3] = {i, j, k};
+      monitor_cell<SPLIT>(g, q, hi, lo,
+                          (i + g.m[0]) * g.st[0] + (j + g.m[1]) * g.st[1] + k + g.m[2], x, acc);
+      k += dk;
+      int carry = k >= n2;
+      if (carry) k -= n2;
+      j += dj + carry;
+      carry = j >= n1;
+      if (carry) j -= n1;
+      i += di + carry;
+    }
   }
   __shared__ double red[8][256];
   for (int q8 = 0; q8 < 8; ++q8) red[q8][threadIdx.x] = acc[q8];

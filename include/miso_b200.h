@@ -224,8 +224,8 @@ int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
  * variant 0 = tiled (TMA plane tiles / streaming lines fed by a producer
  * warp / warp-shuffle rows), 1 = flat (one thread per cell), 2 = pipelined
  * (Runge-Kutta stage: TMA planes with packed FP32x2 differences; x / y
- * sweeps: one warp per line segment marching along the sweep axis; none
- * for z), 3 (Runge-Kutta stage only, the default) = variant 2 with the last
+ * sweeps: one warp per line segment marching along the sweep axis; z sweep:
+ * k rows streamed by TMA), 3 (Runge-Kutta stage only, the default) = variant 2 with the last
  * stage's update deferred into the x sweep: that stage writes its
  * right-hand side and the x sweep forms the new state from it as it streams
  * the state in (this needs x sweep variant 0 and no flat sweep; otherwise

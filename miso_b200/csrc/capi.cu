@@ -19,7 +19,6 @@
 
 #include "../../include/miso_b200.h"
 #include "common.cuh"
-#include "images.cuh"
 #include "kernels.h"
 #include "kernels_s32.h"
 #include "s32_tiled.h"
@@ -37,16 +36,15 @@ constexpr size_t ALIGN = 256;
 size_t round_up(size_t x) { return (x + ALIGN - 1) / ALIGN * ALIGN; }
 
 // FP64 monitors: per-block partial sums of 8 quantities (interior cells).
-// The conserved state and |div B| (4th-order central differences) of cell c
-// at interior coordinates x[3], folded into the accumulators.  The split
-// form takes a neighbour across a face from the interior cell it images (the
-// lo ghost words lag the interior between a step and a download); the FP64
-// form's ghosts are filled after every step.
+// The conserved state and |div B| (4th-order central differences) of cell c,
+// folded into the accumulators.  Neighbours across a face come from the
+// ghost cells, which are current when the kernel runs (miso_b200_monitors
+// brings the split form's lo images up to date first).
 template <bool SPLIT>
 __device__ __forceinline__ void monitor_cell(const Geom &g, const FieldPtrs<const double> &q,
                                              const FieldPtrs<const float> &hi,
                                              const FieldPtrs<const float> &lo, long long c,
-                                             const int x[3], double acc[8]) {
+                                             double acc[8]) {
   double u[NF];
   if (SPLIT) {
     for (int f = 0; f < NF; ++f) u[f] = (double)hi.f[f][c] + (double)lo.f[f][c];
@@ -71,24 +69,10 @@ __device__ __forceinline__ void monitor_cell(const Geom &g, const FieldPtrs<cons
     double p2, p1, m1, m2;
     if (SPLIT) {
       const float *h = hi.f[BX + d], *l = lo.f[BX + d];
-      if (x[d] >= 2 && x[d] < g.n[d] - 2) {
-        p2 = (double)h[c + 2 * s] + l[c + 2 * s];
-        p1 = (double)h[c + s] + l[c + s];
-        m1 = (double)h[c - s] + l[c - s];
-        m2 = (double)h[c - 2 * s] + l[c - 2 * s];
-      } else {
-        auto at = [&](int o) {
-          int side;
-          const int t = ghost_src(g, d, x[d] + o, side);
-          const long long cc = c + (long long)(t - x[d]) * s;
-          const double v = (double)h[cc] + l[cc];
-          return (side >= 0 && ((g.negmask[d][side] >> (BX + d)) & 1u)) ? -v : v;
-        };
-        p2 = at(2);
-        p1 = at(1);
-        m1 = at(-1);
-        m2 = at(-2);
-      }
+      p2 = (double)h[c + 2 * s] + l[c + 2 * s];
+      p1 = (double)h[c + s] + l[c + s];
+      m1 = (double)h[c - s] + l[c - s];
+      m2 = (double)h[c - 2 * s] + l[c - 2 * s];
     } else {
       const double *b = q.f[BX + d];
       p2 = b[c + 2 * s];
@@ -129,9 +113,8 @@ monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
     const int dj = (int)(s1 % n1);
     const int di = (int)(s1 / n1);
     for (; lin < nint; lin += stride) {
-      const int x[3] = {i, j, k};
       monitor_cell<SPLIT>(g, q, hi, lo,
-                          (i + g.m[0]) * g.st[0] + (j + g.m[1]) * g.st[1] + k + g.m[2], x, acc);
+                          (i + g.m[0]) * g.st[0] + (j + g.m[1]) * g.st[1] + k + g.m[2], acc);
       k += dk;
       int carry = k >= n2;
       if (carry) k -= n2;
@@ -1301,7 +1284,11 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
   if (!h || !out) return MISO_B200_ERR_ARG;
   FieldPtrs<const double> q{};
   FieldPtrs<const float> hs{}, ls{};
+  int rc;
   if (h->split()) {
+    // the stencil of div B reads lo ghost words, which lag the interior
+    // between a step and a download
+    if ((rc = h->fresh_lo_shell())) return rc;
     hs = h->cst(h->H(h->cur));
     ls = h->cst(h->L(h->cur));
     monitor_kernel<true><<<h->mon_blocks, 256, 0, h->stream>>>(h->g, q, hs, ls, h->mon_partial);
@@ -1310,7 +1297,7 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
     monitor_kernel<false><<<h->mon_blocks, 256, 0, h->stream>>>(h->g, q, hs, ls, h->mon_partial);
   }
   h->launches++;
-  int rc = h->check_launch("monitors");
+  rc = h->check_launch("monitors");
   if (rc) return rc;
   std::vector<double> part((size_t)h->mon_blocks * 8);
   if ((rc = h->cuda(cudaMemcpyAsync(part.data(), h->mon_partial, part.size() * sizeof(double),

@@ -3,7 +3,8 @@ driven through the reference's integrator interface, cfl(qq, eos) then
 update(dt, eos, bc, src, qq) (mhd_model_base.hpp:57-62).
 
 CPU: the header compiles against the reference's own mhd::Fields and Grid
-types (float and double), and the demo program builds and links.
+types (float and double), its source and boundary calls included, and the
+demo program builds and links.
 GPU: the demo's FP64 result equals the oracle bit for bit, in the default
 (copy in / copy out per call) and the resident mode.
 """
@@ -35,6 +36,11 @@ template <class Real> void drive() {
   integ.set_resident(true);
   integ.push(qq);
   integ.pull(qq);
+  integ.set_point_gravity(1.35e-6);
+  typename miso_b200::Integrator<Real>::Magnetosphere m{5e-4, 3.56e-8, 0.05, -1.5e-4,
+                                                        3.5, 100.0, 1e-8, 1e-10, true};
+  integ.set_magnetosphere_boundary(m);
+  integ.set_blend_state(qq);
 }
 template void drive<double>();
 template void drive<float>();

@@ -366,7 +366,8 @@ struct miso_b200_handle {
     if (rc || !mag.on) return rc;
     const int t = tb();
     launch_magneto_bc(g, f64(set), mag, p.gm, sms, stream);
-    te(t, "magnetosphere_bc", (double)g.cells * 144.0);
+    // every cell: 9 fields read and written, and the reference state read once set
+    te(t, "magnetosphere_bc", (double)g.cells * (mag.blend[0] ? 216.0 : 144.0));
     launches += 1;
     return check_launch("magnetosphere boundary");
   }

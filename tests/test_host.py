@@ -94,3 +94,30 @@ def test_brio_wu_batch_is_seeded():
     assert [x.grid.i_size for x in a] == [x.grid.i_size for x in b]
     assert all(64 <= x.grid.i_size <= 96 for x in a)
     assert all(np.array_equal(x.q, y.q) for x, y in zip(a, b))
+
+
+def test_magnetosphere_initial_state():
+    """The magnetosphere demo's initial condition (demo/mhd3d_magnetosphere/
+    src/ic.hpp) at a few cells, the demo's configuration sections, and the
+    blend state (the initial condition, or zeros)."""
+    from miso_b200 import problems as P
+    prob = P.magnetosphere(16, extent=12.0)
+    g, q, cfg = prob.grid, prob.q, prob.config
+    sw, ms = cfg["solar_wind"], cfg["magnetosphere"]
+    gm = cfg["eos"]["gm"]
+    for i, j, k in [(10, 9, 11), (3, 12, 7), (9, 9, 9)]:
+        x, y, z = g.x[i], g.y[j], g.z[k]
+        r = np.sqrt(x * x + y * y + z * z)
+        assert np.isclose(q[P.RO][i, j, k], max(r ** -3, 0.2 * sw["mass_density"]), rtol=1e-14)
+        assert np.isclose(q[P.BX][i, j, k], -3.0 * x * z * r ** -5, rtol=1e-12)
+        assert np.isclose(q[P.BZ][i, j, k], (x * x + y * y - 2 * z * z) * r ** -5, rtol=1e-12,
+                          atol=1e-300)
+        pr = max(ms["gas_pressure"] * r ** -2, sw["gas_pressure"])
+        assert np.isclose(q[P.EI][i, j, k], pr / (gm - 1.0) / q[P.RO][i, j, k], rtol=1e-13)
+        assert q[P.VX][i, j, k] == 0.0 and q[P.PH][i, j, k] == 0.0
+    # the solar wind on the first layer (x < x_min + 0.8)
+    assert np.all(q[P.RO][0] == sw["mass_density"]) and np.all(q[P.VX][0] == sw["x_velocity_field"])
+    assert cfg["boundary"] == {"kind": "magnetosphere", "cfl_mask": True}
+    assert cfg["source"] == {"kind": "point_gravity", "g": ms["gravitational_acceleration"]}
+    assert np.array_equal(prob.blend, q) and prob.blend is not q
+    assert not np.any(P.magnetosphere(16, extent=12.0, blend_to_initial=False).blend)

@@ -288,21 +288,25 @@ int miso_b200_batch_info(miso_b200_batch *b, long long *interior_cells, int *til
 const char *miso_b200_batch_last_error(miso_b200_batch *b);
 
 /* Allocation-free CFL time step.  No counterpart in the reference: it is an
- * extra entry point for callers that must not let a library allocate device
- * memory -- code running while a stream is captured into a CUDA graph,
- * loops that must not synchronise the device (cudaMalloc may), hosts that
- * own all device memory through their own pool or budget.  It computes the
- * same float-rounded CFL time step as miso_b200_cfl() over the interior of
- * 9 caller-owned DEVICE arrays q[] (FP64 primitives ro, vx, vy, vz, bx, by,
- * bz, ei, ph in the layout above) and returns it in *dt_out (host), with no
+ * extra entry point for callers that cannot let a library allocate device
+ * memory -- applications that give every byte of device memory to their
+ * own pool or hold it to a fixed budget, and applications whose other
+ * streams must not be stalled by the device-wide synchronisation that
+ * cudaMalloc / cudaFree can cause.  It computes the same float-rounded CFL
+ * time step as miso_b200_cfl() over the interior of 9 caller-owned DEVICE
+ * arrays q[] (FP64 primitives ro, vx, vy, vz, bx, by, bz, ei, ph in the
+ * layout above, ghosts included) and returns it in *dt_out (host), with no
  * handle and no cudaMalloc/cudaFree: its scratch is a 65,792-byte array in
  * the library's device memory, held by every GPU that loads the library
  * until the process exits.  Grids of more than 268,435,456 interior cells
- * are rejected with MISO_B200_ERR_ARG.  The first call on a device looks up
- * that device's scratch address, so make it before any stream capture.
- * Every call shares the one scratch array: calls whose work overlaps on the
- * GPU (other threads, other streams) race and must be serialised by the
- * caller.  Synchronises `stream` (a cudaStream_t, NULL = default stream). */
+ * are rejected with MISO_B200_ERR_ARG, and so are pointers that are not
+ * device memory of the current device or arrays shorter than the grid
+ * (checked before any launch, with queries that allocate nothing).  The
+ * first call on a device looks up that device's scratch address.  Every
+ * call shares the one scratch array: calls whose work overlaps on the GPU
+ * (other threads, other streams) race and must be serialised by the
+ * caller.  The call copies the result to the host and waits for `stream`
+ * (a cudaStream_t, NULL = default stream) before it returns. */
 int miso_b200_cfl_noalloc(const miso_b200_grid_desc *grid, const miso_b200_params *params,
                           const double *const q[9], void *stream, double *dt_out);
 

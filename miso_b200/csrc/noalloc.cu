@@ -1,21 +1,24 @@
 // Allocation-free CFL time step over caller-owned FP64 fields.
 //
-// Some callers cannot let a library call cudaMalloc: code that runs while a
-// stream is being captured into a CUDA graph (cudaMalloc is not a stream
-// operation and is refused during capture), real-time or embedded loops that
-// must not synchronise the device (cudaMalloc can), and hosts that own every
-// byte of device memory through their own pool or a fixed budget.  For them
-// miso_b200_cfl_noalloc() computes the same float-rounded CFL time step as
-// miso_b200_cfl() -- the minimum over interior cells of
-// cfl * min(dx, dy, dz) / (cs + |v| + ca) -- on 9 device arrays the caller
-// passes, without allocating anything: its only scratch (per-block partial
-// minima, the result and an error word) is the file-scope device array
-// below, which every GPU that loads the library keeps until the process
-// exits.
+// Some callers cannot let a library call cudaMalloc: applications that
+// hand every byte of device memory to their own pool or hold it to a fixed
+// budget (a cudaMalloc behind their back can fail, or fragment the memory
+// they plan for), and applications whose other streams must not be stalled
+// (cudaMalloc and cudaFree can synchronise the whole device, while this call
+// waits for its own stream only).  For them miso_b200_cfl_noalloc() computes
+// the same float-rounded CFL time step as miso_b200_cfl() -- the minimum
+// over interior cells of cfl * min(dx, dy, dz) / (cs + |v| + ca) -- on 9
+// device arrays the caller passes, without allocating anything: its only
+// scratch (per-block partial minima, the result and an error word) is the
+// file-scope device array below, which every GPU that loads the library
+// keeps until the process exits.  The call copies the result to the host
+// and waits for `stream` before it returns.
 //
 // Compiled with --fmad=false like the FP64 step kernels, so the candidate
 // time step of every cell rounds exactly as on the reference's host path
 // (mhd_integrator_host.hpp:303-334, eos.hpp:36-42, utility.hpp:91-124).
+#include <cuda.h>
+
 #include <cmath>
 #include <cstdio>
 #include <mutex>
@@ -108,6 +111,60 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 
+// cuMemGetAddressRange through the runtime's driver entry point (no link
+// against libcuda); null when the driver does not provide it.
+using AddressRangeFn = CUresult (*)(CUdeviceptr *, size_t *, CUdeviceptr);
+AddressRangeFn address_range_fn() {
+  static AddressRangeFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<AddressRangeFn>(p);
+  }();
+  return fn;
+}
+
+// The array [p, p + bytes) must be device (or managed) memory of device
+// `dev`, inside one allocation.  Host pointers, pinned host memory and
+// arrays shorter than the grid are refused before any launch.  Neither
+// query allocates.
+bool device_array_ok(const void *p, size_t bytes, int dev, std::string &why) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();  // the query's error is not sticky; clear it
+    why = "field pointer is not known to CUDA";
+    return false;
+  }
+  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) {
+    why = "field pointer is not device memory";
+    return false;
+  }
+  if (at.device != dev) {
+    why = "field array lives on another device";
+    return false;
+  }
+  // fail closed: without the extent query nothing is launched
+  AddressRangeFn fn = address_range_fn();
+  if (!fn) {
+    why = "the driver offers no cuMemGetAddressRange to check the field arrays";
+    return false;
+  }
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  if (fn(&base, &size, (CUdeviceptr)p) != CUDA_SUCCESS) {
+    why = "field pointer is not inside a device allocation";
+    return false;
+  }
+  if ((CUdeviceptr)p + bytes > base + size) {
+    why = "field array is shorter than the grid (ghosts included)";
+    return false;
+  }
+  return true;
+}
+
 }  // namespace noalloc
 }  // namespace miso_b200
 
@@ -156,6 +213,11 @@ extern "C" int miso_b200_cfl_noalloc(const miso_b200_grid_desc *gd, const miso_b
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(MISO_B200_ERR_CUDA, cudaGetErrorString(e));
   if (dev < 0 || dev >= MAX_DEVICES) return fail(MISO_B200_ERR_ARG, "device index out of range");
+  for (int f = 0; f < NF; ++f) {
+    std::string why;
+    if (!device_array_ok(q[f], (size_t)g.cells * sizeof(double), dev, why))
+      return fail(MISO_B200_ERR_ARG, why + " (field " + std::to_string(f) + ")");
+  }
   float *scratch = nullptr;
   {
     // once per device, with that device current

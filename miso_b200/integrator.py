@@ -99,7 +99,15 @@ def make_descs(config: dict, grid: Grid, sign=None, precision: str = "fp64"):
 def cfl_noalloc(config: dict, grid: Grid, q, stream: int | None = None) -> float:
     """CFL time step of caller-owned device fields (a CUDA (9, I, J, K)
     float64 tensor) through the allocation-free entry point
-    miso_b200_cfl_noalloc: no handle, no device allocation."""
+    miso_b200_cfl_noalloc: no handle, no device allocation.  Host arrays,
+    CPU tensors and tensors of another shape are refused here, before the
+    library is called; the library refuses non-device pointers itself."""
+    shape = (9,) + tuple(grid.shape)
+    if isinstance(q, np.ndarray) or not hasattr(q, "is_cuda") or not q.is_cuda:
+        raise ValueError("cfl_noalloc needs the fields as a CUDA tensor (device memory)")
+    if tuple(q.shape) != shape or str(q.dtype) != "torch.float64" or not q.is_contiguous():
+        raise ValueError(f"cfl_noalloc needs a contiguous float64 tensor of shape {shape}, "
+                         f"got {tuple(q.shape)} {q.dtype}")
     lib = _lib.load()
     gd, pp = make_descs(config, grid)
     dt = ctypes.c_double()

@@ -25,6 +25,11 @@ REF_F32_SO = os.path.join(HERE, "_ref", "libmiso_ref_f32.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
+# The MISO checkout the reference build and the pymiso reader come from:
+# $MISO_REFERENCE when set, else the default location.
+REFERENCE_ROOT = os.environ.get("MISO_REFERENCE", "/root/reference")
+REFERENCE_INCLUDE = os.path.join(REFERENCE_ROOT, "miso", "include")
+
 
 class Desc(ctypes.Structure):
     _fields_ = [("i_size", ctypes.c_int), ("j_size", ctypes.c_int), ("k_size", ctypes.c_int),
@@ -96,7 +101,7 @@ def _ptrs(q: np.ndarray):
 def build():
     """Compile the restatement (and the reference build where its sources exist)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if os.path.isdir("/root/reference/miso/include"):
+    if os.path.isdir(REFERENCE_INCLUDE):
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 

@@ -29,7 +29,7 @@ def reference():
     """The reference's own host integrator (oracle/_ref), when it was built."""
     from oracle import oracle as om
     if not om.reference_available():
-        if os.path.isdir("/root/reference/miso/include"):
+        if os.path.isdir(om.REFERENCE_INCLUDE):
             subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
         else:
             pytest.skip("reference build (oracle/_ref) not available")

@@ -65,3 +65,20 @@ def test_null_arguments():
     assert lib.miso_b200_update(None, 1e-3) == _lib.ERR_ARG
     assert lib.miso_b200_set_source(None, 1, None, 0) == _lib.ERR_ARG
     assert lib.miso_b200_set_halo(None, 1, 1, None) == _lib.ERR_ARG
+
+
+def test_cfl_noalloc_refuses_host_arrays_before_any_call():
+    """The allocation-free CFL entry point takes device memory only: the
+    Python binding refuses a numpy array, a CPU tensor and a tensor of the
+    wrong shape before the library is called (no GPU needed)."""
+    import numpy as np
+    import torch
+    from miso_b200.integrator import cfl_noalloc
+    prob = P.orszag_tang(16)
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        cfl_noalloc(prob.config, prob.grid, prob.q)
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        cfl_noalloc(prob.config, prob.grid, torch.from_numpy(prob.q))
+    small = np.zeros((9, 4, 4, 1))
+    with pytest.raises(ValueError):
+        cfl_noalloc(prob.config, prob.grid, small)

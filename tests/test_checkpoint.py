@@ -16,8 +16,9 @@ import pytest
 
 from miso_b200 import problems as P
 from miso_b200.checkpoint import Output
+from oracle.oracle import REFERENCE_ROOT
 
-PYMISO_SRC = "/root/reference/pymiso/src"
+PYMISO_SRC = os.path.join(REFERENCE_ROOT, "pymiso", "src")
 
 
 class _FakeHandle:

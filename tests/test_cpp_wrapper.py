@@ -16,8 +16,9 @@ import numpy as np
 import pytest
 
 from conftest import ROOT, interior, rel_l1
+from oracle.oracle import REFERENCE_INCLUDE
 
-REF_INCLUDE = "/root/reference/miso/include"
+REF_INCLUDE = REFERENCE_INCLUDE
 DEMO = os.path.join(ROOT, "tests", "cpp", "wrapper_demo.cpp")
 LIBDIR = os.path.join(ROOT, "miso_b200", "lib")
 

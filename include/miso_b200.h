@@ -240,6 +240,17 @@ int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant);
  * x/y viscosity kernels of the 3-D FP32-split path (defaults 64 and 128). */
 int miso_b200_set_chunks(miso_b200_handle *h, int rk_chunk, int av_chunk);
 
+/* Bound, in SM clock cycles, of the waits in which the consumer threads of
+ * the 3-D FP32-split Runge-Kutta stage and x / y sweep kernels wait for
+ * each plane's TMA copy (default, and cycles <= 0: 4e9, about 2 s).  A wait
+ * that runs out sets the handle's timeout flag; the kernel waits (with the
+ * default bound) for its copies still in flight and returns, and the next
+ * synchronising call reports MISO_B200_ERR_TIMEOUT.  For tests of that
+ * path: a bound far below a copy's latency makes every wait run out.  No
+ * counterpart in the reference, whose CUDA errors abort the process
+ * (miso/include/miso/cuda_util.cuh:17-33).  ERR_STATE on other grids. */
+int miso_b200_set_wait_limit(miso_b200_handle *h, long long cycles);
+
 /* Enable (1) or disable (0) per-kernel CUDA-event timing on the handle's
  * stream (outside graph replays); clears the accumulated totals. */
 int miso_b200_set_timing(miso_b200_handle *h, int enable);

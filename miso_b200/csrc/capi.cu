@@ -23,6 +23,7 @@
 #include "kernels_s32.h"
 #include "s32_tiled.h"
 #include "s32_flat.h"
+#include "tma.cuh"
 
 using namespace miso_b200;
 
@@ -221,6 +222,9 @@ struct miso_b200_handle {
 
   double min_dxyz = 0.0, cfl_dx = 0.0;
   long long launches = 0;
+  // bound (clock cycles) of the consumer waits for each plane's TMA copy in
+  // the Runge-Kutta stage and x / y sweep kernels (miso_b200_set_wait_limit)
+  long long wait_limit = s32t::WAIT_CYCLES;
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -612,6 +616,7 @@ struct miso_b200_handle {
       a.items = rk_items;
       a.src = src;
       a.src_ro = st == 0 ? hi[c][RO] : stg[(st - 1) & 1][RO];
+      a.wait_limit = wait_limit;
       const void *tm = st == 0 ? (const void *)tm_hi[c] : (const void *)tm_stg[(st - 1) & 1];
       const int t = tb();
       if (rk_var == 1)
@@ -664,6 +669,7 @@ struct miso_b200_handle {
       a.cs_fac = (float)p.cs_fac;
       a.vv_fac = (float)p.vv_fac;
       a.ca_fac = (float)p.ca_fac;
+      a.wait_limit = wait_limit;
       const int t = tb();
       if (av_var[d] == 1)
         launch_s32_av_flat(a, d, flat_grid, stream);
@@ -1359,6 +1365,19 @@ int miso_b200_set_chunks(miso_b200_handle *h, int rk_chunk, int av_chunk) {
   s32_rk_items(h->g, h->rk_L, h->rk_tiles_j, h->rk_tiles_k, h->rk_items);
   h->rk_grid = h->rk_items < 2 * h->sms ? h->rk_items : 2 * h->sms;
   if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_wait_limit(miso_b200_handle *h, long long cycles) {
+  if (!h) return MISO_B200_ERR_ARG;
+  if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "the wait limit applies to 3-D split grids");
+  h->wait_limit = cycles > 0 ? cycles : s32t::WAIT_CYCLES;
+  if (h->graph_exec) {  // a captured graph holds the old bound
     cudaGraphExecDestroy(h->graph_exec);
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;

@@ -187,7 +187,7 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
     }
   }
 
-  const bool ok = mbar_wait(&sm.bar[pp.b], pp.par);
+  const bool ok = mbar_wait(&sm.bar[pp.b], pp.par, a.wait_limit);
   const float *pl = reinterpret_cast<const float *>(sm.plane[pp.b]);
   const int fb = pp.seq & 1;
   {

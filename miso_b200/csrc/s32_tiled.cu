@@ -259,13 +259,15 @@ rk_tiled_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
     }
     for (int q = itm.i_start - 2; q <= itm.i_end + 1; ++q, ++seq) {
       const int b = (int)(seq % NBUF);
-      if (tid == 0 && !mbar_wait(&sm.bar[b], (unsigned)((seq / NBUF) & 1))) sm.abort = 1;
+      if (tid == 0 && !mbar_wait(&sm.bar[b], (unsigned)((seq / NBUF) & 1), a.wait_limit))
+        sm.abort = 1;
       __syncthreads();
       if (sm.abort) {
         if (tid == 0) {
           atomicOr(a.err, ERRBIT_TIMEOUT);
-          // drain the copies still in flight (bounded) before the CTA exits
-          for (int s2 = seq + 1; s2 < issued; ++s2)
+          // drain the copies still in flight (bounded; the one whose wait
+          // ran out included) before the CTA exits
+          for (int s2 = seq; s2 < issued; ++s2)
             mbar_wait(&sm.bar[s2 % NBUF], (unsigned)((s2 / NBUF) & 1));
         }
         return;
@@ -471,7 +473,7 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
     const bool active = k < nk;
     for (int p = li.t0 - 2; p <= li.t1 + 1; ++p, ++seq) {
       const int s = (int)(seq % LNB);
-      if (!mbar_wait(&sm.full[s], (unsigned)((seq / LNB) & 1))) {
+      if (!mbar_wait(&sm.full[s], (unsigned)((seq / LNB) & 1), a.wait_limit)) {
         atomicOr(a.err, ERRBIT_TIMEOUT);
         return;
       }

@@ -23,6 +23,7 @@ struct RkArgs {
   int tiles_j, tiles_k, items;
   Source src;           // built-in source term (kind 0: none)
   const float *src_ro;  // density of the stage's argument state (the source's ro)
+  long long wait_limit;  // bound (cycles) of the waits for each plane's copy
 };
 
 // Arguments of one artificial-viscosity sweep launch.
@@ -40,6 +41,7 @@ struct AvArgs {
   // the speed of U^{n+1} = (hi, lo) - dt_4 D goes to cc_out
   float *cc_out;
   float cs_fac, vv_fac, ca_fac;
+  long long wait_limit;  // bound (cycles) of the consumer waits for each plane's copy
 };
 
 // Arrays whose interior shell gets its ghost images (s32_shell.cu); f[n] is

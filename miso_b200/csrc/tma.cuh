@@ -25,8 +25,9 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned
 __device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// Bounded wait for phase `parity`; false on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+// Bounded wait for phase `parity`; false after `limit` cycles.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity,
+                                          long long limit = WAIT_CYCLES) {
   const unsigned a = smem_u32(bar);
   const long long t0 = clock64();
   while (true) {
@@ -38,7 +39,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > WAIT_CYCLES) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 __device__ __forceinline__ void tma4(const CUtensorMap *tm, void *dst, unsigned long long *bar,

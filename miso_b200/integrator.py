@@ -242,6 +242,11 @@ class Integrator:
     def set_chunks(self, rk_chunk: int, av_chunk: int):
         self._check(self._lib.miso_b200_set_chunks(self._h, int(rk_chunk), int(av_chunk)))
 
+    def set_wait_limit(self, cycles: int):
+        """Bound (SM clock cycles) of the consumer waits for each plane's
+        copy in the 3-D split kernels; 0 restores the default (~2 s)."""
+        self._check(self._lib.miso_b200_set_wait_limit(self._h, int(cycles)))
+
     def get_variant(self, kernel_class: int) -> int:
         v = ctypes.c_int()
         self._check(self._lib.miso_b200_get_variant(self._h, int(kernel_class), ctypes.byref(v)))

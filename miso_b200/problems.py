@@ -216,14 +216,16 @@ def magnetosphere(n: int = 128, extent: float = 44.8, radius: float = 3.5,
 
 
 def turbulence(n: int = 256, seed: int = 0, mach: float = 0.5, beta: float = 1.0,
-               gm: float = 5.0 / 3.0, cfl: float = 0.4) -> Problem:
+               gm: float = 5.0 / 3.0, cfl: float = 0.4, shape=None) -> Problem:
     """3-D decaying MHD turbulence on the periodic unit cube.
 
     rho = 1, p = 1/gamma (sound speed 1); v and B are independent random
     solenoidal Fourier sums with 1 <= |k| <= 4, E(k) ~ k^-2, scaled so that
-    the rms speed is ``mach`` and 8 pi p / <B^2> = ``beta``.
+    the rms speed is ``mach`` and 8 pi p / <B^2> = ``beta``.  ``shape``
+    (i, j, k) gives a grid of unequal cell counts on the same cube.
     """
-    g = Grid(n, n, n, 2, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+    ni, nj, nk = (n, n, n) if shape is None else shape
+    g = Grid(ni, nj, nk, 2, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
     rng = np.random.default_rng(seed)
     q = _alloc(g)
     pr = 1.0 / gm
@@ -239,20 +241,22 @@ def turbulence(n: int = 256, seed: int = 0, mach: float = 0.5, beta: float = 1.0
         q[base:base + 3] = f
         del f
     cfgd = make_config(gm, periodic=(True, True, True), cfl_number=cfl)
-    return Problem(f"turbulence_{n}", g, cfgd, q)
+    return Problem(f"turbulence_{ni}x{nj}x{nk}" if shape else f"turbulence_{n}", g, cfgd, q)
 
 
 def blast(n: int = 384, seed: int = 0, gm: float = 5.0 / 3.0, cfl: float = 0.4,
-          smooth: float = 0.0) -> Problem:
+          smooth: float = 0.0, shape=None) -> Problem:
     """3-D magnetised blast wave on [-0.5, 0.5]^3 with mirror (outflow) faces.
 
     Ambient rho = 1, p = 0.1, B_HL = (1, 1, 0)/sqrt(2); inside r < 0.1,
     p = 10 and rho = 1 + 1% seeded uniform noise.  With smooth > 0 the
     sphere's edge is a tanh ramp `smooth` cells wide instead of a step
     (the 100:1 pressure step on fine grids drives the scheme's internal
-    energy negative within the first steps).
+    energy negative within the first steps).  ``shape`` (i, j, k) gives a
+    grid of unequal cell counts on the same cube.
     """
-    g = Grid(n, n, n, 2, -0.5, 0.5, -0.5, 0.5, -0.5, 0.5)
+    ni, nj, nk = (n, n, n) if shape is None else shape
+    g = Grid(ni, nj, nk, 2, -0.5, 0.5, -0.5, 0.5, -0.5, 0.5)
     rng = np.random.default_rng(seed)
     q = _alloc(g)
     X = g.x[:, None, None]
@@ -272,7 +276,7 @@ def blast(n: int = 384, seed: int = 0, gm: float = 5.0 / 3.0, cfl: float = 0.4,
     q[BX] = SQRT4PI / math.sqrt(2.0)
     q[BY] = SQRT4PI / math.sqrt(2.0)
     cfgd = make_config(gm, periodic=(False, False, False), cfl_number=cfl)
-    return Problem(f"blast_{n}", g, cfgd, q)
+    return Problem(f"blast_{ni}x{nj}x{nk}" if shape else f"blast_{n}", g, cfgd, q)
 
 
 def orszag_tang_batch(count: int = 32, n_min: int = 128, n_max: int = 1024, seed: int = 0):

@@ -251,6 +251,17 @@ int miso_b200_set_chunks(miso_b200_handle *h, int rk_chunk, int av_chunk);
  * (miso/include/miso/cuda_util.cuh:17-33).  ERR_STATE on other grids. */
 int miso_b200_set_wait_limit(miso_b200_handle *h, long long cycles);
 
+/* A test of the timeout path without a fault: the next pipelined Runge-Kutta
+ * stage launched outside a CUDA-graph capture (miso_b200_update,
+ * miso_b200_update_device, miso_b200_run without a graph) first waits, with
+ * bound `cycles`, on an mbarrier phase that nothing completes.  The wait
+ * runs out; the kernel sets the timeout flag, waits for its copies in flight
+ * and returns, and the next synchronising call reports
+ * MISO_B200_ERR_TIMEOUT.  The step's state is then invalid; the context and
+ * other handles are not affected.  One launch only.  ERR_STATE unless the
+ * handle runs a 3-D split grid on the pipelined stage (variant 2 or 3). */
+int miso_b200_arm_timeout_test(miso_b200_handle *h, long long cycles);
+
 /* Enable (1) or disable (0) per-kernel CUDA-event timing on the handle's
  * stream (outside graph replays); clears the accumulated totals. */
 int miso_b200_set_timing(miso_b200_handle *h, int enable);

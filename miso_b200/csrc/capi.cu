@@ -225,6 +225,10 @@ struct miso_b200_handle {
   // bound (clock cycles) of the consumer waits for each plane's TMA copy in
   // the Runge-Kutta stage and x / y sweep kernels (miso_b200_set_wait_limit)
   long long wait_limit = s32t::WAIT_CYCLES;
+  // armed by miso_b200_arm_timeout_test: the next pipelined Runge-Kutta
+  // stage launched outside a graph capture stalls on a barrier phase that
+  // nothing completes, with this bound (0: not armed)
+  long long stall_cycles = 0;
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -617,6 +621,11 @@ struct miso_b200_handle {
       a.src = src;
       a.src_ro = st == 0 ? hi[c][RO] : stg[(st - 1) & 1][RO];
       a.wait_limit = wait_limit;
+      a.stall_limit = 0;
+      if (stall_cycles > 0 && rk_var >= 2 && !capturing) {
+        a.stall_limit = stall_cycles;  // one launch only
+        stall_cycles = 0;
+      }
       const void *tm = st == 0 ? (const void *)tm_hi[c] : (const void *)tm_stg[(st - 1) & 1];
       const int t = tb();
       if (rk_var == 1)
@@ -1383,6 +1392,15 @@ int miso_b200_set_wait_limit(miso_b200_handle *h, long long cycles) {
     h->graph_exec = nullptr;
     h->graph = nullptr;
   }
+  return MISO_B200_OK;
+}
+
+int miso_b200_arm_timeout_test(miso_b200_handle *h, long long cycles) {
+  if (!h || cycles <= 0) return MISO_B200_ERR_ARG;
+  if (!h->tiled || h->rk_var < 2)
+    return h->fail(MISO_B200_ERR_STATE,
+                   "the timeout test runs on the pipelined Runge-Kutta stage of 3-D split grids");
+  h->stall_cycles = cycles;
   return MISO_B200_OK;
 }
 

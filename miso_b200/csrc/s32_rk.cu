@@ -139,6 +139,7 @@ struct __align__(128) PipeSmem {
   float2 fz2[2][NPAIR][TJ][HK];             // z fluxes
   float fz1[2][TJ][HK];
   unsigned long long bar[NBUF];
+  unsigned long long stall_bar;  // never arrived at (RkArgs::stall_limit)
   Consts k;       // stage constants (written once by thread 0)
   Producer prod;  // TMA issue cursor (thread 0 only)
 };
@@ -374,6 +375,7 @@ rk_pipe_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int b = 0; b < NBUF; ++b) mbar_init(&sm.bar[b], 1);
+    mbar_init(&sm.stall_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     Consts &k = sm.k;
     const Geom &g = a.g;
@@ -394,6 +396,19 @@ rk_pipe_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
   }
   __syncthreads();
   if ((int)blockIdx.x >= a.items) return;
+  if (a.stall_limit > 0) {
+    // test of the timeout path: a wait on a phase that nothing completes
+    const bool ran_out = !mbar_wait(&sm.stall_bar, 0u, a.stall_limit);
+    if (__syncthreads_or(ran_out)) {
+      if (tid == 0) {
+        atomicOr(a.err, ERRBIT_TIMEOUT);
+        // the copies already issued land before the CTA exits (bounded)
+        for (int s2 = 0; s2 < sm.prod.issued; ++s2)
+          mbar_wait(&sm.bar[s2 % NBUF], (unsigned)((s2 / NBUF) & 1));
+      }
+      return;
+    }
+  }
 
   Pipe pp{0, 0, 0u};
   V9 FA, FB, FC, RA, RB, RC;

@@ -24,6 +24,10 @@ struct RkArgs {
   Source src;           // built-in source term (kind 0: none)
   const float *src_ro;  // density of the stage's argument state (the source's ro)
   long long wait_limit;  // bound (cycles) of the waits for each plane's copy
+  // > 0 (pipelined stage only, a test of the timeout path): before its first
+  // plane every thread waits, with this bound, on a barrier phase that
+  // nothing completes, so the wait runs out and the timeout path is taken
+  long long stall_limit;
 };
 
 // Arguments of one artificial-viscosity sweep launch.

@@ -247,6 +247,12 @@ class Integrator:
         copy in the 3-D split kernels; 0 restores the default (~2 s)."""
         self._check(self._lib.miso_b200_set_wait_limit(self._h, int(cycles)))
 
+    def arm_timeout_test(self, cycles: int):
+        """The next pipelined Runge-Kutta stage waits, with bound ``cycles``,
+        on a barrier phase that nothing completes (a test of the timeout
+        path; the step then reports MISO_B200_ERR_TIMEOUT)."""
+        self._check(self._lib.miso_b200_arm_timeout_test(self._h, int(cycles)))
+
     def get_variant(self, kernel_class: int) -> int:
         v = ctypes.c_int()
         self._check(self._lib.miso_b200_get_variant(self._h, int(kernel_class), ctypes.byref(v)))

@@ -2,12 +2,13 @@
 runs out is reported as a status code, and the context stays usable.
 
 The 3-D FP32-split kernels wait for each plane's TMA copy with a bounded
-mbarrier wait.  With the bound set far below a copy's latency, every
-consumer wait of a Runge-Kutta stage runs out at its first plane: the kernel
-sets the timeout flag, waits (with the default bound) for the copies it has
-in flight, and returns.  The host then reports MISO_B200_ERR_TIMEOUT, where
-the reference would abort the process (cuda_util.cuh:17-33), and a fresh
-handle on the same device steps exactly as before.
+mbarrier wait.  The test arms the pipelined Runge-Kutta stage to first wait,
+with a short bound, on a barrier phase that nothing completes (a flag that
+nothing sets): the wait runs out, the kernel sets the timeout flag, waits
+(with the default bound) for the copies it has in flight, and returns.  The
+host then reports MISO_B200_ERR_TIMEOUT, where the reference would abort the
+process (cuda_util.cuh:17-33), and a fresh handle on the same device steps
+exactly as before.
 """
 import numpy as np
 import pytest
@@ -34,15 +35,14 @@ def _step(prob, nsteps, wait_limit=None):
         integ.close()
 
 
-@pytest.mark.parametrize("variant", [3, 0], ids=["pipelined", "tiled"])
-def test_wait_that_runs_out_is_reported(variant):
+def test_wait_that_runs_out_is_reported():
     prob = P.turbulence(32, seed=6)
     before = _step(prob, 2)
     integ = Integrator(prob.config, prob.grid, precision="fp32_split")
     integ.upload(prob.q)
     integ.apply_boundary_condition()
-    integ.set_variant(0, variant)
-    integ.set_wait_limit(1)  # one clock cycle: no copy lands that fast
+    assert integ.get_variant(0) == 3
+    integ.arm_timeout_test(2_000_000)  # about 1 ms at the SM clock
     dt = integ.cfl()
     with pytest.raises(_lib.MisoError) as exc:
         integ.update(dt)
@@ -54,8 +54,17 @@ def test_wait_that_runs_out_is_reported(variant):
     assert np.array_equal(before, after)
 
 
+def test_timeout_test_needs_the_pipelined_stage():
+    prob = P.turbulence(24, seed=2)
+    with Integrator(prob.config, prob.grid, precision="fp32_split") as integ:
+        integ.set_variant(0, 1)
+        with pytest.raises(_lib.MisoError) as exc:
+            integ.arm_timeout_test(1000)
+        assert exc.value.code == _lib.ERR_STATE
+
+
 def test_wait_limit_default_restored():
-    """Setting the bound back to the default gives the normal step."""
+    """A bound set back to the default (0) gives the normal step."""
     prob = P.turbulence(24, seed=2)
     ref = _step(prob, 1)
     assert np.array_equal(_step(prob, 1, wait_limit=0), ref)

@@ -30,6 +30,7 @@ extern "C" {
 #define MISO_B200_ERR_NOMEM (-5)    /* device allocation failed */
 #define MISO_B200_ERR_TIMEOUT (-6)  /* a bounded device-side wait (TMA copy) ran out */
 #define MISO_B200_ERR_HALO (-7)     /* the halo exchange callback reported an error */
+#define MISO_B200_ERR_CALLBACK (-8) /* the boundary callback reported an error */
 
 #define MISO_B200_FP64 0        /* primitive FP64 state, bit-faithful to the reference */
 #define MISO_B200_FP32_SPLIT 1  /* conserved FP32 hi/lo state, FP32 RHS and viscosity */
@@ -179,6 +180,32 @@ int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, 
  * state and never writes it; a caller passes the initial condition, or
  * zeros for the demo as it runs on zero-filled memory. */
 int miso_b200_set_blend_state(miso_b200_handle *h, const double *const q[9]);
+
+/* Mirror signs of the descriptor's non-periodic faces, set after create:
+ * sign[(axis * 2 + side) * 9 + field], +1 or -1 (axis 0..2 = x, y, z; side
+ * 0 inner, 1 outer), as boundary_condition::symmetric's Sign
+ * (miso/include/miso/boundary_condition.hpp:109-136).  Ghosts keep their
+ * values until the next fill (miso_b200_fill_ghosts or a step). */
+int miso_b200_set_mirror_signs(miso_b200_handle *h, const double *sign);
+
+/* A boundary functor of the caller's own, FP64 form: the `bc` argument of
+ * Integrator::update / apply_boundary_condition for a boundary the built-in
+ * faces do not describe.  After every pass -- where the reference calls
+ * bc.apply(qq.view(), grid.const_view()) and then its halo exchange
+ * (miso/include/miso/mhd_integrator_cuda.cuh:396-401, host twin
+ * mhd_integrator_host.hpp:250-255) -- the library waits for its stream,
+ * calls fn(user, q, stream) with the 9 primitive arrays of the state just
+ * written (on_host != 0: host copies in pinned memory, copied back to the
+ * device after the call; on_host == 0: the device arrays themselves), and
+ * then fills the periodic faces.  The non-periodic faces are left to the
+ * callback.  A nonzero return is reported as MISO_B200_ERR_CALLBACK.  This
+ * is the slow path (a host round trip per pass, 7 per step, and no CUDA
+ * graph: miso_b200_run with use_graph returns MISO_B200_ERR_STATE).
+ * fn == NULL returns to the descriptor's faces.  ERR_STATE on the split
+ * form, with a halo exchange or with the magnetosphere boundary. */
+typedef int (*miso_b200_boundary_fn)(void *user, double *const q[9], void *stream);
+int miso_b200_set_boundary_callback(miso_b200_handle *h, miso_b200_boundary_fn fn, void *user,
+                                    int on_host);
 
 /* Halo exchange of a grid decomposed into shards along i (the slowest
  * axis).  Replaces the reference's HaloExchanger for the neighbour faces of

@@ -46,6 +46,8 @@
 
 namespace miso_b200 {
 
+#ifndef MISO_B200_ERROR_DEFINED
+#define MISO_B200_ERROR_DEFINED
 class Error : public std::runtime_error {
  public:
   Error(int code, const std::string &msg) : std::runtime_error(msg), code_(code) {}
@@ -54,6 +56,7 @@ class Error : public std::runtime_error {
  private:
   int code_;
 };
+#endif
 
 inline void check(int rc, miso_b200_handle *h, const char *what) {
   if (rc != MISO_B200_OK)

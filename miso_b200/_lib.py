@@ -20,6 +20,7 @@ ERR_STATE = -4
 ERR_NOMEM = -5
 ERR_TIMEOUT = -6
 ERR_HALO = -7
+ERR_CALLBACK = -8
 
 FP64 = 0
 FP32_SPLIT = 1
@@ -88,6 +89,9 @@ SIGNATURES = {
     "miso_b200_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "miso_b200_arm_timeout_test": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "miso_b200_set_mirror_signs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "miso_b200_set_boundary_callback": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p, ctypes.c_int]),
     "miso_b200_get_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -185,6 +185,14 @@ struct miso_b200_handle {
   Source src{};
   Magneto mag{};               // the magnetosphere demo's boundary (FP64 form)
   double *blend_block = nullptr;  // its reference state (9 arrays), once set
+  // a boundary callback (miso_b200_set_boundary_callback, FP64 form): called
+  // after every pass in place of the mirror faces, which are then marked
+  // shared (ext) so the fill leaves them to it; on_host: the set is staged
+  // through pinned host memory around the call
+  miso_b200_boundary_fn bc_cb = nullptr;
+  void *bc_user = nullptr;
+  bool bc_host = false;
+  double *bc_stage = nullptr;
   double *axc[3] = {};
   // halo exchange with neighbouring shards along i (miso_b200_set_halo)
   miso_b200_halo_ops halo_ops{};
@@ -370,6 +378,7 @@ struct miso_b200_handle {
   // caller exchanges shared faces after both, as the reference's halo
   // exchange follows its boundary functor)
   int bc64(int set) {
+    if (bc_cb) return bc_callback(set);
     int rc = fill64(set);
     if (rc || !mag.on) return rc;
     const int t = tb();
@@ -378,6 +387,32 @@ struct miso_b200_handle {
     te(t, "magnetosphere_bc", (double)g.cells * (mag.blend[0] ? 216.0 : 144.0));
     launches += 1;
     return check_launch("magnetosphere boundary");
+  }
+  // the caller's boundary functor on the set just written, then the
+  // periodic faces (the reference's bc.apply followed by its halo exchange,
+  // mhd_integrator_cuda.cuh:396-401)
+  int bc_callback(int set) {
+    int rc = cuda(cudaStreamSynchronize(stream), "synchronize before the boundary callback");
+    if (rc) return rc;
+    const size_t bytes = (size_t)g.cells * sizeof(double);
+    double *ptrs[NF];
+    for (int f = 0; f < NF; ++f) {
+      ptrs[f] = bc_host ? bc_stage + (size_t)f * g.cells : q64[set][f];
+      if (bc_host &&
+          (rc = cuda(cudaMemcpyAsync(ptrs[f], q64[set][f], bytes, cudaMemcpyDeviceToHost, stream),
+                     "stage the fields for the boundary callback")))
+        return rc;
+    }
+    if (bc_host && (rc = cuda(cudaStreamSynchronize(stream), "synchronize"))) return rc;
+    const int r = bc_cb(bc_user, ptrs, (void *)stream);
+    if (r) return fail(MISO_B200_ERR_CALLBACK, "boundary callback returned %d", r);
+    if (bc_host)
+      for (int f = 0; f < NF; ++f)
+        if ((rc = cuda(cudaMemcpyAsync(q64[set][f], ptrs[f], bytes, cudaMemcpyHostToDevice,
+                                       stream),
+                       "return the fields from the boundary callback")))
+          return rc;
+    return fill64(set);
   }
   int fill_split(int s) {
     const int t = tb();
@@ -967,6 +1002,7 @@ int miso_b200_destroy(miso_b200_handle *h) {
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->block) cudaFree(h->block);
   if (h->blend_block) cudaFree(h->blend_block);
+  if (h->bc_stage) cudaFreeHost(h->bc_stage);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
   return MISO_B200_OK;
@@ -1100,6 +1136,8 @@ int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, 
   } else if (kind == MISO_B200_BOUNDARY_MAGNETOSPHERE) {
     if (h->split())
       return h->fail(MISO_B200_ERR_STATE, "the magnetosphere boundary runs on the FP64 form");
+    if (h->bc_cb)
+      return h->fail(MISO_B200_ERR_STATE, "a boundary callback is set");
     if (!params || nparams < 9)
       return h->fail(MISO_B200_ERR_ARG, "the magnetosphere boundary takes 9 parameters");
     for (int n = 0; n < 8; ++n)
@@ -1157,9 +1195,72 @@ int miso_b200_set_blend_state(miso_b200_handle *h, const double *const q[9]) {
   return h->cuda(cudaStreamSynchronize(h->stream), "upload blend state");
 }
 
+int miso_b200_set_mirror_signs(miso_b200_handle *h, const double *sign) {
+  if (!h || !sign) return MISO_B200_ERR_ARG;
+  Geom &g = h->g;
+  for (int a = 0; a < 3; ++a)
+    for (int side = 0; side < 2; ++side) {
+      g.negmask[a][side] = 0;
+      for (int f = 0; f < NF; ++f) {
+        const double v = sign[(a * 2 + side) * NF + f];
+        if (v != 1.0 && v != -1.0) return h->fail(MISO_B200_ERR_ARG, "signs must be +1 or -1");
+        g.sign[a][side][f] = (float)v;
+        if (!g.periodic[a] && !g.ext[a][side] && v < 0)
+          g.negmask[a][side] |= (unsigned short)(1u << f);
+      }
+    }
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_boundary_callback(miso_b200_handle *h, miso_b200_boundary_fn fn, void *user,
+                                    int on_host) {
+  if (!h) return MISO_B200_ERR_ARG;
+  Geom &g = h->g;
+  if (fn) {
+    if (h->split())
+      return h->fail(MISO_B200_ERR_STATE, "a boundary callback runs on the FP64 form");
+    if (h->halo_on || h->mag.on)
+      return h->fail(MISO_B200_ERR_STATE,
+                     "a boundary callback excludes the halo exchange and the magnetosphere boundary");
+    if (on_host && !h->bc_stage &&
+        h->cuda(cudaMallocHost((void **)&h->bc_stage, (size_t)g.cells * NF * sizeof(double)),
+                "allocate the boundary callback's host staging"))
+      return MISO_B200_ERR_NOMEM;
+  } else if (h->bc_stage) {
+    cudaFreeHost(h->bc_stage);
+    h->bc_stage = nullptr;
+  }
+  h->bc_cb = fn;
+  h->bc_user = user;
+  h->bc_host = fn && on_host;
+  // the callback owns every non-periodic face: the fill leaves them alone
+  for (int a = 0; a < 3; ++a)
+    for (int side = 0; side < 2; ++side) {
+      g.ext[a][side] = (fn && g.s[a] && !g.periodic[a]) ? 1 : 0;
+      g.negmask[a][side] = 0;
+      if (!g.ext[a][side] && !g.periodic[a])
+        for (int f = 0; f < NF; ++f)
+          if (g.sign[a][side][f] < 0) g.negmask[a][side] |= (unsigned short)(1u << f);
+    }
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
 int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
                        const miso_b200_halo_ops *ops) {
   if (!h) return MISO_B200_ERR_ARG;
+  if (h->bc_cb) return h->fail(MISO_B200_ERR_STATE, "a boundary callback excludes the halo exchange");
   Geom &g = h->g;
   if (ops && !ops->exchange) return h->fail(MISO_B200_ERR_ARG, "halo ops without exchange");
   if (ops && !g.s[0]) return h->fail(MISO_B200_ERR_ARG, "halo exchange needs an i axis of size > 1");
@@ -1203,6 +1304,8 @@ int miso_b200_update_device(miso_b200_handle *h) {
 
 int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
   if (!h || nsteps < 0) return MISO_B200_ERR_ARG;
+  if (h->bc_cb && use_graph)
+    return h->fail(MISO_B200_ERR_STATE, "a boundary callback runs on the host between passes: no graph");
   if (h->halo_on)
     return h->fail(MISO_B200_ERR_STATE, "a shard steps with cfl() and update(dt)");
   int rc;

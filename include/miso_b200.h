@@ -363,6 +363,10 @@ int miso_b200_cfl_noalloc(const miso_b200_grid_desc *grid, const miso_b200_param
  * failed create or miso_b200_cfl_noalloc call). */
 const char *miso_b200_last_error(miso_b200_handle *h);
 
+/* Where a pointer lives: *kind = 1 for device (or managed) memory of any
+ * GPU, 0 for host memory (pageable or pinned).  Allocates nothing. */
+int miso_b200_pointer_kind(const void *p, int *kind);
+
 /* Library version string. */
 const char *miso_b200_version(void);
 

@@ -19,17 +19,24 @@
 // with the reference Grid's i_size .. k_size, i_margin .. k_margin and
 // x_min .. z_max (miso/include/miso/grid.hpp:146-211).
 //
-// The EOS, BC and source arguments are accepted for interface compatibility;
-// the library implements the ideal-gas EOS (gm from Physics), the built-in
-// boundaries of the Boundary descriptor (periodic, or mirror with a sign per
-// field as boundary_condition::symmetric, boundary_condition.hpp:109-136),
-// and no source term (EmptySourceTerm, mhd_model_base.hpp:139-155).
+// The EOS, BC and source arguments are checked, not ignored: the EOS must
+// have the ideal gas's `gm` equal to Physics::gm (else Error); the boundary
+// must be the Boundary descriptor (periodic, or mirror with a sign per field
+// as boundary_condition::symmetric, boundary_condition.hpp:109-136) -- a
+// descriptor with other mirror signs than the last one is applied, another
+// periodicity is an Error; the source must be NoSource (EmptySourceTerm,
+// mhd_model_base.hpp:139-155) or PointGravity<Real>.  Any other boundary or
+// source type is a compile-time error: reference functors run through the
+// backend of include/miso_b200_backend.hpp instead.
 //
-// Residency.  By default every cfl() / update() copies qq to the device and
-// update() copies the result back, so qq always holds the state exactly as
-// with the reference.  set_resident(true) keeps the state on the device
-// between calls (qq is then read only by push() and written only by pull()),
-// which is how a time loop should drive it.
+// Residency.  By default cfl() copies qq to the device, an update() that
+// directly follows a cfl() on the same fields (ModelBase::update's
+// sequence) reuses that copy, and update() copies the result back, so qq
+// always holds the state exactly as with the reference.  set_resident(true)
+// keeps the state on the device between calls (qq is then read only by
+// push() and written only by pull()), which is how a time loop should drive
+// it.  Real = float fields must be host arrays (they are widened through
+// host staging); device float fields are refused with an Error.
 //
 // Errors from the library are thrown as miso_b200::Error (with the status
 // code and the library's message).
@@ -92,6 +99,22 @@ struct Boundary {
   }
 };
 
+// No source term (the reference's mhd::EmptySourceTerm).
+struct NoSource {};
+
+#ifndef MISO_B200_POINT_GRAVITY_DEFINED
+#define MISO_B200_POINT_GRAVITY_DEFINED
+// The magnetosphere demo's point gravity (demo/mhd3d_magnetosphere/src/
+// src.hpp:17-44): force per volume -ro g x / |x|^3 about the origin.
+template <typename Real>
+struct PointGravity {
+  Real g;
+};
+#endif
+
+template <class T>
+struct is_boundary_descriptor : std::is_same<T, Boundary> {};
+
 template <class Real>
 class Integrator {
   static_assert(std::is_same<Real, double>::value || std::is_same<Real, float>::value,
@@ -130,6 +153,8 @@ class Integrator {
     pp.vv_fac = phys.vv_fac;
     pp.precision = precision;
     check(miso_b200_create(&gd, &pp, stream, &h_), nullptr, "miso_b200_create");
+    gm_ = phys.gm;
+    bc_ = bc;
     cells_ = (size_t)(grid.i_size + 2 * grid.i_margin) * (grid.j_size + 2 * grid.j_margin) *
              (grid.k_size + 2 * grid.k_margin);
   }
@@ -141,22 +166,31 @@ class Integrator {
 
   // -- the reference's integrator interface ---------------------------------
   template <class Fields, class EOS>
-  Real cfl(const Fields &qq, const EOS &) {
+  Real cfl(const Fields &qq, const EOS &eos) {
+    check_eos(eos);
     if (!resident_) push(qq);
     double dt = 0.0;
     check(miso_b200_cfl(h_, &dt), h_, "miso_b200_cfl");
+    // the state on the device is qq's: a following update() needs no copy
+    pushed_ = qq.ro.data();
     return (Real)dt;
   }
 
   template <class EOS, class BC, class Src, class Fields>
-  void update(Real dt, const EOS &, const BC &, const Src &, Fields &qq) {
-    if (!resident_) push(qq);
+  void update(Real dt, const EOS &eos, const BC &bc, const Src &src, Fields &qq) {
+    check_eos(eos);
+    set_boundary(bc);
+    set_source(src);
+    if (!resident_ && pushed_ != (const void *)qq.ro.data()) push(qq);
+    pushed_ = nullptr;
     check(miso_b200_update(h_, (double)dt), h_, "miso_b200_update");
     if (!resident_) pull(qq);
   }
 
   template <class BC, class Fields>
-  void apply_boundary_condition(const BC &, Fields &qq) {
+  void apply_boundary_condition(const BC &bc, Fields &qq) {
+    set_boundary(bc);
+    pushed_ = nullptr;
     if (!resident_) push(qq);
     check(miso_b200_fill_ghosts(h_), h_, "miso_b200_fill_ghosts");
     if (!resident_) pull(qq);
@@ -218,6 +252,50 @@ class Integrator {
     check(miso_b200_set_blend_state(h_, q), h_, "miso_b200_set_blend_state");
   }
 
+  // the checks behind update(): see the header comment
+  template <class EOS>
+  void check_eos(const EOS &eos) const {
+    if ((double)eos.gm != gm_ && (Real)eos.gm != (Real)gm_)
+      throw Error(MISO_B200_ERR_ARG, "the EOS's gm differs from Physics::gm");
+  }
+  template <class BC>
+  void set_boundary(const BC &bc) {
+    static_assert(is_boundary_descriptor<BC>::value,
+                  "miso_b200::Integrator takes the miso_b200::Boundary descriptor; reference "
+                  "boundary functors run through include/miso_b200_backend.hpp");
+    for (int a = 0; a < 3; ++a)
+      if (bc.periodic[a] != bc_.periodic[a])
+        throw Error(MISO_B200_ERR_ARG, "the boundary's periodicity differs from the integrator's");
+    bool same = true;
+    for (int a = 0; a < 3; ++a)
+      for (int s = 0; s < 2; ++s)
+        for (int f = 0; f < 9; ++f) same = same && bc.sign[a][s][f] == bc_.sign[a][s][f];
+    if (same) return;
+    check(miso_b200_set_mirror_signs(h_, &bc.sign[0][0][0]), h_, "miso_b200_set_mirror_signs");
+    bc_ = bc;
+  }
+  template <class Src>
+  void set_source(const Src &src) {
+    if constexpr (std::is_same<Src, NoSource>::value) {
+      if (src_on_) {
+        check(miso_b200_set_source(h_, MISO_B200_SOURCE_NONE, nullptr, 0), h_,
+              "miso_b200_set_source");
+        src_on_ = false;
+      }
+    } else if constexpr (std::is_same<Src, PointGravity<Real>>::value) {
+      const double g = (double)src.g;
+      if (!src_on_ || g != src_g_) {
+        check(miso_b200_set_source(h_, MISO_B200_SOURCE_POINT_GRAVITY, &g, 1), h_,
+              "miso_b200_set_source");
+        src_on_ = true;
+        src_g_ = g;
+      }
+    } else {
+      static_assert(sizeof(Src) == 0,
+                    "miso_b200::Integrator takes NoSource or PointGravity<Real> as the source");
+    }
+  }
+
   // nsteps of ModelBase::update() with dt kept on the device (resident state)
   void run(int nsteps, bool graph = true) {
     check(miso_b200_run(h_, nsteps, graph ? 1 : 0), h_, "miso_b200_run");
@@ -233,6 +311,7 @@ class Integrator {
       for (int f = 0; f < 9; ++f) q[f] = reinterpret_cast<const double *>(src[f]);
       return;
     }
+    host_only(src);
     stage_.resize(9 * cells_);
     for (int f = 0; f < 9; ++f) {
       double *d = stage_.data() + (size_t)f * cells_;
@@ -245,6 +324,7 @@ class Integrator {
       for (int f = 0; f < 9; ++f) q[f] = reinterpret_cast<double *>(dst[f]);
       return;
     }
+    host_only(dst);
     stage_.resize(9 * cells_);
     for (int f = 0; f < 9; ++f) q[f] = stage_.data() + (size_t)f * cells_;
   }
@@ -256,10 +336,28 @@ class Integrator {
     }
   }
 
+  // float fields are converted on the host: device arrays are refused
+  template <class P>
+  void host_only(P const p[9]) {
+    for (int f = 0; f < 9; ++f) {
+      int kind = 0;
+      check(miso_b200_pointer_kind(p[f], &kind), h_, "miso_b200_pointer_kind");
+      if (kind == 1)
+        throw Error(MISO_B200_ERR_ARG,
+                    "Real = float fields must be host arrays (device float fields are not "
+                    "converted)");
+    }
+  }
+
   miso_b200_handle *h_ = nullptr;
   size_t cells_ = 0;
   bool resident_ = false;
   std::vector<double> stage_;
+  double gm_ = 0.0;
+  Boundary bc_;
+  const void *pushed_ = nullptr;  // fields whose state cfl() left on the device
+  bool src_on_ = false;
+  double src_g_ = 0.0;
 };
 
 }  // namespace miso_b200

@@ -22,6 +22,10 @@ ERR_TIMEOUT = -6
 ERR_HALO = -7
 ERR_CALLBACK = -8
 
+# int (*)(void *user, double *const q[9], void *stream)
+BOUNDARY_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p,
+                               ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p)
+
 FP64 = 0
 FP32_SPLIT = 1
 
@@ -89,6 +93,7 @@ SIGNATURES = {
     "miso_b200_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "miso_b200_arm_timeout_test": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "miso_b200_pointer_kind": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_set_mirror_signs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "miso_b200_set_boundary_callback": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                                        ctypes.c_void_p, ctypes.c_int]),

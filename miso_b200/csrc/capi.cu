@@ -786,6 +786,19 @@ void miso_b200_set_global_error(const std::string &msg) {
 
 extern "C" {
 
+int miso_b200_pointer_kind(const void *p, int *kind) {
+  if (!kind) return MISO_B200_ERR_ARG;
+  *kind = 0;
+  if (!p) return MISO_B200_OK;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();  // not known to CUDA: host memory
+    return MISO_B200_OK;
+  }
+  *kind = (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) ? 1 : 0;
+  return MISO_B200_OK;
+}
+
 const char *miso_b200_version(void) { return "miso_b200 0.1 (sm_100a)"; }
 
 const char *miso_b200_last_error(miso_b200_handle *h) {

@@ -247,6 +247,40 @@ class Integrator:
         copy in the 3-D split kernels; 0 restores the default (~2 s)."""
         self._check(self._lib.miso_b200_set_wait_limit(self._h, int(cycles)))
 
+    def set_mirror_signs(self, sign):
+        """Mirror signs (3 axes, 2 sides, 9 fields) of the non-periodic faces."""
+        s = np.ascontiguousarray(np.asarray(sign, dtype=np.float64).reshape(54))
+        self._check(self._lib.miso_b200_set_mirror_signs(self._h,
+                                                         s.ctypes.data_as(_lib._dp)))
+        self.bc = BuiltinBoundary(s.reshape(3, 2, 9))
+
+    def set_boundary_callback(self, fn):
+        """A boundary functor of the caller's own (FP64 form): after every
+        pass ``fn(q)`` gets the state just written as a (9, I, J, K) float64
+        numpy array over host copies, fills the non-periodic faces in place
+        (the periodic ones follow on the device), and returns None.
+        ``fn=None`` returns to the built-in faces."""
+        if fn is None:
+            self._check(self._lib.miso_b200_set_boundary_callback(self._h, None, None, 0))
+            self._bc_cb = None
+            return
+        shape = (9,) + tuple(self.grid.shape)
+        cells = int(np.prod(shape[1:]))
+
+        def trampoline(user, q, stream):
+            try:
+                base = ctypes.cast(q[0], ctypes.POINTER(ctypes.c_double))
+                arr = np.ctypeslib.as_array(base, shape=(9 * cells,)).reshape(shape)
+                # the 9 arrays are consecutive in the library's staging
+                assert all(q[f] == q[0] + f * cells * 8 for f in range(9))
+                fn(arr)
+                return 0
+            except Exception:
+                return 1
+        self._bc_cb = _lib.BOUNDARY_FN(trampoline)
+        self._check(self._lib.miso_b200_set_boundary_callback(
+            self._h, ctypes.cast(self._bc_cb, ctypes.c_void_p), None, 1))
+
     def arm_timeout_test(self, cycles: int):
         """The next pipelined Runge-Kutta stage waits, with bound ``cycles``,
         on a barrier phase that nothing completes (a test of the timeout

@@ -34,9 +34,9 @@ struct Grid {
   double x_min, x_max, y_min, y_max, z_min, z_max;
 };
 
-struct IdealEOS {};
-struct NoBC {};
-struct NoSource {};
+struct IdealEOS {
+  double gm;
+};
 
 template <class Real>
 static int run(FILE *in, FILE *out, int nsteps, bool resident) {
@@ -71,9 +71,9 @@ static int run(FILE *in, FILE *out, int nsteps, bool resident) {
   }
   try {
     miso_b200::Integrator<Real> integ(g, ph, bc, MISO_B200_FP64);
-    IdealEOS eos;
-    NoBC nobc;
-    NoSource src;
+    IdealEOS eos{ph.gm};
+    const miso_b200::Boundary &nobc = bc;
+    miso_b200::NoSource src;
     integ.apply_boundary_condition(nobc, qq);
     if (resident) {
       integ.set_resident(true);

@@ -26,14 +26,16 @@ CHECK_TU = r"""
 #include <miso/mhd_fields.hpp>
 #include <miso/grid.hpp>
 #include "miso_b200.hpp"
-struct E {}; struct B {}; struct S {};
+struct E { double gm = 5.0 / 3.0; };
 template <class Real> void drive() {
   miso::Grid<Real, miso::backend::Host> g(16, 16, 1, 2, 0, 1, 0, 1, 0, 1);
   miso::mhd::Fields<Real, miso::backend::Host> qq(g);
-  miso_b200::Integrator<Real> integ(g, miso_b200::Physics(), miso_b200::Boundary::all_mirror());
+  const auto B = miso_b200::Boundary::all_mirror();
+  miso_b200::Integrator<Real> integ(g, miso_b200::Physics(), B);
   Real dt = integ.cfl(qq, E());
-  integ.update(dt, E(), B(), S(), qq);
-  integ.apply_boundary_condition(B(), qq);
+  integ.update(dt, E(), B, miso_b200::NoSource(), qq);
+  integ.update(dt, E(), B, miso_b200::PointGravity<Real>{Real(1e-3)}, qq);
+  integ.apply_boundary_condition(B, qq);
   integ.set_resident(true);
   integ.push(qq);
   integ.pull(qq);
@@ -64,6 +66,36 @@ def test_header_compiles_against_reference_types(tmp_path):
                         "-I" + os.path.join(ROOT, "include"), str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_INCLUDE), reason="reference headers not present")
+@pytest.mark.parametrize("call,message", [
+    ("integ.update(Real(1), E(), Functor(), miso_b200::NoSource(), qq);", "Boundary descriptor"),
+    ("integ.update(Real(1), E(), miso_b200::Boundary(), Src(), qq);", "NoSource or PointGravity"),
+], ids=["functor", "source"])
+def test_header_refuses_unsupported_arguments(tmp_path, call, message):
+    """Boundary functors and source terms the standalone header cannot run
+    are compile-time errors (they were silently ignored before)."""
+    src = tmp_path / "bad.cpp"
+    src.write_text(r"""
+#include <miso/mhd_fields.hpp>
+#include <miso/grid.hpp>
+#include "miso_b200.hpp"
+struct E { double gm = 5.0 / 3.0; };
+struct Functor {};
+struct Src {};
+using Real = double;
+void drive() {
+  miso::Grid<Real, miso::backend::Host> g(16, 16, 1, 2, 0, 1, 0, 1, 0, 1);
+  miso::mhd::Fields<Real, miso::backend::Host> qq(g);
+  miso_b200::Integrator<Real> integ(g, miso_b200::Physics(), miso_b200::Boundary());
+  """ + call + "\n}\n")
+    r = subprocess.run([_gxx(), "-std=c++17", "-fsyntax-only",
+                        "-I" + os.path.join(ROOT, "oracle", "ref_shim"), "-I" + REF_INCLUDE,
+                        "-I" + os.path.join(ROOT, "include"), str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode != 0
+    assert message in r.stderr
 
 
 def _build_demo(out_dir):

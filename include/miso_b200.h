@@ -131,6 +131,15 @@ int miso_b200_last_dt(miso_b200_handle *h, double *dt_out);
  * the non-degenerate axes).  Synchronises. */
 int miso_b200_monitors(miso_b200_handle *h, double out[8]);
 
+/* Fold the monitors' sums into the step (3-D FP32-split grids; ERR_STATE
+ * otherwise): with on != 0 the last viscosity sweep of every step also
+ * leaves FP64 per-block sums of the new state's mass, momentum, energy and
+ * ph^2, and miso_b200_monitors() then reduces only |div B| (a kernel that
+ * reads bx, by, bz) instead of the whole state.  For loops that read the
+ * monitors after every step.  Applies with the default z sweep (variant 0);
+ * the results equal the unfused monitors up to FP64 summation order. */
+int miso_b200_set_monitor_fusion(miso_b200_handle *h, int on);
+
 /* Device pointers of the FP64 primitive state arrays (FP64 form only), valid
  * until the next call that steps or destroys the handle.  Gives user code
  * the reference's FieldsView for custom boundary work

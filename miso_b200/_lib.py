@@ -91,6 +91,7 @@ SIGNATURES = {
                                           ctypes.POINTER(HaloOps)]),
     "miso_b200_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "miso_b200_set_monitor_fusion": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "miso_b200_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "miso_b200_arm_timeout_test": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "miso_b200_pointer_kind": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),

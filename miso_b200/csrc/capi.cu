@@ -226,6 +226,14 @@ struct miso_b200_handle {
   int av_var[3] = {0, 0, 0};
   double *mon_partial = nullptr;
   int mon_blocks = 0;
+  // monitors folded into the step (miso_b200_set_monitor_fusion, 3-D split
+  // path): the z sweep leaves per-block sums of the new state in mon_z and
+  // monitors() adds only the div B kernel
+  bool mon_fuse = false;
+  bool mon_valid = false;  // mon_z holds the sums of the current state
+  double *mon_z = nullptr;
+  double *mon_divb = nullptr;
+  int divb_blocks = 0;
   StepScalars *sc = nullptr;
 
   double min_dxyz = 0.0, cfl_dx = 0.0;
@@ -714,6 +722,7 @@ struct miso_b200_handle {
       a.vv_fac = (float)p.vv_fac;
       a.ca_fac = (float)p.ca_fac;
       a.wait_limit = wait_limit;
+      a.mon = d == 2 && mon_fuse && av_var[2] == 0 ? mon_z : nullptr;
       const int t = tb();
       if (av_var[d] == 1)
         launch_s32_av_flat(a, d, flat_grid, stream);
@@ -754,6 +763,7 @@ struct miso_b200_handle {
     }
     z_parts = av_var[2] == 1 ? flat_grid : av_var[2] == 2 ? zl_grid : z_grid;
     partials_valid = true;
+    mon_valid = mon_fuse && av_var[2] == 0;
     return MISO_B200_OK;
   }
 
@@ -887,6 +897,7 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   h->av_grid = 16 * h->sms;
   h->nparts_alloc = h->nparts > h->z_grid ? h->nparts : h->z_grid;
   h->mon_blocks = h->sms * 4;  // 4 x 148 CTAs of 256: 4.0 -> 2.5 ms at 512^3 against 2 per SM
+  h->divb_blocks = h->sms * 8;
   const size_t cells = (size_t)g.cells;
   size_t total = 0;
   std::vector<std::pair<void **, size_t>> plan;
@@ -911,6 +922,10 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   }
   add((void **)&h->partial, sizeof(float) * h->nparts_alloc);
   add((void **)&h->mon_partial, sizeof(double) * 8 * h->mon_blocks);
+  if (h->split()) {
+    add((void **)&h->mon_z, sizeof(double) * 6 * h->z_grid);
+    add((void **)&h->mon_divb, sizeof(double) * 2 * h->divb_blocks);
+  }
   add((void **)&h->sc, sizeof(StepScalars));
   for (int a = 0; a < 3; ++a) add((void **)&h->axc[a], sizeof(double) * g.t[a]);
   e = cudaMalloc(&h->block, total);
@@ -1036,6 +1051,7 @@ int miso_b200_upload(miso_b200_handle *h, const double *const q[9]) {
     for (int f = 0; f < NF; ++f) src.f[f] = h->io64[f];
     h->cur = 0;
     h->partials_valid = false;
+    h->mon_valid = false;
     h->lo_shell_stale = false;
     launch_s32_to_split(h->g.cells, src, h->H(0), h->L(0), h->sms, h->stream);
     h->launches++;
@@ -1417,6 +1433,36 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
   FieldPtrs<const double> q{};
   FieldPtrs<const float> hs{}, ls{};
   int rc;
+  double dv = 1.0;
+  for (int a = 0; a < 3; ++a)
+    if (h->g.s[a]) dv *= 1.0 / h->g.dsi[a];
+  if (h->split() && h->mon_valid) {
+    // the last z sweep summed the state; only |div B| is left to reduce
+    launch_s32_divb(h->g, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->mon_divb,
+                    h->divb_blocks, h->stream);
+    h->launches++;
+    if ((rc = h->check_launch("divb"))) return rc;
+    std::vector<double> zs((size_t)h->z_grid * 6), db((size_t)h->divb_blocks * 2);
+    if ((rc = h->cuda(cudaMemcpyAsync(zs.data(), h->mon_z, zs.size() * sizeof(double),
+                                      cudaMemcpyDeviceToHost, h->stream),
+                      "read monitors")) ||
+        (rc = h->cuda(cudaMemcpyAsync(db.data(), h->mon_divb, db.size() * sizeof(double),
+                                      cudaMemcpyDeviceToHost, h->stream),
+                      "read monitors")) ||
+        (rc = h->cuda(cudaStreamSynchronize(h->stream), "monitors synchronize")))
+      return rc;
+    for (int q8 = 0; q8 < 8; ++q8) out[q8] = 0.0;
+    const int map[6] = {0, 1, 2, 3, 4, 7};  // ro, mx, my, mz, et, ph^2
+    for (int b = 0; b < h->z_grid; ++b)
+      for (int q = 0; q < 6; ++q) out[map[q]] += zs[(size_t)b * 6 + q];
+    for (int b = 0; b < h->divb_blocks; ++b) {
+      out[5] += db[(size_t)b * 2];
+      out[6] = std::fmax(out[6], db[(size_t)b * 2 + 1]);
+    }
+    for (int q8 = 0; q8 < 8; ++q8)
+      if (q8 != 6) out[q8] *= dv;
+    return MISO_B200_OK;
+  }
   if (h->split()) {
     // the stencil of div B reads lo ghost words, which lag the interior
     // between a step and a download
@@ -1437,9 +1483,6 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
                     "read monitors")))
     return rc;
   if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "monitors synchronize"))) return rc;
-  double dv = 1.0;
-  for (int a = 0; a < 3; ++a)
-    if (h->g.s[a]) dv *= 1.0 / h->g.dsi[a];
   for (int q8 = 0; q8 < 8; ++q8) out[q8] = 0.0;
   for (int b = 0; b < h->mon_blocks; ++b)
     for (int q8 = 0; q8 < 8; ++q8) {
@@ -1490,6 +1533,20 @@ int miso_b200_set_chunks(miso_b200_handle *h, int rk_chunk, int av_chunk) {
   s32_rk_items(h->g, h->rk_L, h->rk_tiles_j, h->rk_tiles_k, h->rk_items);
   h->rk_grid = h->rk_items < 2 * h->sms ? h->rk_items : 2 * h->sms;
   if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_set_monitor_fusion(miso_b200_handle *h, int on) {
+  if (!h) return MISO_B200_ERR_ARG;
+  if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "monitor fusion applies to 3-D split grids");
+  h->mon_fuse = on != 0;
+  h->mon_valid = false;
+  if (h->graph_exec) {  // a captured graph holds the other z sweep
     cudaGraphExecDestroy(h->graph_exec);
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;

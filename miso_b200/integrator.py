@@ -242,6 +242,11 @@ class Integrator:
     def set_chunks(self, rk_chunk: int, av_chunk: int):
         self._check(self._lib.miso_b200_set_chunks(self._h, int(rk_chunk), int(av_chunk)))
 
+    def set_monitor_fusion(self, on: bool = True):
+        """Fold the monitors' sums into every step's last sweep (3-D split
+        grids): monitors() then only reduces |div B|."""
+        self._check(self._lib.miso_b200_set_monitor_fusion(self._h, int(bool(on))))
+
     def set_wait_limit(self, cycles: int):
         """Bound (SM clock cycles) of the consumer waits for each plane's
         copy in the 3-D split kernels; 0 restores the default (~2 s)."""

@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--precision", choices=["fp32_split", "fp64"], default="fp32_split")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched workloads reported beside the headline")
     ap.add_argument("--cpu-n", type=int, default=64, help="reference CPU sample grid size per core")
     ap.add_argument("--workload", choices=["turbulence", "brio_wu_batch", "ot_batch"],
                     default="turbulence",
@@ -378,6 +380,13 @@ def run_b200(args):
     # ---- roofline of the dominant kernel
     roofline = roofline_of(report, args.precision, value / world)
 
+    # ---- the batched workloads beside the headline (same box, same run)
+    batch = None
+    if not args.no_batch:
+        single = {"fp32_split": value / world,
+                  "fp64": fp64["value"] / world if fp64 else None}
+        batch = batch_figures(stream, K, W, single, local, world, rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -405,7 +414,7 @@ def run_b200(args):
                             "GBps": v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] else None}
                         for k, v in report.items()},
             "roofline": roofline, "e2e": e2e, "e2e_host_fields": host_fields, "fp64": fp64, "cpu_baseline": cpu,
-            "clocks": clocks,
+            "clocks": clocks, "batch": batch,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -538,6 +547,58 @@ def run_slab(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def time_batch(probs, precision, stream, K, W, local, world):
+    """Device time of K graph-replayed steps of one batch (CUDA events on the
+    batch's stream, max over ranks), with the clocks sampled meanwhile."""
+    import torch
+
+    from miso_b200.batch import Batch
+    with Batch(probs, precision, stream=stream.cuda_stream) as b:
+        b.upload_all()
+        b.run(W, graph=True)
+        b.sync()
+        info = b.info()
+        cells, l0 = info["interior_cells"], info["launches"]
+        sampler = ClockSampler(local)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sampler.start()
+        e0.record(stream)
+        b.run(K, graph=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = sampler.stop()
+        b.sync()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        launches = b.info()["launches"] - l0
+    return {"value": world * cells * K / (ms / 1e3) / 1e9, "ms_per_step": ms / K,
+            "interior_cells": cells, "instances": len(probs), "gpu_launches": launches,
+            "clocks": clocks}
+
+
+def batch_figures(stream, K, W, single, local, world, rank):
+    """Brio-Wu x4096 (sizes U{512..8192}, left / right values scaled by
+    U[0.8, 1.2]) and Orszag-Tang x32 (sizes U{128..1024}^2), each in the
+    split form and in FP64: Gcell-updates/s and the fraction of the
+    single-grid value per GPU of the same form (`single`)."""
+    from miso_b200 import problems as P
+    out = {}
+    for name, make in (("brio_wu_x4096", lambda: P.brio_wu_batch(4096, 512, 8192, seed=rank)),
+                       ("orszag_tang_x32", lambda: P.orszag_tang_batch(32, 128, 1024, seed=rank))):
+        probs = make()
+        entry = {}
+        for precision in ("fp32_split", "fp64"):
+            r = time_batch(probs, precision, stream, K, W, local, world)
+            if single.get(precision):
+                r["frac_of_single_grid"] = r["value"] / world / single[precision]
+            entry[precision] = r
+        out[name] = entry
+        del probs
+    return out
 
 
 def run_batch(args):

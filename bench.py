@@ -385,7 +385,7 @@ def run_b200(args):
     if not args.no_batch:
         single = {"fp32_split": value / world,
                   "fp64": fp64["value"] / world if fp64 else None}
-        batch = batch_figures(stream, K, W, single, local, world, rank)
+        batch = batch_figures(stream, K, W, single, local, world, rank, prob)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -580,13 +580,28 @@ def time_batch(probs, precision, stream, K, W, local, world):
             "clocks": clocks}
 
 
-def batch_figures(stream, K, W, single, local, world, rank):
+def batch_figures(stream, K, W, single, local, world, rank, big=None):
     """Brio-Wu x4096 (sizes U{512..8192}, left / right values scaled by
     U[0.8, 1.2]) and Orszag-Tang x32 (sizes U{128..1024}^2), each in the
-    split form and in FP64: Gcell-updates/s and the fraction of the
-    single-grid value per GPU of the same form (`single`)."""
+    split form and in FP64; in the split form also 3-D grids of uneven
+    sizes (24 turbulence 64^3 + 16 blast 48^3) and the headline's grid
+    (`big`, 512^3 turbulence) in one batch with the 32 Orszag-Tang grids.
+    Gcell-updates/s and the fraction of the single-grid value per GPU of the
+    same form (`single`)."""
     from miso_b200 import problems as P
     out = {}
+    mixes = [("turbulence64_x24_blast48_x16",
+              lambda: [P.turbulence(64, seed=rank * 64 + s) for s in range(24)] +
+              [P.blast(48, seed=rank * 64 + s) for s in range(16)])]
+    if big is not None:
+        mixes.append(("turbulence512_with_orszag_tang_x32",
+                      lambda: [big] + P.orszag_tang_batch(32, 128, 1024, seed=rank)))
+    for name, make in mixes:
+        probs = make()
+        r = time_batch(probs, "fp32_split", stream, K, W, local, world)
+        r["frac_of_single_grid"] = r["value"] / world / single["fp32_split"]
+        out[name] = {"fp32_split": r}
+        del probs
     for name, make in (("brio_wu_x4096", lambda: P.brio_wu_batch(4096, 512, 8192, seed=rank)),
                        ("orszag_tang_x32", lambda: P.orszag_tang_batch(32, 128, 1024, seed=rank))):
         probs = make()

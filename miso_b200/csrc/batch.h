@@ -25,6 +25,9 @@ struct BatchInst {
   // block-tile axes of the FP32 kernels: R = the last non-degenerate axis
   // (unit stride), C = the one before it, P = the first of three (-1: none)
   int ax_r, ax_c, ax_p;
+  // 1: a 3-D FP32-split instance stepped through a view (view.h) on the
+  // pipelined kernels; the batch-wide kernels and lists leave it out
+  int view;
 };
 
 struct BatchTile {

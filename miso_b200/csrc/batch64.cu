@@ -82,6 +82,7 @@ cfl_kernel(BatchArgs a, FieldPtrs<const double> q) {
 __global__ void finalize_kernel(BatchArgs a) {
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.count; n += gridDim.x * blockDim.x) {
     const BatchInst &in = a.insts[n];
+    if (in.view) continue;  // its view keeps its own step scalars
     const double dt = (double)__uint_as_float(a.dtmin[n]);
     StepScalars &sc = a.sc[n];
     sc.dt = dt;

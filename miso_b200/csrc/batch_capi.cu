@@ -13,6 +13,8 @@
 #include "batch.h"
 #include "common.cuh"
 #include "kernels_s32.h"
+#include "s32_tiled.h"
+#include "view.h"
 
 using namespace miso_b200;
 
@@ -74,6 +76,61 @@ struct miso_b200_batch {
   int graph_steps = 0, graph_cur = 0;
   long long launches = 0, graph_kernels = 0;
 
+  // 3-D FP32-split instances stepped through views on their own streams
+  // (at most VIEW_STREAMS; views on one stream run in turn), forked from
+  // and joined back into the batch's stream every step
+  static constexpr int VIEW_STREAMS = 32;
+  struct View {
+    int index;
+    miso_b200_handle *h;
+    int lane;  // which of the view streams
+  };
+  std::vector<View> views;
+  std::vector<int> view_at;  // per instance: its index in `views`, or -1
+  std::vector<cudaStream_t> vstreams;
+  std::vector<cudaEvent_t> vdone;
+  cudaEvent_t vfork = nullptr;
+
+  int enqueue_views() {
+    if (views.empty()) return MISO_B200_OK;
+    int rc = cuda(cudaEventRecord(vfork, stream), "fork views");
+    for (size_t s = 0; s < vstreams.size() && !rc; ++s)
+      rc = cuda(cudaStreamWaitEvent(vstreams[s], vfork, 0), "fork views");
+    if (rc) return rc;
+    for (auto &v : views) {
+      const long long l0 = b200_view_launches(v.h);
+      int out_cur = 0;
+      if ((rc = b200_view_step(v.h, cur, &out_cur))) {
+        err = std::string("instance ") + std::to_string(v.index) + ": " +
+              miso_b200_last_error(v.h);
+        return rc;
+      }
+      launches += b200_view_launches(v.h) - l0;
+    }
+    return MISO_B200_OK;
+  }
+  int join_views() {
+    int rc = MISO_B200_OK;
+    for (size_t s = 0; s < vstreams.size() && !rc; ++s) {
+      rc = cuda(cudaEventRecord(vdone[s], vstreams[s]), "join views");
+      if (!rc) rc = cuda(cudaStreamWaitEvent(stream, vdone[s], 0), "join views");
+    }
+    return rc;
+  }
+  // every view's ghost layers from its state in set `cur` (after an upload
+  // or a fill of the whole batch), ordered on the batch's stream
+  int fill_views() {
+    if (views.empty()) return MISO_B200_OK;
+    int rc = cuda(cudaEventRecord(vfork, stream), "fork views");
+    for (size_t s = 0; s < vstreams.size() && !rc; ++s)
+      rc = cuda(cudaStreamWaitEvent(vstreams[s], vfork, 0), "fork views");
+    for (auto &v : views)
+      if (!rc && (rc = b200_view_fill(v.h, cur)))
+        err = std::string("instance ") + std::to_string(v.index) + ": " + miso_b200_last_error(v.h);
+    int rj = join_views();
+    return rc ? rc : rj;
+  }
+
   int fail(int code, const std::string &m) {
     err = m;
     return code;
@@ -110,6 +167,8 @@ struct miso_b200_batch {
 
   int enqueue_step() {
     const BatchArgs a = args();
+    // the 3-D split instances run their own pipelined steps concurrently
+    if (int rc = enqueue_views()) return rc;
     if (!split) {
       b64_cfl(a, cst(q64[0]), grid, stream);
       b_finalize(a, stream);
@@ -185,6 +244,7 @@ struct miso_b200_batch {
       }
       cfl_valid = last >= 0;
     }
+    if (int rc = join_views()) return rc;
     return cuda(cudaGetLastError(), "batch step");
   }
 
@@ -199,6 +259,28 @@ struct miso_b200_batch {
       if (e & ERRBIT_NONFINITE)
         return fail(MISO_B200_ERR_NONFINITE,
                     "non-positive or non-finite density / internal energy in a CFL pass");
+    }
+    if (!views.empty()) {
+      // the views' kernels flag their instance's own step scalars
+      std::vector<StepScalars> sc(count);
+      if ((rc = cuda(cudaMemcpyAsync(sc.data(), d_sc, sizeof(StepScalars) * count,
+                                     cudaMemcpyDeviceToHost, stream),
+                     "read")) ||
+          (rc = cuda(cudaStreamSynchronize(stream), "synchronize")))
+        return rc;
+      unsigned int ev = 0;
+      for (auto &v : views) {
+        if (!sc[v.index].err) continue;
+        ev |= sc[v.index].err;
+        cudaMemsetAsync(&d_sc[v.index].err, 0, sizeof(unsigned int), stream);
+      }
+      if (ev) {
+        cudaStreamSynchronize(stream);
+        if (ev & ERRBIT_TIMEOUT)
+          return fail(MISO_B200_ERR_TIMEOUT, "a bounded device-side wait ran out");
+        return fail(MISO_B200_ERR_NONFINITE,
+                    "non-positive or non-finite density / internal energy in a CFL pass");
+      }
     }
     return MISO_B200_OK;
   }
@@ -289,7 +371,16 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
     in.ax_r = nnd > 0 ? nd[nnd - 1] : 2;
     in.ax_c = nnd > 1 ? nd[nnd - 2] : -1;
     in.ax_p = nnd > 2 ? nd[0] : -1;
+    // a 3-D split instance the pipelined kernels can take runs through a
+    // view: the batch-wide lists leave it out
+    in.view = b->split && g.s[0] && g.s[1] && g.s[2] && s32_tiled_supported(g) &&
+              !getenv("MISO_B200_BATCH_BLOCKS");
     b->insts.push_back(in);
+    if (in.view) {
+      off += (g.cells + 63) / 64 * 64;
+      if (g.cells > b->max_cells) b->max_cells = g.cells;
+      continue;
+    }
     for (long long s = 0; s < in.nint; s += BATCH_TILE) tiles.push_back(BatchTile{n, (int)s});
     {
       const int nr = g.n[in.ax_r];
@@ -443,6 +534,47 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
     delete b;
     return bad(MISO_B200_ERR_CUDA, std::string("batch set-up: ") + cudaGetErrorString(e));
   }
+  // the views of the 3-D split instances, over the batch's arrays
+  b->view_at.assign(count, -1);
+  int nviews = 0;
+  for (int n = 0; n < count; ++n) nviews += b->insts[n].view ? 1 : 0;
+  if (nviews) {
+    const int ns = nviews < miso_b200_batch::VIEW_STREAMS ? nviews : miso_b200_batch::VIEW_STREAMS;
+    bool ok = cudaEventCreateWithFlags(&b->vfork, cudaEventDisableTiming) == cudaSuccess;
+    for (int s = 0; s < ns && ok; ++s) {
+      cudaStream_t vs = nullptr;
+      cudaEvent_t ve = nullptr;
+      ok = cudaStreamCreateWithFlags(&vs, cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&ve, cudaEventDisableTiming) == cudaSuccess;
+      if (vs) b->vstreams.push_back(vs);
+      if (ve) b->vdone.push_back(ve);
+    }
+    const size_t pitch = round_up(cells * sizeof(float));
+    int rc = ok ? MISO_B200_OK : MISO_B200_ERR_CUDA;
+    for (int n = 0; n < count && rc == MISO_B200_OK; ++n) {
+      const BatchInst &in = b->insts[n];
+      if (!in.view) continue;
+      float *hi[2][NF], *lo[2][NF], *stg[2][NF];
+      for (int s = 0; s < 2; ++s)
+        for (int f = 0; f < NF; ++f) {
+          hi[s][f] = b->hi[s][f] + in.base;
+          lo[s][f] = b->lo[s][f] + in.base;
+          stg[s][f] = b->stg[s][f] + in.base;
+        }
+      const int lane = (int)b->views.size() % ns;
+      miso_b200_handle *vh = nullptr;
+      rc = b200_view_create(grids[n], params[n], b->vstreams[lane], hi, lo, stg,
+                            b->cc32 + in.base, pitch, b->d_sc + n, &vh);
+      if (rc == MISO_B200_OK) {
+        b->view_at[n] = (int)b->views.size();
+        b->views.push_back({n, vh, lane});
+      }
+    }
+    if (rc != MISO_B200_OK) {
+      miso_b200_batch_destroy(b);
+      return bad(rc, "view set-up of a 3-D instance failed");
+    }
+  }
   *out = b;
   return MISO_B200_OK;
 }
@@ -452,6 +584,13 @@ int miso_b200_batch_destroy(miso_b200_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto &v : b->views) miso_b200_destroy(v.h);
+  for (cudaStream_t s : b->vstreams) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  for (cudaEvent_t e : b->vdone) cudaEventDestroy(e);
+  if (b->vfork) cudaEventDestroy(b->vfork);
   if (b->block) cudaFree(b->block);
   if (b->own_stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -481,7 +620,14 @@ int miso_b200_batch_upload(miso_b200_batch *b, int index, const double *const q[
     launch_s32_to_split(in.g.cells, src, h, l, b->sms, b->stream);
     if ((rc = b->cuda(cudaGetLastError(), "to_split"))) return rc;
   }
-  return b->cuda(cudaStreamSynchronize(b->stream), "upload synchronize");
+  if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "upload synchronize"))) return rc;
+  if (b->view_at.size() && b->view_at[index] >= 0) {
+    // a view's ghost layers and CFL minima follow its new state
+    const auto &v = b->views[b->view_at[index]];
+    if ((rc = b200_view_fill(v.h, b->cur))) return b->fail(rc, miso_b200_last_error(v.h));
+    return b->cuda(cudaStreamSynchronize(b->vstreams[v.lane]), "upload synchronize");
+  }
+  return MISO_B200_OK;
 }
 
 int miso_b200_batch_download(miso_b200_batch *b, int index, double *const q[9]) {
@@ -489,6 +635,14 @@ int miso_b200_batch_download(miso_b200_batch *b, int index, double *const q[9]) 
   const BatchInst &in = b->insts[index];
   const size_t bytes = (size_t)in.g.cells * sizeof(double);
   int rc;
+  if (b->view_at.size() && b->view_at[index] >= 0) {
+    // the lo ghost images of a view lag its interior until a download
+    const auto &v = b->views[b->view_at[index]];
+    if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "download synchronize"))) return rc;
+    if ((rc = b200_view_fresh_lo(v.h, b->cur))) return b->fail(rc, miso_b200_last_error(v.h));
+    if ((rc = b->cuda(cudaStreamSynchronize(b->vstreams[v.lane]), "download synchronize")))
+      return rc;
+  }
   if (b->split) {
     FieldPtrs<const float> h, l;
     FieldPtrs<double> dst;
@@ -519,6 +673,7 @@ int miso_b200_batch_fill_ghosts(miso_b200_batch *b) {
   } else {
     b32_fill(a, b->mut(b->hi[b->cur]), NF, b->grid, b->stream);
     b32_fill(a, b->mut(b->lo[b->cur]), NF, b->grid, b->stream);
+    if (int rc = b->fill_views()) return rc;
   }
   return b->cuda(cudaGetLastError(), "fill_ghosts");
 }

@@ -24,6 +24,7 @@
 #include "s32_tiled.h"
 #include "s32_flat.h"
 #include "tma.cuh"
+#include "view.h"
 
 using namespace miso_b200;
 
@@ -381,6 +382,46 @@ struct miso_b200_handle {
     launches += g.s[0] + g.s[1] + g.s[2] - 1;
     return check_launch("fill_ghosts");
   }
+  // The tiled 3-D FP32-split path: tensor maps of the state, stage and
+  // speed arrays (each set of 9 arrays at one pitch of `pb` bytes), work
+  // items and grids.  Leaves `tiled` false where a map cannot be made.
+  void setup_tiled(size_t pb) {
+    const Geom &g_ = g;
+    bool ok = s32_configure() == 0 && s32_rk_pipe_configure() == 0;
+    for (int s = 0; s < 2 && ok; ++s) {
+      ok = s32_make_tmap(g_, hi[s][0], pb, 0, tm_hi[s]) == 0 &&
+           s32_make_tmap(g_, stg[s][0], pb, 0, tm_stg[s]) == 0 &&
+           s32_make_tmap(g_, hi[s][0], pb, 1, tm_avh[s]) == 0 &&
+           s32_make_tmap(g_, lo[s][0], pb, 1, tm_avl[s]) == 0;
+    }
+    if (ok) ok = s32_make_tmap_cc(g_, cc32, tm_avc) == 0;
+    if (ok) ok = s32_make_tmap(g_, stg[1][0], pb, 1, tm_avd) == 0;
+    for (int s = 0; s < 2 && ok; ++s) ok = s32_make_tmap(g_, hi[s][0], pb, 2, tm_zwh[s]) == 0;
+    if (ok) ok = s32_make_tmap_cc(g_, cc32, tm_zwc, 8) == 0;
+    if (ok) {
+      tiled = true;
+      s32_rk_items(g_, rk_L, rk_tiles_j, rk_tiles_k, rk_items);
+      const int per_sm = 2;
+      rk_grid = rk_items < per_sm * sms ? rk_items : per_sm * sms;
+      av_grid = 2 * sms;  // line sweeps: two CTAs per SM
+      avp_grid = 2 * sms;
+      zl_grid = s32_zline_per_sm() * sms;
+      {
+        const long long want = (s32_shell_cells(g_) + 255) / 256;
+        shell_grid = (int)(want < 8LL * sms ? want : 8LL * sms);
+      }
+      flat_grid = 3 * sms;  // 256 threads x 80 registers: 3 resident CTAs per SM
+      if (const char *v = getenv("MISO_B200_RK"))
+        rk_var = strcmp(v, "flat") == 0    ? 1
+                    : strcmp(v, "tiled") == 0 ? 0
+                    : strcmp(v, "pipe") == 0  ? 2
+                                              : 3;
+      if (const char *v = getenv("MISO_B200_AV"))
+        for (int d = 0; d < 3 && v[d]; ++d)
+          av_var[d] = v[d] == 'f' ? 1 : v[d] == 'p' ? 2 : 0;
+    }
+  }
+
   // Integrator::apply_boundary_condition of the FP64 state: the mirror /
   // periodic fill, then the magnetosphere boundary where it is on (the
   // caller exchanges shared faces after both, as the reference's halo
@@ -819,31 +860,13 @@ const char *miso_b200_last_error(miso_b200_handle *h) {
   return h->err.c_str();
 }
 
-int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, void *stream,
-                     miso_b200_handle **out) {
-  auto create_fail = [](int code, const std::string &msg) {
-    std::lock_guard<std::mutex> lk(g_create_mu);
-    g_create_error = msg;
-    return code;
-  };
-  if (!gd || !pp || !out) return create_fail(MISO_B200_ERR_ARG, "null argument");
-  *out = nullptr;
-  if (gd->margin < 2)
-    return create_fail(MISO_B200_ERR_ARG, "margin must be >= 2 for the 4th-order stencil");
+// Geometry, parameters and CFL spacing of a new handle from its descriptors
+// (validated by the caller).
+static void init_geom(miso_b200_handle *h, const miso_b200_grid_desc *gd,
+                      const miso_b200_params *pp) {
   const int sz[3] = {gd->i_size, gd->j_size, gd->k_size};
   const double lo[3] = {gd->x_min, gd->y_min, gd->z_min};
   const double hi[3] = {gd->x_max, gd->y_max, gd->z_max};
-  for (int a = 0; a < 3; ++a) {
-    if (!valid_axis(sz[a], gd->margin))
-      return create_fail(MISO_B200_ERR_ARG, "invalid grid size");
-    if (!(lo[a] < hi[a])) return create_fail(MISO_B200_ERR_ARG, "invalid grid range");
-  }
-  if (!(pp->gm > 1.0) || !(pp->cfl_number > 0.0) || !(pp->ep >= 0.0) || !(pp->fh >= 0.0))
-    return create_fail(MISO_B200_ERR_ARG, "invalid physics parameters");
-  if (pp->precision != MISO_B200_FP64 && pp->precision != MISO_B200_FP32_SPLIT)
-    return create_fail(MISO_B200_ERR_ARG, "unknown precision");
-
-  auto *h = new miso_b200_handle();
   h->p = *pp;
   Geom &g = h->g;
   double ds[3];
@@ -873,6 +896,35 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   const float m3 = fminf(fminf((float)ds[0], (float)ds[1]), (float)ds[2]);
   h->min_dxyz = (double)m3;
   h->cfl_dx = pp->cfl_number * (double)m3;
+}
+
+int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, void *stream,
+                     miso_b200_handle **out) {
+  auto create_fail = [](int code, const std::string &msg) {
+    std::lock_guard<std::mutex> lk(g_create_mu);
+    g_create_error = msg;
+    return code;
+  };
+  if (!gd || !pp || !out) return create_fail(MISO_B200_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (gd->margin < 2)
+    return create_fail(MISO_B200_ERR_ARG, "margin must be >= 2 for the 4th-order stencil");
+  const int sz[3] = {gd->i_size, gd->j_size, gd->k_size};
+  const double lo[3] = {gd->x_min, gd->y_min, gd->z_min};
+  const double hi[3] = {gd->x_max, gd->y_max, gd->z_max};
+  for (int a = 0; a < 3; ++a) {
+    if (!valid_axis(sz[a], gd->margin))
+      return create_fail(MISO_B200_ERR_ARG, "invalid grid size");
+    if (!(lo[a] < hi[a])) return create_fail(MISO_B200_ERR_ARG, "invalid grid range");
+  }
+  if (!(pp->gm > 1.0) || !(pp->cfl_number > 0.0) || !(pp->ep >= 0.0) || !(pp->fh >= 0.0))
+    return create_fail(MISO_B200_ERR_ARG, "invalid physics parameters");
+  if (pp->precision != MISO_B200_FP64 && pp->precision != MISO_B200_FP32_SPLIT)
+    return create_fail(MISO_B200_ERR_ARG, "unknown precision");
+
+  auto *h = new miso_b200_handle();
+  init_geom(h, gd, pp);
+  Geom &g = h->g;
 
   cudaError_t e = cudaGetDevice(&h->device);
   if (e == cudaSuccess)
@@ -948,42 +1000,8 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
     for (int f = 0; f < NF; ++f) h->io64[f] = (double *)h->stg[0][0] + (size_t)f * cells;
   }
   h->pitch = (long long)(round_up(cells * sizeof(float)) / sizeof(float));
-  if (h->split() && s32_tiled_supported(g) && !getenv("MISO_B200_UNTILED")) {
-    const size_t pb = round_up(cells * sizeof(float));
-    bool ok = s32_configure() == 0 && s32_rk_pipe_configure() == 0;
-    for (int s = 0; s < 2 && ok; ++s) {
-      ok = s32_make_tmap(g, h->hi[s][0], pb, 0, h->tm_hi[s]) == 0 &&
-           s32_make_tmap(g, h->stg[s][0], pb, 0, h->tm_stg[s]) == 0 &&
-           s32_make_tmap(g, h->hi[s][0], pb, 1, h->tm_avh[s]) == 0 &&
-           s32_make_tmap(g, h->lo[s][0], pb, 1, h->tm_avl[s]) == 0;
-    }
-    if (ok) ok = s32_make_tmap_cc(g, h->cc32, h->tm_avc) == 0;
-    if (ok) ok = s32_make_tmap(g, h->stg[1][0], pb, 1, h->tm_avd) == 0;
-    for (int s = 0; s < 2 && ok; ++s) ok = s32_make_tmap(g, h->hi[s][0], pb, 2, h->tm_zwh[s]) == 0;
-    if (ok) ok = s32_make_tmap_cc(g, h->cc32, h->tm_zwc, 8) == 0;
-    if (ok) {
-      h->tiled = true;
-      s32_rk_items(g, h->rk_L, h->rk_tiles_j, h->rk_tiles_k, h->rk_items);
-      const int per_sm = 2;
-      h->rk_grid = h->rk_items < per_sm * h->sms ? h->rk_items : per_sm * h->sms;
-      h->av_grid = 2 * h->sms;  // line sweeps: two CTAs per SM
-      h->avp_grid = 2 * h->sms;
-      h->zl_grid = s32_zline_per_sm() * h->sms;
-      {
-        const long long want = (s32_shell_cells(g) + 255) / 256;
-        h->shell_grid = (int)(want < 8LL * h->sms ? want : 8LL * h->sms);
-      }
-      h->flat_grid = 3 * h->sms;  // 256 threads x 80 registers: 3 resident CTAs per SM
-      if (const char *v = getenv("MISO_B200_RK"))
-        h->rk_var = strcmp(v, "flat") == 0    ? 1
-                    : strcmp(v, "tiled") == 0 ? 0
-                    : strcmp(v, "pipe") == 0  ? 2
-                                              : 3;
-      if (const char *v = getenv("MISO_B200_AV"))
-        for (int d = 0; d < 3 && v[d]; ++d)
-          h->av_var[d] = v[d] == 'f' ? 1 : v[d] == 'p' ? 2 : 0;
-    }
-  }
+  if (h->split() && s32_tiled_supported(g) && !getenv("MISO_B200_UNTILED"))
+    h->setup_tiled(round_up(cells * sizeof(float)));
   e = cudaMemsetAsync(h->block, 0, total, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
@@ -1020,6 +1038,107 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   *out = h;
   return MISO_B200_OK;
 }
+
+}  // extern "C"
+
+// ---- views (view.h): the tiled step over arrays another owner holds
+int miso_b200::b200_view_create(const miso_b200_grid_desc &gd, const miso_b200_params &pp,
+                                cudaStream_t stream, float *const hi[2][NF],
+                                float *const lo[2][NF], float *const stg[2][NF], float *cc,
+                                size_t pitch_bytes, StepScalars *sc, miso_b200_handle **out) {
+  *out = nullptr;
+  if (pp.precision != MISO_B200_FP32_SPLIT) return MISO_B200_ERR_ARG;
+  auto *h = new miso_b200_handle();
+  init_geom(h, &gd, &pp);
+  const Geom &g = h->g;
+  if (!g.s[0] || !g.s[1] || !g.s[2] || !s32_tiled_supported(g)) {
+    delete h;
+    return MISO_B200_ERR_STATE;
+  }
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
+  if (e != cudaSuccess) {
+    delete h;
+    return MISO_B200_ERR_CUDA;
+  }
+  h->stream = stream;
+  h->own_stream = false;
+  for (int s = 0; s < 2; ++s)
+    for (int f = 0; f < NF; ++f) {
+      h->hi[s][f] = hi[s][f];
+      h->lo[s][f] = lo[s][f];
+      h->stg[s][f] = stg[s][f];
+    }
+  h->cc32 = cc;
+  h->sc = sc;
+  h->pitch = (long long)(pitch_bytes / sizeof(float));
+  // the view's own buffers: CFL and monitor partials, cell centres
+  h->nparts = cfl_partial_blocks(h->sms);
+  h->z_grid = 8 * h->sms;
+  h->nparts_alloc = h->nparts > h->z_grid ? h->nparts : h->z_grid;
+  h->mon_blocks = h->sms * 4;
+  h->divb_blocks = h->sms * 8;
+  size_t total = 0;
+  std::vector<std::pair<void **, size_t>> plan;
+  auto add = [&](void **p, size_t b) {
+    plan.emplace_back(p, b);
+    total += round_up(b);
+  };
+  add((void **)&h->partial, sizeof(float) * h->nparts_alloc);
+  add((void **)&h->mon_partial, sizeof(double) * 8 * h->mon_blocks);
+  add((void **)&h->mon_z, sizeof(double) * 6 * h->z_grid);
+  add((void **)&h->mon_divb, sizeof(double) * 2 * h->divb_blocks);
+  for (int a = 0; a < 3; ++a) add((void **)&h->axc[a], sizeof(double) * g.t[a]);
+  e = cudaMalloc(&h->block, total);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->block, 0, total, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    if (h->block) cudaFree(h->block);
+    delete h;
+    return MISO_B200_ERR_NOMEM;
+  }
+  h->bytes = total;
+  size_t off = 0;
+  for (auto &pb : plan) {
+    *pb.first = (char *)h->block + off;
+    off += round_up(pb.second);
+  }
+  h->setup_tiled(pitch_bytes);
+  if (!h->tiled) {
+    cudaFree(h->block);
+    delete h;
+    return MISO_B200_ERR_STATE;
+  }
+  h->src.kind = 0;
+  *out = h;
+  return MISO_B200_OK;
+}
+
+int miso_b200::b200_view_step(miso_b200_handle *h, int cur, int *cur_out) {
+  h->cur = cur;
+  int rc = h->enqueue_cfl();
+  if (!rc) rc = h->enqueue_update();
+  *cur_out = h->cur;
+  return rc;
+}
+
+int miso_b200::b200_view_fill(miso_b200_handle *h, int cur) {
+  h->cur = cur;
+  h->partials_valid = false;
+  h->mon_valid = false;
+  h->lo_shell_stale = false;
+  return h->fill_state();
+}
+
+int miso_b200::b200_view_fresh_lo(miso_b200_handle *h, int cur) {
+  h->cur = cur;
+  return h->fresh_lo_shell();
+}
+
+long long miso_b200::b200_view_launches(const miso_b200_handle *h) { return h->launches; }
+
+extern "C" {
 
 int miso_b200_destroy(miso_b200_handle *h) {
   if (!h) return MISO_B200_ERR_ARG;

@@ -300,7 +300,7 @@ def run_b200(args):
         integ.monitors()
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    d2h_mon = (6 * 8 * sms + 2 * 8 * sms) * 8 if fused else 8 * 4 * sms * 8
+    d2h_mon = (6 * 8 * sms + 8 * 4 * sms) * 8 if fused else 8 * 4 * sms * 8
     e2e = {"value": world * cells * K / e2e_s / 1e9, "unit": UNIT,
            "h2d_bytes_per_step": 96, "d2h_bytes_per_step": 96 + d2h_mon,
            "monitors_fused": fused,

@@ -42,13 +42,15 @@ size_t round_up(size_t x) { return (x + ALIGN - 1) / ALIGN * ALIGN; }
 // folded into the accumulators.  Neighbours across a face come from the
 // ghost cells, which are current when the kernel runs (miso_b200_monitors
 // brings the split form's lo images up to date first).
-template <bool SPLIT>
+// DIVB_ONLY: |div B| alone (the sums come from the z sweep, monitor fusion).
+template <bool SPLIT, bool DIVB_ONLY = false>
 __device__ __forceinline__ void monitor_cell(const Geom &g, const FieldPtrs<const double> &q,
                                              const FieldPtrs<const float> &hi,
                                              const FieldPtrs<const float> &lo, long long c,
                                              double acc[8]) {
   double u[NF];
-  if (SPLIT) {
+  if (DIVB_ONLY) {
+  } else if (SPLIT) {
     for (int f = 0; f < NF; ++f) u[f] = (double)hi.f[f][c] + (double)lo.f[f][c];
   } else {
     const double ro = q.f[RO][c], vx = q.f[VX][c], vy = q.f[VY][c], vz = q.f[VZ][c];
@@ -84,17 +86,18 @@ __device__ __forceinline__ void monitor_cell(const Geom &g, const FieldPtrs<cons
     }
     divb += (-p2 + 8.0 * p1 - 8.0 * m1 + m2) * INV12 * g.dsi[d];
   }
+  acc[5] += fabs(divb);
+  acc[6] = fmax(acc[6], fabs(divb));
+  if (DIVB_ONLY) return;
   acc[0] += u[RO];
   acc[1] += u[MX];
   acc[2] += u[MY];
   acc[3] += u[MZ];
   acc[4] += u[ET];
-  acc[5] += fabs(divb);
-  acc[6] = fmax(acc[6], fabs(divb));
   acc[7] += u[PH] * u[PH];
 }
 
-template <bool SPLIT>
+template <bool SPLIT, bool DIVB_ONLY = false>
 __global__ void __launch_bounds__(256, 4)
 monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
                FieldPtrs<const float> lo, double *__restrict__ partial) {
@@ -115,7 +118,7 @@ monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
     const int dj = (int)(s1 % n1);
     const int di = (int)(s1 / n1);
     for (; lin < nint; lin += stride) {
-      monitor_cell<SPLIT>(g, q, hi, lo,
+      monitor_cell<SPLIT, DIVB_ONLY>(g, q, hi, lo,
                           (i + g.m[0]) * g.st[0] + (j + g.m[1]) * g.st[1] + k + g.m[2], acc);
       k += dk;
       int carry = k >= n2;
@@ -142,6 +145,84 @@ monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
   }
   if (threadIdx.x == 0)
     for (int q8 = 0; q8 < 8; ++q8) partial[blockIdx.x * 8 + q8] = red[q8][0];
+}
+
+// |div B| of the split state (the monitors with their sums folded into the
+// z sweep), the monitor kernel's difference in FP64 from hi + lo, by quads
+// of 4 cells along k that start on a 16-byte boundary (tiled grids: k_total
+// a multiple of 4, margin 2): every neighbour row is one float4 of hi and
+// one of lo, bz takes three per array; lanes on ghost cells of the quad
+// contribute nothing.  The ghost layers must be current (the caller
+// refreshes the lo images first).  Writes slots 5 and 6 of the monitor
+// kernel's per-block layout.
+__device__ __forceinline__ void quad64(const float *h, const float *l, long long c, double v[4]) {
+  const float4 a = __ldg(reinterpret_cast<const float4 *>(h + c));
+  const float4 b = __ldg(reinterpret_cast<const float4 *>(l + c));
+  v[0] = (double)a.x + (double)b.x;
+  v[1] = (double)a.y + (double)b.y;
+  v[2] = (double)a.z + (double)b.z;
+  v[3] = (double)a.w + (double)b.w;
+}
+
+__global__ void __launch_bounds__(256)
+divb_quad_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
+                 double *__restrict__ partial) {
+  const int nq = g.t[2] / 4;
+  const long long work = (long long)g.n[0] * g.n[1] * nq;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  double sum = 0.0, mx = 0.0;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < work; w += stride) {
+    const int q = (int)(w % nq);
+    const long long r = w / nq;
+    const int j = (int)(r % g.n[1]);
+    const int i = (int)(r / g.n[1]);
+    const long long c = (long long)(i + g.m[0]) * g.st[0] + (long long)(j + g.m[1]) * g.st[1] +
+                        4 * q;  // total k = 4q .. 4q+3
+    double xm2[4], xm1[4], xp1[4], xp2[4], ym2[4], ym1[4], yp1[4], yp2[4], z[12];
+    quad64(hi.f[BX], lo.f[BX], c - 2 * g.st[0], xm2);
+    quad64(hi.f[BX], lo.f[BX], c - g.st[0], xm1);
+    quad64(hi.f[BX], lo.f[BX], c + g.st[0], xp1);
+    quad64(hi.f[BX], lo.f[BX], c + 2 * g.st[0], xp2);
+    quad64(hi.f[BY], lo.f[BY], c - 2 * g.st[1], ym2);
+    quad64(hi.f[BY], lo.f[BY], c - g.st[1], ym1);
+    quad64(hi.f[BY], lo.f[BY], c + g.st[1], yp1);
+    quad64(hi.f[BY], lo.f[BY], c + 2 * g.st[1], yp2);
+    quad64(hi.f[BZ], lo.f[BZ], c - 4, z);
+    quad64(hi.f[BZ], lo.f[BZ], c, z + 4);
+    quad64(hi.f[BZ], lo.f[BZ], c + 4, z + 8);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int kk = 4 * q + t - g.m[2];  // interior k of this lane of the quad
+      if (kk < 0 || kk >= g.n[2]) continue;
+      double divb = 0.0;
+      divb += (-xp2[t] + 8.0 * xp1[t] - 8.0 * xm1[t] + xm2[t]) * INV12 * g.dsi[0];
+      divb += (-yp2[t] + 8.0 * yp1[t] - 8.0 * ym1[t] + ym2[t]) * INV12 * g.dsi[1];
+      divb += (-z[t + 6] + 8.0 * z[t + 5] - 8.0 * z[t + 3] + z[t + 2]) * INV12 * g.dsi[2];
+      sum += fabs(divb);
+      mx = fmax(mx, fabs(divb));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  __shared__ double red[8][2];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[wid][0] = sum;
+    red[wid][1] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0, m = 0.0;
+    for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) {
+      s += red[w2][0];
+      m = fmax(m, red[w2][1]);
+    }
+    partial[blockIdx.x * 8 + 5] = s;
+    partial[blockIdx.x * 8 + 6] = m;
+  }
 }
 
 __global__ void set_scalars_kernel(StepScalars *sc, StepScalars v) {
@@ -233,8 +314,7 @@ struct miso_b200_handle {
   bool mon_fuse = false;
   bool mon_valid = false;  // mon_z holds the sums of the current state
   double *mon_z = nullptr;
-  double *mon_divb = nullptr;
-  int divb_blocks = 0;
+
   StepScalars *sc = nullptr;
 
   double min_dxyz = 0.0, cfl_dx = 0.0;
@@ -949,7 +1029,6 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   h->av_grid = 16 * h->sms;
   h->nparts_alloc = h->nparts > h->z_grid ? h->nparts : h->z_grid;
   h->mon_blocks = h->sms * 4;  // 4 x 148 CTAs of 256: 4.0 -> 2.5 ms at 512^3 against 2 per SM
-  h->divb_blocks = h->sms * 8;
   const size_t cells = (size_t)g.cells;
   size_t total = 0;
   std::vector<std::pair<void **, size_t>> plan;
@@ -976,7 +1055,6 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
   add((void **)&h->mon_partial, sizeof(double) * 8 * h->mon_blocks);
   if (h->split()) {
     add((void **)&h->mon_z, sizeof(double) * 6 * h->z_grid);
-    add((void **)&h->mon_divb, sizeof(double) * 2 * h->divb_blocks);
   }
   add((void **)&h->sc, sizeof(StepScalars));
   for (int a = 0; a < 3; ++a) add((void **)&h->axc[a], sizeof(double) * g.t[a]);
@@ -1078,7 +1156,6 @@ int miso_b200::b200_view_create(const miso_b200_grid_desc &gd, const miso_b200_p
   h->z_grid = 8 * h->sms;
   h->nparts_alloc = h->nparts > h->z_grid ? h->nparts : h->z_grid;
   h->mon_blocks = h->sms * 4;
-  h->divb_blocks = h->sms * 8;
   size_t total = 0;
   std::vector<std::pair<void **, size_t>> plan;
   auto add = [&](void **p, size_t b) {
@@ -1088,7 +1165,6 @@ int miso_b200::b200_view_create(const miso_b200_grid_desc &gd, const miso_b200_p
   add((void **)&h->partial, sizeof(float) * h->nparts_alloc);
   add((void **)&h->mon_partial, sizeof(double) * 8 * h->mon_blocks);
   add((void **)&h->mon_z, sizeof(double) * 6 * h->z_grid);
-  add((void **)&h->mon_divb, sizeof(double) * 2 * h->divb_blocks);
   for (int a = 0; a < 3; ++a) add((void **)&h->axc[a], sizeof(double) * g.t[a]);
   e = cudaMalloc(&h->block, total);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->block, 0, total, stream);
@@ -1556,16 +1632,18 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
   for (int a = 0; a < 3; ++a)
     if (h->g.s[a]) dv *= 1.0 / h->g.dsi[a];
   if (h->split() && h->mon_valid) {
-    // the last z sweep summed the state; only |div B| is left to reduce
-    launch_s32_divb(h->g, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->mon_divb,
-                    h->divb_blocks, h->stream);
+    // the last z sweep summed the state; only |div B| is left to reduce (its
+    // stencil reads lo ghost words, which lag the interior until refreshed)
+    if ((rc = h->fresh_lo_shell())) return rc;
+    divb_quad_kernel<<<h->mon_blocks, 256, 0, h->stream>>>(
+        h->g, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->mon_partial);
     h->launches++;
     if ((rc = h->check_launch("divb"))) return rc;
-    std::vector<double> zs((size_t)h->z_grid * 6), db((size_t)h->divb_blocks * 2);
+    std::vector<double> zs((size_t)h->z_grid * 6), db((size_t)h->mon_blocks * 8);
     if ((rc = h->cuda(cudaMemcpyAsync(zs.data(), h->mon_z, zs.size() * sizeof(double),
                                       cudaMemcpyDeviceToHost, h->stream),
                       "read monitors")) ||
-        (rc = h->cuda(cudaMemcpyAsync(db.data(), h->mon_divb, db.size() * sizeof(double),
+        (rc = h->cuda(cudaMemcpyAsync(db.data(), h->mon_partial, db.size() * sizeof(double),
                                       cudaMemcpyDeviceToHost, h->stream),
                       "read monitors")) ||
         (rc = h->cuda(cudaStreamSynchronize(h->stream), "monitors synchronize")))
@@ -1574,9 +1652,9 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
     const int map[6] = {0, 1, 2, 3, 4, 7};  // ro, mx, my, mz, et, ph^2
     for (int b = 0; b < h->z_grid; ++b)
       for (int q = 0; q < 6; ++q) out[map[q]] += zs[(size_t)b * 6 + q];
-    for (int b = 0; b < h->divb_blocks; ++b) {
-      out[5] += db[(size_t)b * 2];
-      out[6] = std::fmax(out[6], db[(size_t)b * 2 + 1]);
+    for (int b = 0; b < h->mon_blocks; ++b) {
+      out[5] += db[(size_t)b * 8 + 5];
+      out[6] = std::fmax(out[6], db[(size_t)b * 8 + 6]);
     }
     for (int q8 = 0; q8 < 8; ++q8)
       if (q8 != 6) out[q8] *= dv;

@@ -747,97 +747,6 @@ av_z_kernel(const AvArgs a) {
   }
 }
 
-// |div B| of the split state over the interior: a warp takes 32 consecutive
-// k cells of a row and finishes the inner 28 (bz neighbours by shuffles),
-// reading bx and by at i +- 1, 2 and j +- 1, 2 (their rows stay in L2); a
-// neighbour across a face is the interior cell it images, with its mirror
-// sign, so the ghost layers need not be current.  The same difference as
-// the monitor kernel: (-p2 + 8 p1 - 8 m1 + m2) / 12 * dsi per axis.
-__device__ __forceinline__ double bval(const CFSet &hi, const CFSet &lo, int f, int cell) {
-  return (double)__ldg(hi.f[f] + cell) + (double)__ldg(lo.f[f] + cell);
-}
-
-__global__ void __launch_bounds__(128)
-divb_kernel(const Geom g, const CFSet hi, const CFSet lo, double *__restrict__ partial) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int nk = g.n[2];
-  const int segs = g.s[2] ? (nk + 27) / 28 : 1;
-  const int work = g.n[0] * g.n[1] * segs;
-  const int warps = gridDim.x * (blockDim.x >> 5);
-  double sum = 0.0, mx = 0.0;
-  for (int wi = blockIdx.x * (blockDim.x >> 5) + wid; wi < work; wi += warps) {
-    const int sg = wi % segs;
-    const int row = wi / segs;
-    const int j = row % g.n[1];
-    const int i = row / g.n[1];
-    // z: this lane's bz (the imaged interior cell across a k face)
-    int k = g.s[2] ? sg * 28 + lane - 2 : lane;
-    double bz = 0.0;
-    if (g.s[2]) {
-      int side;
-      const int ks = ghost_src(g, 2, min(k, nk + 1), side);
-      bz = bval(hi, lo, BZ, cell_of(g, i, j, ks));
-      if (side >= 0 && ((g.negmask[2][side] >> BZ) & 1u)) bz = -bz;
-    }
-    const double zm2 = __shfl_up_sync(0xffffffffu, bz, 2), zm1 = __shfl_up_sync(0xffffffffu, bz, 1);
-    const double zp1 = __shfl_down_sync(0xffffffffu, bz, 1), zp2 = __shfl_down_sync(0xffffffffu, bz, 2);
-    const bool out = g.s[2] ? (lane >= 2 && lane < 30 && k < nk) : (lane == 0);
-    if (!out) continue;
-    if (!g.s[2]) k = 0;
-    double divb = 0.0;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      if (!g.s[d]) continue;
-      double p2, p1, m1, m2;
-      if (d == 2) {
-        p2 = zp2;
-        p1 = zp1;
-        m1 = zm1;
-        m2 = zm2;
-      } else {
-        const int x = d == 0 ? i : j;
-        double v[4];
-        const int offs[4] = {2, 1, -1, -2};
-#pragma unroll
-        for (int n = 0; n < 4; ++n) {
-          int side;
-          const int xs = ghost_src(g, d, x + offs[n], side);
-          const int cell = d == 0 ? cell_of(g, xs, j, k) : cell_of(g, i, xs, k);
-          v[n] = bval(hi, lo, BX + d, cell);
-          if (side >= 0 && ((g.negmask[d][side] >> (BX + d)) & 1u)) v[n] = -v[n];
-        }
-        p2 = v[0];
-        p1 = v[1];
-        m1 = v[2];
-        m2 = v[3];
-      }
-      divb += (-p2 + 8.0 * p1 - 8.0 * m1 + m2) * INV12 * g.dsi[d];
-    }
-    sum += fabs(divb);
-    mx = fmax(mx, fabs(divb));
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  }
-  __shared__ double red[4][2];
-  if (lane == 0) {
-    red[wid][0] = sum;
-    red[wid][1] = mx;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0, m = 0.0;
-    for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) {
-      s += red[w2][0];
-      m = fmax(m, red[w2][1]);
-    }
-    partial[blockIdx.x * 2] = s;
-    partial[blockIdx.x * 2 + 1] = m;
-  }
-}
-
 // ---- z sweep as a streaming line (sweep variant 2) ----
 // The x / y line structure applied to the contiguous axis: a CTA owns ZK
 // consecutive k cells of one i plane and walks a chunk of j rows; per row a
@@ -1158,10 +1067,6 @@ void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st) {
     s32t::av_z_kernel<false><<<grid, 128, 0, st>>>(a);
 }
 
-void launch_s32_divb(const Geom &g, const CFSet &hi, const CFSet &lo, double *partial, int grid,
-                     cudaStream_t st) {
-  s32t::divb_kernel<<<grid, 128, 0, st>>>(g, hi, lo, partial);
-}
 
 int s32_zline_per_sm() {
   int n = 0;

@@ -90,11 +90,7 @@ void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cu
 void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, const AvArgs &a,
                         int dir, bool defer, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);
-// FP64 sum and maximum of |div B| (4th-order central differences) over the
-// interior of the split state hi + lo, per block (2 per block); neighbours
-// across a face come from the interior cells they image
-void launch_s32_divb(const Geom &g, const CFSet &hi, const CFSet &lo, double *partial, int grid,
-                     cudaStream_t st);
+
 // z sweep as a streaming line (TMA rows of 132 k cells, wrap copies of 8 for
 // periodic k faces); writes a.partial[blockIdx.x]
 int s32_zline_per_sm();  // resident z line CTAs per SM (after s32_configure)

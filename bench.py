@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched workloads reported beside the headline")
     ap.add_argument("--cpu-n", type=int, default=64, help="reference CPU sample grid size per core")
-    ap.add_argument("--workload", choices=["turbulence", "brio_wu_batch", "ot_batch"],
+    ap.add_argument("--workload", choices=["turbulence", "brio_wu_batch", "ot_batch",
+                                           "turbulence_blast_batch", "turbulence512_ot_batch"],
                     default="turbulence",
                     help="turbulence: one 3-D grid (the headline); the batch workloads run "
                          "many instances through the batched solver")
@@ -628,8 +629,15 @@ def run_batch(args):
     torch.cuda.set_device(local)
     if args.workload == "brio_wu_batch":
         probs = P.brio_wu_batch(args.count or 4096, seed=rank)
-    else:
+    elif args.workload == "ot_batch":
         probs = P.orszag_tang_batch(args.count or 32, seed=rank)
+    elif args.workload == "turbulence_blast_batch":
+        # 3-D grids of uneven sizes: 24 turbulence 64^3 + 16 blast 48^3
+        probs = ([P.turbulence(64, seed=rank * 64 + s) for s in range(24)] +
+                 [P.blast(48, seed=rank * 64 + s) for s in range(16)])
+    else:
+        # the 512^3 turbulence grid in one batch with 32 Orszag-Tang grids
+        probs = [P.turbulence(args.n, seed=rank)] + P.orszag_tang_batch(32, seed=rank)
     K, W = args.steps, args.warmup
     stream = torch.cuda.Stream()
     with Batch(probs, args.precision, stream=stream.cuda_stream) as b:

@@ -179,8 +179,12 @@ int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, in
  * params: [0] ro_sw, [1] pr_sw, [2] vx_sw, [3] bz_imf, [4] radius, [5] a0,
  * [6] ro_floor, [7] pr_floor, [8] nonzero: miso_b200_cfl masks the sphere
  * r <= radius as the demo's TimeStep::cfl does (timestep.hpp:15-49).
- * FP64 form and non-periodic axes only (ERR_STATE / ERR_ARG otherwise).
- * The FP64 form stays bit for bit the reference's. */
+ * Non-periodic axes only (ERR_ARG otherwise).  The FP64 form stays bit for
+ * bit the reference's.  The FP32 split form applies the same steps to the
+ * primitives it forms in FP64 from its conserved state, after every pass,
+ * and runs its per-cell kernels (which read every ghost cell) while the
+ * boundary is on; on a grid decomposed into shards it is refused
+ * (ERR_STATE). */
 #define MISO_B200_BOUNDARY_FACES 0
 #define MISO_B200_BOUNDARY_MAGNETOSPHERE 1
 int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, int nparams);

@@ -79,7 +79,7 @@ struct miso_b200_batch {
   // 3-D FP32-split instances stepped through views on their own streams
   // (at most VIEW_STREAMS; views on one stream run in turn), forked from
   // and joined back into the batch's stream every step
-  static constexpr int VIEW_STREAMS = 32;
+  static constexpr int VIEW_STREAMS = 64;
   struct View {
     int index;
     miso_b200_handle *h;

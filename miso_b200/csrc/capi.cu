@@ -260,8 +260,10 @@ struct miso_b200_handle {
   int nparts = 0;         // CFL partial minima used by the FP64 / untiled passes
   int nparts_alloc = 0;   // capacity of `partial`
 
-  // tiled FP32-split path (3-D grids)
-  bool tiled = false;
+  // tiled FP32-split path (3-D grids); tiled_ok: the grid can take it (the
+  // magnetosphere boundary, which reads every ghost between passes, runs
+  // the per-cell kernels instead)
+  bool tiled = false, tiled_ok = false;
   // built-in source term (miso_b200_set_source) and the cell centres it
   // reads, one array per axis (ghosts included)
   Source src{};
@@ -479,7 +481,7 @@ struct miso_b200_handle {
     for (int s = 0; s < 2 && ok; ++s) ok = s32_make_tmap(g_, hi[s][0], pb, 2, tm_zwh[s]) == 0;
     if (ok) ok = s32_make_tmap_cc(g_, cc32, tm_zwc, 8) == 0;
     if (ok) {
-      tiled = true;
+      tiled = tiled_ok = true;
       s32_rk_items(g_, rk_L, rk_tiles_j, rk_tiles_k, rk_items);
       const int per_sm = 2;
       rk_grid = rk_items < per_sm * sms ? rk_items : per_sm * sms;
@@ -559,8 +561,24 @@ struct miso_b200_handle {
     return check_launch("fill_ghosts");
   }
 
+  // the magnetosphere boundary on the split state (hi / lo of set s) or on
+  // a stage buffer (stg[s]), after its mirror fill
+  int magneto32(int s, bool stage) {
+    if (!mag.on) return MISO_B200_OK;
+    const int t = tb();
+    if (stage)
+      launch_s32_magneto(g, S(s), S(s), false, mag, p.gm, sms, stream);
+    else
+      launch_s32_magneto(g, H(s), L(s), true, mag, p.gm, sms, stream);
+    te(t, "magnetosphere_bc", (double)g.cells * (stage ? 72.0 : 144.0) +
+                                  (mag.blend[0] ? (double)g.cells * 72.0 : 0.0));
+    launches += 1;
+    return check_launch("magnetosphere boundary");
+  }
+
   int fill_state() {
     int rc = split() ? fill_split(cur) : bc64(0);
+    if (!rc && split()) rc = magneto32(cur, false);
     if (rc) return rc;
     return split() ? halo_f(hi[cur], lo[cur]) : halo_d(q64[0]);
   }
@@ -656,7 +674,7 @@ struct miso_b200_handle {
     const int t = tb();
     if (split() && tiled) {
       if (!partials_valid) {
-        launch_s32_cfl_partial(g, cst(H(cur)), partial, z_grid, sc, p.gm, cfl_dx, stream);
+        launch_s32_cfl_partial(g, cst(H(cur)), partial, z_grid, sc, p.gm, cfl_dx, stream, mag);
         te(t, "cfl", interior() * 32.0);
         const int t2 = tb();
         launch_cfl_finalize(partial, z_grid, sc, p.cfl_number, min_dxyz, stream);
@@ -668,7 +686,7 @@ struct miso_b200_handle {
       return check_launch("cfl");
     }
     if (split()) {
-      launch_s32_cfl_partial(g, cst(H(cur)), partial, nparts, sc, p.gm, cfl_dx, stream);
+      launch_s32_cfl_partial(g, cst(H(cur)), partial, nparts, sc, p.gm, cfl_dx, stream, mag);
       launch_cfl_finalize(partial, nparts, sc, p.cfl_number, min_dxyz, stream);
       te(t, "cfl", interior() * 32.0);
     } else {
@@ -724,9 +742,11 @@ struct miso_b200_handle {
       if ((rc = check_launch("rk_stage"))) return rc;
       if (s < 3) {
         if ((rc = fill_stage(s & 1))) return rc;
+        if ((rc = magneto32(s & 1, true))) return rc;
         if ((rc = halo_f(stg[s & 1]))) return rc;
       } else {
         if ((rc = fill_split(c))) return rc;
+        if ((rc = magneto32(c, false))) return rc;
         if ((rc = halo_f(hi[c], lo[c]))) return rc;
       }
     }
@@ -742,6 +762,7 @@ struct miso_b200_handle {
       if ((rc = check_launch("av_sweep"))) return rc;
       cur ^= 1;
       if ((rc = fill_split(cur))) return rc;
+      if ((rc = magneto32(cur, false))) return rc;
       if ((rc = halo_f(hi[cur], lo[cur]))) return rc;
     }
     return MISO_B200_OK;
@@ -755,6 +776,12 @@ struct miso_b200_handle {
   // stg[1]; av_line_kernel<0, true> forms U^{n+1} from hi, lo and D as it
   // streams them).  Needs the line x sweep and no flat sweep, which would
   // read the images of U^{n+1} and its speed.
+  // persistent grid of a line sweep: two CTAs per SM, or one per work item
+  // on a small grid
+  int line_grid(int d) const {
+    const int items = s32_av_line_items(g, d, av_L);
+    return items < av_grid ? items : av_grid;
+  }
   bool defer_last() const {
     return rk_var == 3 && av_var[0] == 0 && av_var[1] != 1 && av_var[2] != 1;
   }
@@ -850,9 +877,9 @@ struct miso_b200_handle {
       else if (av_var[d] == 2 && d < 2)
         launch_s32_av_march(a, d, avp_grid, stream);
       else if (d == 0 && defer)
-        launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avd, a, 0, true, av_grid, stream);
+        launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avd, a, 0, true, line_grid(0), stream);
       else if (d < 2)
-        launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, false, av_grid, stream);
+        launch_s32_av_line(tm_avh[cur], tm_avl[cur], tm_avc, a, d, false, line_grid(d), stream);
       else if (av_var[2] == 2)
         launch_s32_av_zline(tm_avh[cur], tm_avl[cur], tm_avc, tm_zwh[cur], tm_zwc, a, zl_grid,
                             stream);
@@ -1357,9 +1384,11 @@ int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, 
   if (kind == MISO_B200_BOUNDARY_FACES) {
     h->mag.on = 0;
     h->mag.mask_cfl = 0;
+    h->tiled = h->tiled_ok;
   } else if (kind == MISO_B200_BOUNDARY_MAGNETOSPHERE) {
-    if (h->split())
-      return h->fail(MISO_B200_ERR_STATE, "the magnetosphere boundary runs on the FP64 form");
+    if (h->split() && h->halo_on)
+      return h->fail(MISO_B200_ERR_STATE,
+                     "the split form's magnetosphere boundary runs on a single grid");
     if (h->bc_cb)
       return h->fail(MISO_B200_ERR_STATE, "a boundary callback is set");
     if (!params || nparams < 9)
@@ -1386,6 +1415,9 @@ int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, 
     m.y = h->axc[1];
     m.z = h->axc[2];
     m.on = 1;
+    // the split form runs the per-cell kernels, which read every ghost
+    // cell the boundary writes between passes
+    h->tiled = false;
   } else {
     return h->fail(MISO_B200_ERR_ARG, "unknown boundary kind %d", kind);
   }
@@ -1485,6 +1517,9 @@ int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
                        const miso_b200_halo_ops *ops) {
   if (!h) return MISO_B200_ERR_ARG;
   if (h->bc_cb) return h->fail(MISO_B200_ERR_STATE, "a boundary callback excludes the halo exchange");
+  if (h->split() && h->mag.on && ops)
+    return h->fail(MISO_B200_ERR_STATE,
+                   "the split form's magnetosphere boundary runs on a single grid");
   Geom &g = h->g;
   if (ops && !ops->exchange) return h->fail(MISO_B200_ERR_ARG, "halo ops without exchange");
   if (ops && !g.s[0]) return h->fail(MISO_B200_ERR_ARG, "halo exchange needs an i axis of size > 1");

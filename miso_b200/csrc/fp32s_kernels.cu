@@ -254,7 +254,7 @@ av_sweep_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
 
 __global__ void __launch_bounds__(256)
 cfl_partial_kernel(Geom g, FieldPtrs<const float> u, float *__restrict__ partial,
-                   unsigned int *__restrict__ err, float gm, float cfl_dx) {
+                   unsigned int *__restrict__ err, float gm, float cfl_dx, Magneto mg) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
   float best = 1.e10f;
   bool bad = false;
@@ -271,9 +271,15 @@ cfl_partial_kernel(Geom g, FieldPtrs<const float> u, float *__restrict__ partial
     const float cs = sqrtf(gm * (gm - 1.0f) * e);
     const float vv = sqrtf(mm) * inv;
     const float ca = sqrtf(bb * inv * FPII4);
-    const float tv = cs + vv + ca;
-    best = fminf(best, cfl_dx / tv);
+    float tv = cs + vv + ca;
     bad |= !(q.ro > 0.0f) || !(e >= 0.0f) || !isfinite(tv);
+    if (mg.mask_cfl) {
+      // the magnetosphere demo's CFL (timestep.hpp:15-49): the sphere
+      // r <= r_inner moves at 1e-10
+      const double x = mg.x[i], y = mg.y[j], z = mg.z[k];
+      if (sqrt(x * x + y * y + z * z) <= mg.r_inner) tv = 1.e-10f;
+    }
+    best = fminf(best, cfl_dx / tv);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
@@ -287,6 +293,76 @@ cfl_partial_kernel(Geom g, FieldPtrs<const float> u, float *__restrict__ partial
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
     if (lane == 0) partial[blockIdx.x] = best;
+  }
+}
+
+// The magnetosphere demo's boundary (demo/mhd3d_magnetosphere/src/bc.hpp:
+// 39-158) on the split state, every cell, ghosts included, after the
+// mirror fill: the FP64 form's steps (magneto_bc_kernel) on the cell's
+// primitive variables formed in FP64 from the conserved state -- hi + lo
+// (PAIR) or a stage buffer's single words -- written back in the same form.
+template <bool PAIR>
+__global__ void __launch_bounds__(256)
+magneto_split_kernel(Geom g, FieldPtrs<float> hi, FieldPtrs<float> lo, Magneto mg, double gm) {
+  const bool inflow = g.s[0] && !g.periodic[0] && !g.ext[0][0];
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.cells;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(c % g.t[2]);
+    const long long r1 = c / g.t[2];
+    const int j = (int)(r1 % g.t[1]);
+    const int i = (int)(r1 / g.t[1]);
+    double u[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+      u[f] = PAIR ? (double)hi.f[f][c] + (double)lo.f[f][c] : (double)hi.f[f][c];
+    // conserved -> primitive
+    double p[NF];
+    p[RO] = u[RO];
+    p[VX] = u[MX] / u[RO];
+    p[VY] = u[MY] / u[RO];
+    p[VZ] = u[MZ] / u[RO];
+    p[BX] = u[BX];
+    p[BY] = u[BY];
+    p[BZ] = u[BZ];
+    p[EI] = (u[ET] - 0.5 * u[RO] * (p[VX] * p[VX] + p[VY] * p[VY] + p[VZ] * p[VZ]) -
+             PII8 * (u[BX] * u[BX] + u[BY] * u[BY] + u[BZ] * u[BZ])) /
+            u[RO];
+    p[PH] = u[PH];
+    if (inflow && i < g.m[0]) {
+      p[RO] = mg.ro_sw;
+      p[VX] = mg.vx_sw;
+      p[EI] = mg.pr_sw / (gm - 1.0) / p[RO];
+      p[BZ] = mg.bz_sw;
+    }
+    const double x = mg.x[i], y = mg.y[j], z = mg.z[k];
+    const double rr = sqrt(x * x + y * y + z * z);
+    const double r1n = rr / mg.r_inner;
+    const double hh = fmax2f(0.0, r1n * r1n - 1.0);
+    const double w = mg.a0 * hh / (mg.a0 * hh + 1.0);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const double b = mg.blend[f] ? mg.blend[f][c] : 0.0;
+      p[f] = p[f] * w + b * (1.0 - w);
+    }
+    p[RO] = fmax2f(p[RO], mg.ro_floor);
+    p[EI] = fmax2f(p[EI], mg.pr_floor / (gm - 1.0) / p[RO]);
+    // primitive -> conserved
+    u[RO] = p[RO];
+    u[MX] = p[RO] * p[VX];
+    u[MY] = p[RO] * p[VY];
+    u[MZ] = p[RO] * p[VZ];
+    u[BX] = p[BX];
+    u[BY] = p[BY];
+    u[BZ] = p[BZ];
+    u[ET] = p[RO] * p[EI] + 0.5 * p[RO] * (p[VX] * p[VX] + p[VY] * p[VY] + p[VZ] * p[VZ]) +
+            PII8 * (p[BX] * p[BX] + p[BY] * p[BY] + p[BZ] * p[BZ]);
+    u[PH] = p[PH];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const float h = __double2float_rn(u[f]);
+      hi.f[f][c] = h;
+      if (PAIR) lo.f[f][c] = __double2float_rn(u[f] - (double)h);
+    }
   }
 }
 
@@ -379,9 +455,18 @@ void launch_s32_av_sweep(const Geom &g, const FieldPtrs<const float> &hi,
 
 void launch_s32_cfl_partial(const Geom &g, const FieldPtrs<const float> &u, float *partial,
                             int nparts, StepScalars *sc, double gm, double cfl_dx,
-                            cudaStream_t st) {
+                            cudaStream_t st, const Magneto &mg) {
   s32::cfl_partial_kernel<<<nparts, 256, 0, st>>>(g, u, partial, &sc->err, (float)gm,
-                                                  (float)cfl_dx);
+                                                  (float)cfl_dx, mg);
+}
+
+void launch_s32_magneto(const Geom &g, const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
+                        bool pair, const Magneto &mg, double gm, int sms, cudaStream_t st) {
+  const int grid = blocks_for(g.cells, 256, sms, 8);
+  if (pair)
+    s32::magneto_split_kernel<true><<<grid, 256, 0, st>>>(g, hi, lo, mg, gm);
+  else
+    s32::magneto_split_kernel<false><<<grid, 256, 0, st>>>(g, hi, lo, mg, gm);
 }
 
 void launch_s32_to_split(long long cells, const FieldPtrs<const double> &q,

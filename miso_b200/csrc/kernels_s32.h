@@ -17,9 +17,13 @@ void launch_s32_av_sweep(const Geom &g, const FieldPtrs<const float> &hi,
                          const FieldPtrs<const float> &lo, const FieldPtrs<float> &hi2,
                          const FieldPtrs<float> &lo2, const float *cc, const StepScalars *sc,
                          int dir, double ep, double fh, int sms, cudaStream_t st);
+// the magnetosphere demo's boundary on the split state: hi + lo (pair) or
+// a stage buffer's single words (hi), every cell
+void launch_s32_magneto(const Geom &g, const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
+                        bool pair, const Magneto &mg, double gm, int sms, cudaStream_t st);
 void launch_s32_cfl_partial(const Geom &g, const FieldPtrs<const float> &u, float *partial,
                             int nparts, StepScalars *sc, double gm, double cfl_dx,
-                            cudaStream_t st);
+                            cudaStream_t st, const Magneto &mg = Magneto{});
 void launch_s32_to_split(long long cells, const FieldPtrs<const double> &q,
                          const FieldPtrs<float> &hi, const FieldPtrs<float> &lo, int sms,
                          cudaStream_t st);

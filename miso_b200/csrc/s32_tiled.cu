@@ -1060,6 +1060,11 @@ void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, c
     s32t::av_line_kernel<1, false><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, a);
 }
 
+int s32_av_line_items(const Geom &g, int dir, int L) {
+  const int oth = dir == 0 ? 1 : 0;
+  return ((g.n[2] + s32t::LK - 1) / s32t::LK) * g.n[oth] * ((g.n[dir] + L - 1) / L);
+}
+
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st) {
   if (a.mon)
     s32t::av_z_kernel<true><<<grid, 128, 0, st>>>(a);

@@ -90,6 +90,8 @@ void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cu
 void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, const AvArgs &a,
                         int dir, bool defer, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);
+// work items of the x (dir 0) / y (dir 1) line sweep: k blocks x lines x chunks of L
+int s32_av_line_items(const Geom &g, int dir, int L);
 
 // z sweep as a streaming line (TMA rows of 132 k cells, wrap copies of 8 for
 // periodic k faces); writes a.partial[blockIdx.x]

@@ -15,7 +15,7 @@ MHD demos use: ideal gas with ``eos.gm``; periodic faces where
 ``domain.periodic`` says so and the symmetric mirror (per-field sign) on the
 other faces; no source, or the magnetosphere demo's point gravity when
 ``source.kind`` is ``"point_gravity"`` (``source.g`` its acceleration).
-With ``boundary.kind == "magnetosphere"`` (FP64 form) the magnetosphere
+With ``boundary.kind == "magnetosphere"`` (both forms) the magnetosphere
 demo's boundary and masked CFL replace the plain faces, configured from the
 demo's own ``solar_wind``, ``magnetosphere`` and ``floor`` sections; the
 state it blends toward is the ``blend`` argument (zeros if None).

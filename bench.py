@@ -555,10 +555,14 @@ def time_batch(probs, precision, stream, K, W, local, world):
     batch's stream, max over ranks), with the clocks sampled meanwhile."""
     import torch
 
+    from miso_b200.autotune import autotune_batch
     from miso_b200.batch import Batch
     with Batch(probs, precision, stream=stream.cuda_stream) as b:
         b.upload_all()
         b.run(W, graph=True)
+        b.sync()
+        tuning = autotune_batch(b) if b.views() else {}
+        b.run(1, graph=True)
         b.sync()
         info = b.info()
         cells, l0 = info["interior_cells"], info["launches"]
@@ -578,7 +582,7 @@ def time_batch(probs, precision, stream, K, W, local, world):
         launches = b.info()["launches"] - l0
     return {"value": world * cells * K / (ms / 1e3) / 1e9, "ms_per_step": ms / K,
             "interior_cells": cells, "instances": len(probs), "gpu_launches": launches,
-            "clocks": clocks}
+            "tuning": tuning, "clocks": clocks}
 
 
 def batch_figures(stream, K, W, single, local, world, rank, big=None):
@@ -644,6 +648,10 @@ def run_batch(args):
         b.upload_all()
         b.run(W, graph=True)
         b.sync()
+        from miso_b200.autotune import autotune_batch
+        tuning = autotune_batch(b) if b.views() else {}
+        b.run(1, graph=True)
+        b.sync()
         cells = b.info()["interior_cells"]
         l0 = b.info()["launches"]
         sampler = ClockSampler(local)
@@ -670,7 +678,7 @@ def run_batch(args):
             "config": {"workload": args.workload, "instances": len(probs),
                        "interior_cells": cells, "precision": args.precision,
                        "launch": "one persistent launch per pass, CUDA graph per step"},
-            "gpu_launches": launches, "clocks": clocks}), flush=True)
+            "gpu_launches": launches, "tuning": tuning, "clocks": clocks}), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -347,6 +347,16 @@ int miso_b200_batch_dt(miso_b200_batch *b, double *dt);
 /* Interior cells of all instances, tiles in the work list, kernels enqueued. */
 int miso_b200_batch_info(miso_b200_batch *b, long long *interior_cells, int *tiles,
                          long long *launches);
+/* Planes per work item of the 3-D instances' Runge-Kutta stage and x / y
+ * sweeps (as miso_b200_set_chunks; defaults 64 and 128).  3-D FP32-split
+ * instances that take the tiled path run the single grid's pipelined
+ * kernels, each instance on its own stream forked from the batch's stream
+ * every step; short work items keep more of them in flight at once.  The
+ * autotuner (miso_b200/autotune.py, autotune_batch) picks these per batch
+ * composition. */
+int miso_b200_batch_set_chunks(miso_b200_batch *b, int rk_chunk, int av_chunk);
+/* Number of instances the batch runs through the pipelined kernels. */
+int miso_b200_batch_views(miso_b200_batch *b, int *views);
 const char *miso_b200_batch_last_error(miso_b200_batch *b);
 
 /* Allocation-free CFL time step.  No counterpart in the reference: it is an

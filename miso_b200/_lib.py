@@ -95,6 +95,8 @@ SIGNATURES = {
     "miso_b200_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "miso_b200_arm_timeout_test": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "miso_b200_pointer_kind": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "miso_b200_batch_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "miso_b200_batch_views": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_set_mirror_signs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "miso_b200_set_boundary_callback": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                                        ctypes.c_void_p, ctypes.c_int]),

@@ -146,3 +146,73 @@ def autotune(integ, steps: int = 2, use_cache: bool = True) -> dict:
     if use_cache:
         _save(cache)
     return choice
+
+
+# ---------------------------------------------------------------------------
+# Batched solver: work-item lengths of the 3-D instances' pipelined kernels
+# ---------------------------------------------------------------------------
+BATCH_CHUNKS = ((64, 128), (32, 64), (16, 32), (16, 16), (8, 16))
+
+
+def _batch_key(batch) -> str:
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    shapes = {}
+    for p in batch.problems:
+        g = p.grid
+        k = f"{g.i_size}x{g.j_size}x{g.k_size}"
+        shapes[k] = shapes.get(k, 0) + 1
+    comp = ",".join(f"{n}*{k}" for k, n in sorted(shapes.items()))
+    return f"batch:{batch.precision}:{comp}:sm{sms}"
+
+
+def autotune_batch(batch, steps: int = 3, use_cache: bool = True) -> dict:
+    """Pick and apply the work-item lengths (Runge-Kutta, x / y sweep
+    chunks) of a batch's 3-D instances by timing whole graph-replayed steps
+    of the batch itself (CUDA events); cached per batch composition (the
+    count of each grid shape), precision and SM count.  Short items keep
+    more small grids in flight at once; long ones spend less on halo
+    planes.  The state advances by the steps timed."""
+    import torch
+    if batch.views() == 0:
+        return {}
+    key = _batch_key(batch)
+    cache = _load() if use_cache else {}
+    if key in cache:
+        c = cache[key]
+        batch.set_chunks(c["rk_chunk"], c["av_chunk"])
+        return c
+    import time
+    # events on the batch's own stream when the caller gave it one, else the
+    # host's clock around the synchronised steps
+    stream = torch.cuda.ExternalStream(batch.stream) if batch.stream else None
+    best = None
+    times = {}
+    for rk_chunk, av_chunk in BATCH_CHUNKS:
+        batch.set_chunks(rk_chunk, av_chunk)
+        batch.run(2, graph=True)  # capture (and warm) outside the timing
+        batch.sync()
+        torch.cuda.synchronize()
+        if stream is not None:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            batch.run(steps, graph=True)
+            e1.record(stream)
+            batch.sync()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+        else:
+            t0 = time.perf_counter()
+            batch.run(steps, graph=True)
+            batch.sync()
+            ms = (time.perf_counter() - t0) * 1e3 / steps
+        times[f"{rk_chunk}/{av_chunk}"] = ms
+        if best is None or ms < best[0]:
+            best = (ms, rk_chunk, av_chunk)
+    choice = {"rk_chunk": best[1], "av_chunk": best[2], "ms_per_step": times}
+    batch.set_chunks(choice["rk_chunk"], choice["av_chunk"])
+    cache[key] = choice
+    if use_cache:
+        _save(cache)
+    return choice

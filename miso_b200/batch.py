@@ -29,6 +29,7 @@ class Batch:
         _lib.check(lib.miso_b200_batch_create(n, grids, params, ctypes.c_void_p(stream or 0),
                                               ctypes.byref(h)), None)
         self._h, self._lib = h, lib
+        self.stream = stream  # the cudaStream_t handle given, or None (the library's own)
         self.problems = list(problems)
         self.precision = precision
 
@@ -80,6 +81,16 @@ class Batch:
         out = np.empty(len(self.problems))
         self._check(self._lib.miso_b200_batch_dt(self._h, out.ctypes.data_as(_lib._dp)))
         return out
+
+    def set_chunks(self, rk_chunk: int, av_chunk: int):
+        """Planes per work item of the 3-D instances' pipelined kernels."""
+        self._check(self._lib.miso_b200_batch_set_chunks(self._h, int(rk_chunk), int(av_chunk)))
+
+    def views(self) -> int:
+        """Instances that run the single grid's pipelined kernels."""
+        n = ctypes.c_int()
+        self._check(self._lib.miso_b200_batch_views(self._h, ctypes.byref(n)))
+        return n.value
 
     def info(self) -> dict:
         cells, tiles, launches = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_longlong()

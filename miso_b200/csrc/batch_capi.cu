@@ -737,6 +737,27 @@ int miso_b200_batch_run(miso_b200_batch *b, int nsteps, int use_graph) {
   return MISO_B200_OK;
 }
 
+int miso_b200_batch_set_chunks(miso_b200_batch *b, int rk_chunk, int av_chunk) {
+  if (!b || rk_chunk < 1 || av_chunk < 1) return MISO_B200_ERR_ARG;
+  for (auto &v : b->views) {
+    const int rc = miso_b200_set_chunks(v.h, rk_chunk, av_chunk);
+    if (rc) return b->fail(rc, miso_b200_last_error(v.h));
+  }
+  if (b->graph_exec) {  // the captured step holds the old work lists
+    cudaGraphExecDestroy(b->graph_exec);
+    cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_batch_views(miso_b200_batch *b, int *views) {
+  if (!b || !views) return MISO_B200_ERR_ARG;
+  *views = (int)b->views.size();
+  return MISO_B200_OK;
+}
+
 int miso_b200_batch_sync(miso_b200_batch *b) {
   if (!b) return MISO_B200_ERR_ARG;
   return b->read_err();

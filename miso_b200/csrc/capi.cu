@@ -1433,8 +1433,6 @@ int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, 
 
 int miso_b200_set_blend_state(miso_b200_handle *h, const double *const q[9]) {
   if (!h || !q) return MISO_B200_ERR_ARG;
-  if (h->split())
-    return h->fail(MISO_B200_ERR_STATE, "the magnetosphere boundary runs on the FP64 form");
   const size_t bytes = (size_t)h->g.cells * sizeof(double);
   int rc;
   if (!h->blend_block &&

@@ -259,6 +259,20 @@ typedef struct miso_b200_halo_ops {
 int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
                        const miso_b200_halo_ops *ops);
 
+/* Overlap each halo exchange with the pass after it (3-D FP32-split grids on
+ * the pipelined Runge-Kutta stage and the line x sweep, the defaults;
+ * ERR_STATE otherwise or without a halo exchange).  The exchange callback
+ * is then called with `comm_stream` (a cudaStream_t of the caller's) as its
+ * stream, ordered after the pass that wrote the planes; the next pass that
+ * reads across i -- a Runge-Kutta stage or the x sweep -- first finishes the
+ * planes [2, n-2), which read no ghost plane, then waits for the exchange
+ * and finishes the two boundary groups [0, 2) and [n-2, n).  The results
+ * are the same bits as without overlap.  Shards of one process on one GPU
+ * share one comm stream, as they share one stream.  comm_stream == NULL
+ * turns the overlap off.  No counterpart in the reference, whose halo
+ * exchange blocks between passes (mhd_halo_exchange.hpp:451-621). */
+int miso_b200_set_halo_overlap(miso_b200_handle *h, void *comm_stream);
+
 /* Kernel variant of one kernel class on the 3-D FP32-split path:
  * kernel_class 0 = Runge-Kutta stage, 1/2/3 = viscosity sweep x/y/z;
  * variant 0 = tiled (TMA plane tiles / streaming lines fed by a producer

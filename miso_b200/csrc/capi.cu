@@ -281,6 +281,13 @@ struct miso_b200_handle {
   // halo exchange with neighbouring shards along i (miso_b200_set_halo)
   miso_b200_halo_ops halo_ops{};
   bool halo_on = false;
+  // overlap of the exchange with the next pass (miso_b200_set_halo_overlap):
+  // the callback runs on `comm` after event ev_pass; the next pass finishes
+  // the planes that need no ghost first and waits for ev_xchg before the
+  // two boundary plane groups
+  cudaStream_t comm = nullptr;
+  cudaEvent_t ev_pass = nullptr, ev_xchg = nullptr;
+  bool xchg_pending = false;
   alignas(64) unsigned char tm_hi[2][128];   // RK plane-tile maps of hi[set] (4-D: k, j, i, field)
   alignas(64) unsigned char tm_stg[2][128];  // RK plane-tile maps of stg[set]
   alignas(64) unsigned char tm_avh[2][128];  // AV line maps of hi[set]
@@ -577,7 +584,9 @@ struct miso_b200_handle {
   }
 
   int fill_state() {
-    int rc = split() ? fill_split(cur) : bc64(0);
+    int rc = join_xchg();
+    if (rc) return rc;
+    rc = split() ? fill_split(cur) : bc64(0);
     if (!rc && split()) rc = magneto32(cur, false);
     if (rc) return rc;
     return split() ? halo_f(hi[cur], lo[cur]) : halo_d(q64[0]);
@@ -598,11 +607,34 @@ struct miso_b200_handle {
       rlo[a] = b;                                       // low ghost planes
       rhi[a] = b + (size_t)(ni + m) * plane * elem;    // high ghost planes
     }
+    cudaStream_t xs = stream;
+    if (comm) {
+      // behind everything the pass wrote, on the exchange's own stream
+      int rc = join_xchg();
+      if (!rc) rc = cuda(cudaEventRecord(ev_pass, stream), "record pass event");
+      if (!rc) rc = cuda(cudaStreamWaitEvent(comm, ev_pass, 0), "order the exchange");
+      if (rc) return rc;
+      xs = comm;
+    }
     const int r = halo_ops.exchange(halo_ops.user, n, (size_t)m * plane * elem, g.ext[0][0],
-                                    g.ext[0][1], slo, shi, rlo, rhi, (void *)stream);
+                                    g.ext[0][1], slo, shi, rlo, rhi, (void *)xs);
     if (r) return fail(MISO_B200_ERR_HALO, "halo exchange callback returned %d", r);
+    if (comm) {
+      int rc = cuda(cudaEventRecord(ev_xchg, comm), "record exchange event");
+      if (rc) return rc;
+      xchg_pending = true;
+    }
     return MISO_B200_OK;
   }
+  // the ghost planes of the last exchange are in place before what follows
+  // on the handle's stream
+  int join_xchg() {
+    if (!xchg_pending) return MISO_B200_OK;
+    xchg_pending = false;
+    return cuda(cudaStreamWaitEvent(stream, ev_xchg, 0), "wait for the exchange");
+  }
+  // the pass runs its planes that need no ghost before the exchange lands
+  bool split_pass() const { return comm && xchg_pending && g.n[0] > 4; }
   int halo_d(double *const *set) {
     void *arr[NF];
     for (int f = 0; f < NF; ++f) arr[f] = set[f];
@@ -778,8 +810,8 @@ struct miso_b200_handle {
   // read the images of U^{n+1} and its speed.
   // persistent grid of a line sweep: two CTAs per SM, or one per work item
   // on a small grid
-  int line_grid(int d) const {
-    const int items = s32_av_line_items(g, d, av_L);
+  int line_grid(int d, int r0 = 0, int r1 = -1) const {
+    const int items = s32_av_line_items(g, d, av_L, r0, r1 < 0 ? g.n[d] : r1);
     return items < av_grid ? items : av_grid;
   }
   bool defer_last() const {
@@ -817,16 +849,34 @@ struct miso_b200_handle {
         a.stall_limit = stall_cycles;  // one launch only
         stall_cycles = 0;
       }
+      a.i0 = 0;
+      a.i1 = g.n[0];
       const void *tm = st == 0 ? (const void *)tm_hi[c] : (const void *)tm_stg[(st - 1) & 1];
       const int t = tb();
-      if (rk_var == 1)
-        launch_s32_rk_flat(st == 0 ? cfs(hi[c]) : cfs(stg[(st - 1) & 1]), a, st, flat_grid,
-                           stream);
-      else if (rk_var >= 2)
-        launch_s32_rk_pipe(tm, a, defer && st == 3 ? 4 : st, rk_grid, stream);
-
-      else
-        launch_s32_rk_tiled(tm, a, st, rk_grid, stream);
+      if (rk_var >= 2 && split_pass()) {
+        // a shard with the exchange in flight: the planes [2, n-2) first,
+        // then, with the ghost planes in place, the two boundary groups
+        const int n0 = g.n[0];
+        const int ranges[3][2] = {{2, n0 - 2}, {0, 2}, {n0 - 2, n0}};
+        for (int r = 0; r < 3; ++r) {
+          if (r == 1 && (rc = join_xchg())) return rc;
+          a.i0 = ranges[r][0];
+          a.i1 = ranges[r][1];
+          a.items = s32_rk_items_range(g, rk_L, a.i0, a.i1);
+          const int grid = a.items < 2 * sms ? a.items : 2 * sms;
+          launch_s32_rk_pipe(tm, a, defer && st == 3 ? 4 : st, grid, stream);
+          a.stall_limit = 0;
+        }
+      } else {
+        if ((rc = join_xchg())) return rc;
+        if (rk_var == 1)
+          launch_s32_rk_flat(st == 0 ? cfs(hi[c]) : cfs(stg[(st - 1) & 1]), a, st, flat_grid,
+                             stream);
+        else if (rk_var >= 2)
+          launch_s32_rk_pipe(tm, a, defer && st == 3 ? 4 : st, rk_grid, stream);
+        else
+          launch_s32_rk_tiled(tm, a, st, rk_grid, stream);
+      }
       te(t, "rk_stage",
          interior() * (st == 0 || (defer && st == 3) ? 72.0 : st < 3 ? 108.0 : 184.0));
       if ((rc = check_launch("rk_stage"))) return rc;
@@ -871,8 +921,24 @@ struct miso_b200_handle {
       a.ca_fac = (float)p.ca_fac;
       a.wait_limit = wait_limit;
       a.mon = d == 2 && mon_fuse && av_var[2] == 0 ? mon_z : nullptr;
+      a.r0 = 0;
+      a.r1 = d < 2 ? g.n[d] : 0;
       const int t = tb();
-      if (av_var[d] == 1)
+      if (d == 0 && av_var[0] == 0 && split_pass()) {
+        // a shard with the exchange in flight: the x sweep finishes the
+        // planes [2, n-2) first, the boundary groups after the exchange
+        const int n0 = g.n[0];
+        const int ranges[3][2] = {{2, n0 - 2}, {0, 2}, {n0 - 2, n0}};
+        for (int r = 0; r < 3; ++r) {
+          if (r == 1 && (rc = join_xchg())) return rc;
+          a.r0 = ranges[r][0];
+          a.r1 = ranges[r][1];
+          launch_s32_av_line(tm_avh[cur], tm_avl[cur], defer ? tm_avd : tm_avc, a, 0, defer,
+                             line_grid(0, a.r0, a.r1), stream);
+        }
+      } else if (((rc = join_xchg()))) {
+        return rc;
+      } else if (av_var[d] == 1)
         launch_s32_av_flat(a, d, flat_grid, stream);
       else if (av_var[d] == 2 && d < 2)
         launch_s32_av_march(a, d, avp_grid, stream);
@@ -917,8 +983,10 @@ struct miso_b200_handle {
 
   int read_err() {
     unsigned int e = 0;
-    int rc = cuda(cudaMemcpyAsync(&e, &sc->err, sizeof e, cudaMemcpyDeviceToHost, stream),
-                  "read error flags");
+    int rc = join_xchg();
+    if (rc) return rc;
+    rc = cuda(cudaMemcpyAsync(&e, &sc->err, sizeof e, cudaMemcpyDeviceToHost, stream),
+              "read error flags");
     if (rc) return rc;
     if ((rc = cuda(cudaStreamSynchronize(stream), "synchronize"))) return rc;
     if (e & (ERRBIT_NONFINITE | ERRBIT_TIMEOUT)) {
@@ -1245,7 +1313,10 @@ extern "C" {
 
 int miso_b200_destroy(miso_b200_handle *h) {
   if (!h) return MISO_B200_ERR_ARG;
+  h->join_xchg();
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->ev_pass) cudaEventDestroy(h->ev_pass);
+  if (h->ev_xchg) cudaEventDestroy(h->ev_xchg);
   h->harvest();
   for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
@@ -1260,6 +1331,7 @@ int miso_b200_destroy(miso_b200_handle *h) {
 
 int miso_b200_upload(miso_b200_handle *h, const double *const q[9]) {
   if (!h || !q) return MISO_B200_ERR_ARG;
+  if (int rc0 = h->join_xchg()) return rc0;
   const size_t bytes = (size_t)h->g.cells * sizeof(double);
   int rc;
   for (int f = 0; f < NF; ++f) {
@@ -1289,7 +1361,8 @@ int miso_b200_upload(miso_b200_handle *h, const double *const q[9]) {
 int miso_b200_download_async(miso_b200_handle *h, double *const q[9], void *event) {
   if (!h || !q) return MISO_B200_ERR_ARG;
   const size_t bytes = (size_t)h->g.cells * sizeof(double);
-  int rc;
+  int rc = h->join_xchg();
+  if (rc) return rc;
   for (int f = 0; f < NF; ++f)
     if (!q[f]) return h->fail(MISO_B200_ERR_ARG, "null field pointer %d", f);
   if ((rc = h->fresh_lo_shell())) return rc;
@@ -1312,7 +1385,8 @@ int miso_b200_download_async(miso_b200_handle *h, double *const q[9], void *even
 int miso_b200_download(miso_b200_handle *h, double *const q[9]) {
   if (!h || !q) return MISO_B200_ERR_ARG;
   const size_t bytes = (size_t)h->g.cells * sizeof(double);
-  int rc;
+  int rc = h->join_xchg();
+  if (rc) return rc;
   if ((rc = h->fresh_lo_shell())) return rc;
   if (h->split()) {
     launch_s32_from_split(h->g.cells, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->IO(), h->sms,
@@ -1511,9 +1585,33 @@ int miso_b200_set_boundary_callback(miso_b200_handle *h, miso_b200_boundary_fn f
   return MISO_B200_OK;
 }
 
+int miso_b200_set_halo_overlap(miso_b200_handle *h, void *comm_stream) {
+  if (!h) return MISO_B200_ERR_ARG;
+  if (int rc = h->join_xchg()) return rc;
+  if (!comm_stream) {
+    h->comm = nullptr;
+    return MISO_B200_OK;
+  }
+  if (!h->halo_on) return h->fail(MISO_B200_ERR_STATE, "no halo exchange is set");
+  if (!h->tiled || h->rk_var < 2 || h->av_var[0] != 0)
+    return h->fail(MISO_B200_ERR_STATE,
+                   "the overlapped exchange runs on the pipelined split path "
+                   "(3-D FP32-split grid, Runge-Kutta variant 2 or 3, line x sweep)");
+  int rc = MISO_B200_OK;
+  if (!h->ev_pass)
+    rc = h->cuda(cudaEventCreateWithFlags(&h->ev_pass, cudaEventDisableTiming), "event");
+  if (!rc && !h->ev_xchg)
+    rc = h->cuda(cudaEventCreateWithFlags(&h->ev_xchg, cudaEventDisableTiming), "event");
+  if (rc) return rc;
+  h->comm = (cudaStream_t)comm_stream;
+  return MISO_B200_OK;
+}
+
 int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
                        const miso_b200_halo_ops *ops) {
   if (!h) return MISO_B200_ERR_ARG;
+  if (int rc = h->join_xchg()) return rc;
+  if (!ops) h->comm = nullptr;
   if (h->bc_cb) return h->fail(MISO_B200_ERR_STATE, "a boundary callback excludes the halo exchange");
   if (h->split() && h->mag.on && ops)
     return h->fail(MISO_B200_ERR_STATE,
@@ -1658,6 +1756,7 @@ int miso_b200_last_dt(miso_b200_handle *h, double *dt_out) {
 
 int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
   if (!h || !out) return MISO_B200_ERR_ARG;
+  if (int rc0 = h->join_xchg()) return rc0;
   FieldPtrs<const double> q{};
   FieldPtrs<const float> hs{}, ls{};
   int rc;
@@ -1736,6 +1835,10 @@ int miso_b200_fields_view(miso_b200_handle *h, double *ptrs[9]) {
 }
 
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
+  if (h && h->comm && ((kernel_class == 0 && variant < 2) || (kernel_class == 1 && variant != 0))) {
+    h->join_xchg();
+    h->comm = nullptr;  // the overlapped exchange needs the pipelined stage and the line x sweep
+  }
   if (!h || kernel_class < 0 || kernel_class > 3 || variant < 0 ||
       variant > (kernel_class == 0 ? 3 : 2))
     return MISO_B200_ERR_ARG;

@@ -97,8 +97,8 @@ __device__ __forceinline__ Item item_of(const RkArgs &a, int it) {
   const int tj = rem / a.tiles_k;
   r.jj = tj * TJ;
   r.kk = (rem - tj * a.tiles_k) * TK;
-  r.i_start = ch * a.L;
-  r.i_end = min(a.g.n[0], r.i_start + a.L);
+  r.i_start = a.i0 + ch * a.L;
+  r.i_end = min(a.i1, r.i_start + a.L);
   return r;
 }
 

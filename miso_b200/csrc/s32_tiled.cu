@@ -192,8 +192,8 @@ __device__ __forceinline__ Item item_of(const RkArgs &a, int it) {
   const int ch = it / per_chunk, rem = it % per_chunk;
   r.tj = rem / a.tiles_k;
   r.tk = rem % a.tiles_k;
-  r.i_start = ch * a.L;
-  r.i_end = min(a.g.n[0], r.i_start + a.L);
+  r.i_start = a.i0 + ch * a.L;
+  r.i_end = min(a.i1, r.i_start + a.L);
   return r;
 }
 
@@ -357,8 +357,8 @@ __device__ __forceinline__ LineItem line_item(const AvArgs &a, int it, int kbloc
   const int r1 = it / kblocks;
   r.u = r1 % nu;
   const int ch = r1 / nu;
-  r.t0 = ch * a.L;
-  r.t1 = min(a.g.n[DIR], r.t0 + a.L);
+  r.t0 = a.r0 + ch * a.L;
+  r.t1 = min(a.r1, r.t0 + a.L);
   return r;
 }
 
@@ -422,7 +422,7 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
   const int tid = threadIdx.x, lane = tid & 31;
   const int nk = g.n[2], nu = g.n[OTH];
   const int kblocks = (nk + LK - 1) / LK;
-  const int chunks = (g.n[DIR] + a.L - 1) / a.L;
+  const int chunks = (a.r1 - a.r0 + a.L - 1) / a.L;
   const int items = kblocks * nu * chunks;
   if (tid == 0) {
     for (int b = 0; b < LNB; ++b) {
@@ -1027,6 +1027,12 @@ int s32_configure() {
   return e == cudaSuccess ? 0 : -1;
 }
 
+int s32_rk_items_range(const Geom &g, int L, int i0, int i1) {
+  const int tj = (g.n[1] + s32t::TJ - 1) / s32t::TJ;
+  const int tk = (g.n[2] + s32t::TK - 1) / s32t::TK;
+  return tj * tk * ((i1 - i0 + L - 1) / L);
+}
+
 void s32_rk_items(const Geom &g, int L, int &tiles_j, int &tiles_k, int &items) {
   tiles_j = (g.n[1] + s32t::TJ - 1) / s32t::TJ;
   tiles_k = (g.n[2] + s32t::TK - 1) / s32t::TK;
@@ -1060,9 +1066,9 @@ void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, c
     s32t::av_line_kernel<1, false><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, a);
 }
 
-int s32_av_line_items(const Geom &g, int dir, int L) {
+int s32_av_line_items(const Geom &g, int dir, int L, int r0, int r1) {
   const int oth = dir == 0 ? 1 : 0;
-  return ((g.n[2] + s32t::LK - 1) / s32t::LK) * g.n[oth] * ((g.n[dir] + L - 1) / L);
+  return ((g.n[2] + s32t::LK - 1) / s32t::LK) * g.n[oth] * ((r1 - r0 + L - 1) / L);
 }
 
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st) {

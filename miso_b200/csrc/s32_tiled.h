@@ -20,6 +20,7 @@ struct RkArgs {
   unsigned int *err;
   float gm, gm1, cs_fac, vv_fac, ca_fac;
   int L;  // planes per work item along i
+  int i0, i1;  // the planes [i0, i1) this launch finishes (a shard's interior / boundary part)
   int tiles_j, tiles_k, items;
   Source src;           // built-in source term (kind 0: none)
   const float *src_ro;  // density of the stage's argument state (the source's ro)
@@ -41,6 +42,7 @@ struct AvArgs {
   float *partial;  // z sweep: per-block CFL minima of the new state (nullable)
   float ep, fh, gm, gm1, cfl_dx;
   int L;  // cells per work item along the sweep axis (x, y sweeps)
+  int r0, r1;  // x / y sweeps: the cells [r0, r1) of the sweep axis this launch finishes
   // x sweep with the last RK update deferred into it: hi / lo hold U^n, and
   // the speed of U^{n+1} = (hi, lo) - dt_4 D goes to cc_out
   float *cc_out;
@@ -79,6 +81,8 @@ int s32_make_tmap(const Geom &g, const float *field0, size_t pitch_bytes, int ki
 int s32_make_tmap_cc(const Geom &g, const float *cc, void *tm_out, int kbox = 132);
 int s32_configure();
 void s32_rk_items(const Geom &g, int L, int &tiles_j, int &tiles_k, int &items);
+// work items of an RK stage launch over the planes [i0, i1)
+int s32_rk_items_range(const Geom &g, int L, int i0, int i1);
 void launch_s32_rk_tiled(const void *tm, const RkArgs &a, int stage, int grid, cudaStream_t st);
 // Pipelined RK stage (s32_rk.cu): same tensor map and work items as the
 // tiled kernel, one barrier per plane, packed FP32x2 differences.
@@ -90,8 +94,9 @@ void launch_s32_rk_pipe(const void *tm, const RkArgs &a, int stage, int grid, cu
 void launch_s32_av_line(const void *tm_hi, const void *tm_lo, const void *tm3, const AvArgs &a,
                         int dir, bool defer, int grid, cudaStream_t st);
 void launch_s32_av_z(const AvArgs &a, int grid, cudaStream_t st);
-// work items of the x (dir 0) / y (dir 1) line sweep: k blocks x lines x chunks of L
-int s32_av_line_items(const Geom &g, int dir, int L);
+// work items of the x (dir 0) / y (dir 1) line sweep over the cells [r0, r1)
+// of its axis: k blocks x lines x chunks of L
+int s32_av_line_items(const Geom &g, int dir, int L, int r0, int r1);
 
 // z sweep as a streaming line (TMA rows of 132 k cells, wrap copies of 8 for
 // periodic k faces); writes a.partial[blockIdx.x]

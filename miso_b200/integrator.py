@@ -242,6 +242,14 @@ class Integrator:
     def set_chunks(self, rk_chunk: int, av_chunk: int):
         self._check(self._lib.miso_b200_set_chunks(self._h, int(rk_chunk), int(av_chunk)))
 
+    def set_halo_overlap(self, comm_stream: int | None):
+        """Overlap each halo exchange with the next pass: the exchange runs
+        on ``comm_stream`` (a cudaStream_t handle; shards of one process
+        share one), the next pass finishes the planes that need no ghost
+        first.  ``None`` turns it off."""
+        self._check(self._lib.miso_b200_set_halo_overlap(self._h,
+                                                         ctypes.c_void_p(comm_stream or 0)))
+
     def set_monitor_fusion(self, on: bool = True):
         """Fold the monitors' sums into every step's last sweep (3-D split
         grids): monitors() then only reduces |div B|."""

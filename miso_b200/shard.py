@@ -277,11 +277,13 @@ class _nullcontext:
 
 
 def run_local_shards(prob, count: int, steps: int, precision: str = "fp64", variants=None,
-                     stream=None) -> tuple[np.ndarray, list[float]]:
+                     stream=None, overlap: bool = False) -> tuple[np.ndarray, list[float]]:
     """Advance ``prob`` by ``steps`` host-dt steps (cfl, then update) as
     ``count`` shards on the current GPU, one host thread per shard, all on
     one CUDA stream (``stream``, or a new one); return the gathered global
-    interior and the time steps taken."""
+    interior and the time steps taken.  With ``overlap`` the exchanges run
+    on a second stream shared by the shards while each next pass finishes
+    the planes that need no ghost (``Integrator.set_halo_overlap``)."""
     import torch
     periodic_x = bool(prob.config["domain"]["periodic"]["x"])
     specs = split_grid(prob.grid, count, periodic_x)
@@ -295,6 +297,7 @@ def run_local_shards(prob, count: int, steps: int, precision: str = "fp64", vari
     if not stream:
         raise ValueError("the shards need one explicit (non-null) CUDA stream")
     st = stream
+    comm = torch.cuda.Stream() if overlap else None
     integs = []
     for s in specs:
         blend = getattr(prob, "blend", None)
@@ -303,6 +306,8 @@ def run_local_shards(prob, count: int, steps: int, precision: str = "fp64", vari
         for cls, var in (variants or {}).items():
             integ.set_variant(cls, var)
         halo.attach(integ, s)
+        if comm is not None:
+            integ.set_halo_overlap(comm.cuda_stream)
         integ.upload(split_state(prob.q, prob.grid, s))
         integs.append(integ)
     dts = [[] for _ in specs]

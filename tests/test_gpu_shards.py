@@ -50,6 +50,31 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("make,count", [(lambda: P.turbulence(40, seed=3), 2),
+                                        (lambda: P.blast(36, seed=1), 3),
+                                        (lambda: P.turbulence(32, seed=4), 4)],
+                         ids=["turb40_x2", "blast36_x3", "turb32_x4"])
+def test_overlapped_exchange_equals_single_grid(make, count):
+    """The exchange on its own stream while each next pass finishes the
+    planes that need no ghost, the boundary plane groups after it: the same
+    bits as the single grid (and so as the blocking exchange)."""
+    prob = make()
+    steps = 4
+    ref, dts = single(prob, steps, "fp32_split")
+    got, sdts = run_local_shards(prob, count, steps, "fp32_split", overlap=True)
+    assert sdts == dts
+    assert np.array_equal(got, ref)
+
+
+def test_overlap_refused_off_the_pipelined_path():
+    from miso_b200 import _lib
+    prob = P.turbulence(24, seed=1)
+    with Integrator(prob.config, prob.grid, precision="fp32_split") as integ:
+        with pytest.raises(_lib.MisoError) as e:
+            integ.set_halo_overlap(1)  # no halo exchange set
+        assert e.value.code == _lib.ERR_STATE
+
+
 @pytest.mark.parametrize("name,make,precision,count,variants", CASES,
                          ids=[c[0] for c in CASES])
 def test_shards_equal_single_grid(name, make, precision, count, variants):

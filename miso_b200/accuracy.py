@@ -71,8 +71,19 @@ def compare(prob, steps: int, every: int, emit=print) -> dict:
     inner = (slice(None),) + prob.grid.interior
     rec = {}
     t = 0.0
+    from . import _lib
     for s in range(1, steps + 1):
-        dt = forms["fp64"].cfl()
+        try:
+            dt = forms["fp64"].cfl()
+        except _lib.MisoError as exc:
+            # the FP64 form (the reference's arithmetic) met a non-positive
+            # density or internal energy: record where, and stop
+            q = forms["fp64"].download()[inner]
+            rec = {"problem": prob.name, "failed_at_step": s, "time": t, "form": "fp64",
+                   "error": str(exc), "min_rho": float(q[P.RO].min()),
+                   "min_ei": float(q[P.EI].min())}
+            emit(json.dumps(rec))
+            break
         forms["fp64"].update(dt)
         forms["fp32_split"].update(dt)
         t += dt

@@ -119,6 +119,22 @@ int miso_b200_update_device(miso_b200_handle *h);
  * replayed.  Asynchronous. */
 int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph);
 
+/* The time loop of ModelBase::run between two outputs, kept on the device
+ * (mhd_model_base.hpp:108-111 with ModelBase::update, :57-62, and
+ * Time::update, time.hpp:64-67): steps -- CFL, update, time += dt, dt kept
+ * on the device as miso_b200_run does -- while time < t_end and fewer than
+ * max_steps steps were taken, checked after every step as the reference's
+ * loop checks it.  *time is the time before (in) and after (out); *steps
+ * the steps taken.  With use_graph the loop is one CUDA graph launch: a
+ * conditional WHILE node whose condition a one-thread kernel sets after
+ * each step from the device-held time (where a step swaps the FP32-split
+ * hi / lo sets the body holds two steps, the second under an IF node with
+ * the same condition).  Without it, or with a boundary callback, the steps
+ * are launched from the host and the time is read after each.
+ * Synchronises.  ERR_STATE on a shard (its dt is reduced on the host). */
+int miso_b200_run_until(miso_b200_handle *h, double *time, double t_end, int max_steps,
+                        int use_graph, int *steps);
+
 /* Wait for the handle's stream; reports device-side error flags. */
 int miso_b200_sync(miso_b200_handle *h);
 

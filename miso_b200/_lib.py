@@ -97,6 +97,9 @@ SIGNATURES = {
     "miso_b200_pointer_kind": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_batch_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_batch_views": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "miso_b200_run_until": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_set_halo_overlap": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "miso_b200_set_mirror_signs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "miso_b200_set_boundary_callback": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,

@@ -225,6 +225,32 @@ divb_quad_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
   }
 }
 
+// The time loop of ModelBase::run kept on the device
+// (miso_b200_run_until): after every step, time += dt (Time::update,
+// time.hpp), and the loop goes on while time < t_end and fewer than
+// max_steps steps were taken (mhd_model_base.hpp:108-111).
+struct RunState {
+  double time, t_end;
+  int steps, max_steps;
+};
+
+__global__ void advance_kernel(RunState *rs, const StepScalars *sc) {
+  rs->time += sc->dt;
+  rs->steps += 1;
+}
+
+// the same inside the loop's graph: the conditions of the WHILE node and
+// (a body of two steps) of the IF node around the second step
+__global__ void advance_cond_kernel(RunState *rs, const StepScalars *sc,
+                                    cudaGraphConditionalHandle h_while,
+                                    cudaGraphConditionalHandle h_if, int set_if) {
+  rs->time += sc->dt;
+  rs->steps += 1;
+  const unsigned go = rs->time < rs->t_end && rs->steps < rs->max_steps ? 1u : 0u;
+  cudaGraphSetConditional(h_while, go);
+  if (set_if) cudaGraphSetConditional(h_if, go);
+}
+
 __global__ void set_scalars_kernel(StepScalars *sc, StepScalars v) {
   const unsigned int err = sc->err;
   *sc = v;
@@ -335,6 +361,22 @@ struct miso_b200_handle {
   // stage launched outside a graph capture stalls on a barrier phase that
   // nothing completes, with this bound (0: not armed)
   long long stall_cycles = 0;
+
+  void drop_loop() {
+    if (loop_exec) cudaGraphExecDestroy(loop_exec);
+    if (loop_graph) cudaGraphDestroy(loop_graph);
+    loop_exec = nullptr;
+    loop_graph = nullptr;
+    loop_cur = -1;
+  }
+  // the device-held time loop (miso_b200_run_until): one graph with a WHILE
+  // node around one step (or two, the second under an IF node, where a step
+  // swaps the hi / lo sets)
+  RunState *rs = nullptr;
+  cudaGraph_t loop_graph = nullptr;
+  cudaGraphExec_t loop_exec = nullptr;
+  int loop_cur = -1, loop_steps = 0;
+  long long loop_kernels = 0;  // kernels per step
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -1152,6 +1194,7 @@ int miso_b200_create(const miso_b200_grid_desc *gd, const miso_b200_params *pp, 
     add((void **)&h->mon_z, sizeof(double) * 6 * h->z_grid);
   }
   add((void **)&h->sc, sizeof(StepScalars));
+  add((void **)&h->rs, sizeof(RunState));
   for (int a = 0; a < 3; ++a) add((void **)&h->axc[a], sizeof(double) * g.t[a]);
   e = cudaMalloc(&h->block, total);
   if (e != cudaSuccess) {
@@ -1321,6 +1364,8 @@ int miso_b200_destroy(miso_b200_handle *h) {
   for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->loop_exec) cudaGraphExecDestroy(h->loop_exec);
+  if (h->loop_graph) cudaGraphDestroy(h->loop_graph);
   if (h->block) cudaFree(h->block);
   if (h->blend_block) cudaFree(h->blend_block);
   if (h->bc_stage) cudaFreeHost(h->bc_stage);
@@ -1449,6 +1494,7 @@ int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, in
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   return MISO_B200_OK;
 }
@@ -1501,6 +1547,7 @@ int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, 
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   return MISO_B200_OK;
 }
@@ -1542,6 +1589,7 @@ int miso_b200_set_mirror_signs(miso_b200_handle *h, const double *sign) {
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   return MISO_B200_OK;
 }
@@ -1581,6 +1629,7 @@ int miso_b200_set_boundary_callback(miso_b200_handle *h, miso_b200_boundary_fn f
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   return MISO_B200_OK;
 }
@@ -1635,6 +1684,7 @@ int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   h->partials_valid = false;
   return MISO_B200_OK;
@@ -1689,6 +1739,7 @@ int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   if (!h->graph_exec) {
     const int before = h->cur;
@@ -1735,6 +1786,154 @@ int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
     if ((rc = h->enqueue_cfl())) return rc;
     if ((rc = h->enqueue_update())) return rc;
   }
+  return MISO_B200_OK;
+}
+
+// The loop graph: WHILE { step; advance } with the condition set by the
+// advance kernel; where a step swaps the hi / lo sets the body holds two
+// steps, the second under an IF node with the same condition, so the loop
+// still stops after the step that reaches t_end.
+static int build_loop_graph(miso_b200_handle *h) {
+  if (h->loop_exec) cudaGraphExecDestroy(h->loop_exec);
+  if (h->loop_graph) cudaGraphDestroy(h->loop_graph);
+  h->loop_exec = nullptr;
+  h->loop_graph = nullptr;
+  cudaGraph_t g = nullptr;
+  int rc = h->cuda(cudaGraphCreate(&g, 0), "graph create");
+  if (rc) return rc;
+  cudaGraphConditionalHandle h_while;
+  rc = h->cuda(cudaGraphConditionalHandleCreate(&h_while, g, 1, cudaGraphCondAssignDefault),
+               "conditional handle");
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = h_while;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  if (!rc) rc = h->cuda(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp), "while node");
+  if (rc) {
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  const int before = h->cur;
+  const bool valid_before = h->partials_valid;
+  const long long l0 = h->launches;
+  cudaGraph_t tmp = nullptr;
+  // the IF node's handle (used where a step swaps the hi / lo sets)
+  cudaGraphConditionalHandle h_if = 0;
+  rc = h->cuda(cudaGraphConditionalHandleCreate(&h_if, wp.conditional.phGraph_out[0], 0,
+                                                cudaGraphCondAssignDefault),
+               "conditional handle");
+  if (rc) {
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  h->capturing = true;
+  rc = h->cuda(cudaStreamBeginCaptureToGraph(h->stream, wp.conditional.phGraph_out[0], nullptr,
+                                             nullptr, 0, cudaStreamCaptureModeThreadLocal),
+               "begin capture");
+  if (!rc) rc = h->enqueue_cfl();
+  if (!rc) rc = h->enqueue_update();
+  const long long per_step = h->launches - l0 + 1;
+  const bool two = !rc && h->cur != before;
+  if (!rc) {
+    advance_cond_kernel<<<1, 1, 0, h->stream>>>(h->rs, h->sc, h_while, h_if, two ? 1 : 0);
+    rc = h->check_launch("advance");
+  }
+  cudaGraphNodeParams ip = {};
+  if (!rc && two) {
+    // the second step under an IF node with the loop's condition
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    rc = h->cuda(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &cg, &deps, &nd),
+                 "capture info");
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = h_if;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    if (!rc) rc = h->cuda(cudaGraphAddNode(&inode, cg, deps, nd, &ip), "if node");
+    if (!rc)
+      rc = h->cuda(cudaStreamUpdateCaptureDependencies(h->stream, &inode, 1,
+                                                        cudaStreamSetCaptureDependencies),
+                   "capture dependencies");
+  }
+  cudaError_t e = cudaStreamEndCapture(h->stream, &tmp);
+  if (!rc) rc = h->cuda(e, "end capture");
+  if (!rc && two) {
+    rc = h->cuda(cudaStreamBeginCaptureToGraph(h->stream, ip.conditional.phGraph_out[0], nullptr,
+                                               nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                 "begin capture");
+    if (!rc) rc = h->enqueue_cfl();
+    if (!rc) rc = h->enqueue_update();
+    if (!rc) {
+      advance_cond_kernel<<<1, 1, 0, h->stream>>>(h->rs, h->sc, h_while, h_if, 0);
+      rc = h->check_launch("advance");
+    }
+    e = cudaStreamEndCapture(h->stream, &tmp);
+    if (!rc) rc = h->cuda(e, "end capture");
+  }
+  h->capturing = false;
+  h->cur = before;
+  h->partials_valid = valid_before;
+  h->launches = l0;
+  if (!rc) rc = h->cuda(cudaGraphInstantiate(&h->loop_exec, g, 0), "graph instantiate");
+  if (rc) {
+    cudaGraphDestroy(g);
+    h->loop_exec = nullptr;
+    return rc;
+  }
+  h->loop_graph = g;
+  h->loop_cur = before;
+  h->loop_steps = two ? 2 : 1;
+  h->loop_kernels = per_step;
+  return MISO_B200_OK;
+}
+
+int miso_b200_run_until(miso_b200_handle *h, double *time, double t_end, int max_steps,
+                        int use_graph, int *steps_out) {
+  if (!h || !time || !steps_out || max_steps < 0) return MISO_B200_ERR_ARG;
+  *steps_out = 0;
+  if (h->halo_on)
+    return h->fail(MISO_B200_ERR_STATE, "a shard steps with cfl() and update(dt)");
+  if (h->bc_cb) use_graph = 0;  // a host callback between passes cannot be captured
+  if (!(*time < t_end) || max_steps == 0) return MISO_B200_OK;
+  RunState st{*time, t_end, 0, max_steps};
+  int rc = h->cuda(cudaMemcpyAsync(h->rs, &st, sizeof st, cudaMemcpyHostToDevice, h->stream),
+                   "set the run state");
+  if (!rc) rc = h->cuda(cudaStreamSynchronize(h->stream), "synchronize");
+  if (rc) return rc;
+  // eager steps: without a graph, and until the tiled split path holds the
+  // CFL minima its captured step relies on
+  while (!use_graph || (h->tiled && !h->partials_valid)) {
+    if ((rc = h->enqueue_cfl()) || (rc = h->enqueue_update())) return rc;
+    advance_kernel<<<1, 1, 0, h->stream>>>(h->rs, h->sc);
+    h->launches++;
+    if ((rc = h->check_launch("advance"))) return rc;
+    rc = h->cuda(cudaMemcpyAsync(&st, h->rs, sizeof st, cudaMemcpyDeviceToHost, h->stream),
+                 "read the run state");
+    if (!rc) rc = h->read_err();
+    if (rc) return rc;
+    *time = st.time;
+    *steps_out = st.steps;
+    if (!(st.time < t_end) || st.steps >= max_steps) return MISO_B200_OK;
+  }
+  if (!h->loop_exec || h->loop_cur != h->cur)
+    if ((rc = build_loop_graph(h))) return rc;
+  if ((rc = h->cuda(cudaGraphLaunch(h->loop_exec, h->stream), "graph launch"))) return rc;
+  rc = h->cuda(cudaMemcpyAsync(&st, h->rs, sizeof st, cudaMemcpyDeviceToHost, h->stream),
+               "read the run state");
+  if (!rc) rc = h->read_err();
+  if (rc) return rc;
+  const int taken = st.steps - *steps_out;
+  h->launches += h->loop_kernels * taken;
+  // each step swaps the sets where the body holds two steps
+  if (h->loop_steps == 2 && (taken & 1)) h->cur ^= 1;
+  if (h->tiled) h->partials_valid = true;
+  *time = st.time;
+  *steps_out = st.steps;
   return MISO_B200_OK;
 }
 
@@ -1854,6 +2053,7 @@ int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   return MISO_B200_OK;
 }
@@ -1870,6 +2070,7 @@ int miso_b200_set_chunks(miso_b200_handle *h, int rk_chunk, int av_chunk) {
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   return MISO_B200_OK;
 }
@@ -1884,6 +2085,7 @@ int miso_b200_set_monitor_fusion(miso_b200_handle *h, int on) {
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   return MISO_B200_OK;
 }
@@ -1897,6 +2099,7 @@ int miso_b200_set_wait_limit(miso_b200_handle *h, long long cycles) {
     cudaGraphDestroy(h->graph);
     h->graph_exec = nullptr;
     h->graph = nullptr;
+    h->drop_loop();
   }
   return MISO_B200_OK;
 }

@@ -242,6 +242,19 @@ class Integrator:
     def set_chunks(self, rk_chunk: int, av_chunk: int):
         self._check(self._lib.miso_b200_set_chunks(self._h, int(rk_chunk), int(av_chunk)))
 
+    def run_until(self, time: float, t_end: float, max_steps: int = 2**31 - 1,
+                  graph: bool = True) -> tuple[float, int]:
+        """Steps (cfl, update, time += dt) with dt and the time on the
+        device while time < t_end (and fewer than max_steps); with ``graph``
+        one CUDA graph launch (a conditional WHILE node) runs the loop.
+        Returns the new time and the steps taken."""
+        t = ctypes.c_double(time)
+        n = ctypes.c_int()
+        self._check(self._lib.miso_b200_run_until(self._h, ctypes.byref(t), float(t_end),
+                                                  int(max_steps), int(bool(graph)),
+                                                  ctypes.byref(n)))
+        return t.value, n.value
+
     def set_halo_overlap(self, comm_stream: int | None):
         """Overlap each halo exchange with the next pass: the exchange runs
         on ``comm_stream`` (a cudaStream_t handle; shards of one process

@@ -12,6 +12,14 @@ that follow it.
 
 Configuration keys, as the reference reads them: ``time.tend``,
 ``time.dt_output``, ``io.enabled``, ``io.continue``, ``io.save_dir``.
+
+``run(device_loop=True)`` keeps the steps between two outputs on the device:
+one ``Integrator.run_until`` call -- a CUDA graph whose WHILE node runs
+steps until the device-held time reaches the next output time or
+``time.tend`` -- per output interval.  The steps are the same; dt stays on
+the device (the GLM damping factor from the device exp, as
+``Integrator.run``), so the FP64 form then agrees with the host loop to
+rounding, not bit for bit.
 """
 from __future__ import annotations
 
@@ -77,7 +85,7 @@ class Model:
             self.save_state()
             self.n_output += 1
 
-    def run(self):
+    def run(self, device_loop: bool = False):
         """ModelBase::run (mhd_model_base.hpp:88-116)."""
         self.mhd.apply_initial_condition(self.q0)
         if (self.resume and self.output is not None and
@@ -87,7 +95,14 @@ class Model:
             self.output.write_setup()
         self.save_if_needed()
         while self.time < self.tend:
-            self.update()
+            if device_loop:
+                # the steps up to the next output (or the end) in one launch;
+                # the loop stops after the step that reaches it, as here
+                t_next = min(self.tend, self.dt_output * self.n_output)
+                self.time, n = self.mhd.integrator.run_until(self.time, t_next)
+                self.n_step += n
+            else:
+                self.update()
             self.save_if_needed()
         if self.output is not None:
             self.output.wait()

@@ -58,6 +58,7 @@ struct miso_b200_batch {
   int nscells = 0;
   StepScalars *d_sc = nullptr;
   unsigned int *d_dtmin = nullptr;
+  unsigned int *d_dtinit = nullptr;  // 1e10 per instance: the running minima's start
   unsigned int *d_err = nullptr;
   // FP64
   double *q64[3][NF] = {};
@@ -184,6 +185,11 @@ struct miso_b200_batch {
       launches += 2 + 4 + 1 + 3;
     } else {
       if (!cfl_valid) {
+        // a replaced state: the minima the last sweep folded in are stale
+        if (int rc = cuda(cudaMemcpyAsync(d_dtmin, d_dtinit, sizeof(unsigned int) * count,
+                                          cudaMemcpyDeviceToDevice, stream),
+                          "reset the CFL minima"))
+          return rc;
         b32_cfl(a, cst(hi[cur]), grid, stream);
         ++launches;
       }
@@ -471,6 +477,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   add((void **)&b->d_scells, sizeof(int4) * (scells.empty() ? 1 : scells.size()));
   add((void **)&b->d_sc, sizeof(StepScalars) * count);
   add((void **)&b->d_dtmin, sizeof(unsigned int) * count);
+  add((void **)&b->d_dtinit, sizeof(unsigned int) * count);
   add((void **)&b->d_err, sizeof(unsigned int));
   if (!b->split) {
     for (int s = 0; s < 3; ++s)
@@ -526,6 +533,9 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   for (auto &v : init) v = bits;
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->d_dtmin, init.data(), sizeof(unsigned int) * count,
+                        cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_dtinit, init.data(), sizeof(unsigned int) * count,
                         cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) {

@@ -451,6 +451,7 @@ struct miso_b200_handle {
   }
   int cuda(cudaError_t e, const char *what) {
     if (e == cudaSuccess) return MISO_B200_OK;
+    cudaGetLastError();  // a non-sticky error must not surface at a later launch check
     return fail(MISO_B200_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   }
   int check_launch(const char *what) { return cuda(cudaGetLastError(), what); }
@@ -760,7 +761,8 @@ struct miso_b200_handle {
       return check_launch("cfl");
     }
     if (split()) {
-      launch_s32_cfl_partial(g, cst(H(cur)), partial, nparts, sc, p.gm, cfl_dx, stream, mag);
+      launch_s32_cfl_partial(g, cst(H(cur)), partial, nparts, sc, p.gm, cfl_dx, stream, mag,
+                             cst(L(cur)));
       launch_cfl_finalize(partial, nparts, sc, p.cfl_number, min_dxyz, stream);
       te(t, "cfl", interior() * 32.0);
     } else {
@@ -1819,14 +1821,19 @@ static int build_loop_graph(miso_b200_handle *h) {
   const bool valid_before = h->partials_valid;
   const long long l0 = h->launches;
   cudaGraph_t tmp = nullptr;
-  // the IF node's handle (used where a step swaps the hi / lo sets)
+  // where a step swaps the hi / lo sets (the split form's odd number of
+  // viscosity sweeps) the body holds two steps, the second under an IF node
+  const int sweeps = h->tiled ? 3 : h->g.s[0] + h->g.s[1] + h->g.s[2];
+  const bool two = h->split() && (sweeps & 1);
   cudaGraphConditionalHandle h_if = 0;
-  rc = h->cuda(cudaGraphConditionalHandleCreate(&h_if, wp.conditional.phGraph_out[0], 0,
-                                                cudaGraphCondAssignDefault),
-               "conditional handle");
-  if (rc) {
-    cudaGraphDestroy(g);
-    return rc;
+  if (two) {
+    rc = h->cuda(cudaGraphConditionalHandleCreate(&h_if, wp.conditional.phGraph_out[0], 0,
+                                                  cudaGraphCondAssignDefault),
+                 "conditional handle");
+    if (rc) {
+      cudaGraphDestroy(g);
+      return rc;
+    }
   }
   h->capturing = true;
   rc = h->cuda(cudaStreamBeginCaptureToGraph(h->stream, wp.conditional.phGraph_out[0], nullptr,
@@ -1835,7 +1842,8 @@ static int build_loop_graph(miso_b200_handle *h) {
   if (!rc) rc = h->enqueue_cfl();
   if (!rc) rc = h->enqueue_update();
   const long long per_step = h->launches - l0 + 1;
-  const bool two = !rc && h->cur != before;
+  if (!rc && (h->cur != before) != two)
+    rc = h->fail(MISO_B200_ERR_STATE, "a step swapped the state sets unexpectedly");
   if (!rc) {
     advance_cond_kernel<<<1, 1, 0, h->stream>>>(h->rs, h->sc, h_while, h_if, two ? 1 : 0);
     rc = h->check_launch("advance");

@@ -252,9 +252,29 @@ av_sweep_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
   }
 }
 
+// With the magnetosphere boundary the state is read in FP64 from hi + lo:
+// its strong dipole field makes the magnetic energy dwarf the thermal one
+// near the body, and the internal energy formed from the FP32 hi words
+// alone can cancel below zero where hi + lo holds a positive one.
+__device__ __forceinline__ float cfl_cell64(const FieldPtrs<const float> &u,
+                                            const FieldPtrs<const float> &lo, long long c,
+                                            double gm, bool &bad) {
+  double q[NF];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) q[f] = (double)__ldg(u.f[f] + c) + (double)__ldg(lo.f[f] + c);
+  const double inv = 1.0 / q[RO];
+  const double mm = q[MX] * q[MX] + q[MY] * q[MY] + q[MZ] * q[MZ];
+  const double bb = q[BX] * q[BX] + q[BY] * q[BY] + q[BZ] * q[BZ];
+  const double e = (q[ET] - 0.5 * mm * inv - bb * PII8) * inv;
+  const double tv = sqrt(gm * (gm - 1.0) * e) + sqrt(mm) * inv + sqrt(bb * inv * PII4);
+  bad |= !(q[RO] > 0.0) || !(e >= 0.0) || !isfinite(tv);
+  return (float)tv;
+}
+
 __global__ void __launch_bounds__(256)
 cfl_partial_kernel(Geom g, FieldPtrs<const float> u, float *__restrict__ partial,
-                   unsigned int *__restrict__ err, float gm, float cfl_dx, Magneto mg) {
+                   unsigned int *__restrict__ err, float gm, float cfl_dx, Magneto mg,
+                   FieldPtrs<const float> lo) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
   float best = 1.e10f;
   bool bad = false;
@@ -263,16 +283,21 @@ cfl_partial_kernel(Geom g, FieldPtrs<const float> u, float *__restrict__ partial
     int i, j, k;
     decode_index(g, lin, i, j, k);
     const long long c = i * g.st[0] + j * g.st[1] + k;
-    const Cons q = load_cons(u, c);
-    const float inv = 1.0f / q.ro;
-    const float mm = q.m[0] * q.m[0] + q.m[1] * q.m[1] + q.m[2] * q.m[2];
-    const float bb = q.b[0] * q.b[0] + q.b[1] * q.b[1] + q.b[2] * q.b[2];
-    const float e = (q.et - 0.5f * mm * inv - bb * FPII8) * inv;
-    const float cs = sqrtf(gm * (gm - 1.0f) * e);
-    const float vv = sqrtf(mm) * inv;
-    const float ca = sqrtf(bb * inv * FPII4);
-    float tv = cs + vv + ca;
-    bad |= !(q.ro > 0.0f) || !(e >= 0.0f) || !isfinite(tv);
+    float tv;
+    if (mg.on) {
+      tv = cfl_cell64(u, lo, c, (double)gm, bad);
+    } else {
+      const Cons q = load_cons(u, c);
+      const float inv = 1.0f / q.ro;
+      const float mm = q.m[0] * q.m[0] + q.m[1] * q.m[1] + q.m[2] * q.m[2];
+      const float bb = q.b[0] * q.b[0] + q.b[1] * q.b[1] + q.b[2] * q.b[2];
+      const float e = (q.et - 0.5f * mm * inv - bb * FPII8) * inv;
+      const float cs = sqrtf(gm * (gm - 1.0f) * e);
+      const float vv = sqrtf(mm) * inv;
+      const float ca = sqrtf(bb * inv * FPII4);
+      tv = cs + vv + ca;
+      bad |= !(q.ro > 0.0f) || !(e >= 0.0f) || !isfinite(tv);
+    }
     if (mg.mask_cfl) {
       // the magnetosphere demo's CFL (timestep.hpp:15-49): the sphere
       // r <= r_inner moves at 1e-10
@@ -455,9 +480,10 @@ void launch_s32_av_sweep(const Geom &g, const FieldPtrs<const float> &hi,
 
 void launch_s32_cfl_partial(const Geom &g, const FieldPtrs<const float> &u, float *partial,
                             int nparts, StepScalars *sc, double gm, double cfl_dx,
-                            cudaStream_t st, const Magneto &mg) {
+                            cudaStream_t st, const Magneto &mg,
+                            const FieldPtrs<const float> &lo) {
   s32::cfl_partial_kernel<<<nparts, 256, 0, st>>>(g, u, partial, &sc->err, (float)gm,
-                                                  (float)cfl_dx, mg);
+                                                  (float)cfl_dx, mg, lo);
 }
 
 void launch_s32_magneto(const Geom &g, const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,

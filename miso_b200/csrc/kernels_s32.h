@@ -23,7 +23,8 @@ void launch_s32_magneto(const Geom &g, const FieldPtrs<float> &hi, const FieldPt
                         bool pair, const Magneto &mg, double gm, int sms, cudaStream_t st);
 void launch_s32_cfl_partial(const Geom &g, const FieldPtrs<const float> &u, float *partial,
                             int nparts, StepScalars *sc, double gm, double cfl_dx,
-                            cudaStream_t st, const Magneto &mg = Magneto{});
+                            cudaStream_t st, const Magneto &mg = Magneto{},
+                            const FieldPtrs<const float> &lo = FieldPtrs<const float>{});
 void launch_s32_to_split(long long cells, const FieldPtrs<const double> &q,
                          const FieldPtrs<float> &hi, const FieldPtrs<float> &lo, int sms,
                          cudaStream_t st);

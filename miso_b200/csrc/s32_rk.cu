@@ -81,34 +81,6 @@ __device__ __forceinline__ float d4(float A, float B, float D, float E) {
   return fmaf(8.f, D - B, A - E);
 }
 
-// Flux vector of direction D (flux_dir's values) formed as the packed pairs
-// the stage exchanges and differences: (ro, mx) (my, mz) (bx, by) (bz, et)
-// and ph alone.  Each pair of like terms is one FP32x2 multiply and one
-// FP32x2 fused multiply-add.
-template <int D>
-__device__ __forceinline__ void flux_pk(const float u[NF], const PrimF &p, float ch2, V9 &F) {
-  const float vd = p.v[D], bd = u[BX + D];
-  const float bd4 = bd * FPII4;
-  const float2 vd2 = f2(vd, vd);
-  // momentum m_e vd - b_e bd4, plus the total pressure on e == D
-  const float fmx = fmaf(u[MX], vd, -(u[BX] * bd4));
-  F.p[0] = f2(u[MX + D], D == 0 ? fmx + p.ptot : fmx);
-  float2 myz = fma2(f2(u[MY], u[MZ]), vd2, mul2(f2(u[BY], u[BZ]), f2(-bd4, -bd4)));
-  if (D == 1) myz.x += p.ptot;
-  if (D == 2) myz.y += p.ptot;
-  F.p[1] = myz;
-  // induction vd b_e - v_e bd (ph on e == D)
-  float2 bxy = fma2(vd2, f2(u[BX], u[BY]), mul2(f2(p.v[0], p.v[1]), f2(-bd, -bd)));
-  if (D == 0) bxy.x = u[PH];
-  if (D == 1) bxy.y = u[PH];
-  F.p[2] = bxy;
-  // (bz, et): vd bz - v_z bd, e_tot vd - vb bd4
-  float2 bze = fma2(f2(u[BZ], p.e_tot), vd2, mul2(f2(p.v[2], p.vb), f2(-bd, -bd4)));
-  if (D == 2) bze.x = u[PH];
-  F.p[3] = bze;
-  F.s = ch2 * bd;
-}
-
 struct Consts {
   float2 wx2, wy2, wz2, mdt2;
   float wx, wy, wz, dt, decay, ch2;
@@ -220,28 +192,29 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
   const float *pl = reinterpret_cast<const float *>(sm.plane[pp.b]);
   const int fb = pp.seq & 1;
   {
-    float u[NF];
+    float u[NF], F[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) u[f] = pl[(f * HJ + ty + 2) * HK + tx + 2];
     PrimF p;
     prim(u, a.gm1, p);
-    flux_pk<0>(u, p, k.ch2, Fn);
+    flux_dir<0>(u, p, k.ch2, F);
+#pragma unroll
+    for (int i = 0; i < NPAIR; ++i) Fn.p[i] = f2(F[2 * i], F[2 * i + 1]);
+    Fn.s = F[8];
     if (need_yz) {
-      V9 F;
-      flux_pk<1>(u, p, k.ch2, F);
+      flux_dir<1>(u, p, k.ch2, F);
 #pragma unroll
-      for (int i = 0; i < NPAIR; ++i) sm.fy2[fb][i][ty + 2][tx] = F.p[i];
-      sm.fy1[fb][ty + 2][tx] = F.s;
-      flux_pk<2>(u, p, k.ch2, F);
+      for (int i = 0; i < NPAIR; ++i) sm.fy2[fb][i][ty + 2][tx] = f2(F[2 * i], F[2 * i + 1]);
+      sm.fy1[fb][ty + 2][tx] = F[8];
+      flux_dir<2>(u, p, k.ch2, F);
 #pragma unroll
-      for (int i = 0; i < NPAIR; ++i) sm.fz2[fb][i][ty][tx + 2] = F.p[i];
-      sm.fz1[fb][ty][tx + 2] = F.s;
+      for (int i = 0; i < NPAIR; ++i) sm.fz2[fb][i][ty][tx + 2] = f2(F[2 * i], F[2 * i + 1]);
+      sm.fz1[fb][ty][tx + 2] = F[8];
     }
   }
   // halo fluxes: warps 0-3 the y rows above / below, warp 4 the z columns
   if (need_yz && tid < 4 * TK + 4 * TJ) {
-    float uh[NF];
-    V9 Fh;
+    float uh[NF], Fh[NF];
     PrimF ph;
     if (tid < 4 * TK) {
       const int r = tid >> 5, col = tid & 31;
@@ -249,10 +222,10 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
 #pragma unroll
       for (int f = 0; f < NF; ++f) uh[f] = pl[(f * HJ + row) * HK + col + 2];
       prim(uh, a.gm1, ph);
-      flux_pk<1>(uh, ph, k.ch2, Fh);
+      flux_dir<1>(uh, ph, k.ch2, Fh);
 #pragma unroll
-      for (int i = 0; i < NPAIR; ++i) sm.fy2[fb][i][row][col] = Fh.p[i];
-      sm.fy1[fb][row][col] = Fh.s;
+      for (int i = 0; i < NPAIR; ++i) sm.fy2[fb][i][row][col] = f2(Fh[2 * i], Fh[2 * i + 1]);
+      sm.fy1[fb][row][col] = Fh[8];
     } else {
       const int e = tid - 4 * TK;
       const int row = e >> 2, cz = e & 3;
@@ -260,10 +233,10 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
 #pragma unroll
       for (int f = 0; f < NF; ++f) uh[f] = pl[(f * HJ + row + 2) * HK + col];
       prim(uh, a.gm1, ph);
-      flux_pk<2>(uh, ph, k.ch2, Fh);
+      flux_dir<2>(uh, ph, k.ch2, Fh);
 #pragma unroll
-      for (int i = 0; i < NPAIR; ++i) sm.fz2[fb][i][row][col] = Fh.p[i];
-      sm.fz1[fb][row][col] = Fh.s;
+      for (int i = 0; i < NPAIR; ++i) sm.fz2[fb][i][row][col] = f2(Fh[2 * i], Fh[2 * i + 1]);
+      sm.fz1[fb][row][col] = Fh[8];
     }
   }
 

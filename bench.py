@@ -562,8 +562,12 @@ def time_batch(probs, precision, stream, K, W, local, world):
         b.run(W, graph=True)
         b.sync()
         tuning = autotune_batch(b) if b.views() else {}
-        b.run(1, graph=True)
+        # a captured step graph holds two steps where a step swaps the hi / lo
+        # sets: two graph steps here leave the graph matching the state, so
+        # nothing is captured inside the timed region
+        b.run(2, graph=True)
         b.sync()
+        K = K + (K & 1)
         info = b.info()
         cells, l0 = info["interior_cells"], info["launches"]
         sampler = ClockSampler(local)
@@ -650,8 +654,9 @@ def run_batch(args):
         b.sync()
         from miso_b200.autotune import autotune_batch
         tuning = autotune_batch(b) if b.views() else {}
-        b.run(1, graph=True)
+        b.run(2, graph=True)  # the captured graph matches the state's hi / lo set
         b.sync()
+        K = K + (K & 1)
         cells = b.info()["interior_cells"]
         l0 = b.info()["launches"]
         sampler = ClockSampler(local)

@@ -166,7 +166,7 @@ def _batch_key(batch) -> str:
     return f"batch:{batch.precision}:{comp}:sm{sms}"
 
 
-def autotune_batch(batch, steps: int = 3, use_cache: bool = True) -> dict:
+def autotune_batch(batch, steps: int = 4, use_cache: bool = True) -> dict:
     """Pick and apply the work-item lengths (Runge-Kutta, x / y sweep
     chunks) of a batch's 3-D instances by timing whole graph-replayed steps
     of the batch itself (CUDA events); cached per batch composition (the
@@ -176,6 +176,7 @@ def autotune_batch(batch, steps: int = 3, use_cache: bool = True) -> dict:
     import torch
     if batch.views() == 0:
         return {}
+    steps += steps & 1  # whole replays of a two-step graph: no eager step timed
     key = _batch_key(batch)
     cache = _load() if use_cache else {}
     if key in cache:

@@ -385,6 +385,10 @@ int miso_b200_batch_info(miso_b200_batch *b, long long *interior_cells, int *til
  * autotuner (miso_b200/autotune.py, autotune_batch) picks these per batch
  * composition. */
 int miso_b200_batch_set_chunks(miso_b200_batch *b, int rk_chunk, int av_chunk);
+/* Kernel variant (as miso_b200_set_variant) of the 3-D instances that run
+ * the pipelined kernels; the autotuner tries the warp-march x / y sweeps,
+ * which suit grids narrower than the line sweeps' 128-cell k blocks. */
+int miso_b200_batch_set_variant(miso_b200_batch *b, int kernel_class, int variant);
 /* Number of instances the batch runs through the pipelined kernels. */
 int miso_b200_batch_views(miso_b200_batch *b, int *views);
 const char *miso_b200_batch_last_error(miso_b200_batch *b);

@@ -96,6 +96,7 @@ SIGNATURES = {
     "miso_b200_arm_timeout_test": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "miso_b200_pointer_kind": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_batch_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "miso_b200_batch_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_batch_views": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_run_until": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                            ctypes.c_double, ctypes.c_int, ctypes.c_int,

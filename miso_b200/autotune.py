@@ -152,6 +152,10 @@ def autotune(integ, steps: int = 2, use_cache: bool = True) -> dict:
 # Batched solver: work-item lengths of the 3-D instances' pipelined kernels
 # ---------------------------------------------------------------------------
 BATCH_CHUNKS = ((64, 128), (32, 64), (16, 32), (16, 16), (8, 16))
+# (RK stage, x sweep, y sweep) variants tried with each chunk pair: the
+# default (deferred last stage, line sweeps); the warp-march x / y sweeps,
+# whose 32-cell segments fit grids narrower than a line's 128-cell k block
+BATCH_VARIANTS = ((3, 0, 0), (2, 2, 2), (3, 0, 2))
 
 
 def _batch_key(batch) -> str:
@@ -164,6 +168,14 @@ def _batch_key(batch) -> str:
         shapes[k] = shapes.get(k, 0) + 1
     comp = ",".join(f"{n}*{k}" for k, n in sorted(shapes.items()))
     return f"batch:{batch.precision}:{comp}:sm{sms}"
+
+
+def _apply_batch(batch, c: dict):
+    vr, vx, vy = c.get("variants", (3, 0, 0))
+    batch.set_variant(1, vx)
+    batch.set_variant(2, vy)
+    batch.set_variant(0, vr)
+    batch.set_chunks(c["rk_chunk"], c["av_chunk"])
 
 
 def autotune_batch(batch, steps: int = 4, use_cache: bool = True) -> dict:
@@ -181,7 +193,7 @@ def autotune_batch(batch, steps: int = 4, use_cache: bool = True) -> dict:
     cache = _load() if use_cache else {}
     if key in cache:
         c = cache[key]
-        batch.set_chunks(c["rk_chunk"], c["av_chunk"])
+        _apply_batch(batch, c)
         return c
     import time
     # events on the batch's own stream when the caller gave it one, else the
@@ -189,7 +201,11 @@ def autotune_batch(batch, steps: int = 4, use_cache: bool = True) -> dict:
     stream = torch.cuda.ExternalStream(batch.stream) if batch.stream else None
     best = None
     times = {}
-    for rk_chunk, av_chunk in BATCH_CHUNKS:
+    for (vr, vx, vy), (rk_chunk, av_chunk) in [(v, c) for v in BATCH_VARIANTS
+                                               for c in BATCH_CHUNKS]:
+        batch.set_variant(1, vx)
+        batch.set_variant(2, vy)
+        batch.set_variant(0, vr)
         batch.set_chunks(rk_chunk, av_chunk)
         batch.run(2, graph=True)  # capture (and warm) outside the timing
         batch.sync()
@@ -208,11 +224,12 @@ def autotune_batch(batch, steps: int = 4, use_cache: bool = True) -> dict:
             batch.run(steps, graph=True)
             batch.sync()
             ms = (time.perf_counter() - t0) * 1e3 / steps
-        times[f"{rk_chunk}/{av_chunk}"] = ms
+        times[f"{vr}{vx}{vy}:{rk_chunk}/{av_chunk}"] = ms
         if best is None or ms < best[0]:
-            best = (ms, rk_chunk, av_chunk)
-    choice = {"rk_chunk": best[1], "av_chunk": best[2], "ms_per_step": times}
-    batch.set_chunks(choice["rk_chunk"], choice["av_chunk"])
+            best = (ms, rk_chunk, av_chunk, (vr, vx, vy))
+    choice = {"rk_chunk": best[1], "av_chunk": best[2], "variants": list(best[3]),
+              "ms_per_step": times}
+    _apply_batch(batch, choice)
     cache[key] = choice
     if use_cache:
         _save(cache)

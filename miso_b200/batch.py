@@ -86,6 +86,11 @@ class Batch:
         """Planes per work item of the 3-D instances' pipelined kernels."""
         self._check(self._lib.miso_b200_batch_set_chunks(self._h, int(rk_chunk), int(av_chunk)))
 
+    def set_variant(self, kernel_class: int, variant: int):
+        """Kernel variant of the 3-D instances' pipelined path."""
+        self._check(self._lib.miso_b200_batch_set_variant(self._h, int(kernel_class),
+                                                          int(variant)))
+
     def views(self) -> int:
         """Instances that run the single grid's pipelined kernels."""
         n = ctypes.c_int()

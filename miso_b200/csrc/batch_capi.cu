@@ -762,6 +762,21 @@ int miso_b200_batch_set_chunks(miso_b200_batch *b, int rk_chunk, int av_chunk) {
   return MISO_B200_OK;
 }
 
+int miso_b200_batch_set_variant(miso_b200_batch *b, int kernel_class, int variant) {
+  if (!b) return MISO_B200_ERR_ARG;
+  for (auto &v : b->views) {
+    const int rc = miso_b200_set_variant(v.h, kernel_class, variant);
+    if (rc) return b->fail(rc, miso_b200_last_error(v.h));
+  }
+  if (b->graph_exec) {
+    cudaGraphExecDestroy(b->graph_exec);
+    cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+  }
+  return MISO_B200_OK;
+}
+
 int miso_b200_batch_views(miso_b200_batch *b, int *views) {
   if (!b || !views) return MISO_B200_ERR_ARG;
   *views = (int)b->views.size();

@@ -141,9 +141,10 @@ def test_batch_autotune_picks_and_caches(tmp_path, monkeypatch):
     """The batch tuner times the work-item lengths of the 3-D instances on
     whole graph-replayed steps, applies the fastest and caches it per batch
     composition; the chunk lengths leave every instance's result unchanged
-    (each item is computed the same wherever it is cut)."""
+    (each item is computed the same wherever it is cut); the variants agree
+    to FP32 rounding."""
     import torch
-    from miso_b200.autotune import BATCH_CHUNKS, autotune_batch
+    from miso_b200.autotune import BATCH_CHUNKS, BATCH_VARIANTS, autotune_batch
     monkeypatch.setenv("MISO_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     probs = [P.turbulence(32, seed=1), P.blast(24, seed=2), P.orszag_tang(40)]
     stream = torch.cuda.Stream()
@@ -155,12 +156,12 @@ def test_batch_autotune_picks_and_caches(tmp_path, monkeypatch):
             if tune:
                 c = autotune_batch(b, steps=1)
                 assert (c["rk_chunk"], c["av_chunk"]) in BATCH_CHUNKS
-                assert len(c["ms_per_step"]) == len(BATCH_CHUNKS)
+                assert len(c["ms_per_step"]) == len(BATCH_CHUNKS) * len(BATCH_VARIANTS)
                 # cached: the second call returns the same choice at once
                 assert autotune_batch(b) == c
                 b.upload_all()
             b.run(4, graph=True)
             b.sync()
             outs.append([b.download(i) for i in range(len(probs))])
-    for a, c in zip(*outs):
-        assert np.array_equal(a, c)
+    for p, a, c in zip(probs, *outs):
+        assert rel_l1(interior(p, a)[P.RO], interior(p, c)[P.RO]) <= 1e-5

@@ -58,14 +58,22 @@ def test_masked_cfl_and_boundary_act(oracle):
     assert dt_plain == oracle.cfl(plain, q) and dt_plain != oracle.cfl(prob, q)
 
 
-@pytest.mark.parametrize("n,steps", [(16, 6), (24, 4)], ids=["n16", "n24"])
+@pytest.mark.parametrize("n,steps", [(24, 6), (32, 4)], ids=["n24", "n32"])
 def test_split_form_follows_fp64(n, steps):
     """The FP32 split form with the magnetosphere boundary (its per-cell
     kernels, the boundary on the split state after every pass, the masked
     CFL) stepped with the FP64 form's dt sequence: relative L1 of rho
-    <= 1e-6, of p and B <= 1e-5; its own CFL within 1e-4 of FP64's (the
-    time step is the minimum over cells, so it follows the few cells that
-    set it, not the L1 average)."""
+    <= 1e-7, of p <= 1e-5 and of B <= 1e-6; its own CFL within 1e-4 of
+    FP64's (the time step is the minimum over cells, so it follows the few
+    cells that set it, not the L1 average).
+
+    The grids keep the FP64 solution off the floors.  On a coarser one
+    (16 cells over [-12, 12]) a single step drives the cells just outside
+    the inner sphere to the pressure floor (1e-10, beta near 1e-14), where
+    the thermal energy is 1e-7 of the total: below what an FP32 word of the
+    total energy resolves, so the split form's pressure there is rounding
+    (relative L1 of p 3.6e-5 after one step, of rho 3.6e-6), while the same
+    grid with a zero blend state stays at 5e-8 in rho."""
     prob = P.magnetosphere(n, extent=12.0)
     ref = Integrator(prob.config, prob.grid, sign=prob.sign, precision="fp64", blend=prob.blend)
     ref.upload(prob.q)
@@ -86,9 +94,9 @@ def test_split_form_follows_fp64(n, steps):
 
     def rl1(x, y):
         return float(np.sum(np.abs(x - y)) / np.sum(np.abs(y)))
-    assert rl1(a[P.RO], b[P.RO]) <= 1e-6
+    assert rl1(a[P.RO], b[P.RO]) <= 1e-7
     assert rl1(a[P.RO] * a[P.EI] * (gm - 1), b[P.RO] * b[P.EI] * (gm - 1)) <= 1e-5
-    assert rl1(a[P.BX:P.BZ + 1], b[P.BX:P.BZ + 1]) <= 1e-5
+    assert rl1(a[P.BX:P.BZ + 1], b[P.BX:P.BZ + 1]) <= 1e-6
 
 
 def test_refusals():

@@ -152,8 +152,9 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]);
  * leaves FP64 per-block sums of the new state's mass, momentum, energy and
  * ph^2, and miso_b200_monitors() then reduces only |div B| (a kernel that
  * reads bx, by, bz) instead of the whole state.  For loops that read the
- * monitors after every step.  Applies with the default z sweep (variant 0);
- * the results equal the unfused monitors up to FP64 summation order. */
+ * monitors after every step.  Applies with the default z sweep (variant 0)
+ * and with the fused y and z sweeps (y variant 3); the results equal the
+ * unfused monitors up to FP64 summation order. */
 int miso_b200_set_monitor_fusion(miso_b200_handle *h, int on);
 
 /* Device pointers of the FP64 primitive state arrays (FP64 form only), valid
@@ -299,9 +300,14 @@ int miso_b200_set_halo_overlap(miso_b200_handle *h, void *comm_stream);
  * stage's update deferred into the x sweep: that stage writes its
  * right-hand side and the x sweep forms the new state from it as it streams
  * the state in (this needs x sweep variant 0 and no flat sweep; otherwise
- * it runs as variant 2).  All compute the same step up to FP32 rounding
- * order; the autotuner (miso_b200/autotune.py) times them and keeps the
- * fastest.
+ * it runs as variant 2), and 3 (y sweep only) = the y and z sweeps fused
+ * into one pass: each k column of a plane is swept along j and each finished
+ * row along k, with the separate sweeps' arithmetic, so the step gives the
+ * same bits as the y line sweep followed by the z sweep without writing
+ * and re-reading the y-swept state (the z variant is then unused; refused
+ * with ERR_STATE for a batch's instances, whose steps keep one hi / lo swap
+ * per sweep).  All compute the same step up to FP32 rounding order; the
+ * autotuner (miso_b200/autotune.py) times them and keeps the fastest.
  * ERR_STATE on grids that use the simple per-cell kernels only. */
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant);
 int miso_b200_get_variant(miso_b200_handle *h, int kernel_class, int *variant);

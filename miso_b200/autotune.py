@@ -8,7 +8,9 @@ Runge-Kutta stage also the pipelined plane kernel -- and a few
 work-item lengths along the march axis, and keeps the fastest of each.
 Where the pipelined RK stage and the line x sweep win, it also times the
 pipelined stage with its last update deferred into the x sweep (RK variant
-3), which moves work from one class to the other, on the whole step.
+3), which moves work from one class to the other, on the whole step, and
+then the y and z sweeps fused into one pass (y variant 3), also on the whole
+step.
 Results are cached in a JSON file keyed by precision, grid shape and SM
 count ($MISO_B200_TUNE_CACHE, default ~/.cache/miso_b200/tune.json), so a
 later run of the same shape skips the search.
@@ -25,8 +27,9 @@ CLASSES = {"rk_stage": 0, "av_x": 1, "av_y": 2, "av_z": 3}
 # variants per class: 0 tiled, 1 flat, 2 pipelined (RK: planes with packed
 # differences; x / y sweeps: one warp per line segment marching along the
 # axis; z sweep: rows streamed by TMA); RK 3: variant 2 with the last stage's update deferred into the x
-# sweep (compared on the whole step, not per class)
-VARIANTS = {"rk_stage": (0, 1, 2, 3), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1, 2)}
+# sweep (compared on the whole step, not per class); y 3: the y and z sweeps
+# fused into one pass (the z variant then unused; also on the whole step)
+VARIANTS = {"rk_stage": (0, 1, 2, 3), "av_x": (0, 1, 2), "av_y": (0, 1, 2, 3), "av_z": (0, 1, 2)}
 PER_CLASS = {"rk_stage": (0, 1, 2), "av_x": (0, 1, 2), "av_y": (0, 1, 2), "av_z": (0, 1, 2)}
 CHUNKS = (32, 64, 128)
 
@@ -76,7 +79,7 @@ def _times(integ, steps):
 
 def _step_ms(t: dict) -> float:
     return (t.get("rk_stage", 0) * 4 + t.get("av_x", 0) + t.get("av_y", 0) +
-            t.get("av_z", 0))
+            t.get("av_z", 0) + t.get("av_yz", 0))
 
 
 def _try_variant(integ, kc: int, var: int) -> bool:
@@ -130,6 +133,18 @@ def autotune(integ, steps: int = 2, use_cache: bool = True) -> dict:
             best["av_x"] = (0, t3["av_x"])
         else:
             integ.set_variant(0, 2)
+    if choice["av_y"] != 1 and choice["av_z"] != 1:
+        # the y and z sweeps in one pass: one write and one read of the state
+        # fewer, both sweeps' arithmetic in one kernel
+        t_sep = _times(integ, steps)
+        integ.set_variant(2, 3)
+        t_fused = _times(integ, steps)
+        if _step_ms(t_fused) < _step_ms(t_sep):
+            choice["av_y"] = 3
+            best["av_y"] = (3, t_fused["av_yz"])
+            best.pop("av_z", None)
+        else:
+            integ.set_variant(2, choice["av_y"])
     # work-item lengths for the winning variants
     chunk_best = None
     for rk_chunk in CHUNKS:

@@ -266,6 +266,7 @@ struct miso_b200_handle {
   int sms = 148;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  bool is_view = false;  // a batch instance's view: its step keeps the batch's set parity
   std::string err;
 
   void *block = nullptr;  // one allocation holds every device buffer
@@ -322,11 +323,13 @@ struct miso_b200_handle {
   alignas(64) unsigned char tm_avd[128];     // AV line map of stg[1] (deferred last-stage D)
   alignas(64) unsigned char tm_zwh[2][128];  // z line sweep: 8-wide wrap maps of hi[set]
   alignas(64) unsigned char tm_zwc[128];     // and of the characteristic speed
+  alignas(64) unsigned char tm_zwl[2][128];  // fused y and z sweeps: wrap maps of lo[set]
   long long pitch = 0;                       // elements between consecutive field arrays
   int rk_L = 64, rk_tiles_j = 0, rk_tiles_k = 0, rk_items = 0, rk_grid = 0;
   int av_L = 128, av_grid = 0, z_grid = 0;
   int avp_grid = 0;  // warp-march x / y sweep: 2 resident CTAs of 8 warps per SM
   int zl_grid = 0;   // z line sweep: resident CTAs per SM x SMs
+  int yz_grid = 0;   // fused y and z sweeps: resident CTAs per SM x SMs
   int shell_grid = 0;
   // The flat kernels run exactly one resident wave (grid = resident blocks)
   // and stride over tiles in order, so the CTAs in flight always cover one
@@ -338,9 +341,16 @@ struct miso_b200_handle {
   // kernel variant per class on the 3-D split path: 0 = tiled (TMA plane
   // tiles / streaming lines), 1 = flat (one thread per cell); 2: RK =
   // pipelined TMA planes with packed FP32x2 differences (default), x / y
-  // sweeps = one warp per line segment marching along the sweep axis
-  int rk_var = 3;  // pipelined stages, the last update deferred into the x sweep
+  // sweeps = one warp per line segment marching along the sweep axis; 3:
+  // RK = variant 2 with the last update deferred into the x sweep (default),
+  // y sweep = the y and z sweeps fused into one pass (the z variant unused)
+  int rk_var = 3;
   int av_var[3] = {0, 0, 0};
+  bool fused_yz() const { return av_var[1] == 3; }
+  // hi / lo set swaps of one step: one per viscosity pass
+  int sweep_passes() const {
+    return tiled ? (fused_yz() ? 2 : 3) : g.s[0] + g.s[1] + g.s[2];
+  }
   double *mon_partial = nullptr;
   int mon_blocks = 0;
   // monitors folded into the step (miso_b200_set_monitor_fusion, 3-D split
@@ -528,7 +538,9 @@ struct miso_b200_handle {
     }
     if (ok) ok = s32_make_tmap_cc(g_, cc32, tm_avc) == 0;
     if (ok) ok = s32_make_tmap(g_, stg[1][0], pb, 1, tm_avd) == 0;
-    for (int s = 0; s < 2 && ok; ++s) ok = s32_make_tmap(g_, hi[s][0], pb, 2, tm_zwh[s]) == 0;
+    for (int s = 0; s < 2 && ok; ++s)
+      ok = s32_make_tmap(g_, hi[s][0], pb, 2, tm_zwh[s]) == 0 &&
+           s32_make_tmap(g_, lo[s][0], pb, 2, tm_zwl[s]) == 0;
     if (ok) ok = s32_make_tmap_cc(g_, cc32, tm_zwc, 8) == 0;
     if (ok) {
       tiled = tiled_ok = true;
@@ -538,6 +550,7 @@ struct miso_b200_handle {
       av_grid = 2 * sms;  // line sweeps: two CTAs per SM
       avp_grid = 2 * sms;
       zl_grid = s32_zline_per_sm() * sms;
+      yz_grid = s32_yz_per_sm() * sms;
       {
         const long long want = (s32_shell_cells(g_) + 255) / 256;
         shell_grid = (int)(want < 8LL * sms ? want : 8LL * sms);
@@ -967,6 +980,22 @@ struct miso_b200_handle {
       a.mon = d == 2 && mon_fuse && av_var[2] == 0 ? mon_z : nullptr;
       a.r0 = 0;
       a.r1 = d < 2 ? g.n[d] : 0;
+      if (d == 1 && fused_yz()) {
+        // the y and z sweeps in one pass: CFL minima and monitor sums as
+        // the z sweep leaves them
+        if ((rc = join_xchg())) return rc;
+        a.partial = partial;
+        a.mon = mon_fuse ? mon_z : nullptr;
+        const int t = tb();
+        launch_s32_av_yz(tm_avh[cur], tm_avl[cur], tm_avc, tm_zwh[cur], tm_zwl[cur], tm_zwc, a,
+                         yz_grid, stream);
+        te(t, "av_yz", interior() * 148.0);
+        if ((rc = check_launch("av_yz"))) return rc;
+        if ((rc = shell(hi[cur ^ 1], SHELL_ALL))) return rc;
+        lo_shell_stale = true;
+        cur ^= 1;
+        break;
+      }
       const int t = tb();
       if (d == 0 && av_var[0] == 0 && split_pass()) {
         // a shard with the exchange in flight: the x sweep finishes the
@@ -1019,9 +1048,12 @@ struct miso_b200_handle {
       if ((rc = fresh_lo_shell())) return rc;
       if ((rc = halo_f(hi[cur], lo[cur]))) return rc;
     }
-    z_parts = av_var[2] == 1 ? flat_grid : av_var[2] == 2 ? zl_grid : z_grid;
+    z_parts = fused_yz()        ? yz_grid
+              : av_var[2] == 1 ? flat_grid
+              : av_var[2] == 2 ? zl_grid
+                               : z_grid;
     partials_valid = true;
-    mon_valid = mon_fuse && av_var[2] == 0;
+    mon_valid = mon_fuse && (av_var[2] == 0 || fused_yz());
     return MISO_B200_OK;
   }
 
@@ -1282,6 +1314,7 @@ int miso_b200::b200_view_create(const miso_b200_grid_desc &gd, const miso_b200_p
   }
   h->stream = stream;
   h->own_stream = false;
+  h->is_view = true;
   for (int s = 0; s < 2; ++s)
     for (int f = 0; f < NF; ++f) {
       h->hi[s][f] = hi[s][f];
@@ -1823,8 +1856,7 @@ static int build_loop_graph(miso_b200_handle *h) {
   cudaGraph_t tmp = nullptr;
   // where a step swaps the hi / lo sets (the split form's odd number of
   // viscosity sweeps) the body holds two steps, the second under an IF node
-  const int sweeps = h->tiled ? 3 : h->g.s[0] + h->g.s[1] + h->g.s[2];
-  const bool two = h->split() && (sweeps & 1);
+  const bool two = h->split() && (h->sweep_passes() & 1);
   cudaGraphConditionalHandle h_if = 0;
   if (two) {
     rc = h->cuda(cudaGraphConditionalHandleCreate(&h_if, wp.conditional.phGraph_out[0], 0,
@@ -1978,7 +2010,8 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
         h->g, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->mon_partial);
     h->launches++;
     if ((rc = h->check_launch("divb"))) return rc;
-    std::vector<double> zs((size_t)h->z_grid * 6), db((size_t)h->mon_blocks * 8);
+    // per-block sums of the sweep that left them (z_parts blocks)
+    std::vector<double> zs((size_t)h->z_parts * 6), db((size_t)h->mon_blocks * 8);
     if ((rc = h->cuda(cudaMemcpyAsync(zs.data(), h->mon_z, zs.size() * sizeof(double),
                                       cudaMemcpyDeviceToHost, h->stream),
                       "read monitors")) ||
@@ -1989,7 +2022,7 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
       return rc;
     for (int q8 = 0; q8 < 8; ++q8) out[q8] = 0.0;
     const int map[6] = {0, 1, 2, 3, 4, 7};  // ro, mx, my, mz, et, ph^2
-    for (int b = 0; b < h->z_grid; ++b)
+    for (int b = 0; b < h->z_parts; ++b)
       for (int q = 0; q < 6; ++q) out[map[q]] += zs[(size_t)b * 6 + q];
     for (int b = 0; b < h->mon_blocks; ++b) {
       out[5] += db[(size_t)b * 8 + 5];
@@ -2047,9 +2080,12 @@ int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
     h->comm = nullptr;  // the overlapped exchange needs the pipelined stage and the line x sweep
   }
   if (!h || kernel_class < 0 || kernel_class > 3 || variant < 0 ||
-      variant > (kernel_class == 0 ? 3 : 2))
+      variant > (kernel_class == 0 || kernel_class == 2 ? 3 : 2))
     return MISO_B200_ERR_ARG;
   if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "kernel variants apply to 3-D split grids");
+  if (kernel_class == 2 && variant == 3 && h->is_view)
+    return h->fail(MISO_B200_ERR_STATE,
+                   "a batch instance keeps one hi / lo swap per sweep: no fused y and z sweeps");
   if (kernel_class == 0 && variant < 2 && h->src.kind != 0)
     return h->fail(MISO_B200_ERR_STATE, "with a source term the RK stage runs variant 2 or 3");
   if (kernel_class == 0)

@@ -942,6 +942,319 @@ av_zline_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__
   }
 }
 
+// ---- y and z sweeps in one pass (y sweep variant 3) ----
+// The two sweeps of one i plane fused: a CTA owns ZK consecutive k cells of
+// a plane and marches along j over a chunk of rows, as the z line sweep
+// does.  Per row a producer warp copies hi, lo and the characteristic speed
+// of the x-swept state (k box of 132 from 2 cells before the block; for a
+// periodic k face also the 8-wide wrap boxes of hi, lo and the speed) into
+// a ring slot by TMA; rows across a j face come from the interior row they
+// image.  Each lane of the four consumer warps runs the y sweep down its
+// column with the line sweep's register queue, which yields the y-swept
+// state of the row two back; the warp then runs the z sweep on that row by
+// shuffles (z_flux_diff) and updates its inner 28 lanes.  A lane across a
+// k face runs the y sweep of the interior column it images and takes the
+// face's mirror signs afterwards -- the values the separate z sweep reads
+// there -- so the pass gives the bits of the y line sweep followed by the z
+// sweep, without writing the y-swept state and reading it back (144 B per
+// cell).  The CFL candidate of the new state, and with MON the monitors'
+// FP64 sums, are folded into per-CTA partials as the z sweep folds them.
+constexpr int YZ_NB = 6;                                     // ring slots
+constexpr int YZ_LO = L_LO;                                  // hi at 0, then lo
+constexpr int YZ_CC = 2 * L_LO;                              // the speed
+constexpr int YZ_WB = (NF * ZWB * 4 + 127) / 128 * 128;      // one 8-wide wrap box of 9 fields
+constexpr int YZ_WL = YZ_CC + (LBOX * 4 + 127) / 128 * 128;  // left wrap: hi, lo, speed
+constexpr int YZ_WR = YZ_WL + 2 * YZ_WB + 128;               // right wrap
+constexpr int YZ_SLOT = YZ_WR + 2 * YZ_WB + 128;
+constexpr unsigned YZ_TXW = (2 * NF + 1) * ZWB * 4;  // bytes of one side's wrap copies
+
+struct __align__(128) YzSmem {
+  unsigned char slot[YZ_NB][YZ_SLOT];
+  unsigned long long full[YZ_NB];   // the row's copies landed
+  unsigned long long empty[YZ_NB];  // the row read by every consumer warp (LCW arrivals)
+};
+
+template <bool MON>
+__global__ void __launch_bounds__(LK + 32, 2)
+av_yz_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CUtensorMap tlo,
+             const __grid_constant__ CUtensorMap tcc, const __grid_constant__ CUtensorMap twh,
+             const __grid_constant__ CUtensorMap twl, const __grid_constant__ CUtensorMap twc,
+             const AvArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  YzSmem &sm = *reinterpret_cast<YzSmem *>(smem_raw);
+  const Geom &g = a.g;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int nk = g.n[2];
+  const int kblocks = (nk + ZK - 1) / ZK;
+  const int chunks = (g.n[1] + a.L - 1) / a.L;
+  const int items = kblocks * g.n[0] * chunks;
+  const int xl = nk - nk % 4;  // first array column of the left wrap copy
+  if (tid == 0) {
+    for (int b = 0; b < YZ_NB; ++b) {
+      mbar_init(&sm.full[b], 1);
+      mbar_init(&sm.empty[b], LCW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();  // the only CTA-wide barrier
+  if (tid >= LK) {
+    // producer warp: one lane fills the slots row by row, rows t0-2 .. t1+1
+    // of each item
+    if (tid == LK) {
+      int s = 0;
+      bool stop = false;
+      for (int it = blockIdx.x; it < items && !stop; it += gridDim.x) {
+        const ZItem z = z_item(a, it, kblocks);
+        // wrap copies for the blocks with lanes across a periodic k face
+        // (the last lane of block kb sits at k = kb * ZK + 113)
+        const bool wl = g.periodic[2] && z.kb == 0;
+        const bool wr = g.periodic[2] && z.kb * ZK + 4 * 28 + 1 >= nk;
+        const unsigned tx = ZL_TX + (wl ? YZ_TXW : 0u) + (wr ? YZ_TXW : 0u);
+        for (int p = z.t0 - 2; p <= z.t1 + 1; ++p, ++s) {
+          const int b = s % YZ_NB;
+          if (s >= YZ_NB && !mbar_wait(&sm.empty[b], (unsigned)(((s / YZ_NB) - 1) & 1))) {
+            atomicOr(a.err, ERRBIT_TIMEOUT);
+            stop = true;
+            break;
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          unsigned char *sl = sm.slot[b];
+          int side;
+          const int ps = ghost_src(g, 1, p, side);  // a row across a j face: its image
+          const int x = z.kb * ZK, y = ps + g.m[1], zc = z.i + g.m[0];
+          mbar_expect_tx(&sm.full[b], tx);
+          tma4(&thi, sl, &sm.full[b], x, y, zc, 0);
+          tma4(&tlo, sl + YZ_LO, &sm.full[b], x, y, zc, 0);
+          tma3(&tcc, sl + YZ_CC, &sm.full[b], x, y, zc);
+          if (wl) {
+            tma4(&twh, sl + YZ_WL, &sm.full[b], xl, y, zc, 0);
+            tma4(&twl, sl + YZ_WL + YZ_WB, &sm.full[b], xl, y, zc, 0);
+            tma3(&twc, sl + YZ_WL + 2 * YZ_WB, &sm.full[b], xl, y, zc);
+          }
+          if (wr) {
+            tma4(&twh, sl + YZ_WR, &sm.full[b], 0, y, zc, 0);
+            tma4(&twl, sl + YZ_WR + YZ_WB, &sm.full[b], 0, y, zc, 0);
+            tma3(&twc, sl + YZ_WR + 2 * YZ_WB, &sm.full[b], 0, y, zc);
+          }
+        }
+      }
+      // the last copies land before the CTA exits (bounded)
+      for (int s2 = s > YZ_NB ? s - YZ_NB : 0; s2 < s; ++s2)
+        mbar_wait(&sm.full[s2 % YZ_NB], (unsigned)((s2 / YZ_NB) & 1));
+    }
+    return;
+  }
+
+  const float facy = (float)(g.dsi[1] * a.sc->dt);
+  const float facz = (float)(g.dsi[2] * a.sc->dt);
+  const float2 ep2 = vs<float2>(a.ep), fh2 = vs<float2>(a.fh), mfac2 = vs<float2>(-facy);
+  float best = 1.e10f;
+  bool bad = false, stop = false;
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // MON: ro, mx, my, mz, et, ph^2
+  int seq = 0;
+  // y sweep queue on field pairs, as av_line_kernel
+  W9 wm2, wm1, w0, w1, dq0, F0;
+  float ccm1 = 0.f, cc0 = 0.f, cc1 = 0.f;
+  for (int it = blockIdx.x; it < items && !stop; it += gridDim.x) {
+    const ZItem z = z_item(a, it, kblocks);
+    const int k = z.kb * ZK + 28 * w + lane - 2;
+    const int kk = min(k, nk + 1);
+    // where this lane's words sit in a slot, and the k face's mirror signs
+    // its y-swept values take
+    int region = 0, off = 28 * w + lane;
+    unsigned negz = 0;
+    if (kk < 0 || kk >= nk) {
+      int side;
+      const int img = ghost_src(g, 2, kk, side);
+      if (g.periodic[2]) {
+        region = kk < 0 ? 1 : 2;
+        off = img + 2 - (kk < 0 ? xl : 0);
+      } else {
+        off = img - (z.kb * ZK - 2);
+        negz = g.negmask[2][side];
+      }
+    }
+    const int o_hi = region == 0 ? 0 : region == 1 ? YZ_WL : YZ_WR;
+    const int o_lo = region == 0 ? YZ_LO : o_hi + YZ_WB;
+    const int o_cc = region == 0 ? YZ_CC : o_hi + 2 * YZ_WB;
+    const int stride = region == 0 ? LBOX : ZWB;
+    const bool out = lane >= 2 && lane < 30 && k < nk;
+    for (int p = z.t0 - 2; p <= z.t1 + 1; ++p, ++seq) {
+      const int s = seq % YZ_NB;
+      if (!mbar_wait(&sm.full[s], (unsigned)((seq / YZ_NB) & 1), a.wait_limit)) {
+        // leave the loops (every consumer warp still meets the barrier below)
+        atomicOr(a.err, ERRBIT_TIMEOUT);
+        stop = true;
+        break;
+      }
+      W9 wp;
+      float ccp;
+      {
+        const float *sh = reinterpret_cast<const float *>(sm.slot[s] + o_hi);
+        float u[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) u[f] = sh[f * stride + off];
+        if (p < 0 || p >= g.n[1]) {
+          // the row was copied from the interior row it images: the mirror
+          // signs of that j face (none on a periodic axis)
+          const unsigned neg = g.negmask[1][p < 0 ? 0 : 1];
+#pragma unroll
+          for (int f = 0; f < NF; ++f)
+            if ((neg >> f) & 1u) u[f] = -u[f];
+        }
+        limited_w9(u, wp);
+        ccp = reinterpret_cast<const float *>(sm.slot[s] + o_cc)[off];
+      }
+      const int r = p - z.t0;  // -2 .. t1-t0+1
+      if (r == -2) {
+        wm2 = wp;
+      } else if (r == -1) {
+        wm1 = wp;
+        ccm1 = ccp;
+      } else if (r == 0) {
+        w0 = wp;
+        cc0 = ccp;
+      } else if (r == 1) {
+        w1 = wp;
+        // -1/2 of the face speed 0.5 (cc[t-1] + cc[t])
+        const float hcc = -0.25f * (ccm1 + cc0);
+        const float2 hcc2 = vs<float2>(hcc);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float2 dqm = dqq_t(wm2.p[i], wm1.p[i], w0.p[i], ep2);
+          dq0.p[i] = dqq_t(wm1.p[i], w0.p[i], w1.p[i], ep2);
+          F0.p[i] = flux_t(wm1.p[i], w0.p[i], dqm, dq0.p[i], hcc2, fh2);
+        }
+        const float dqm = dqq_t(wm2.s, wm1.s, w0.s, a.ep);
+        dq0.s = dqq_t(wm1.s, w0.s, w1.s, a.ep);
+        F0.s = flux_t(wm1.s, w0.s, dqm, dq0.s, hcc, a.fh);
+        cc1 = ccp;
+      } else {
+        // centre row t = p - 2; its copies sit two slots back
+        const int t = p - 2;
+        const int sc_ = (int)((seq - 2) % YZ_NB);
+        const float *chi = reinterpret_cast<const float *>(sm.slot[sc_] + o_hi);
+        const float *clo = reinterpret_cast<const float *>(sm.slot[sc_] + o_lo);
+        const float cct = cc0;  // speed of the centre cell
+        const float hcc = -0.25f * (cc0 + cc1);
+        const float2 hcc2 = vs<float2>(hcc);
+        W9 dF;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float2 dq1 = dqq_t(w0.p[i], w1.p[i], wp.p[i], ep2);
+          const float2 F1 = flux_t(w0.p[i], w1.p[i], dq0.p[i], dq1, hcc2, fh2);
+          dF.p[i] = vsub(F1, F0.p[i]);
+          F0.p[i] = F1;
+          dq0.p[i] = dq1;
+        }
+        {
+          const float dq1 = dqq_t(w0.s, w1.s, wp.s, a.ep);
+          const float F1 = flux_t(w0.s, w1.s, dq0.s, dq1, hcc, a.fh);
+          dF.s = vsub(F1, F0.s);
+          F0.s = F1;
+          dq0.s = dq1;
+        }
+        w0 = w1;
+        w1 = wp;
+        cc0 = cc1;
+        cc1 = ccp;
+        // the y-swept state of the centre cell (the y line sweep's update)
+        float sy[NF], ey[NF];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int f0 = field_of(2 * i), f1 = field_of(2 * i + 1);
+          const float2 h = make_float2(chi[f0 * stride + off], chi[f1 * stride + off]);
+          const float2 l = make_float2(clo[f0 * stride + off], clo[f1 * stride + off]);
+          float2 sv, e;
+          two_sum(h, vfma(dF.p[i], mfac2, l), sv, e);
+          sy[f0] = sv.x;
+          sy[f1] = sv.y;
+          ey[f0] = e.x;
+          ey[f1] = e.y;
+        }
+        two_sum(chi[ET * stride + off], vfma(dF.s, -facy, clo[ET * stride + off]), sy[ET],
+                ey[ET]);
+        if (negz) {
+#pragma unroll
+          for (int f = 0; f < NF; ++f)
+            if ((negz >> f) & 1u) {
+              sy[f] = -sy[f];
+              ey[f] = -ey[f];
+            }
+        }
+        // the z sweep of row t
+        W9 dFz;
+        z_flux_diff(sy, cct, a.ep, a.fh, dFz);
+        if (out) {
+          float sv[NF], e[NF];
+          av_update(sy, ey, dFz, facz, sv, e);
+          const int c = cell_of(g, z.i, t, k);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            a.hi2.f[f][c] = sv[f];  // interior only: the shell kernel fills the images
+            a.lo2.f[f][c] = e[f];
+          }
+          if (MON) {
+            acc[0] += (double)sv[RO] + (double)e[RO];
+            acc[1] += (double)sv[MX] + (double)e[MX];
+            acc[2] += (double)sv[MY] + (double)e[MY];
+            acc[3] += (double)sv[MZ] + (double)e[MZ];
+            acc[4] += (double)sv[ET] + (double)e[ET];
+            const double ph = (double)sv[PH] + (double)e[PH];
+            acc[5] += ph * ph;
+          }
+          if (a.partial) {
+            // CFL candidate of the new state (mhd_integrator_host.hpp:303-334)
+            float cs, vv, ca, ein;
+            speeds(sv, a.gm, a.gm1, cs, vv, ca, ein);
+            const float tv = cs + vv + ca;
+            best = fminf(best, a.cfl_dx / tv);
+            bad |= !(sv[RO] > 0.0f) || !(ein >= 0.0f) || !isfinite(tv);
+          }
+        }
+      }
+      // release the slots this warp is done with: row p-2 (the centre just
+      // finished, or a leading halo row), and at the item's last row the two
+      // trailing halo rows
+      __syncwarp();
+      if (lane == 0) {
+        if (r >= 0) mbar_arrive(&sm.empty[(seq - 2) % YZ_NB]);
+        if (p == z.t1 + 1) {
+          mbar_arrive(&sm.empty[(seq - 1) % YZ_NB]);
+          mbar_arrive(&sm.empty[seq % YZ_NB]);
+        }
+      }
+    }
+  }
+  __shared__ float red[LCW];
+  __shared__ double mred[LCW][6];
+  if (a.partial) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0) red[w] = best;
+    if (bad) atomicOr(a.err, ERRBIT_NONFINITE);
+  }
+  if (MON) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+      if (lane == 0) mred[w][q] = acc[q];
+    }
+  }
+  asm volatile("bar.sync 1, %0;" ::"r"(LK) : "memory");  // the consumer warps only
+  if (a.partial && tid == 0) {
+    float b = red[0];
+    for (int w2 = 1; w2 < LCW; ++w2) b = fminf(b, red[w2]);
+    a.partial[blockIdx.x] = b;
+  }
+  if (MON && tid < 6) {
+    double v = 0.0;
+    for (int w2 = 0; w2 < LCW; ++w2) v += mred[w2][tid];
+    a.mon[blockIdx.x * 6 + tid] = v;
+  }
+}
+
 }  // namespace s32t
 
 // ---------------------------------------------------------------------------
@@ -1012,6 +1325,7 @@ int s32_configure() {
   const int ln = (int)sizeof(s32t::LineSmem);
   const int lnd = (int)sizeof(s32t::LineSmemT<true>);
   const int zl = (int)sizeof(s32t::ZLineSmem);
+  const int yz = (int)sizeof(s32t::YzSmem);
   cudaError_t e = cudaSuccess;
 #define MISO_SET(k, b) \
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b)
@@ -1023,6 +1337,8 @@ int s32_configure() {
   MISO_SET((s32t::av_line_kernel<1, false>), ln);
   MISO_SET((s32t::av_line_kernel<0, true>), lnd);
   MISO_SET(s32t::av_zline_kernel, zl);
+  MISO_SET(s32t::av_yz_kernel<false>, yz);
+  MISO_SET(s32t::av_yz_kernel<true>, yz);
 #undef MISO_SET
   return e == cudaSuccess ? 0 : -1;
 }
@@ -1094,6 +1410,28 @@ void launch_s32_av_zline(const void *tm_hi, const void *tm_lo, const void *tm_cc
   s32t::av_zline_kernel<<<grid, s32t::LK + 32, sizeof(s32t::ZLineSmem), st>>>(
       *(const CUtensorMap *)tm_hi, *(const CUtensorMap *)tm_lo, *(const CUtensorMap *)tm_cc,
       *(const CUtensorMap *)tm_wh, *(const CUtensorMap *)tm_wc, a);
+}
+
+int s32_yz_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, s32t::av_yz_kernel<true>, s32t::LK + 32,
+                                                    sizeof(s32t::YzSmem)) != cudaSuccess ||
+      n < 1)
+    n = 1;
+  return n;
+}
+
+void launch_s32_av_yz(const void *tm_hi, const void *tm_lo, const void *tm_cc, const void *tm_wh,
+                      const void *tm_wl, const void *tm_wc, const AvArgs &a, int grid,
+                      cudaStream_t st) {
+  const CUtensorMap &h = *(const CUtensorMap *)tm_hi, &l = *(const CUtensorMap *)tm_lo;
+  const CUtensorMap &c = *(const CUtensorMap *)tm_cc, &wh = *(const CUtensorMap *)tm_wh;
+  const CUtensorMap &wl = *(const CUtensorMap *)tm_wl, &wc = *(const CUtensorMap *)tm_wc;
+  const size_t smem = sizeof(s32t::YzSmem);
+  if (a.mon)
+    s32t::av_yz_kernel<true><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, wh, wl, wc, a);
+  else
+    s32t::av_yz_kernel<false><<<grid, s32t::LK + 32, smem, st>>>(h, l, c, wh, wl, wc, a);
 }
 
 }  // namespace miso_b200

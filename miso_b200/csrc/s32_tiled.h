@@ -104,6 +104,13 @@ int s32_zline_per_sm();  // resident z line CTAs per SM (after s32_configure)
 void launch_s32_av_zline(const void *tm_hi, const void *tm_lo, const void *tm_cc,
                          const void *tm_wh, const void *tm_wc, const AvArgs &a, int grid,
                          cudaStream_t st);
+// y and z sweeps in one pass (y sweep variant 3): the z line sweep's rows
+// and wrap copies (of hi, lo and the speed) with the y sweep run down each
+// column; writes a.partial[blockIdx.x] and, with a.mon, the monitor sums
+int s32_yz_per_sm();  // resident fused-sweep CTAs per SM (after s32_configure)
+void launch_s32_av_yz(const void *tm_hi, const void *tm_lo, const void *tm_cc, const void *tm_wh,
+                      const void *tm_wl, const void *tm_wc, const AvArgs &a, int grid,
+                      cudaStream_t st);
 // x / y sweep, one warp per 32-cell line segment marching along the sweep
 // axis (s32_av.cu): no shared memory, no CTA barrier; interior-only writes
 void launch_s32_av_march(const AvArgs &a, int dir, int grid, cudaStream_t st);

@@ -959,6 +959,9 @@ av_zline_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__
 // sweep, without writing the y-swept state and reading it back (144 B per
 // cell).  The CFL candidate of the new state, and with MON the monitors'
 // FP64 sums, are folded into per-CTA partials as the z sweep folds them.
+// The first four rows of an item run apart from the steady loop, so the
+// queue's leading entries are dead there: 128 registers, three CTAs (15
+// warps) per SM beside 219 KB of slots.
 constexpr int YZ_NB = 6;                                     // ring slots
 constexpr int YZ_LO = L_LO;                                  // hi at 0, then lo
 constexpr int YZ_CC = 2 * L_LO;                              // the speed
@@ -974,8 +977,55 @@ struct __align__(128) YzSmem {
   unsigned long long empty[YZ_NB];  // the row read by every consumer warp (LCW arrivals)
 };
 
+// A consumer lane's place in a slot: offsets of its hi, lo and speed words
+// (the main box or a wrap box) and the stride between fields.
+struct YzLane {
+  int o_hi, o_lo, o_cc, stride, off;
+};
+
+// Row p of the fused sweeps' march: wait for its slot (seq), then the
+// limited quantities of the lane's column -- with the mirror signs of the
+// j face for a row copied from the interior row it images -- and its speed.
+// false (error bit set) when the wait ran out.
+__device__ __forceinline__ bool yz_row(YzSmem &sm, int seq, long long limit, const YzLane &ln,
+                                       int p, const Geom &g, W9 &wp, float &ccp,
+                                       unsigned *err) {
+  const int s = seq % YZ_NB;
+  if (!mbar_wait(&sm.full[s], (unsigned)((seq / YZ_NB) & 1), limit)) {
+    atomicOr(err, ERRBIT_TIMEOUT);
+    return false;
+  }
+  const float *sh = reinterpret_cast<const float *>(sm.slot[s] + ln.o_hi);
+  float u[NF];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) u[f] = sh[f * ln.stride + ln.off];
+  if (p < 0 || p >= g.n[1]) {
+    const unsigned neg = g.negmask[1][p < 0 ? 0 : 1];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+      if ((neg >> f) & 1u) u[f] = -u[f];
+  }
+  limited_w9(u, wp);
+  ccp = reinterpret_cast<const float *>(sm.slot[s] + ln.o_cc)[ln.off];
+  return true;
+}
+
+// Release the slots a warp is done with after row `seq` of an item: the row
+// two back (the centre just finished, or a leading halo row), and after the
+// item's last row the two trailing halo rows.
+__device__ __forceinline__ void yz_release(YzSmem &sm, int seq, int lane, bool last) {
+  __syncwarp();
+  if (lane == 0) {
+    mbar_arrive(&sm.empty[(seq - 2) % YZ_NB]);
+    if (last) {
+      mbar_arrive(&sm.empty[(seq - 1) % YZ_NB]);
+      mbar_arrive(&sm.empty[seq % YZ_NB]);
+    }
+  }
+}
+
 template <bool MON>
-__global__ void __launch_bounds__(LK + 32, 2)
+__global__ void __launch_bounds__(LK + 32, 3)
 av_yz_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CUtensorMap tlo,
              const __grid_constant__ CUtensorMap tcc, const __grid_constant__ CUtensorMap twh,
              const __grid_constant__ CUtensorMap twl, const __grid_constant__ CUtensorMap twc,
@@ -1052,9 +1102,6 @@ av_yz_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CU
   bool bad = false, stop = false;
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // MON: ro, mx, my, mz, et, ph^2
   int seq = 0;
-  // y sweep queue on field pairs, as av_line_kernel
-  W9 wm2, wm1, w0, w1, dq0, F0;
-  float ccm1 = 0.f, cc0 = 0.f, cc1 = 0.f;
   for (int it = blockIdx.x; it < items && !stop; it += gridDim.x) {
     const ZItem z = z_item(a, it, kblocks);
     const int k = z.kb * ZK + 28 * w + lane - 2;
@@ -1074,156 +1121,136 @@ av_yz_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CU
         negz = g.negmask[2][side];
       }
     }
-    const int o_hi = region == 0 ? 0 : region == 1 ? YZ_WL : YZ_WR;
-    const int o_lo = region == 0 ? YZ_LO : o_hi + YZ_WB;
-    const int o_cc = region == 0 ? YZ_CC : o_hi + 2 * YZ_WB;
-    const int stride = region == 0 ? LBOX : ZWB;
+    YzLane ln;
+    ln.o_hi = region == 0 ? 0 : region == 1 ? YZ_WL : YZ_WR;
+    ln.o_lo = region == 0 ? YZ_LO : ln.o_hi + YZ_WB;
+    ln.o_cc = region == 0 ? YZ_CC : ln.o_hi + 2 * YZ_WB;
+    ln.stride = region == 0 ? LBOX : ZWB;
+    ln.off = off;
     const bool out = lane >= 2 && lane < 30 && k < nk;
-    for (int p = z.t0 - 2; p <= z.t1 + 1; ++p, ++seq) {
-      const int s = seq % YZ_NB;
-      if (!mbar_wait(&sm.full[s], (unsigned)((seq / YZ_NB) & 1), a.wait_limit)) {
-        // leave the loops (every consumer warp still meets the barrier below)
-        atomicOr(a.err, ERRBIT_TIMEOUT);
+    // the y sweep's queue on field pairs, as av_line_kernel: the first four
+    // rows of the item (t0-2 .. t0+1) give the limited quantities of rows
+    // t0, t0+1, the slope of row t0 and the flux of face t0 - 1/2
+    W9 w0, w1, dq0, F0;
+    float cc0, cc1;
+    {
+      W9 wm2, wm1;
+      float ccm1, cx;
+      // (a wait that ran out leaves the loops; every consumer warp still
+      // meets the barrier below)
+      if (!yz_row(sm, seq, a.wait_limit, ln, z.t0 - 2, g, wm2, cx, a.err)) break;
+      ++seq;
+      if (!yz_row(sm, seq, a.wait_limit, ln, z.t0 - 1, g, wm1, ccm1, a.err)) break;
+      ++seq;
+      if (!yz_row(sm, seq, a.wait_limit, ln, z.t0, g, w0, cc0, a.err)) break;
+      yz_release(sm, seq, lane, false);
+      ++seq;
+      if (!yz_row(sm, seq, a.wait_limit, ln, z.t0 + 1, g, w1, cc1, a.err)) break;
+      // -1/2 of the face speed 0.5 (cc[t-1] + cc[t])
+      const float hcc = -0.25f * (ccm1 + cc0);
+      const float2 hcc2 = vs<float2>(hcc);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 dqm = dqq_t(wm2.p[i], wm1.p[i], w0.p[i], ep2);
+        dq0.p[i] = dqq_t(wm1.p[i], w0.p[i], w1.p[i], ep2);
+        F0.p[i] = flux_t(wm1.p[i], w0.p[i], dqm, dq0.p[i], hcc2, fh2);
+      }
+      const float dqm = dqq_t(wm2.s, wm1.s, w0.s, a.ep);
+      dq0.s = dqq_t(wm1.s, w0.s, w1.s, a.ep);
+      F0.s = flux_t(wm1.s, w0.s, dqm, dq0.s, hcc, a.fh);
+      yz_release(sm, seq, lane, false);
+      ++seq;
+    }
+    for (int p = z.t0 + 2; p <= z.t1 + 1; ++p, ++seq) {
+      W9 wp;
+      float ccp;
+      if (!yz_row(sm, seq, a.wait_limit, ln, p, g, wp, ccp, a.err)) {
         stop = true;
         break;
       }
-      W9 wp;
-      float ccp;
+      // centre row t = p - 2; its copies sit two slots back
+      const int t = p - 2;
+      const int sc_ = (int)((seq - 2) % YZ_NB);
+      const float *chi = reinterpret_cast<const float *>(sm.slot[sc_] + ln.o_hi);
+      const float *clo = reinterpret_cast<const float *>(sm.slot[sc_] + ln.o_lo);
+      const float cct = cc0;  // speed of the centre cell
+      const float hcc = -0.25f * (cc0 + cc1);
+      const float2 hcc2 = vs<float2>(hcc);
+      W9 dF;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 dq1 = dqq_t(w0.p[i], w1.p[i], wp.p[i], ep2);
+        const float2 F1 = flux_t(w0.p[i], w1.p[i], dq0.p[i], dq1, hcc2, fh2);
+        dF.p[i] = vsub(F1, F0.p[i]);
+        F0.p[i] = F1;
+        dq0.p[i] = dq1;
+      }
       {
-        const float *sh = reinterpret_cast<const float *>(sm.slot[s] + o_hi);
-        float u[NF];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) u[f] = sh[f * stride + off];
-        if (p < 0 || p >= g.n[1]) {
-          // the row was copied from the interior row it images: the mirror
-          // signs of that j face (none on a periodic axis)
-          const unsigned neg = g.negmask[1][p < 0 ? 0 : 1];
-#pragma unroll
-          for (int f = 0; f < NF; ++f)
-            if ((neg >> f) & 1u) u[f] = -u[f];
-        }
-        limited_w9(u, wp);
-        ccp = reinterpret_cast<const float *>(sm.slot[s] + o_cc)[off];
+        const float dq1 = dqq_t(w0.s, w1.s, wp.s, a.ep);
+        const float F1 = flux_t(w0.s, w1.s, dq0.s, dq1, hcc, a.fh);
+        dF.s = vsub(F1, F0.s);
+        F0.s = F1;
+        dq0.s = dq1;
       }
-      const int r = p - z.t0;  // -2 .. t1-t0+1
-      if (r == -2) {
-        wm2 = wp;
-      } else if (r == -1) {
-        wm1 = wp;
-        ccm1 = ccp;
-      } else if (r == 0) {
-        w0 = wp;
-        cc0 = ccp;
-      } else if (r == 1) {
-        w1 = wp;
-        // -1/2 of the face speed 0.5 (cc[t-1] + cc[t])
-        const float hcc = -0.25f * (ccm1 + cc0);
-        const float2 hcc2 = vs<float2>(hcc);
+      w0 = w1;
+      w1 = wp;
+      cc0 = cc1;
+      cc1 = ccp;
+      // the y-swept state of the centre cell (the y line sweep's update)
+      float sy[NF], ey[NF];
+      const int st = ln.stride, o = ln.off;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float2 dqm = dqq_t(wm2.p[i], wm1.p[i], w0.p[i], ep2);
-          dq0.p[i] = dqq_t(wm1.p[i], w0.p[i], w1.p[i], ep2);
-          F0.p[i] = flux_t(wm1.p[i], w0.p[i], dqm, dq0.p[i], hcc2, fh2);
-        }
-        const float dqm = dqq_t(wm2.s, wm1.s, w0.s, a.ep);
-        dq0.s = dqq_t(wm1.s, w0.s, w1.s, a.ep);
-        F0.s = flux_t(wm1.s, w0.s, dqm, dq0.s, hcc, a.fh);
-        cc1 = ccp;
-      } else {
-        // centre row t = p - 2; its copies sit two slots back
-        const int t = p - 2;
-        const int sc_ = (int)((seq - 2) % YZ_NB);
-        const float *chi = reinterpret_cast<const float *>(sm.slot[sc_] + o_hi);
-        const float *clo = reinterpret_cast<const float *>(sm.slot[sc_] + o_lo);
-        const float cct = cc0;  // speed of the centre cell
-        const float hcc = -0.25f * (cc0 + cc1);
-        const float2 hcc2 = vs<float2>(hcc);
-        W9 dF;
+      for (int i = 0; i < 4; ++i) {
+        const int f0 = field_of(2 * i), f1 = field_of(2 * i + 1);
+        const float2 h = make_float2(chi[f0 * st + o], chi[f1 * st + o]);
+        const float2 l = make_float2(clo[f0 * st + o], clo[f1 * st + o]);
+        float2 sv, e;
+        two_sum(h, vfma(dF.p[i], mfac2, l), sv, e);
+        sy[f0] = sv.x;
+        sy[f1] = sv.y;
+        ey[f0] = e.x;
+        ey[f1] = e.y;
+      }
+      two_sum(chi[ET * st + o], vfma(dF.s, -facy, clo[ET * st + o]), sy[ET], ey[ET]);
+      if (negz) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float2 dq1 = dqq_t(w0.p[i], w1.p[i], wp.p[i], ep2);
-          const float2 F1 = flux_t(w0.p[i], w1.p[i], dq0.p[i], dq1, hcc2, fh2);
-          dF.p[i] = vsub(F1, F0.p[i]);
-          F0.p[i] = F1;
-          dq0.p[i] = dq1;
-        }
-        {
-          const float dq1 = dqq_t(w0.s, w1.s, wp.s, a.ep);
-          const float F1 = flux_t(w0.s, w1.s, dq0.s, dq1, hcc, a.fh);
-          dF.s = vsub(F1, F0.s);
-          F0.s = F1;
-          dq0.s = dq1;
-        }
-        w0 = w1;
-        w1 = wp;
-        cc0 = cc1;
-        cc1 = ccp;
-        // the y-swept state of the centre cell (the y line sweep's update)
-        float sy[NF], ey[NF];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int f0 = field_of(2 * i), f1 = field_of(2 * i + 1);
-          const float2 h = make_float2(chi[f0 * stride + off], chi[f1 * stride + off]);
-          const float2 l = make_float2(clo[f0 * stride + off], clo[f1 * stride + off]);
-          float2 sv, e;
-          two_sum(h, vfma(dF.p[i], mfac2, l), sv, e);
-          sy[f0] = sv.x;
-          sy[f1] = sv.y;
-          ey[f0] = e.x;
-          ey[f1] = e.y;
-        }
-        two_sum(chi[ET * stride + off], vfma(dF.s, -facy, clo[ET * stride + off]), sy[ET],
-                ey[ET]);
-        if (negz) {
-#pragma unroll
-          for (int f = 0; f < NF; ++f)
-            if ((negz >> f) & 1u) {
-              sy[f] = -sy[f];
-              ey[f] = -ey[f];
-            }
-        }
-        // the z sweep of row t
-        W9 dFz;
-        z_flux_diff(sy, cct, a.ep, a.fh, dFz);
-        if (out) {
-          float sv[NF], e[NF];
-          av_update(sy, ey, dFz, facz, sv, e);
-          const int c = cell_of(g, z.i, t, k);
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            a.hi2.f[f][c] = sv[f];  // interior only: the shell kernel fills the images
-            a.lo2.f[f][c] = e[f];
+        for (int f = 0; f < NF; ++f)
+          if ((negz >> f) & 1u) {
+            sy[f] = -sy[f];
+            ey[f] = -ey[f];
           }
-          if (MON) {
-            acc[0] += (double)sv[RO] + (double)e[RO];
-            acc[1] += (double)sv[MX] + (double)e[MX];
-            acc[2] += (double)sv[MY] + (double)e[MY];
-            acc[3] += (double)sv[MZ] + (double)e[MZ];
-            acc[4] += (double)sv[ET] + (double)e[ET];
-            const double ph = (double)sv[PH] + (double)e[PH];
-            acc[5] += ph * ph;
-          }
-          if (a.partial) {
-            // CFL candidate of the new state (mhd_integrator_host.hpp:303-334)
-            float cs, vv, ca, ein;
-            speeds(sv, a.gm, a.gm1, cs, vv, ca, ein);
-            const float tv = cs + vv + ca;
-            best = fminf(best, a.cfl_dx / tv);
-            bad |= !(sv[RO] > 0.0f) || !(ein >= 0.0f) || !isfinite(tv);
-          }
+      }
+      // the z sweep of row t
+      W9 dFz;
+      z_flux_diff(sy, cct, a.ep, a.fh, dFz);
+      if (out) {
+        float sv[NF], e[NF];
+        av_update(sy, ey, dFz, facz, sv, e);
+        const int c = cell_of(g, z.i, t, k);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          a.hi2.f[f][c] = sv[f];  // interior only: the shell kernel fills the images
+          a.lo2.f[f][c] = e[f];
+        }
+        if (MON) {
+          acc[0] += (double)sv[RO] + (double)e[RO];
+          acc[1] += (double)sv[MX] + (double)e[MX];
+          acc[2] += (double)sv[MY] + (double)e[MY];
+          acc[3] += (double)sv[MZ] + (double)e[MZ];
+          acc[4] += (double)sv[ET] + (double)e[ET];
+          const double ph = (double)sv[PH] + (double)e[PH];
+          acc[5] += ph * ph;
+        }
+        if (a.partial) {
+          // CFL candidate of the new state (mhd_integrator_host.hpp:303-334)
+          float cs, vv, ca, ein;
+          speeds(sv, a.gm, a.gm1, cs, vv, ca, ein);
+          const float tv = cs + vv + ca;
+          best = fminf(best, a.cfl_dx / tv);
+          bad |= !(sv[RO] > 0.0f) || !(ein >= 0.0f) || !isfinite(tv);
         }
       }
-      // release the slots this warp is done with: row p-2 (the centre just
-      // finished, or a leading halo row), and at the item's last row the two
-      // trailing halo rows
-      __syncwarp();
-      if (lane == 0) {
-        if (r >= 0) mbar_arrive(&sm.empty[(seq - 2) % YZ_NB]);
-        if (p == z.t1 + 1) {
-          mbar_arrive(&sm.empty[(seq - 1) % YZ_NB]);
-          mbar_arrive(&sm.empty[seq % YZ_NB]);
-        }
-      }
+      yz_release(sm, seq, lane, p == z.t1 + 1);
     }
   }
   __shared__ float red[LCW];

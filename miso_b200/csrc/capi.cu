@@ -345,7 +345,7 @@ struct miso_b200_handle {
   // RK = variant 2 with the last update deferred into the x sweep (default),
   // y sweep = the y and z sweeps fused into one pass (the z variant unused)
   int rk_var = 3;
-  int av_var[3] = {0, 0, 0};
+  int av_var[3] = {0, 3, 0};  // the y and z sweeps fused by default
   bool fused_yz() const { return av_var[1] == 3; }
   // hi / lo set swaps of one step: one per viscosity pass
   int sweep_passes() const {
@@ -563,7 +563,7 @@ struct miso_b200_handle {
                                               : 3;
       if (const char *v = getenv("MISO_B200_AV"))
         for (int d = 0; d < 3 && v[d]; ++d)
-          av_var[d] = v[d] == 'f' ? 1 : v[d] == 'p' ? 2 : 0;
+          av_var[d] = v[d] == 'f' ? 1 : v[d] == 'p' ? 2 : (v[d] == 'u' && d == 1) ? 3 : 0;
     }
   }
 
@@ -1359,6 +1359,7 @@ int miso_b200::b200_view_create(const miso_b200_grid_desc &gd, const miso_b200_p
     delete h;
     return MISO_B200_ERR_STATE;
   }
+  h->av_var[1] = 0;  // one hi / lo swap per sweep, as the batch's other instances
   h->src.kind = 0;
   *out = h;
   return MISO_B200_OK;

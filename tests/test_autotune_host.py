@@ -1,6 +1,7 @@
 """The autotuner's choices on a stand-in integrator with scripted kernel
 times (no GPU): per-class picks, the whole-step comparison of the deferred
-last RK stage (variant 3 moves time from the RK class to the x sweep), the
+last RK stage (variant 3 moves time from the RK class to the x sweep) and of
+the fused y and z sweeps (y variant 3: one pass in place of two), the
 refusal of RK variants under a source term, and the cache."""
 import pytest
 
@@ -10,10 +11,11 @@ from miso_b200 import _lib, autotune
 class FakeInteg:
     """Kernel times per class as functions of the variants set."""
 
-    def __init__(self, defer_gain, refuse_rk=()):
-        self.var = {0: 3, 1: 0, 2: 0, 3: 0}
+    def __init__(self, defer_gain, refuse_rk=(), fused_ms=20.0):
+        self.var = {0: 3, 1: 0, 2: 3, 3: 0}
         self.chunks = (64, 128)
         self.defer_gain = defer_gain
+        self.fused_ms = fused_ms
         self.refuse_rk = refuse_rk
         self.config, self.precision = {}, "fp32_split"
 
@@ -42,12 +44,15 @@ class FakeInteg:
         # variant 3 takes the update into the x sweep: the sweep pays part of it
         avx = {0: 4.3, 1: 6.0, 2: 5.2}[self.var[1]] + (0.5 * 4 * self.defer_gain
                                                         if self.var[0] == 3 else 0.0)
-        avy = {0: 4.3, 1: 6.0, 2: 5.2}[self.var[2]]
-        avz = {0: 5.0, 1: 7.0, 2: 6.2}[self.var[3]]
         chunk = 0.01 * abs(self.chunks[0] - 64) / 64
-        return {"rk_stage": {"ms": 4 * (rk + chunk), "launches": 4},
-                "av_x": {"ms": avx, "launches": 1}, "av_y": {"ms": avy, "launches": 1},
-                "av_z": {"ms": avz, "launches": 1}}
+        rep = {"rk_stage": {"ms": 4 * (rk + chunk), "launches": 4},
+               "av_x": {"ms": avx, "launches": 1}}
+        if self.var[2] == 3:  # the fused y and z sweeps: one pass
+            rep["av_yz"] = {"ms": self.fused_ms, "launches": 1}
+        else:
+            rep["av_y"] = {"ms": {0: 4.3, 1: 6.0, 2: 5.2}[self.var[2]], "launches": 1}
+            rep["av_z"] = {"ms": {0: 5.0, 1: 7.0, 2: 6.2}[self.var[3]], "launches": 1}
+        return rep
 
 
 @pytest.fixture
@@ -76,3 +81,16 @@ def test_refused_variants_are_skipped(cache):
     integ = FakeInteg(defer_gain=0.8, refuse_rk=(0, 1))  # a source term pins RK to 2 / 3
     choice = autotune.autotune(integ, steps=1)
     assert choice["rk_stage"] in (2, 3)
+
+
+def test_fused_sweeps_kept_when_the_step_gains(cache):
+    integ = FakeInteg(defer_gain=0.8, fused_ms=7.0)  # 7.0 ms against 4.3 + 5.0
+    choice = autotune.autotune(integ, steps=1)
+    assert choice["av_y"] == 3 and integ.get_variant(2) == 3
+    assert choice["ms"]["av_y"] == 7.0 and "av_z" not in choice["ms"]
+
+
+def test_fused_sweeps_dropped_when_the_step_loses(cache):
+    integ = FakeInteg(defer_gain=0.8, fused_ms=9.5)
+    choice = autotune.autotune(integ, steps=1)
+    assert choice["av_y"] == 0 and integ.get_variant(2) == 0

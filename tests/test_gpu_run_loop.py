@@ -14,29 +14,35 @@ from miso_b200.integrator import Integrator
 pytestmark = pytest.mark.gpu
 
 
-def _fresh(prob, precision):
+def _fresh(prob, precision, yvar=None):
     integ = Integrator(prob.config, prob.grid, sign=prob.sign, precision=precision)
+    if yvar is not None:
+        integ.set_variant(2, yvar)
     integ.upload(prob.q)
     integ.apply_boundary_condition()
     return integ
 
 
-@pytest.mark.parametrize("make,precision,nsteps", [
-    (lambda: P.orszag_tang(64), "fp64", 7),          # one step per body
-    (lambda: P.turbulence(32, seed=2), "fp32_split", 5),   # two per body, odd count
-    (lambda: P.turbulence(32, seed=2), "fp32_split", 6),
-    (lambda: P.orszag_tang(64), "fp32_split", 5),
-], ids=["ot64_fp64_7", "turb32_split_5", "turb32_split_6", "ot64_split_5"])
-def test_graph_loop_equals_host_launched_steps(make, precision, nsteps):
+@pytest.mark.parametrize("make,precision,nsteps,yvar", [
+    (lambda: P.orszag_tang(64), "fp64", 7, None),          # one step per body
+    # the separate y and z sweeps: three swaps a step, two steps per body
+    (lambda: P.turbulence(32, seed=2), "fp32_split", 5, 0),   # odd count
+    (lambda: P.turbulence(32, seed=2), "fp32_split", 6, 0),
+    # the fused y and z sweeps (the default): two swaps, one step per body
+    (lambda: P.turbulence(32, seed=2), "fp32_split", 5, None),
+    (lambda: P.orszag_tang(64), "fp32_split", 5, None),
+], ids=["ot64_fp64_7", "turb32_split_sep_5", "turb32_split_sep_6", "turb32_split_5",
+        "ot64_split_5"])
+def test_graph_loop_equals_host_launched_steps(make, precision, nsteps, yvar):
     """t_end = the time after `nsteps` host-launched steps: the graph loop
     stops after the same step, with the same time and the same bits."""
     prob = make()
-    a = _fresh(prob, precision)
+    a = _fresh(prob, precision, yvar)
     t, n = a.run_until(0.0, 1e30, max_steps=nsteps, graph=False)
     assert n == nsteps
     ref = a.download()
     a.close()
-    b = _fresh(prob, precision)
+    b = _fresh(prob, precision, yvar)
     t2, n2 = b.run_until(0.0, t, graph=True)
     assert n2 == nsteps and t2 == t
     out = b.download()

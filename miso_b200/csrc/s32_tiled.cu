@@ -296,7 +296,7 @@ rk_tiled_kernel(const __grid_constant__ CUtensorMap tm, const RkArgs a) {
 // ---- x / y line sweep ----
 constexpr int LK = 128;       // k cells per CTA
 constexpr int LBOX = LK + 4;  // k box of the TMA copies
-constexpr int LNB = 6;        // slots (3 planes in use, 3 in flight)
+constexpr int LNB = 5;        // slots (3 planes in use, 2 in flight; 6 measured slower)
 constexpr int L_HI = 0;
 constexpr int L_LO = (NF * LBOX * 4 + 127) / 128 * 128;
 constexpr int L_CC = L_LO + L_LO;
@@ -405,13 +405,81 @@ __device__ __forceinline__ void line_issue(const CUtensorMap *thi, const CUtenso
     tma3(t3, sl + L_CC, &sm.full[s], k0, cj, ci);
 }
 
+// Plane p of a line sweep's march: wait for its slot (seq), then the
+// limited quantities of the thread's cell -- with DEFER formed from U^n and
+// the deferred stage's D, with the mirror signs of the sweep axis's face for
+// a plane copied from the interior plane it images -- and its speed.  false
+// (error bit set) when the wait ran out.
+template <int DIR, bool DEFER>
+__device__ __forceinline__ bool line_row(LineSmemT<DEFER> &sm, int seq, int p, const AvArgs &a,
+                                         int tid, float dt4, float decay4, W9 &wp, float &ccp) {
+  constexpr int NB = LNB;
+  const int s = seq % NB;
+  if (!mbar_wait(&sm.full[s], (unsigned)((seq / NB) & 1), a.wait_limit)) {
+    atomicOr(a.err, ERRBIT_TIMEOUT);
+    return false;
+  }
+  const float *shi = reinterpret_cast<const float *>(sm.slot[s] + L_HI);
+  float u[NF];
+  if (DEFER) {
+    const float *slo = reinterpret_cast<const float *>(sm.slot[s] + L_LO);
+    const float *sd = reinterpret_cast<const float *>(sm.slot[s] + L_D);
+    const int o = tid + 2;
+    float e;
+    last_stage_field<RO>(shi[RO * LBOX + o], slo[RO * LBOX + o], sd[RO * LBOX + o], dt4, decay4, u[RO], e);
+    last_stage_field<MX>(shi[MX * LBOX + o], slo[MX * LBOX + o], sd[MX * LBOX + o], dt4, decay4, u[MX], e);
+    last_stage_field<MY>(shi[MY * LBOX + o], slo[MY * LBOX + o], sd[MY * LBOX + o], dt4, decay4, u[MY], e);
+    last_stage_field<MZ>(shi[MZ * LBOX + o], slo[MZ * LBOX + o], sd[MZ * LBOX + o], dt4, decay4, u[MZ], e);
+    last_stage_field<BX>(shi[BX * LBOX + o], slo[BX * LBOX + o], sd[BX * LBOX + o], dt4, decay4, u[BX], e);
+    last_stage_field<BY>(shi[BY * LBOX + o], slo[BY * LBOX + o], sd[BY * LBOX + o], dt4, decay4, u[BY], e);
+    last_stage_field<BZ>(shi[BZ * LBOX + o], slo[BZ * LBOX + o], sd[BZ * LBOX + o], dt4, decay4, u[BZ], e);
+    last_stage_field<ET>(shi[ET * LBOX + o], slo[ET * LBOX + o], sd[ET * LBOX + o], dt4, decay4, u[ET], e);
+    last_stage_field<PH>(shi[PH * LBOX + o], slo[PH * LBOX + o], sd[PH * LBOX + o], dt4, decay4, u[PH], e);
+    ccp = last_stage_cc(u, a);
+  } else {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) u[f] = shi[f * LBOX + tid + 2];
+    ccp = reinterpret_cast<const float *>(sm.slot[s] + L_CC)[tid + 2];
+  }
+  if (p < 0 || p >= a.g.n[DIR]) {
+    // the plane was copied from the interior plane it images: apply the
+    // mirror signs of that face (none on a periodic axis)
+    const unsigned neg = a.g.negmask[DIR][p < 0 ? 0 : 1];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+      if ((neg >> f) & 1u) u[f] = -u[f];
+  }
+  limited_w9(u, wp);
+  return true;
+}
+
+// Release the slots a consumer warp is done with after plane `seq` of an
+// item: the plane two back (read for the cell just finished, or a leading
+// halo plane), and after the item's last plane the two trailing halo planes.
+template <bool DEFER>
+__device__ __forceinline__ void line_release(LineSmemT<DEFER> &sm, int seq, int lane, bool last) {
+  constexpr int NB = LNB;
+  __syncwarp();
+  if (lane == 0) {
+    mbar_arrive(&sm.empty[(seq - 2) % NB]);
+    if (last) {
+      mbar_arrive(&sm.empty[(seq - 1) % NB]);
+      mbar_arrive(&sm.empty[seq % NB]);
+    }
+  }
+}
+
 // DEFER (x sweep only): the state is U^{n+1} = (hi, lo) - dt_4 D of the
 // deferred last Runge-Kutta stage (rk_pipe_kernel<4>); t3 maps D in place of
 // the characteristic speed.  Each plane's state and speed are formed as the
 // plane arrives, and the sweep writes the speed of the cells it finishes
 // for the y and z sweeps.
+// Registers are held to three CTAs' worth (<= 128), and the march's first
+// four planes run apart from its steady loop so that the queue's leading
+// entries are dead there; the grid keeps two CTAs per SM (three resident
+// measured 1.2x slower: their copies in flight crowd each other).
 template <int DIR, bool DEFER>
-__global__ void __launch_bounds__(LK + 32, 2)
+__global__ void __launch_bounds__(LK + 32, 3)
 av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CUtensorMap tlo,
                const __grid_constant__ CUtensorMap t3, const AvArgs a) {
   static_assert(!DEFER || DIR == 0, "the deferred update rides on the x sweep");
@@ -419,13 +487,14 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
   LineSmemT<DEFER> &sm = *reinterpret_cast<LineSmemT<DEFER> *>(smem_raw);
   const Geom &g = a.g;
   constexpr int OTH = DIR == 0 ? 1 : 0;
+  constexpr int NB = LNB;
   const int tid = threadIdx.x, lane = tid & 31;
   const int nk = g.n[2], nu = g.n[OTH];
   const int kblocks = (nk + LK - 1) / LK;
   const int chunks = (a.r1 - a.r0 + a.L - 1) / a.L;
   const int items = kblocks * nu * chunks;
   if (tid == 0) {
-    for (int b = 0; b < LNB; ++b) {
+    for (int b = 0; b < NB; ++b) {
       mbar_init(&sm.full[b], 1);
       mbar_init(&sm.empty[b], LCW);
     }
@@ -442,8 +511,8 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
       prod.begin(a, kblocks, nu, items);
       int s = 0;
       for (; prod.valid(items); ++s) {
-        const int b = s % LNB;
-        if (s >= LNB && !mbar_wait(&sm.empty[b], (unsigned)(((s / LNB) - 1) & 1))) {
+        const int b = s % NB;
+        if (s >= NB && !mbar_wait(&sm.empty[b], (unsigned)(((s / NB) - 1) & 1))) {
           atomicOr(a.err, ERRBIT_TIMEOUT);
           break;
         }
@@ -452,8 +521,8 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
         prod.next(a, kblocks, nu, items);
       }
       // the last copies land before the CTA exits (bounded)
-      for (int s2 = s > LNB ? s - LNB : 0; s2 < s; ++s2)
-        mbar_wait(&sm.full[s2 % LNB], (unsigned)((s2 / LNB) & 1));
+      for (int s2 = s > NB ? s - NB : 0; s2 < s; ++s2)
+        mbar_wait(&sm.full[s2 % NB], (unsigned)((s2 / NB) & 1));
     }
     return;
   }
@@ -465,163 +534,120 @@ av_line_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ 
   // limiter state on field pairs: W9 holds (ro, mx) (my, mz) (bx, by) (bz, ph)
   // as packed pairs and ro*e alone
   const float2 ep2 = vs<float2>(a.ep), fh2 = vs<float2>(a.fh), mfac2 = vs<float2>(-fac);
-  W9 wm2, wm1, w0, w1, dq0, F0;
-  float ccm1 = 0.f, cc0 = 0.f, cc1 = 0.f;
   for (int it = blockIdx.x; it < items; it += gridDim.x) {
     const LineItem li = line_item<DIR>(a, it, kblocks, nu);
     const int k = li.kb * LK + tid;
     const bool active = k < nk;
-    for (int p = li.t0 - 2; p <= li.t1 + 1; ++p, ++seq) {
-      const int s = (int)(seq % LNB);
-      if (!mbar_wait(&sm.full[s], (unsigned)((seq / LNB) & 1), a.wait_limit)) {
-        atomicOr(a.err, ERRBIT_TIMEOUT);
-        return;
+    // the first four planes of the item (t0-2 .. t0+1) give the limited
+    // quantities of planes t0, t0+1, the slope of plane t0 and the flux of
+    // face t0 - 1/2; they run apart from the steady loop, so the queue's
+    // leading entries are dead there
+    W9 w0, w1, dq0, F0;
+    float cc0, cc1;
+    {
+      W9 wm2, wm1;
+      float ccm1, cx;
+      if (!line_row<DIR, DEFER>(sm, seq, li.t0 - 2, a, tid, dt4, decay4, wm2, cx)) return;
+      ++seq;
+      if (!line_row<DIR, DEFER>(sm, seq, li.t0 - 1, a, tid, dt4, decay4, wm1, ccm1)) return;
+      ++seq;
+      if (!line_row<DIR, DEFER>(sm, seq, li.t0, a, tid, dt4, decay4, w0, cc0)) return;
+      line_release<DEFER>(sm, seq, lane, false);
+      ++seq;
+      if (!line_row<DIR, DEFER>(sm, seq, li.t0 + 1, a, tid, dt4, decay4, w1, cc1)) return;
+      // -1/2 of the face speed 0.5 (cc[t-1] + cc[t])
+      const float hcc = -0.25f * (ccm1 + cc0);
+      const float2 hcc2 = vs<float2>(hcc);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 dqm = dqq_t(wm2.p[i], wm1.p[i], w0.p[i], ep2);
+        dq0.p[i] = dqq_t(wm1.p[i], w0.p[i], w1.p[i], ep2);
+        F0.p[i] = flux_t(wm1.p[i], w0.p[i], dqm, dq0.p[i], hcc2, fh2);
       }
-      const float *shi = reinterpret_cast<const float *>(sm.slot[s] + L_HI);
+      const float dqm = dqq_t(wm2.s, wm1.s, w0.s, a.ep);
+      dq0.s = dqq_t(wm1.s, w0.s, w1.s, a.ep);
+      F0.s = flux_t(wm1.s, w0.s, dqm, dq0.s, hcc, a.fh);
+      line_release<DEFER>(sm, seq, lane, false);
+      ++seq;
+    }
+    for (int p = li.t0 + 2; p <= li.t1 + 1; ++p, ++seq) {
       W9 wp;
       float ccp;
-      {
-        float u[NF];
-        if (DEFER) {
-          const float *slo = reinterpret_cast<const float *>(sm.slot[s] + L_LO);
-          const float *sd = reinterpret_cast<const float *>(sm.slot[s] + L_D);
-          const int o = tid + 2;
-          float e;
-          last_stage_field<RO>(shi[RO * LBOX + o], slo[RO * LBOX + o], sd[RO * LBOX + o], dt4, decay4, u[RO], e);
-          last_stage_field<MX>(shi[MX * LBOX + o], slo[MX * LBOX + o], sd[MX * LBOX + o], dt4, decay4, u[MX], e);
-          last_stage_field<MY>(shi[MY * LBOX + o], slo[MY * LBOX + o], sd[MY * LBOX + o], dt4, decay4, u[MY], e);
-          last_stage_field<MZ>(shi[MZ * LBOX + o], slo[MZ * LBOX + o], sd[MZ * LBOX + o], dt4, decay4, u[MZ], e);
-          last_stage_field<BX>(shi[BX * LBOX + o], slo[BX * LBOX + o], sd[BX * LBOX + o], dt4, decay4, u[BX], e);
-          last_stage_field<BY>(shi[BY * LBOX + o], slo[BY * LBOX + o], sd[BY * LBOX + o], dt4, decay4, u[BY], e);
-          last_stage_field<BZ>(shi[BZ * LBOX + o], slo[BZ * LBOX + o], sd[BZ * LBOX + o], dt4, decay4, u[BZ], e);
-          last_stage_field<ET>(shi[ET * LBOX + o], slo[ET * LBOX + o], sd[ET * LBOX + o], dt4, decay4, u[ET], e);
-          last_stage_field<PH>(shi[PH * LBOX + o], slo[PH * LBOX + o], sd[PH * LBOX + o], dt4, decay4, u[PH], e);
-          ccp = last_stage_cc(u, a);
-        } else {
+      if (!line_row<DIR, DEFER>(sm, seq, p, a, tid, dt4, decay4, wp, ccp)) return;
+      // centre cell t = p - 2; its plane sits two slots back
+      const int t = p - 2;
+      const int sc_ = (int)((seq - 2) % LNB);
+      const float *chi = reinterpret_cast<const float *>(sm.slot[sc_] + L_HI);
+      const float *clo = reinterpret_cast<const float *>(sm.slot[sc_] + L_LO);
+      const float *cd = reinterpret_cast<const float *>(sm.slot[sc_] + (DEFER ? L_D : L_LO));
+      const float cct = cc0;  // speed of the centre cell
+      const float hcc = -0.25f * (cc0 + cc1);
+      const float2 hcc2 = vs<float2>(hcc);
+      W9 dF;
 #pragma unroll
-          for (int f = 0; f < NF; ++f) u[f] = shi[f * LBOX + tid + 2];
-          ccp = reinterpret_cast<const float *>(sm.slot[s] + L_CC)[tid + 2];
-        }
-        if (p < 0 || p >= g.n[DIR]) {
-          // the plane was copied from the interior plane it images: apply
-          // the mirror signs of that face (none on a periodic axis)
-          const unsigned neg = g.negmask[DIR][p < 0 ? 0 : 1];
-#pragma unroll
-          for (int f = 0; f < NF; ++f)
-            if ((neg >> f) & 1u) u[f] = -u[f];
-        }
-        limited_w9(u, wp);
+      for (int i = 0; i < 4; ++i) {
+        const float2 dq1 = dqq_t(w0.p[i], w1.p[i], wp.p[i], ep2);
+        const float2 F1 = flux_t(w0.p[i], w1.p[i], dq0.p[i], dq1, hcc2, fh2);
+        dF.p[i] = vsub(F1, F0.p[i]);
+        F0.p[i] = F1;
+        dq0.p[i] = dq1;
       }
-      const int r = p - li.t0;  // -2 .. t1-t0+1
-      if (r == -2) {
-        wm2 = wp;
-      } else if (r == -1) {
-        wm1 = wp;
-        ccm1 = ccp;
-      } else if (r == 0) {
-        w0 = wp;
-        cc0 = ccp;
-      } else if (r == 1) {
-        w1 = wp;
-        // -1/2 of the face speed 0.5 (cc[t-1] + cc[t])
-        const float hcc = -0.25f * (ccm1 + cc0);
-        const float2 hcc2 = vs<float2>(hcc);
+      {
+        const float dq1 = dqq_t(w0.s, w1.s, wp.s, a.ep);
+        const float F1 = flux_t(w0.s, w1.s, dq0.s, dq1, hcc, a.fh);
+        dF.s = vsub(F1, F0.s);
+        F0.s = F1;
+        dq0.s = dq1;
+      }
+      w0 = w1;
+      w1 = wp;
+      cc0 = cc1;
+      cc1 = ccp;
+      if (active) {
+        const int x0 = DIR == 0 ? t : li.u;
+        const int x1 = DIR == 0 ? li.u : t;
+        const int cell = cell_of(g, x0, x1, k);
+        const int o = tid + 2;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          const float2 dqm = dqq_t(wm2.p[i], wm1.p[i], w0.p[i], ep2);
-          dq0.p[i] = dqq_t(wm1.p[i], w0.p[i], w1.p[i], ep2);
-          F0.p[i] = flux_t(wm1.p[i], w0.p[i], dqm, dq0.p[i], hcc2, fh2);
-        }
-        const float dqm = dqq_t(wm2.s, wm1.s, w0.s, a.ep);
-        dq0.s = dqq_t(wm1.s, w0.s, w1.s, a.ep);
-        F0.s = flux_t(wm1.s, w0.s, dqm, dq0.s, hcc, a.fh);
-        cc1 = ccp;
-      } else {
-        // centre cell t = p - 2; its plane sits two slots back
-        const int t = p - 2;
-        const int sc_ = (int)((seq - 2) % LNB);
-        const float *chi = reinterpret_cast<const float *>(sm.slot[sc_] + L_HI);
-        const float *clo = reinterpret_cast<const float *>(sm.slot[sc_] + L_LO);
-        const float *cd = reinterpret_cast<const float *>(sm.slot[sc_] + (DEFER ? L_D : L_LO));
-        const float cct = cc0;  // speed of the centre cell
-        const float hcc = -0.25f * (cc0 + cc1);
-        const float2 hcc2 = vs<float2>(hcc);
-        W9 dF;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float2 dq1 = dqq_t(w0.p[i], w1.p[i], wp.p[i], ep2);
-          const float2 F1 = flux_t(w0.p[i], w1.p[i], dq0.p[i], dq1, hcc2, fh2);
-          dF.p[i] = vsub(F1, F0.p[i]);
-          F0.p[i] = F1;
-          dq0.p[i] = dq1;
+          const int f0 = field_of(2 * i), f1 = field_of(2 * i + 1);
+          float2 h = make_float2(chi[f0 * LBOX + o], chi[f1 * LBOX + o]);
+          float2 l = make_float2(clo[f0 * LBOX + o], clo[f1 * LBOX + o]);
+          if (DEFER) {
+            // the centre's U^{n+1} pair, formed again from its slot
+            if (i == 0) {
+              last_stage_field<RO>(h.x, l.x, cd[RO * LBOX + o], dt4, decay4, h.x, l.x);
+              last_stage_field<MX>(h.y, l.y, cd[MX * LBOX + o], dt4, decay4, h.y, l.y);
+            } else if (i == 1) {
+              last_stage_field<MY>(h.x, l.x, cd[MY * LBOX + o], dt4, decay4, h.x, l.x);
+              last_stage_field<MZ>(h.y, l.y, cd[MZ * LBOX + o], dt4, decay4, h.y, l.y);
+            } else if (i == 2) {
+              last_stage_field<BX>(h.x, l.x, cd[BX * LBOX + o], dt4, decay4, h.x, l.x);
+              last_stage_field<BY>(h.y, l.y, cd[BY * LBOX + o], dt4, decay4, h.y, l.y);
+            } else {
+              last_stage_field<BZ>(h.x, l.x, cd[BZ * LBOX + o], dt4, decay4, h.x, l.x);
+              last_stage_field<PH>(h.y, l.y, cd[PH * LBOX + o], dt4, decay4, h.y, l.y);
+            }
+          }
+          float2 sv, e;
+          two_sum(h, vfma(dF.p[i], mfac2, l), sv, e);
+          // interior only: the shell kernel fills the images
+          a.hi2.f[f0][cell] = sv.x;
+          a.hi2.f[f1][cell] = sv.y;
+          a.lo2.f[f0][cell] = e.x;
+          a.lo2.f[f1][cell] = e.y;
         }
         {
-          const float dq1 = dqq_t(w0.s, w1.s, wp.s, a.ep);
-          const float F1 = flux_t(w0.s, w1.s, dq0.s, dq1, hcc, a.fh);
-          dF.s = vsub(F1, F0.s);
-          F0.s = F1;
-          dq0.s = dq1;
+          float h = chi[ET * LBOX + o], l = clo[ET * LBOX + o];
+          if (DEFER) last_stage_field<ET>(h, l, cd[ET * LBOX + o], dt4, decay4, h, l);
+          float sv, e;
+          two_sum(h, vfma(dF.s, -fac, l), sv, e);
+          a.hi2.f[ET][cell] = sv;
+          a.lo2.f[ET][cell] = e;
         }
-        w0 = w1;
-        w1 = wp;
-        cc0 = cc1;
-        cc1 = ccp;
-        if (active) {
-          const int x0 = DIR == 0 ? t : li.u;
-          const int x1 = DIR == 0 ? li.u : t;
-          const int cell = cell_of(g, x0, x1, k);
-          const int o = tid + 2;
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int f0 = field_of(2 * i), f1 = field_of(2 * i + 1);
-            float2 h = make_float2(chi[f0 * LBOX + o], chi[f1 * LBOX + o]);
-            float2 l = make_float2(clo[f0 * LBOX + o], clo[f1 * LBOX + o]);
-            if (DEFER) {
-              // the centre's U^{n+1} pair, formed again from its slot
-              if (i == 0) {
-                last_stage_field<RO>(h.x, l.x, cd[RO * LBOX + o], dt4, decay4, h.x, l.x);
-                last_stage_field<MX>(h.y, l.y, cd[MX * LBOX + o], dt4, decay4, h.y, l.y);
-              } else if (i == 1) {
-                last_stage_field<MY>(h.x, l.x, cd[MY * LBOX + o], dt4, decay4, h.x, l.x);
-                last_stage_field<MZ>(h.y, l.y, cd[MZ * LBOX + o], dt4, decay4, h.y, l.y);
-              } else if (i == 2) {
-                last_stage_field<BX>(h.x, l.x, cd[BX * LBOX + o], dt4, decay4, h.x, l.x);
-                last_stage_field<BY>(h.y, l.y, cd[BY * LBOX + o], dt4, decay4, h.y, l.y);
-              } else {
-                last_stage_field<BZ>(h.x, l.x, cd[BZ * LBOX + o], dt4, decay4, h.x, l.x);
-                last_stage_field<PH>(h.y, l.y, cd[PH * LBOX + o], dt4, decay4, h.y, l.y);
-              }
-            }
-            float2 sv, e;
-            two_sum(h, vfma(dF.p[i], mfac2, l), sv, e);
-            // interior only: the shell kernel fills the images
-            a.hi2.f[f0][cell] = sv.x;
-            a.hi2.f[f1][cell] = sv.y;
-            a.lo2.f[f0][cell] = e.x;
-            a.lo2.f[f1][cell] = e.y;
-          }
-          {
-            float h = chi[ET * LBOX + o], l = clo[ET * LBOX + o];
-            if (DEFER) last_stage_field<ET>(h, l, cd[ET * LBOX + o], dt4, decay4, h, l);
-            float sv, e;
-            two_sum(h, vfma(dF.s, -fac, l), sv, e);
-            a.hi2.f[ET][cell] = sv;
-            a.lo2.f[ET][cell] = e;
-          }
-          if (DEFER) a.cc_out[cell] = cct;  // read by the y and z sweeps
-        }
+        if (DEFER) a.cc_out[cell] = cct;  // read by the y and z sweeps
       }
-      // release the slots this warp is done with: plane p-2 (read for the
-      // cell just finished, or a leading halo plane), and at the item's last
-      // plane the two trailing halo planes
-      __syncwarp();
-      if (lane == 0) {
-        if (r >= 0) mbar_arrive(&sm.empty[(seq - 2) % LNB]);
-        if (p == li.t1 + 1) {
-          mbar_arrive(&sm.empty[(seq - 1) % LNB]);
-          mbar_arrive(&sm.empty[seq % LNB]);
-        }
-      }
+      line_release<DEFER>(sm, seq, lane, p == li.t1 + 1);
     }
   }
 }

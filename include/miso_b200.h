@@ -304,9 +304,8 @@ int miso_b200_set_halo_overlap(miso_b200_handle *h, void *comm_stream);
  * into one pass: each k column of a plane is swept along j and each finished
  * row along k, with the separate sweeps' arithmetic, so the step gives the
  * same bits as the y line sweep followed by the z sweep without writing
- * and re-reading the y-swept state (the z variant is then unused; refused
- * with ERR_STATE for a batch's instances, whose steps keep one hi / lo swap
- * per sweep).  All compute the same step up to FP32 rounding order; the
+ * and re-reading the y-swept state (the z variant is then unused).  All
+ * compute the same step up to FP32 rounding order; the
  * autotuner (miso_b200/autotune.py) times them and keeps the fastest.
  * ERR_STATE on grids that use the simple per-cell kernels only. */
 int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant);

@@ -168,9 +168,10 @@ def autotune(integ, steps: int = 2, use_cache: bool = True) -> dict:
 # ---------------------------------------------------------------------------
 BATCH_CHUNKS = ((64, 128), (32, 64), (16, 32), (16, 16), (8, 16))
 # (RK stage, x sweep, y sweep) variants tried with each chunk pair: the
-# default (deferred last stage, line sweeps); the warp-march x / y sweeps,
+# default (deferred last stage, line x sweep, the y and z sweeps in one
+# pass); the same with the separate sweeps; the warp-march x / y sweeps,
 # whose 32-cell segments fit grids narrower than a line's 128-cell k block
-BATCH_VARIANTS = ((3, 0, 0), (2, 2, 2), (3, 0, 2))
+BATCH_VARIANTS = ((3, 0, 3), (3, 0, 0), (2, 2, 2), (3, 0, 2))
 
 
 def _batch_key(batch) -> str:
@@ -186,7 +187,7 @@ def _batch_key(batch) -> str:
 
 
 def _apply_batch(batch, c: dict):
-    vr, vx, vy = c.get("variants", (3, 0, 0))
+    vr, vx, vy = c.get("variants", (3, 0, 3))
     batch.set_variant(1, vx)
     batch.set_variant(2, vy)
     batch.set_variant(0, vr)

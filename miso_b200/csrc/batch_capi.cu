@@ -101,7 +101,8 @@ struct miso_b200_batch {
     for (auto &v : views) {
       const long long l0 = b200_view_launches(v.h);
       int out_cur = 0;
-      if ((rc = b200_view_step(v.h, cur, &out_cur))) {
+      // each view steps from the set its own last step left it in
+      if ((rc = b200_view_step(v.h, -1, &out_cur))) {
         err = std::string("instance ") + std::to_string(v.index) + ": " +
               miso_b200_last_error(v.h);
         return rc;
@@ -118,15 +119,15 @@ struct miso_b200_batch {
     }
     return rc;
   }
-  // every view's ghost layers from its state in set `cur` (after an upload
-  // or a fill of the whole batch), ordered on the batch's stream
+  // every view's ghost layers from its current state (after an upload or a
+  // fill of the whole batch), ordered on the batch's stream
   int fill_views() {
     if (views.empty()) return MISO_B200_OK;
     int rc = cuda(cudaEventRecord(vfork, stream), "fork views");
     for (size_t s = 0; s < vstreams.size() && !rc; ++s)
       rc = cuda(cudaStreamWaitEvent(vstreams[s], vfork, 0), "fork views");
     for (auto &v : views)
-      if (!rc && (rc = b200_view_fill(v.h, cur)))
+      if (!rc && (rc = b200_view_fill(v.h, b200_view_cur(v.h))))
         err = std::string("instance ") + std::to_string(v.index) + ": " + miso_b200_last_error(v.h);
     int rj = join_views();
     return rc ? rc : rj;
@@ -619,22 +620,26 @@ int miso_b200_batch_upload(miso_b200_batch *b, int index, const double *const q[
     if ((rc = b->cuda(cudaMemcpyAsync(dst, q[f], bytes, cudaMemcpyDefault, b->stream), "upload")))
       return rc;
   }
+  // a view's state goes to the view's own set (with the fused y and z pass
+  // its steps keep one set while the batch's other instances alternate)
+  const bool is_view = b->view_at.size() && b->view_at[index] >= 0;
+  const int set = is_view ? b200_view_cur(b->views[b->view_at[index]].h) : b->cur;
   if (b->split) {
     FieldPtrs<const double> src;
     FieldPtrs<float> h, l;
     for (int f = 0; f < NF; ++f) {
       src.f[f] = b->io64[f];
-      h.f[f] = b->hi[b->cur][f] + in.base;
-      l.f[f] = b->lo[b->cur][f] + in.base;
+      h.f[f] = b->hi[set][f] + in.base;
+      l.f[f] = b->lo[set][f] + in.base;
     }
     launch_s32_to_split(in.g.cells, src, h, l, b->sms, b->stream);
     if ((rc = b->cuda(cudaGetLastError(), "to_split"))) return rc;
   }
   if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "upload synchronize"))) return rc;
-  if (b->view_at.size() && b->view_at[index] >= 0) {
+  if (is_view) {
     // a view's ghost layers and CFL minima follow its new state
     const auto &v = b->views[b->view_at[index]];
-    if ((rc = b200_view_fill(v.h, b->cur))) return b->fail(rc, miso_b200_last_error(v.h));
+    if ((rc = b200_view_fill(v.h, set))) return b->fail(rc, miso_b200_last_error(v.h));
     return b->cuda(cudaStreamSynchronize(b->vstreams[v.lane]), "upload synchronize");
   }
   return MISO_B200_OK;
@@ -645,11 +650,13 @@ int miso_b200_batch_download(miso_b200_batch *b, int index, double *const q[9]) 
   const BatchInst &in = b->insts[index];
   const size_t bytes = (size_t)in.g.cells * sizeof(double);
   int rc;
+  int set = b->cur;  // a view's state sits in the view's own set
   if (b->view_at.size() && b->view_at[index] >= 0) {
     // the lo ghost images of a view lag its interior until a download
     const auto &v = b->views[b->view_at[index]];
+    set = b200_view_cur(v.h);
     if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "download synchronize"))) return rc;
-    if ((rc = b200_view_fresh_lo(v.h, b->cur))) return b->fail(rc, miso_b200_last_error(v.h));
+    if ((rc = b200_view_fresh_lo(v.h, set))) return b->fail(rc, miso_b200_last_error(v.h));
     if ((rc = b->cuda(cudaStreamSynchronize(b->vstreams[v.lane]), "download synchronize")))
       return rc;
   }
@@ -657,8 +664,8 @@ int miso_b200_batch_download(miso_b200_batch *b, int index, double *const q[9]) 
     FieldPtrs<const float> h, l;
     FieldPtrs<double> dst;
     for (int f = 0; f < NF; ++f) {
-      h.f[f] = b->hi[b->cur][f] + in.base;
-      l.f[f] = b->lo[b->cur][f] + in.base;
+      h.f[f] = b->hi[set][f] + in.base;
+      l.f[f] = b->lo[set][f] + in.base;
       dst.f[f] = b->io64[f];
     }
     launch_s32_from_split(in.g.cells, h, l, dst, b->sms, b->stream);
@@ -710,6 +717,8 @@ int miso_b200_batch_run(miso_b200_batch *b, int nsteps, int use_graph) {
   }
   if (!b->graph_exec) {
     const int before = b->cur;
+    std::vector<int> vbefore;  // the views' own sets (restored with the batch's)
+    for (auto &v : b->views) vbefore.push_back(b200_view_cur(v.h));
     const long long l0 = b->launches;
     if ((rc = b->cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal),
                       "begin capture")))
@@ -723,6 +732,7 @@ int miso_b200_batch_run(miso_b200_batch *b, int nsteps, int use_graph) {
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     b->cur = before;
+    for (size_t n = 0; n < b->views.size(); ++n) b200_view_set_cur(b->views[n].h, vbefore[n]);
     const long long kernels = b->launches - l0;
     b->launches = l0;
     if (rc) {

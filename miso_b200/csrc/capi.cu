@@ -266,7 +266,6 @@ struct miso_b200_handle {
   int sms = 148;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  bool is_view = false;  // a batch instance's view: its step keeps the batch's set parity
   std::string err;
 
   void *block = nullptr;  // one allocation holds every device buffer
@@ -1314,7 +1313,6 @@ int miso_b200::b200_view_create(const miso_b200_grid_desc &gd, const miso_b200_p
   }
   h->stream = stream;
   h->own_stream = false;
-  h->is_view = true;
   for (int s = 0; s < 2; ++s)
     for (int f = 0; f < NF; ++f) {
       h->hi[s][f] = hi[s][f];
@@ -1359,14 +1357,13 @@ int miso_b200::b200_view_create(const miso_b200_grid_desc &gd, const miso_b200_p
     delete h;
     return MISO_B200_ERR_STATE;
   }
-  h->av_var[1] = 0;  // one hi / lo swap per sweep, as the batch's other instances
   h->src.kind = 0;
   *out = h;
   return MISO_B200_OK;
 }
 
 int miso_b200::b200_view_step(miso_b200_handle *h, int cur, int *cur_out) {
-  h->cur = cur;
+  if (cur >= 0) h->cur = cur;
   int rc = h->enqueue_cfl();
   if (!rc) rc = h->enqueue_update();
   *cur_out = h->cur;
@@ -1387,6 +1384,10 @@ int miso_b200::b200_view_fresh_lo(miso_b200_handle *h, int cur) {
 }
 
 long long miso_b200::b200_view_launches(const miso_b200_handle *h) { return h->launches; }
+
+int miso_b200::b200_view_cur(const miso_b200_handle *h) { return h->cur; }
+
+void miso_b200::b200_view_set_cur(miso_b200_handle *h, int cur) { h->cur = cur; }
 
 extern "C" {
 
@@ -2084,9 +2085,6 @@ int miso_b200_set_variant(miso_b200_handle *h, int kernel_class, int variant) {
       variant > (kernel_class == 0 || kernel_class == 2 ? 3 : 2))
     return MISO_B200_ERR_ARG;
   if (!h->tiled) return h->fail(MISO_B200_ERR_STATE, "kernel variants apply to 3-D split grids");
-  if (kernel_class == 2 && variant == 3 && h->is_view)
-    return h->fail(MISO_B200_ERR_STATE,
-                   "a batch instance keeps one hi / lo swap per sweep: no fused y and z sweeps");
   if (kernel_class == 0 && variant < 2 && h->src.kind != 0)
     return h->fail(MISO_B200_ERR_STATE, "with a source term the RK stage runs variant 2 or 3");
   if (kernel_class == 0)

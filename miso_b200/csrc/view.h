@@ -20,9 +20,16 @@ int b200_view_create(const miso_b200_grid_desc &gd, const miso_b200_params &pp,
                      cudaStream_t stream, float *const hi[2][NF], float *const lo[2][NF],
                      float *const stg[2][NF], float *cc, size_t pitch_bytes, StepScalars *sc,
                      miso_b200_handle **out);
-// One step (CFL, then the update) with the state in set `cur`; returns the
-// set that holds the new state.
+// One step (CFL, then the update) with the state in set `cur` (cur < 0: the
+// set the view's last step, fill or upload left it in); returns the set that
+// holds the new state.  A view keeps its own set: with the fused y and z
+// pass a step swaps the sets twice, while the batch's other instances swap
+// once per sweep.
 int b200_view_step(miso_b200_handle *h, int cur, int *cur_out);
+// The set that holds the view's current state, and its reset (after a
+// graph capture, which records steps without leaving their effect).
+int b200_view_cur(const miso_b200_handle *h);
+void b200_view_set_cur(miso_b200_handle *h, int cur);
 // The state in set `cur` was replaced: fill its ghosts, forget the CFL minima.
 int b200_view_fill(miso_b200_handle *h, int cur);
 // Bring the lo ghost images up to date (before a download).

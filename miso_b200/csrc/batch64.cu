@@ -10,30 +10,24 @@
 namespace miso_b200 {
 namespace b64 {
 
-struct TileState {
-  BatchInst inst;
-  int idx;
-  int start;
-};
-
-// Thread 0 brings the tile's instance record into shared memory.
-__device__ __forceinline__ void load_tile(const BatchArgs &a, int t, TileState &ts) {
-  if (threadIdx.x == 0) {
-    const BatchTile bt = a.tiles[t];
-    ts.idx = bt.inst;
-    ts.start = bt.start;
-    ts.inst = a.insts[bt.inst];
-  }
-  __syncthreads();
+// A tile's instance record, read by every thread of the CTA from the same
+// addresses (one L1 broadcast): no shared copy and no barrier per tile.
+__device__ __forceinline__ const BatchInst &tile_of(const BatchArgs &a, int t, int &idx,
+                                                    int &start) {
+  const BatchTile bt = a.tiles[t];
+  idx = bt.inst;
+  start = bt.start;
+  return a.insts[bt.inst];
 }
 
 // interior coordinates and local cell index of linear interior index lin
-__device__ __forceinline__ long long decode(const Geom &g, long long lin, int &x0, int &x1,
-                                            int &x2) {
-  x2 = (int)(lin % g.n[2]);
-  const long long r = lin / g.n[2];
-  x1 = (int)(r % g.n[1]);
-  x0 = (int)(r / g.n[1]);
+// (32-bit: an instance holds fewer than 2^31 interior cells, as its tiles'
+// int start indices do)
+__device__ __forceinline__ long long decode(const Geom &g, int lin, int &x0, int &x1, int &x2) {
+  x2 = lin % g.n[2];
+  const int r = lin / g.n[2];
+  x1 = r % g.n[1];
+  x0 = r / g.n[1];
   return (long long)(x0 + g.m[0]) * g.st[0] + (long long)(x1 + g.m[1]) * g.st[1] + x2 + g.m[2];
 }
 
@@ -47,12 +41,11 @@ __device__ __forceinline__ P shift(const P &p, long long base) {
 
 __global__ void __launch_bounds__(BATCH_TILE)
 cfl_kernel(BatchArgs a, FieldPtrs<const double> q) {
-  __shared__ TileState ts;
   __shared__ float red[BATCH_TILE / 32];
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    load_tile(a, t, ts);
-    const BatchInst &in = ts.inst;
-    const long long lin = ts.start + threadIdx.x;
+    int idx, start;
+    const BatchInst &in = tile_of(a, t, idx, start);
+    const int lin = start + threadIdx.x;
     float best = 1.e10f;
     if (lin < in.nint) {
       int x0, x1, x2;
@@ -70,7 +63,7 @@ cfl_kernel(BatchArgs a, FieldPtrs<const double> q) {
       float b = red[0];
       for (int w = 1; w < BATCH_TILE / 32; ++w) b = fminf(b, red[w]);
       // non-negative floats order as their bit patterns
-      atomicMin(a.dtmin + ts.idx, __float_as_uint(b));
+      atomicMin(a.dtmin + idx, __float_as_uint(b));
     }
     __syncthreads();
   }
@@ -98,19 +91,25 @@ __global__ void finalize_kernel(BatchArgs a) {
   }
 }
 
-__global__ void __launch_bounds__(BATCH_TILE)
+// The right-hand side and viscosity kernels run 128-thread CTAs, each thread
+// on two cells of a 256-cell tile: at their ~170 registers three CTAs (12
+// warps) fit an SM, as for the single grid's per-cell kernels, where one
+// 256-thread CTA (8 warps) did.
+constexpr int HALF = BATCH_TILE / 2;
+
+__global__ void __launch_bounds__(HALF, 3)
 rhs_kernel(BatchArgs a, FieldPtrs<const double> o, FieldPtrs<const double> ar,
            FieldPtrs<double> r, int stage) {
-  __shared__ TileState ts;
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    load_tile(a, t, ts);
-    const BatchInst &in = ts.inst;
-    const long long lin = ts.start + threadIdx.x;
+  for (int t2 = blockIdx.x; t2 < 2 * a.ntiles; t2 += gridDim.x) {
+    const int t = t2 >> 1;
+    int idx, start;
+    const BatchInst &in = tile_of(a, t, idx, start);
+    const int lin = start + (t2 & 1) * HALF + threadIdx.x;
     if (lin < in.nint) {
       const Geom &g = in.g;
       int x0, x1, x2;
       const long long c = decode(g, lin, x0, x1, x2);
-      const StepScalars &sc = a.sc[ts.idx];
+      const StepScalars &sc = a.sc[idx];
       double out[NF];
       fp64::rhs_cell(g, shift(o, in.base), shift(ar, in.base), c, sc.dts[stage], sc.ch2,
                      sc.ph_decay[stage], in.gm, out);
@@ -120,17 +119,15 @@ rhs_kernel(BatchArgs a, FieldPtrs<const double> o, FieldPtrs<const double> ar,
 #pragma unroll
       for (int f = 0; f < NF; ++f) store_cell(r.f[f] + in.base, c, nb, im, f, out[f]);
     }
-    __syncthreads();
   }
 }
 
 __global__ void __launch_bounds__(BATCH_TILE)
 cc_kernel(BatchArgs a, FieldPtrs<const double> q, double *cc) {
-  __shared__ TileState ts;
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    load_tile(a, t, ts);
-    const BatchInst &in = ts.inst;
-    const long long lin = ts.start + threadIdx.x;
+    int idx, start;
+    const BatchInst &in = tile_of(a, t, idx, start);
+    const int lin = start + threadIdx.x;
     if (lin < in.nint) {
       const Geom &g = in.g;
       int x0, x1, x2;
@@ -141,24 +138,23 @@ cc_kernel(BatchArgs a, FieldPtrs<const double> q, double *cc) {
       if (nb) make_img(g, x0, x1, x2, im);
       store_cell(cc + in.base, c, nb, im, NF, v);
     }
-    __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(BATCH_TILE)
+__global__ void __launch_bounds__(HALF, 3)
 av_kernel(BatchArgs a, FieldPtrs<const double> q, FieldPtrs<double> r, const double *cc,
           int dir) {
-  __shared__ TileState ts;
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    load_tile(a, t, ts);
-    const BatchInst &in = ts.inst;
-    const long long lin = ts.start + threadIdx.x;
+  for (int t2 = blockIdx.x; t2 < 2 * a.ntiles; t2 += gridDim.x) {
+    const int t = t2 >> 1;
+    int idx, start;
+    const BatchInst &in = tile_of(a, t, idx, start);
+    const int lin = start + (t2 & 1) * HALF + threadIdx.x;
     if (lin < in.nint) {
       const Geom &g = in.g;
       int x0, x1, x2;
       const long long c = decode(g, lin, x0, x1, x2);
       double out[NF];
-      fp64::av_cell(g, shift(q, in.base), cc + in.base, c, dir, a.sc[ts.idx].dt, in.ep, in.fh,
+      fp64::av_cell(g, shift(q, in.base), cc + in.base, c, dir, a.sc[idx].dt, in.ep, in.fh,
                     out);
       const bool nb = near_boundary(g, x0, x1, x2);
       Img im;
@@ -166,18 +162,16 @@ av_kernel(BatchArgs a, FieldPtrs<const double> q, FieldPtrs<double> r, const dou
 #pragma unroll
       for (int f = 0; f < NF; ++f) store_cell(r.f[f] + in.base, c, nb, im, f, out[f]);
     }
-    __syncthreads();
   }
 }
 
 // Write the ghost images of every interior value (after an upload).
 __global__ void __launch_bounds__(BATCH_TILE)
 fill_kernel(BatchArgs a, FieldPtrs<double> q) {
-  __shared__ TileState ts;
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    load_tile(a, t, ts);
-    const BatchInst &in = ts.inst;
-    const long long lin = ts.start + threadIdx.x;
+    int idx, start;
+    const BatchInst &in = tile_of(a, t, idx, start);
+    const int lin = start + threadIdx.x;
     if (lin < in.nint) {
       const Geom &g = in.g;
       int x0, x1, x2;
@@ -192,7 +186,6 @@ fill_kernel(BatchArgs a, FieldPtrs<double> q) {
         }
       }
     }
-    __syncthreads();
   }
 }
 
@@ -207,7 +200,7 @@ void b_finalize(const BatchArgs &a, cudaStream_t st) {
 void b64_rhs(const BatchArgs &a, const FieldPtrs<const double> &o,
              const FieldPtrs<const double> &ar, const FieldPtrs<double> &r, int stage, int grid,
              cudaStream_t st) {
-  b64::rhs_kernel<<<grid, BATCH_TILE, 0, st>>>(a, o, ar, r, stage);
+  b64::rhs_kernel<<<2 * grid, b64::HALF, 0, st>>>(a, o, ar, r, stage);
 }
 void b64_cc(const BatchArgs &a, const FieldPtrs<const double> &q, double *cc, int grid,
             cudaStream_t st) {
@@ -215,7 +208,7 @@ void b64_cc(const BatchArgs &a, const FieldPtrs<const double> &q, double *cc, in
 }
 void b64_av(const BatchArgs &a, const FieldPtrs<const double> &q, const FieldPtrs<double> &r,
             const double *cc, int dir, int grid, cudaStream_t st) {
-  b64::av_kernel<<<grid, BATCH_TILE, 0, st>>>(a, q, r, cc, dir);
+  b64::av_kernel<<<2 * grid, b64::HALF, 0, st>>>(a, q, r, cc, dir);
 }
 void b64_fill(const BatchArgs &a, const FieldPtrs<double> &q, int grid, cudaStream_t st) {
   b64::fill_kernel<<<grid, BATCH_TILE, 0, st>>>(a, q);

@@ -89,6 +89,11 @@ void b64_cc(const BatchArgs &a, const FieldPtrs<const double> &q, double *cc, in
 void b64_av(const BatchArgs &a, const FieldPtrs<const double> &q, const FieldPtrs<double> &r,
             const double *cc, int dir, int grid, cudaStream_t st);
 void b64_fill(const BatchArgs &a, const FieldPtrs<double> &q, int grid, cudaStream_t st);
+// the sweep along the own axes of the 1-D / 2-D instances (b64_av leaves
+// them out): R by warp shuffles over `rows`, C by a march over `rows_c`
+void b64_av_rows(const BatchArgs &a, const RowItem *rows, int nrows, const RowItem *rows_c,
+                 int nrows_c, const FieldPtrs<const double> &q, const FieldPtrs<double> &r,
+                 const double *cc, int dir, int grid, cudaStream_t st);
 
 // FP32 split (conserved hi/lo state)
 void b32_cfl(const BatchArgs &a, const FieldPtrs<const float> &hi, int grid, cudaStream_t st);

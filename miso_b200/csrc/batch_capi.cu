@@ -181,9 +181,16 @@ struct miso_b200_batch {
       // every sweep runs, degenerate ones included: in FP64 the reference's
       // degenerate sweep is a round-off step of its own
       const int src[3] = {2, 0, 1}, dst[3] = {0, 1, 0};
-      for (int d = 0; d < 3; ++d)
+      for (int d = 0; d < 3; ++d) {
+        // 3-D instances and degenerate axes on the tile list; the own axes
+        // of the 1-D / 2-D instances by rows
         b64_av(a, cst(q64[src[d]]), mut(q64[dst[d]]), cc64, d, grid, stream);
-      launches += 2 + 4 + 1 + 3;
+        const int nc = sweep_c[d] ? nrows_c : 0;
+        b64_av_rows(a, d_rows, nrows, d_rows_c, nc, cst(q64[src[d]]), mut(q64[dst[d]]), cc64, d,
+                    grid, stream);
+        launches += 1 + (nrows > 0) + (nc > 0);
+      }
+      launches += 2 + 4 + 1;
     } else {
       if (!cfl_valid) {
         // a replaced state: the minima the last sweep folded in are stale

@@ -152,6 +152,23 @@ __device__ __forceinline__ double av_dflux(const double w[5], double ccl, double
   return f_up - f_dw;
 }
 
+// The limited quantities of cell c as av_cell forms them -- ro, the
+// momenta ro v, B, ph and ro ei -- and its characteristic speed.
+__device__ __forceinline__ void av_load_w(const FieldPtrs<const double> &q, const double *cc,
+                                          long long c, double w[NF], double &ccv) {
+  const double ro = __ldg(q.f[RO] + c);
+  w[0] = ro;
+  w[1] = ro * __ldg(q.f[VX] + c);
+  w[2] = ro * __ldg(q.f[VY] + c);
+  w[3] = ro * __ldg(q.f[VZ] + c);
+  w[4] = __ldg(q.f[BX] + c);
+  w[5] = __ldg(q.f[BY] + c);
+  w[6] = __ldg(q.f[BZ] + c);
+  w[7] = __ldg(q.f[PH] + c);
+  w[8] = ro * __ldg(q.f[EI] + c);
+  ccv = __ldg(cc + c);
+}
+
 // One Runge-Kutta stage for interior cell c: out = orgn + dt * R(argm)
 // (mhd_integrator_host.hpp:106-244, expression by expression).
 // The source's force per volume at cell (i, j, k) (array indices) from the

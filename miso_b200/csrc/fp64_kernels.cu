@@ -87,6 +87,7 @@ av_sweep_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<double> r,
   }
 }
 
+
 // A viscosity sweep marching along the sweep axis: a warp owns 32
 // neighbouring lines (along `lane_ax`) and walks a chunk of L cells of them
 // along `dir`, carrying the limited variables, their slopes and the face
@@ -95,21 +96,6 @@ av_sweep_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<double> r,
 // every dqq_eval and flux_core call are the per-cell sweep's (av_cell), so
 // every output is bit for bit the same.  Interior cells only; ghost cells
 // along `dir` are read as neighbours.
-__device__ __forceinline__ void av_load_w(const FieldPtrs<const double> &q, const double *cc,
-                                          long long c, double w[NF], double &ccv) {
-  const double ro = __ldg(q.f[RO] + c);
-  w[0] = ro;
-  w[1] = ro * __ldg(q.f[VX] + c);
-  w[2] = ro * __ldg(q.f[VY] + c);
-  w[3] = ro * __ldg(q.f[VZ] + c);
-  w[4] = __ldg(q.f[BX] + c);
-  w[5] = __ldg(q.f[BY] + c);
-  w[6] = __ldg(q.f[BZ] + c);
-  w[7] = __ldg(q.f[PH] + c);
-  w[8] = ro * __ldg(q.f[EI] + c);
-  ccv = __ldg(cc + c);
-}
-
 __global__ void __launch_bounds__(128)
 av_march_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<double> r,
                 const double *__restrict__ cc, const StepScalars *__restrict__ sc, int dir,

@@ -32,6 +32,34 @@ def test_batch_fp64_matches_oracle(oracle):
             assert rel_l1(interior(p, out), interior(p, ref)) <= 1e-12, p.name
 
 
+def test_batch_fp64_equals_single_grids():
+    """Every FP64 batch instance evolves bit for bit as its grid on its own
+    handle with the device-held dt (both take the damping factor from the
+    device exp): the row sweeps of the 1-D / 2-D instances (shuffles along
+    the unit-stride axis, a march along the other) and the closed-form
+    degenerate sweeps give the per-cell sweep's bits."""
+    from miso_b200.integrator import Integrator
+    probs = mixed()
+    nsteps = 6
+    with Batch(probs, "fp64") as b:
+        b.upload_all()
+        b.run(nsteps, graph=True)
+        b.sync()
+        dts = b.dt()
+        outs = [b.download(i) for i in range(len(probs))]
+    for i, p in enumerate(probs):
+        integ = Integrator(p.config, p.grid, sign=p.sign, precision="fp64")
+        integ.upload(p.q)
+        integ.apply_boundary_condition()
+        integ.run(nsteps, graph=False)
+        ref = integ.download()
+        dt = integ.last_dt()
+        integ.close()
+        assert dt == dts[i], (p.name, dt, dts[i])
+        a, r = interior(p, outs[i]), interior(p, ref)
+        assert np.array_equal(a, r), (p.name, int(np.sum(a != r)))
+
+
 def test_batch_per_instance_dt(oracle):
     probs = mixed()
     with Batch(probs, "fp64") as b:

@@ -115,18 +115,26 @@ void b32_shell_fill(const BatchArgs &a, const int4 *cells, int n, const FieldPtr
 // `combo` (b32_row_combo) selects the axis pair of every item in `items`
 int b32_row_combo(int ax_r, int ax_c);
 constexpr int ROW_COMBOS = 6;
+// defer (stage 3): write the stage's right-hand side D to `out` and leave
+// the update to the step's first sweep
 void b32_rk_rows(const BatchArgs &a, const RowItem *items, int n, int combo,
                  const FieldPtrs<const float> &prev, const FieldPtrs<const float> &u0,
                  const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
-                 const FieldPtrs<float> &out, float *cc, int stage, int grid, cudaStream_t st);
+                 const FieldPtrs<float> &out, float *cc, int stage, int defer, int grid,
+                 cudaStream_t st);
+// d4.f[0] != nullptr: the first sweep of a step whose last update was
+// deferred -- every cell read is U^{n+1} = (hi, lo) - dt_4 D, and the sweep
+// writes the speed of U^{n+1} to cc_out for the later sweeps
 void b32_av_rows_r(const BatchArgs &a, const RowItem *items, int n,
                    const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
                    const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc,
-                   int dir, int fuse_cfl, int grid, cudaStream_t st);
+                   int dir, int fuse_cfl, const FieldPtrs<const float> &d4, float *cc_out,
+                   int grid, cudaStream_t st);
 void b32_av_rows_c(const BatchArgs &a, const RowItem *items, int n,
                    const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
                    const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc,
-                   int dir, int fuse_cfl, int grid, cudaStream_t st);
+                   int dir, int fuse_cfl, const FieldPtrs<const float> &d4, float *cc_out,
+                   int grid, cudaStream_t st);
 // resident CTAs of the block-tile kernels on `sms` SMs (their persistent grid)
 int b32_block_grid(int sms);
 

@@ -81,15 +81,49 @@ struct StageK {
   float dt, decay, ch2, gm, gm1, cs_fac, vv_fac, ca_fac;
 };
 
+// The last stage's update U^{n+1} = (h, l) - dt D of one cell as a
+// compensated pair (sv, e), the GLM damping on ph, and the speed of the new
+// state, with explicitly rounded operations: the fourth stage forms it, or
+// -- with the update deferred -- the first sweep of the step, for every
+// cell it reads, with the same bits.
+__device__ __forceinline__ void last_update(float dt, float decay, const float h[NF],
+                                            const float l[NF], const float D[NF], float sv[NF],
+                                            float e[NF]) {
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    const float t = __fmaf_rn(-dt, D[f], l[f]);
+    if (f == PH) {
+      float tt;
+      two_sum(h[f], t, sv[f], tt);
+      const float pr = __fmul_rn(sv[f], decay);
+      const float pe = __fmaf_rn(sv[f], decay, -pr);
+      two_sum(pr, __fmaf_rn(tt, decay, pe), sv[f], e[f]);
+    } else {
+      two_sum(h[f], t, sv[f], e[f]);
+    }
+  }
+}
+__device__ __forceinline__ float last_speed(const float sv[NF], float gm, float gm1,
+                                            float cs_fac, float vv_fac, float ca_fac) {
+  float cs, vv, ca, ein;
+  speeds(sv, gm, gm1, cs, vv, ca, ein);
+  return __fmaf_rn(ca, ca_fac, __fmaf_rn(vv, vv_fac, __fmul_rn(cs, cs_fac)));
+}
+
 // write the finished cell `cell` of a stage (centre values A0 / A1; LAST: the
-// fourth stage, which updates hi / lo and writes the speed)
-template <bool LAST>
+// fourth stage, which updates hi / lo and writes the speed -- or with DEFER
+// writes its right-hand side D to `out` and leaves the update to the step's
+// first sweep)
+template <bool LAST, bool DEFER>
 __device__ __forceinline__ void rk_finish(const StageK &k, long long base, int cell,
                                           const float D[NF], const float A0[NF],
                                           const float A1[NF], const FieldPtrs<float> &hi,
                                           const FieldPtrs<float> &lo, const FieldPtrs<float> &out,
                                           float *cc) {
-  if (!LAST) {
+  if (DEFER) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) out.f[f][base + cell] = D[f];
+  } else if (!LAST) {
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
       float v = A0[f] - k.dt * D[f];
@@ -97,25 +131,14 @@ __device__ __forceinline__ void rk_finish(const StageK &k, long long base, int c
       out.f[f][base + cell] = v;
     }
   } else {
-    float sv[NF];
+    float sv[NF], e[NF];
+    last_update(k.dt, k.decay, A0, A1, D, sv, e);
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-      float e;
-      if (f == PH) {
-        float tt;
-        two_sum(A0[f], A1[f] - k.dt * D[f], sv[f], tt);
-        const float pr = sv[f] * k.decay;
-        const float pe = fmaf(sv[f], k.decay, -pr);
-        two_sum(pr, pe + tt * k.decay, sv[f], e);
-      } else {
-        two_sum(A0[f], A1[f] - k.dt * D[f], sv[f], e);
-      }
       hi.f[f][base + cell] = sv[f];
-      lo.f[f][base + cell] = e;
+      lo.f[f][base + cell] = e[f];
     }
-    float cs, vv, ca, ein;
-    speeds(sv, k.gm, k.gm1, cs, vv, ca, ein);
-    cc[base + cell] = cs * k.cs_fac + vv * k.vv_fac + ca * k.ca_fac;
+    cc[base + cell] = last_speed(sv, k.gm, k.gm1, k.cs_fac, k.vv_fac, k.ca_fac);
   }
 }
 
@@ -137,7 +160,7 @@ __device__ __forceinline__ void load_centre(long long base, int cell,
 
 // One row q of a 2-D march: F(q) -> Fn, F(q-1) in F1, F(q-2) in F2;
 // R(q) -> Rn, R(q-2) in R2 (see the file comment for P, N and R).
-template <int AR, int AC, bool LAST>
+template <int AR, int AC, bool LAST, bool DEFER>
 __device__ __forceinline__ void rk_row(const StageK &k, const RowGeo &q,
                                        const RowItem &it, int qrow, int rt, bool lane_out,
                                        const FieldPtrs<const float> &prev,
@@ -169,16 +192,16 @@ __device__ __forceinline__ void rk_row(const StageK &k, const RowGeo &q,
   }
   if (fin) {
     float A0[NF], A1[NF], D[NF];
-    load_centre<LAST>(q.base, ccell, u0, hi, lo, A0, A1);
+    if (!DEFER) load_centre<LAST>(q.base, ccell, u0, hi, lo, A0, A1);
 #pragma unroll
     for (int f = 0; f < NF; ++f)
       D[f] = __fsub_rn(R2[f], __fmul_rn(q.wC, fmaf(-8.f, F1[f], Fn[f])));
-    rk_finish<LAST>(k, q.base, ccell, D, A0, A1, hi, lo, out, cc);
+    rk_finish<LAST, DEFER>(k, q.base, ccell, D, A0, A1, hi, lo, out, cc);
   }
 }
 
 // One item of the Runge-Kutta stage: axes AR (unit stride) and AC (-1: 1-D)
-template <int AR, int AC, bool LAST>
+template <int AR, int AC, bool LAST, bool DEFER>
 __device__ __forceinline__ void rk_item(const RowItem &it, const RowGeo &q, const StageK &k,
                                         const FieldPtrs<const float> &prev,
                                         const FieldPtrs<const float> &u0,
@@ -192,14 +215,14 @@ __device__ __forceinline__ void rk_item(const RowItem &it, const RowGeo &q, cons
     // 1-D: one row
     const int cell = rt * q.sR;
     float A0[NF], A1[NF];
-    if (lane_out) load_centre<LAST>(q.base, cell, u0, hi, lo, A0, A1);
+    if (lane_out && !DEFER) load_centre<LAST>(q.base, cell, u0, hi, lo, A0, A1);
     float u[NF], F[NF], D[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) u[f] = __ldg(prev.f[f] + q.base + cell);
     flux_of<AR < 0 ? 0 : AR>(u, k.gm1, k.ch2, F);
 #pragma unroll
     for (int f = 0; f < NF; ++f) D[f] = q.wR * dR(F[f]);
-    if (lane_out) rk_finish<LAST>(k, q.base, cell, D, A0, A1, hi, lo, out, cc);
+    if (lane_out) rk_finish<LAST, DEFER>(k, q.base, cell, D, A0, A1, hi, lo, out, cc);
     return;
   }
   constexpr int CC = AC < 0 ? 0 : AC;
@@ -208,20 +231,20 @@ __device__ __forceinline__ void rk_item(const RowItem &it, const RowGeo &q, cons
   for (int f = 0; f < NF; ++f) FA[f] = FB[f] = FC[f] = RA[f] = RB[f] = RC[f] = 0.f;
   const int qe = it.c1 + 1;
   for (int qr = it.c0 - 2; qr <= qe; qr += 3) {
-    rk_row<AR, CC, LAST>(k, q, it, qr, rt, lane_out, prev, u0, hi, lo, out, cc, FA, FC, FB, RA,
-                         RB);
+    rk_row<AR, CC, LAST, DEFER>(k, q, it, qr, rt, lane_out, prev, u0, hi, lo, out, cc, FA, FC,
+                                FB, RA, RB);
     if (qr + 1 > qe) break;
-    rk_row<AR, CC, LAST>(k, q, it, qr + 1, rt, lane_out, prev, u0, hi, lo, out, cc, FB, FA, FC,
-                         RB, RC);
+    rk_row<AR, CC, LAST, DEFER>(k, q, it, qr + 1, rt, lane_out, prev, u0, hi, lo, out, cc, FB,
+                                FA, FC, RB, RC);
     if (qr + 2 > qe) break;
-    rk_row<AR, CC, LAST>(k, q, it, qr + 2, rt, lane_out, prev, u0, hi, lo, out, cc, FC, FB, FA,
-                         RC, RA);
+    rk_row<AR, CC, LAST, DEFER>(k, q, it, qr + 2, rt, lane_out, prev, u0, hi, lo, out, cc, FC,
+                                FB, FA, RC, RA);
   }
 }
 
 // Runge-Kutta stage over the items of one axis pair (AR unit-stride axis,
 // AC the other one, -1 for 1-D instances)
-template <int AR, int AC, bool LAST>
+template <int AR, int AC, bool LAST, bool DEFER>
 __global__ void __launch_bounds__(256, 2)
 rk_rows_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const float> prev,
                FieldPtrs<const float> u0, FieldPtrs<float> hi, FieldPtrs<float> lo,
@@ -241,7 +264,7 @@ rk_rows_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const fl
     k.cs_fac = (float)in.cs_fac;
     k.vv_fac = (float)in.vv_fac;
     k.ca_fac = (float)in.ca_fac;
-    rk_item<AR, AC, LAST>(it, q, k, prev, u0, hi, lo, out, cc);
+    rk_item<AR, AC, LAST, DEFER>(it, q, k, prev, u0, hi, lo, out, cc);
   }
 }
 
@@ -263,12 +286,49 @@ __device__ __forceinline__ void cfl_commit(const BatchArgs &a, int inst, float b
   if ((threadIdx.x & 31) == 0) atomicMin(a.dtmin + inst, __float_as_uint(best));
 }
 
+// The first sweep of a step whose last Runge-Kutta update was deferred: the
+// stage's right-hand side D and the speed array the sweep writes for the
+// later sweeps (d4.f[0] == nullptr: no deferred update).
+struct Defer {
+  FieldPtrs<const float> d4;
+  float *cc_out;
+};
+
+// The words of one cell as the sweep reads them: hi / lo of the state, or
+// with a deferred update U^{n+1} formed from them and D, with its speed.
+__device__ __forceinline__ void sweep_cell(const BatchArgs &a, const BatchInst &in, int inst,
+                                           long long at, const FieldPtrs<const float> &hi,
+                                           const FieldPtrs<const float> &lo, const Defer &df,
+                                           const float *cc, float u[NF], float l[NF],
+                                           float &ccv) {
+  if (df.d4.f[0]) {
+    float h[NF], lw[NF], d[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      h[f] = __ldg(hi.f[f] + at);
+      lw[f] = __ldg(lo.f[f] + at);
+      d[f] = __ldg(df.d4.f[f] + at);
+    }
+    const StepScalars &sc = a.sc[inst];
+    last_update((float)sc.dts[3], (float)sc.ph_decay[3], h, lw, d, u, l);
+    ccv = last_speed(u, (float)in.gm, (float)(in.gm - 1.0), (float)in.cs_fac, (float)in.vv_fac,
+                     (float)in.ca_fac);
+  } else {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      u[f] = __ldg(hi.f[f] + at);
+      l[f] = __ldg(lo.f[f] + at);
+    }
+    ccv = cc ? __ldg(cc + at) : 0.f;
+  }
+}
+
 // Viscosity sweep along R (shuffles), or -- for an instance whose axis
 // `dir` is degenerate -- the state copied through unchanged.
 __global__ void __launch_bounds__(256)
 av_rows_r_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const float> hi,
                  FieldPtrs<const float> lo, FieldPtrs<float> hi2, FieldPtrs<float> lo2,
-                 const float *cc, int dir, int fuse_cfl) {
+                 const float *cc, int dir, int fuse_cfl, Defer df) {
   const int lane = threadIdx.x & 31;
   const int nw = (int)((gridDim.x * blockDim.x) >> 5);
   for (int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); w < nitems; w += nw) {
@@ -286,16 +346,12 @@ av_rows_r_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const 
     bool bad = false;
     for (int c = it.c0; c < it.c1; ++c) {
       const int cell = row_cell(q, c, rt);
-      float u[NF], l[NF], w[NW];
-#pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        u[f] = __ldg(hi.f[f] + q.base + cell);
-        l[f] = __ldg(lo.f[f] + q.base + cell);
-      }
+      float u[NF], l[NF], w[NW], ccc;
+      sweep_cell(a, in, it.inst, q.base + cell, hi, lo, df, sweep ? cc : nullptr, u, l, ccc);
+      if (df.d4.f[0] && lane_out) df.cc_out[q.base + cell] = ccc;  // read by the later sweeps
       float dF[NW];
       if (sweep) {
         limited_vars(u, w);
-        const float ccc = __ldg(cc + q.base + cell);
         const float cup = 0.5f * (ccc + __shfl_down_sync(FULL, ccc, 1));
 #pragma unroll
         for (int n = 0; n < NW; ++n) {
@@ -332,7 +388,7 @@ av_rows_r_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const 
 __global__ void __launch_bounds__(256, 2)
 av_rows_c_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const float> hi,
                  FieldPtrs<const float> lo, FieldPtrs<float> hi2, FieldPtrs<float> lo2,
-                 const float *cc, int dir, int fuse_cfl) {
+                 const float *cc, int dir, int fuse_cfl, Defer df) {
   const int lane = threadIdx.x & 31;
   const int nw = (int)((gridDim.x * blockDim.x) >> 5);
   for (int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); w < nitems; w += nw) {
@@ -348,10 +404,15 @@ av_rows_c_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const 
     auto load_w = [&](int row, float w[NW], float &ccv) {
       const int cell = row_cell(q, row, rt);
       float u[NF];
+      if (df.d4.f[0]) {
+        float l[NF];
+        sweep_cell(a, in, it.inst, q.base + cell, hi, lo, df, cc, u, l, ccv);
+      } else {
 #pragma unroll
-      for (int f = 0; f < NF; ++f) u[f] = __ldg(hi.f[f] + q.base + cell);
+        for (int f = 0; f < NF; ++f) u[f] = __ldg(hi.f[f] + q.base + cell);
+        ccv = __ldg(cc + q.base + cell);
+      }
       limited_vars(u, w);
-      ccv = __ldg(cc + q.base + cell);
     };
     // prologue: rows c0-2 .. c0+1 give the slope at c0 and the face flux
     // between c0-1 and c0
@@ -377,11 +438,9 @@ av_rows_c_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const 
       const int ccell = row_cell(q, c, rt);
       float H[NF], L[NF];
       if (active) {
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-          H[f] = __ldg(hi.f[f] + q.base + ccell);
-          L[f] = __ldg(lo.f[f] + q.base + ccell);
-        }
+        float ccv;
+        sweep_cell(a, in, it.inst, q.base + ccell, hi, lo, df, nullptr, H, L, ccv);
+        if (df.d4.f[0]) df.cc_out[q.base + ccell] = ccv;  // read by the later sweeps
       }
       float wp[NW], ccp;
       load_w(c + 2, wp, ccp);
@@ -420,15 +479,19 @@ av_rows_c_kernel(BatchArgs a, const RowItem *items, int nitems, FieldPtrs<const 
 void b32_rk_rows(const BatchArgs &a, const RowItem *items, int n, int combo,
                  const FieldPtrs<const float> &prev, const FieldPtrs<const float> &u0,
                  const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,
-                 const FieldPtrs<float> &out, float *cc, int stage, int grid, cudaStream_t st) {
+                 const FieldPtrs<float> &out, float *cc, int stage, int defer, int grid,
+                 cudaStream_t st) {
   if (n <= 0) return;
-#define MISO_RK_ROWS(R, C)                                                                   \
-  if (stage == 3)                                                                          \
-    b32r::rk_rows_kernel<R, C, true><<<grid, 256, 0, st>>>(a, items, n, prev, u0, hi, lo, out, \
-                                                           cc, stage);                     \
-  else                                                                                     \
-    b32r::rk_rows_kernel<R, C, false><<<grid, 256, 0, st>>>(a, items, n, prev, u0, hi, lo,     \
-                                                            out, cc, stage)
+#define MISO_RK_ROWS(R, C)                                                                    \
+  if (stage == 3 && defer)                                                                  \
+    b32r::rk_rows_kernel<R, C, true, true><<<grid, 256, 0, st>>>(a, items, n, prev, u0, hi,   \
+                                                                 lo, out, cc, stage);         \
+  else if (stage == 3)                                                                      \
+    b32r::rk_rows_kernel<R, C, true, false><<<grid, 256, 0, st>>>(a, items, n, prev, u0, hi,  \
+                                                                  lo, out, cc, stage);        \
+  else                                                                                      \
+    b32r::rk_rows_kernel<R, C, false, false><<<grid, 256, 0, st>>>(a, items, n, prev, u0, hi, \
+                                                                   lo, out, cc, stage)
   switch (combo) {
     case 0: MISO_RK_ROWS(0, -1); break;
     case 1: MISO_RK_ROWS(1, -1); break;
@@ -448,17 +511,21 @@ int b32_row_combo(int ax_r, int ax_c) {
 void b32_av_rows_r(const BatchArgs &a, const RowItem *items, int n,
                    const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
                    const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc,
-                   int dir, int fuse_cfl, int grid, cudaStream_t st) {
+                   int dir, int fuse_cfl, const FieldPtrs<const float> &d4, float *cc_out,
+                   int grid, cudaStream_t st) {
   if (n > 0)
-    b32r::av_rows_r_kernel<<<grid, 256, 0, st>>>(a, items, n, hi, lo, hi2, lo2, cc, dir, fuse_cfl);
+    b32r::av_rows_r_kernel<<<grid, 256, 0, st>>>(a, items, n, hi, lo, hi2, lo2, cc, dir,
+                                                 fuse_cfl, b32r::Defer{d4, cc_out});
 }
 
 void b32_av_rows_c(const BatchArgs &a, const RowItem *items, int n,
                    const FieldPtrs<const float> &hi, const FieldPtrs<const float> &lo,
                    const FieldPtrs<float> &hi2, const FieldPtrs<float> &lo2, const float *cc,
-                   int dir, int fuse_cfl, int grid, cudaStream_t st) {
+                   int dir, int fuse_cfl, const FieldPtrs<const float> &d4, float *cc_out,
+                   int grid, cudaStream_t st) {
   if (n > 0)
-    b32r::av_rows_c_kernel<<<grid, 256, 0, st>>>(a, items, n, hi, lo, hi2, lo2, cc, dir, fuse_cfl);
+    b32r::av_rows_c_kernel<<<grid, 256, 0, st>>>(a, items, n, hi, lo, hi2, lo2, cc, dir,
+                                                 fuse_cfl, b32r::Defer{d4, cc_out});
 }
 
 }  // namespace miso_b200

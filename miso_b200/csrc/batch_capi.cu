@@ -47,6 +47,7 @@ struct miso_b200_batch {
   int nrows = 0, nrows_c = 0;
   int rgrid = 0;
   bool sweep[3] = {false, false, false};  // some instance is non-degenerate along d
+  bool defer_rows = true;  // RK variant 3: the rows' last update deferred into the first sweep
   bool sweep_c[3] = {false, false, false};  // d is the C axis of some 2-D instance
 
   void *block = nullptr;
@@ -203,6 +204,16 @@ struct miso_b200_batch {
       }
       b_finalize(a, stream);
       const int c = cur;
+      // the 1-D / 2-D instances' last Runge-Kutta update deferred into the
+      // step's first sweep (their fourth stage writes its right-hand side D
+      // to stg[1]; the first sweep forms U^{n+1} from hi, lo and D)
+      const bool defer = defer_rows && nrows > 0;
+      int first = -1, last = -1;
+      for (int d = 0; d < 3; ++d)
+        if (sweep[d]) {
+          if (first < 0) first = d;
+          last = d;
+        }
       for (int s = 0; s < 4; ++s) {
         FieldPtrs<const float> prev = s == 0 ? cst(hi[c]) : cst(stg[(s - 1) & 1]);
         if (nbtiles) {
@@ -214,28 +225,30 @@ struct miso_b200_batch {
           const int n = row_off[cb + 1] - row_off[cb];
           if (!n) continue;
           b32_rk_rows(a, d_rows + row_off[cb], n, cb, prev, cst(hi[c]), mut(hi[c]), mut(lo[c]),
-                      mut(stg[s & 1]), cc32, s, rgrid, stream);
+                      mut(stg[s & 1]), cc32, s, defer && s == 3 ? 1 : 0, rgrid, stream);
           ++launches;
         }
         // the block kernels write the interior; images of what the next pass reads
-        if (s < 3) {
+        if (s < 3 || defer) {  // the stage output, or with the deferred update D
           b32_shell_fill(a, d_scells, nscells, mut(stg[s & 1]), NF, -1, stream);
-        } else {
+          ++launches;
+        }
+        if (s == 3 && (!defer || nbtiles)) {  // the block instances' new state and speed
           b32_shell_fill(a, d_scells, nscells, mut(hi[c]), NF, -1, stream);
           FieldPtrs<float> ccf{};
           ccf.f[0] = cc32;
           b32_shell_fill(a, d_scells, nscells, ccf, 1, NF, stream);
-          ++launches;
+          launches += 2;
         }
-        ++launches;
       }
       launches += 1;
-      int last = -1;
-      for (int d = 0; d < 3; ++d)
-        if (sweep[d]) last = d;
+      FieldPtrs<const float> none{};
       for (int d = 0; d < 3; ++d) {
         if (!sweep[d]) continue;  // degenerate for every instance: the state is unchanged
         const int fuse = d == last ? 1 : 0;
+        const bool dd = defer && d == first;  // the rows take the deferred update here
+        const FieldPtrs<const float> d4 = dd ? cst(stg[1]) : none;
+        float *cc_out = dd ? cc32 : nullptr;
         if (nbtiles) {
           b32_av(a, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]), mut(lo[cur ^ 1]), cc32, d, fuse,
                  bgrid, stream);
@@ -243,16 +256,22 @@ struct miso_b200_batch {
         }
         if (nrows) {  // sweeps along R and degenerate ones of the 1-D / 2-D instances
           b32_av_rows_r(a, d_rows, nrows, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]),
-                        mut(lo[cur ^ 1]), cc32, d, fuse, rgrid, stream);
+                        mut(lo[cur ^ 1]), cc32, d, fuse, d4, cc_out, rgrid, stream);
           ++launches;
         }
         if (nrows_c && sweep_c[d]) {  // sweeps along C of the 2-D instances
           b32_av_rows_c(a, d_rows_c, nrows_c, cst(hi[cur]), cst(lo[cur]), mut(hi[cur ^ 1]),
-                        mut(lo[cur ^ 1]), cc32, d, fuse, rgrid, stream);
+                        mut(lo[cur ^ 1]), cc32, d, fuse, d4, cc_out, rgrid, stream);
           ++launches;
         }
         b32_shell_fill(a, d_scells, nscells, mut(hi[cur ^ 1]), NF, -1, stream);
         b32_shell_fill(a, d_scells, nscells, mut(lo[cur ^ 1]), NF, -1, stream);
+        if (dd && d != last) {  // the speed the first sweep wrote, read across faces later
+          FieldPtrs<float> ccf{};
+          ccf.f[0] = cc32;
+          b32_shell_fill(a, d_scells, nscells, ccf, 1, NF, stream);
+          ++launches;
+        }
         cur ^= 1;
         launches += 2;
       }
@@ -781,6 +800,10 @@ int miso_b200_batch_set_chunks(miso_b200_batch *b, int rk_chunk, int av_chunk) {
 
 int miso_b200_batch_set_variant(miso_b200_batch *b, int kernel_class, int variant) {
   if (!b) return MISO_B200_ERR_ARG;
+  if (kernel_class == 0 && (variant < 0 || variant > 3)) return MISO_B200_ERR_ARG;
+  // the 1-D / 2-D instances: RK variant 3 defers their last update into the
+  // step's first sweep (with the same bits), any other keeps it in the stage
+  if (kernel_class == 0) b->defer_rows = variant == 3;
   for (auto &v : b->views) {
     const int rc = miso_b200_set_variant(v.h, kernel_class, variant);
     if (rc) return b->fail(rc, miso_b200_last_error(v.h));

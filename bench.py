@@ -301,13 +301,30 @@ def run_b200(args):
         integ.monitors()
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    d2h_mon = (6 * 8 * sms + 8 * 4 * sms) * 8 if fused else 8 * 4 * sms * 8
+    # the monitors' read-back: the last sweep's per-block sums (6 doubles per
+    # block of the fused y and z pass, 3 CTAs per SM, or of the z sweep, 8
+    # per SM) and the div B kernel's (8 doubles per block, 4 per SM)
+    zparts = (3 if tuning.get("av_y") == 3 else 8) * sms
+    d2h_mon = (6 * zparts + 8 * 4 * sms) * 8 if fused else 8 * 4 * sms * 8
     e2e = {"value": world * cells * K / e2e_s / 1e9, "unit": UNIT,
            "h2d_bytes_per_step": 96, "d2h_bytes_per_step": 96 + d2h_mon,
            "monitors_fused": fused,
            "path": "Integrator.cfl() -> update(dt) -> monitors() per step, host dt"}
     if fused:
         integ.set_monitor_fusion(False)
+    # ---- the reference's own ModelBase::update (mhd_model_base.hpp:57-62):
+    # cfl() -> host dt -> update(dt), no monitors
+    integ.update(integ.cfl())
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        integ.update(integ.cfl())
+    torch.cuda.synchronize()
+    eu_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_update = {"value": world * cells * K / eu_s / 1e9, "unit": UNIT,
+                  "h2d_bytes_per_step": 96, "d2h_bytes_per_step": 96,
+                  "path": "Integrator.cfl() -> update(dt) per step (ModelBase::update), host dt"}
 
     # ---- the same step with the whole FP64 primitive state crossing PCIe
     # both ways every step (pinned host fields, upload -> cfl -> update ->
@@ -414,7 +431,8 @@ def run_b200(args):
             "kernels": {k: {"launches": v["launches"], "ms_per_step": v["ms"] / K,
                             "GBps": v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] else None}
                         for k, v in report.items()},
-            "roofline": roofline, "e2e": e2e, "e2e_host_fields": host_fields, "fp64": fp64, "cpu_baseline": cpu,
+            "roofline": roofline, "e2e": e2e, "e2e_model_update": e2e_update,
+            "e2e_host_fields": host_fields, "fp64": fp64, "cpu_baseline": cpu,
             "clocks": clocks, "batch": batch,
         }
         print(json.dumps(line), flush=True)

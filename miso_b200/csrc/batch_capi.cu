@@ -85,7 +85,7 @@ struct miso_b200_batch {
   struct View {
     int index;
     miso_b200_handle *h;
-    int lane;  // which of the view streams
+    int lane;  // which of the view streams; -1: the batch's own stream (a grid that fills the GPU)
   };
   std::vector<View> views;
   std::vector<int> view_at;  // per instance: its index in `views`, or -1
@@ -95,7 +95,8 @@ struct miso_b200_batch {
 
   int enqueue_views() {
     if (views.empty()) return MISO_B200_OK;
-    int rc = cuda(cudaEventRecord(vfork, stream), "fork views");
+    int rc = MISO_B200_OK;
+    if (!vstreams.empty()) rc = cuda(cudaEventRecord(vfork, stream), "fork views");
     for (size_t s = 0; s < vstreams.size() && !rc; ++s)
       rc = cuda(cudaStreamWaitEvent(vstreams[s], vfork, 0), "fork views");
     if (rc) return rc;
@@ -124,7 +125,7 @@ struct miso_b200_batch {
   // fill of the whole batch), ordered on the batch's stream
   int fill_views() {
     if (views.empty()) return MISO_B200_OK;
-    int rc = cuda(cudaEventRecord(vfork, stream), "fork views");
+    int rc = vstreams.empty() ? MISO_B200_OK : cuda(cudaEventRecord(vfork, stream), "fork views");
     for (size_t s = 0; s < vstreams.size() && !rc; ++s)
       rc = cuda(cudaStreamWaitEvent(vstreams[s], vfork, 0), "fork views");
     for (auto &v : views)
@@ -575,8 +576,17 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
   b->view_at.assign(count, -1);
   int nviews = 0;
   for (int n = 0; n < count; ++n) nviews += b->insts[n].view ? 1 : 0;
+  // A grid large enough to fill the GPU with its own persistent kernels
+  // steps on the batch's stream, in turn with the rest (run beside other
+  // work, its persistent CTAs would not all be resident, and their static
+  // share of the work items would finish unevenly); smaller grids run
+  // concurrently on the view streams.
+  const long long whole_gpu = 1LL << 24;
+  int nsmall = 0;
+  for (int n = 0; n < count; ++n)
+    nsmall += b->insts[n].view && b->insts[n].nint < whole_gpu ? 1 : 0;
   if (nviews) {
-    const int ns = nviews < miso_b200_batch::VIEW_STREAMS ? nviews : miso_b200_batch::VIEW_STREAMS;
+    const int ns = nsmall < miso_b200_batch::VIEW_STREAMS ? nsmall : miso_b200_batch::VIEW_STREAMS;
     bool ok = cudaEventCreateWithFlags(&b->vfork, cudaEventDisableTiming) == cudaSuccess;
     for (int s = 0; s < ns && ok; ++s) {
       cudaStream_t vs = nullptr;
@@ -588,6 +598,7 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
     }
     const size_t pitch = round_up(cells * sizeof(float));
     int rc = ok ? MISO_B200_OK : MISO_B200_ERR_CUDA;
+    int nlane = 0;
     for (int n = 0; n < count && rc == MISO_B200_OK; ++n) {
       const BatchInst &in = b->insts[n];
       if (!in.view) continue;
@@ -598,10 +609,14 @@ int miso_b200_batch_create(int count, const miso_b200_grid_desc *grids,
           lo[s][f] = b->lo[s][f] + in.base;
           stg[s][f] = b->stg[s][f] + in.base;
         }
-      const int lane = (int)b->views.size() % ns;
+      int lane = -1;
+      if (in.nint < whole_gpu) {
+        lane = nlane % ns;
+        ++nlane;
+      }
       miso_b200_handle *vh = nullptr;
-      rc = b200_view_create(grids[n], params[n], b->vstreams[lane], hi, lo, stg,
-                            b->cc32 + in.base, pitch, b->d_sc + n, &vh);
+      rc = b200_view_create(grids[n], params[n], lane >= 0 ? b->vstreams[lane] : b->stream, hi,
+                            lo, stg, b->cc32 + in.base, pitch, b->d_sc + n, &vh);
       if (rc == MISO_B200_OK) {
         b->view_at[n] = (int)b->views.size();
         b->views.push_back({n, vh, lane});
@@ -666,7 +681,8 @@ int miso_b200_batch_upload(miso_b200_batch *b, int index, const double *const q[
     // a view's ghost layers and CFL minima follow its new state
     const auto &v = b->views[b->view_at[index]];
     if ((rc = b200_view_fill(v.h, set))) return b->fail(rc, miso_b200_last_error(v.h));
-    return b->cuda(cudaStreamSynchronize(b->vstreams[v.lane]), "upload synchronize");
+    return b->cuda(cudaStreamSynchronize(v.lane >= 0 ? b->vstreams[v.lane] : b->stream),
+                   "upload synchronize");
   }
   return MISO_B200_OK;
 }
@@ -683,7 +699,8 @@ int miso_b200_batch_download(miso_b200_batch *b, int index, double *const q[9]) 
     set = b200_view_cur(v.h);
     if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "download synchronize"))) return rc;
     if ((rc = b200_view_fresh_lo(v.h, set))) return b->fail(rc, miso_b200_last_error(v.h));
-    if ((rc = b->cuda(cudaStreamSynchronize(b->vstreams[v.lane]), "download synchronize")))
+    if ((rc = b->cuda(cudaStreamSynchronize(v.lane >= 0 ? b->vstreams[v.lane] : b->stream),
+                      "download synchronize")))
       return rc;
   }
   if (b->split) {

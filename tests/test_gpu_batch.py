@@ -84,6 +84,30 @@ def test_batch_rows_deferred_update_bit_identical():
         assert np.array_equal(interior(p, outs[0][0][i]), interior(p, outs[1][0][i])), p.name
 
 
+def test_batch_whole_gpu_view_on_batch_stream():
+    """A 3-D instance large enough to fill the GPU (256^3) steps on the
+    batch's own stream, in turn with the 2-D instances' kernels, not beside
+    them: it still equals its grid stepped alone, bit for bit, through
+    eager and graph-replayed steps and a download."""
+    from miso_b200.integrator import Integrator
+    probs = [P.turbulence(256, seed=4), P.orszag_tang(64)]
+    with Batch(probs, "fp32_split") as b:
+        assert b.views() == 1
+        b.upload_all()
+        b.run(1, graph=False)
+        b.run(2, graph=True)
+        b.sync()
+        big = b.download(0)
+    p = probs[0]
+    integ = Integrator(p.config, p.grid, precision="fp32_split")
+    integ.upload(p.q)
+    integ.apply_boundary_condition()
+    integ.run(3, graph=False)
+    ref = integ.download()
+    integ.close()
+    assert np.array_equal(interior(p, big), interior(p, ref))
+
+
 def test_batch_per_instance_dt(oracle):
     probs = mixed()
     with Batch(probs, "fp64") as b:

@@ -276,6 +276,26 @@ typedef struct miso_b200_halo_ops {
 int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
                        const miso_b200_halo_ops *ops);
 
+/* A source functor of the caller's own for the FP64 form: the reference's
+ * Source concept (src.vx, src.vy, src.vz, src.ei evaluated on the stage's
+ * argument state, mhd_model_base.hpp:131-155), as update_sc4 uses it
+ * (mhd_integrator_host.hpp:134, 151, 168: the forces inside the dt factor
+ * of the momentum equations; 241: src.ei added to the new total energy
+ * outside it).  Before every Runge-Kutta stage `fn` gets the stage's
+ * argument state q[9] (primitive fields, ghosts included, the handle's
+ * field layout) and fills s[0..3] (four arrays of the same layout) with the
+ * four terms of every interior cell; it returns 0, or any other value to
+ * stop the step with MISO_B200_ERR_CALLBACK.  on_host != 0: q and s are
+ * host copies that the library stages (exact, and slow); 0: device arrays,
+ * with the handle's stream as the last argument.  While set it replaces the
+ * built-in source; fn == NULL removes it.  ERR_STATE on the FP32 split form
+ * and on a grid in shards; no graph capture (miso_b200_run with use_graph
+ * refuses, miso_b200_run_until launches the steps from the host). */
+typedef int (*miso_b200_source_fn)(void *user, const double *const q[9], double *const s[4],
+                                   void *stream);
+int miso_b200_set_source_callback(miso_b200_handle *h, miso_b200_source_fn fn, void *user,
+                                  int on_host);
+
 /* Overlap each halo exchange with the pass after it (3-D FP32-split grids on
  * the pipelined Runge-Kutta stage and the line x sweep, the defaults;
  * ERR_STATE otherwise or without a halo exchange).  The exchange callback

@@ -25,6 +25,9 @@ ERR_CALLBACK = -8
 # int (*)(void *user, double *const q[9], void *stream)
 BOUNDARY_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p,
                                ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p)
+# miso_b200_source_fn: (user, const double *const q[9], double *const s[4], stream)
+SOURCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                             ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p)
 
 FP64 = 0
 FP32_SPLIT = 1
@@ -105,6 +108,8 @@ SIGNATURES = {
     "miso_b200_set_mirror_signs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "miso_b200_set_boundary_callback": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                                        ctypes.c_void_p, ctypes.c_int]),
+    "miso_b200_set_source_callback": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                                     ctypes.c_void_p, ctypes.c_int]),
     "miso_b200_get_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int)]),
     "miso_b200_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

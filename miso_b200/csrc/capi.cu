@@ -299,6 +299,12 @@ struct miso_b200_handle {
   // after every pass in place of the mirror faces, which are then marked
   // shared (ext) so the fill leaves them to it; on_host: the set is staged
   // through pinned host memory around the call
+  // a source functor of the caller's (FP64): before every RK stage it fills
+  // src_dev (4 arrays) from the stage's argument state
+  miso_b200_source_fn src_cb = nullptr;
+  void *src_user = nullptr;
+  bool src_host = false;
+  double *src_dev = nullptr, *src_stage = nullptr;  // device terms; host staging (q then s)
   miso_b200_boundary_fn bc_cb = nullptr;
   void *bc_user = nullptr;
   bool bc_host = false;
@@ -581,6 +587,38 @@ struct miso_b200_handle {
     launches += 1;
     return check_launch("magnetosphere boundary");
   }
+  // the caller's source functor on the argument state of the stage at hand
+  // (set `set`): its four terms into src_dev, which the stage kernel reads
+  int src_callback(int set) {
+    int rc = cuda(cudaStreamSynchronize(stream), "synchronize before the source callback");
+    if (rc) return rc;
+    const size_t bytes = (size_t)g.cells * sizeof(double);
+    const double *qp[NF];
+    double *sp[4];
+    for (int f = 0; f < NF; ++f) {
+      if (src_host) {
+        double *dst = src_stage + (size_t)f * g.cells;
+        if ((rc = cuda(cudaMemcpyAsync(dst, q64[set][f], bytes, cudaMemcpyDeviceToHost, stream),
+                       "stage the fields for the source callback")))
+          return rc;
+        qp[f] = dst;
+      } else {
+        qp[f] = q64[set][f];
+      }
+    }
+    for (int t = 0; t < 4; ++t)
+      sp[t] = src_host ? src_stage + (size_t)(NF + t) * g.cells : src_dev + (size_t)t * g.cells;
+    if (src_host && (rc = cuda(cudaStreamSynchronize(stream), "synchronize"))) return rc;
+    const int r = src_cb(src_user, qp, sp, (void *)stream);
+    if (r) return fail(MISO_B200_ERR_CALLBACK, "source callback returned %d", r);
+    if (src_host)
+      for (int t = 0; t < 4; ++t)
+        if ((rc = cuda(cudaMemcpyAsync(src_dev + (size_t)t * g.cells, sp[t], bytes,
+                                       cudaMemcpyHostToDevice, stream),
+                       "return the source terms")))
+          return rc;
+    return MISO_B200_OK;
+  }
   // the caller's boundary functor on the set just written, then the
   // periodic faces (the reference's bc.apply followed by its halo exchange,
   // mhd_integrator_cuda.cuh:396-401)
@@ -793,6 +831,7 @@ struct miso_b200_handle {
       const int seq_a[4] = {0, 1, 2, 1};
       const int seq_r[4] = {1, 2, 1, 2};
       for (int s = 0; s < 4; ++s) {
+        if (src_cb && (rc = src_callback(seq_a[s]))) return rc;
         const int t = tb();
         launch_fp64_rhs_stage(g, c64(0), c64(seq_a[s]), f64(seq_r[s]), sc, s, p.gm, src, sms,
                               stream);
@@ -1406,6 +1445,8 @@ int miso_b200_destroy(miso_b200_handle *h) {
   if (h->block) cudaFree(h->block);
   if (h->blend_block) cudaFree(h->blend_block);
   if (h->bc_stage) cudaFreeHost(h->bc_stage);
+  if (h->src_stage) cudaFreeHost(h->src_stage);
+  if (h->src_dev) cudaFree(h->src_dev);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
   return MISO_B200_OK;
@@ -1513,6 +1554,7 @@ int miso_b200_cfl(miso_b200_handle *h, double *dt_out) {
 
 int miso_b200_set_source(miso_b200_handle *h, int kind, const double *params, int nparams) {
   if (!h) return MISO_B200_ERR_ARG;
+  if (h->src_cb) return h->fail(MISO_B200_ERR_STATE, "a source callback is set");
   if (kind == MISO_B200_SOURCE_NONE) {
     h->src.kind = 0;
     h->src.g = 0.0;
@@ -1631,6 +1673,49 @@ int miso_b200_set_mirror_signs(miso_b200_handle *h, const double *sign) {
   return MISO_B200_OK;
 }
 
+int miso_b200_set_source_callback(miso_b200_handle *h, miso_b200_source_fn fn, void *user,
+                                  int on_host) {
+  if (!h) return MISO_B200_ERR_ARG;
+  const size_t bytes = (size_t)h->g.cells * sizeof(double);
+  if (fn) {
+    if (h->split())
+      return h->fail(MISO_B200_ERR_STATE, "a source callback runs on the FP64 form");
+    if (h->halo_on)
+      return h->fail(MISO_B200_ERR_STATE, "a source callback runs on a single grid");
+    if (!h->src_dev && h->cuda(cudaMalloc((void **)&h->src_dev, 4 * bytes),
+                               "allocate the source terms"))
+      return MISO_B200_ERR_NOMEM;
+    if (on_host && !h->src_stage &&
+        h->cuda(cudaMallocHost((void **)&h->src_stage, (NF + 4) * bytes),
+                "allocate the source callback's host staging"))
+      return MISO_B200_ERR_NOMEM;
+    if (h->cuda(cudaMemsetAsync(h->src_dev, 0, 4 * bytes, h->stream), "clear the source terms"))
+      return MISO_B200_ERR_CUDA;
+    h->src.kind = 2;
+    for (int t = 0; t < 4; ++t) h->src.arr[t] = h->src_dev + (size_t)t * h->g.cells;
+  } else {
+    if (h->src_stage) cudaFreeHost(h->src_stage);
+    if (h->src_dev) {
+      cudaStreamSynchronize(h->stream);
+      cudaFree(h->src_dev);
+    }
+    h->src_stage = nullptr;
+    h->src_dev = nullptr;
+    if (h->src.kind == 2) h->src.kind = 0;
+  }
+  h->src_cb = fn;
+  h->src_user = user;
+  h->src_host = fn && on_host;
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+    h->drop_loop();
+  }
+  return MISO_B200_OK;
+}
+
 int miso_b200_set_boundary_callback(miso_b200_handle *h, miso_b200_boundary_fn fn, void *user,
                                     int on_host) {
   if (!h) return MISO_B200_ERR_ARG;
@@ -1698,7 +1783,8 @@ int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
   if (!h) return MISO_B200_ERR_ARG;
   if (int rc = h->join_xchg()) return rc;
   if (!ops) h->comm = nullptr;
-  if (h->bc_cb) return h->fail(MISO_B200_ERR_STATE, "a boundary callback excludes the halo exchange");
+  if (h->bc_cb || h->src_cb)
+    return h->fail(MISO_B200_ERR_STATE, "a callback excludes the halo exchange");
   if (h->split() && h->mag.on && ops)
     return h->fail(MISO_B200_ERR_STATE,
                    "the split form's magnetosphere boundary runs on a single grid");
@@ -1746,8 +1832,8 @@ int miso_b200_update_device(miso_b200_handle *h) {
 
 int miso_b200_run(miso_b200_handle *h, int nsteps, int use_graph) {
   if (!h || nsteps < 0) return MISO_B200_ERR_ARG;
-  if (h->bc_cb && use_graph)
-    return h->fail(MISO_B200_ERR_STATE, "a boundary callback runs on the host between passes: no graph");
+  if ((h->bc_cb || h->src_cb) && use_graph)
+    return h->fail(MISO_B200_ERR_STATE, "a callback runs on the host between passes: no graph");
   if (h->halo_on)
     return h->fail(MISO_B200_ERR_STATE, "a shard steps with cfl() and update(dt)");
   int rc;
@@ -1940,7 +2026,7 @@ int miso_b200_run_until(miso_b200_handle *h, double *time, double t_end, int max
   *steps_out = 0;
   if (h->halo_on)
     return h->fail(MISO_B200_ERR_STATE, "a shard steps with cfl() and update(dt)");
-  if (h->bc_cb) use_graph = 0;  // a host callback between passes cannot be captured
+  if (h->bc_cb || h->src_cb) use_graph = 0;  // a host callback between passes cannot be captured
   if (!(*time < t_end) || max_steps == 0) return MISO_B200_OK;
   RunState st{*time, t_end, 0, max_steps};
   int rc = h->cuda(cudaMemcpyAsync(h->rs, &st, sizeof st, cudaMemcpyHostToDevice, h->stream),

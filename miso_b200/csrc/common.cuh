@@ -59,9 +59,12 @@ struct Magneto {
 };
 
 struct Source {
-  int kind;  // 0 none, 1 point gravity
+  int kind;  // 0 none, 1 point gravity, 2 a caller's functor (arrays filled per stage)
   double g;  // gravitational constant: force per volume -ro g x / |x|^3
   const double *x, *y, *z;
+  // kind 2: src.vx, src.vy, src.vz and src.ei of every cell for the stage
+  // at hand (arrays of the field layout), filled by the caller's functor
+  const double *arr[4];
 };
 
 // Per-step scalars, resident in device memory so a whole step can run

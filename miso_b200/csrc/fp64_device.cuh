@@ -177,7 +177,11 @@ __device__ __forceinline__ void source_force(const Source &s, const FieldPtrs<co
                                              long long c, int i, int j, int k, double &sx,
                                              double &sy, double &sz) {
   sx = sy = sz = 0.0;
-  if (s.kind == 1) {
+  if (s.kind == 2) {
+    sx = s.arr[0][c];
+    sy = s.arr[1][c];
+    sz = s.arr[2][c];
+  } else if (s.kind == 1) {
     const double X = s.x[i], Y = s.y[j], Z = s.z[k];
     const double rr = sqrt(X * X + Y * Y + Z * Z);
     const double r3 = rr * rr * rr;  // util::pow3
@@ -188,14 +192,20 @@ __device__ __forceinline__ void source_force(const Source &s, const FieldPtrs<co
   }
 }
 
+// The source's energy term src.ei (mhd_integrator_host.hpp:241, added to the
+// new total energy outside the dt factor): 0 for every built-in source.
+__device__ __forceinline__ double source_heat(const Source &s, long long c) {
+  return s.kind == 2 ? s.arr[3][c] : 0.0;
+}
+
 __device__ __forceinline__ void rhs_cell(const Geom &g, const FieldPtrs<const double> &o,
                                          const FieldPtrs<const double> &a, long long c,
                                          double dt, double ch2, double decay, double gm,
                                          double out[NF], double sx = 0.0, double sy = 0.0,
-                                         double sz = 0.0) {
-  // sx, sy, sz: the source's force per volume (0 for EmptySourceTerm,
-  // mhd_model_base.hpp:131-155); src.ei adds 0 for every built-in source
-  const double src = 0.0;
+                                         double sz = 0.0, double se = 0.0) {
+  // sx, sy, sz: the source's force per volume, se its energy term (0 for
+  // EmptySourceTerm, mhd_model_base.hpp:131-155)
+  const double src = se;
     DirTerms X, Y, Z;
     dir_terms(a, c, g.st[0] * g.s[0], 0, g.dsi[0], gm, X);
     dir_terms(a, c, g.st[1] * g.s[1], 1, g.dsi[1], gm, Y);

@@ -41,7 +41,7 @@ rhs_stage_kernel(Geom g, FieldPtrs<const double> o, FieldPtrs<const double> a,
 
     double out[NF], sx, sy, sz;
     source_force(src, a, c, i, j, k, sx, sy, sz);
-    rhs_cell(g, o, a, c, dt, ch2, decay, gm, out, sx, sy, sz);
+    rhs_cell(g, o, a, c, dt, ch2, decay, gm, out, sx, sy, sz, source_heat(src, c));
 #pragma unroll
     for (int f = 0; f < NF; ++f) r.f[f][c] = out[f];
   }

@@ -148,7 +148,9 @@ class Integrator:
         lib, h = self._lib, self._h
         src = cfg.get("source") or {}
         kind = src.get("kind", "none")
-        if kind != "none":
+        if kind == "callback":
+            self.set_source_callback(src["fn"])
+        elif kind != "none":
             kinds = {"point_gravity": 1}
             if kind not in kinds:
                 raise ValueError(f"unknown source kind {kind!r}")
@@ -306,6 +308,43 @@ class Integrator:
         self._bc_cb = _lib.BOUNDARY_FN(trampoline)
         self._check(self._lib.miso_b200_set_boundary_callback(
             self._h, ctypes.cast(self._bc_cb, ctypes.c_void_p), None, 1))
+
+    def set_source_callback(self, fn, on_host: bool = True):
+        """A source functor of the caller's own (FP64 form; the reference's
+        Source concept, mhd_model_base.hpp:131-155): before every
+        Runge-Kutta stage ``fn(q, s)`` gets the stage's argument state ``q``
+        (the 9 primitive fields with ghosts, (9, I, J, K) float64) and fills
+        ``s`` ((4, I, J, K): src.vx, src.vy, src.vz, src.ei of every
+        interior cell) in place.  With ``on_host`` both are numpy arrays over
+        host copies; otherwise ``fn(q, s, stream)`` gets lists of device
+        addresses (9 and 4) and the cudaStream_t of the handle.
+        ``fn=None`` removes it."""
+        if fn is None:
+            self._check(self._lib.miso_b200_set_source_callback(self._h, None, None, 0))
+            self._src_cb = None
+            return
+        shape = tuple(self.grid.shape)
+        cells = int(np.prod(shape))
+
+        def view(p, n):
+            base = ctypes.cast(p, ctypes.POINTER(ctypes.c_double))
+            return np.ctypeslib.as_array(base, shape=(n * cells,)).reshape((n,) + shape)
+
+        def trampoline(user, q, s, stream):
+            try:
+                if on_host:
+                    # the library stages q and then s as consecutive arrays
+                    assert all(q[f] == q[0] + f * cells * 8 for f in range(9))
+                    assert all(s[t] == s[0] + t * cells * 8 for t in range(4))
+                    fn(view(q[0], 9), view(s[0], 4))
+                else:
+                    fn([q[f] for f in range(9)], [s[t] for t in range(4)], stream)
+                return 0
+            except Exception:
+                return 1
+        self._src_cb = _lib.SOURCE_FN(trampoline)
+        self._check(self._lib.miso_b200_set_source_callback(
+            self._h, ctypes.cast(self._src_cb, ctypes.c_void_p), None, int(bool(on_host))))
 
     def arm_timeout_test(self, cycles: int):
         """The next pipelined Runge-Kutta stage waits, with bound ``cycles``,

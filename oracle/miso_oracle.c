@@ -241,13 +241,29 @@ static inline double D3(const double *a, const double *b, const double *e, long 
 /* mhd_integrator_host.hpp:57-247 with the derived arrays of eos.hpp:25-31
  * and lines 64-89.  The source term (src.vx/vy/vz inside dt * (...), src.ei
  * added to the new total energy, lines 134-168 and 241) is the empty one
- * (adds 0.0) or the point gravity of the magnetosphere demo
+ * (adds 0.0), the point gravity of the magnetosphere demo
  * (demo/mhd3d_magnetosphere/src/src.hpp:17-44): force per volume
- * -ro g x / |x|^3 on the stage's argument state, no heating. */
-static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
-                  double *const a[NF], double *const r[NF], double dt, double ch2,
-                  double tau, double *pr, double *bb, double *ht, double *vb) {
+ * -ro g x / |x|^3 on the stage's argument state, no heating -- or a
+ * caller's functor (its four values per cell, from the argument state),
+ * or four constants.  Returns the callback's nonzero status. */
+static int stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
+                 double *const a[NF], double *const r[NF], double dt, double ch2,
+                 double tau, double *pr, double *bb, double *ht, double *vb) {
   const double gm = d->gm;
+  double *s4[4] = {NULL, NULL, NULL, NULL};
+  if (d->source == 2) {
+    double *blk = (double *)malloc(sizeof(double) * 4 * (size_t)g->cells);
+    if (!blk) return -1;
+    for (int q = 0; q < 4; ++q) {
+      s4[q] = blk + (size_t)q * g->cells;
+      for (long n = 0; n < g->cells; ++n) s4[q][n] = 0.0;
+    }
+    const int rc = d->src_fn ? d->src_fn(d->src_user, a, s4) : -1;
+    if (rc) {
+      free(blk);
+      return rc;
+    }
+  }
   for (long n = 0; n < g->cells; ++n) {
     pr[n] = (gm - 1.0) * a[RO][n] * a[EI][n];
     bb[n] = a[BX][n] * a[BX][n] + a[BY][n] * a[BY][n] + a[BZ][n] * a[BZ][n];
@@ -266,8 +282,18 @@ static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
       for (int k = g->m[2]; k < g->t[2] - g->m[2]; ++k) {
         const double dzi = g->daxi[2][k];
         const long c = IDX(g, i, j, k);
-        double sx = src, sy = src, sz = src;
-        if (d->source == 1) {
+        double sx = src, sy = src, sz = src, se = src;
+        if (d->source == 2) {
+          sx = s4[0][c];
+          sy = s4[1][c];
+          sz = s4[2][c];
+          se = s4[3][c];
+        } else if (d->source == 3) {
+          sx = d->src_const[0];
+          sy = d->src_const[1];
+          sz = d->src_const[2];
+          se = d->src_const[3];
+        } else if (d->source == 1) {
           const double X = g->ax[0][i], Y = g->ax[1][j], Z = g->ax[2][k];
           const double rr = sqrt(X * X + Y * Y + Z * Z);
           const double r3 = rr * rr * rr; /* util::pow3 */
@@ -333,10 +359,12 @@ static void stage(const geom *g, const miso_oracle_desc *d, double *const o[NF],
                                       r[VZ][c] * r[VZ][c]) -
                     PII8 * (+r[BX][c] * r[BX][c] + r[BY][c] * r[BY][c] +
                             r[BZ][c] * r[BZ][c]) +
-                    src) / r[RO][c];
+                    se) / r[RO][c];
       }
     }
   }
+  if (s4[0]) free(s4[0]);
+  return 0;
 }
 
 /* ---------------------------------------------------------------------- */
@@ -520,24 +548,29 @@ static void apply_av(const geom *g, const miso_oracle_desc *d, double *const q[N
 }
 
 /* mhd_integrator_host.hpp:258-277 and 337-350. */
-static void update(const geom *g, const miso_oracle_desc *d, double *const q[NF], work *w,
-                   double dt) {
+static int update(const geom *g, const miso_oracle_desc *d, double *const q[NF], work *w,
+                  double dt) {
   const double ch = 0.8 * d->cfl_number * g->min_dxyz / dt;
   const double ch2 = ch * ch;
   const double tau = 2.0 * dt;
-  stage(g, d, q, q, w->rslt, dt / 4.0, ch2, tau, w->pr, w->bb, w->ht, w->vb);
+  int rc;
+  if ((rc = stage(g, d, q, q, w->rslt, dt / 4.0, ch2, tau, w->pr, w->bb, w->ht, w->vb))) return rc;
   copy_fields(g, w->argm, w->rslt);
   fill_ghosts(g, d, w->argm);
-  stage(g, d, q, w->argm, w->rslt, dt / 3.0, ch2, tau, w->pr, w->bb, w->ht, w->vb);
+  if ((rc = stage(g, d, q, w->argm, w->rslt, dt / 3.0, ch2, tau, w->pr, w->bb, w->ht, w->vb)))
+    return rc;
   copy_fields(g, w->argm, w->rslt);
   fill_ghosts(g, d, w->argm);
-  stage(g, d, q, w->argm, w->rslt, dt / 2.0, ch2, tau, w->pr, w->bb, w->ht, w->vb);
+  if ((rc = stage(g, d, q, w->argm, w->rslt, dt / 2.0, ch2, tau, w->pr, w->bb, w->ht, w->vb)))
+    return rc;
   copy_fields(g, w->argm, w->rslt);
   fill_ghosts(g, d, w->argm);
-  stage(g, d, q, w->argm, w->rslt, dt, ch2, tau, w->pr, w->bb, w->ht, w->vb);
+  if ((rc = stage(g, d, q, w->argm, w->rslt, dt, ch2, tau, w->pr, w->bb, w->ht, w->vb)))
+    return rc;
   copy_fields(g, q, w->rslt);
   fill_ghosts(g, d, q);
   apply_av(g, d, q, w, dt);
+  return 0;
 }
 
 /* ---------------------------------------------------------------------- */
@@ -566,10 +599,11 @@ int miso_oracle_stage(const miso_oracle_desc *d, double *const orgn[9],
   if (geom_init(&g, d)) return -1;
   work w;
   if (work_alloc(&w, &g)) { geom_free(&g); return -2; }
-  stage(&g, d, orgn, argm, rslt, dt, ch_divb_square, tau_divb, w.pr, w.bb, w.ht, w.vb);
+  const int rc = stage(&g, d, orgn, argm, rslt, dt, ch_divb_square, tau_divb, w.pr, w.bb, w.ht,
+                       w.vb);
   free(w.block);
   geom_free(&g);
-  return 0;
+  return rc;
 }
 
 int miso_oracle_av(const miso_oracle_desc *d, double *const q[9], double dt) {
@@ -591,10 +625,10 @@ int miso_oracle_update(const miso_oracle_desc *d, double *const q[9], double dt)
   if (work_alloc(&w, &g)) { geom_free(&g); return -2; }
   copy_fields(&g, w.rslt, q);
   copy_fields(&g, w.argm, q);
-  update(&g, d, q, &w, dt);
+  const int rc = update(&g, d, q, &w, dt);
   free(w.block);
   geom_free(&g);
-  return 0;
+  return rc;
 }
 
 int miso_oracle_run(const miso_oracle_desc *d, double *const q[9], int nsteps,
@@ -606,14 +640,15 @@ int miso_oracle_run(const miso_oracle_desc *d, double *const q[9], int nsteps,
   if (fill_first) fill_ghosts(&g, d, q);
   copy_fields(&g, w.rslt, q);
   copy_fields(&g, w.argm, q);
-  for (int n = 0; n < nsteps; ++n) {
+  int rc = 0;
+  for (int n = 0; n < nsteps && !rc; ++n) {
     double dt = cfl(&g, d, q);
     if (dt_out) dt_out[n] = dt;
-    update(&g, d, q, &w, dt);
+    rc = update(&g, d, q, &w, dt);
   }
   free(w.block);
   geom_free(&g);
-  return 0;
+  return rc;
 }
 
 int miso_oracle_axis(const miso_oracle_desc *d, int axis, double *s, double *ds,

@@ -34,7 +34,7 @@ typedef struct miso_oracle_desc {
   double cfl_number;
   double ep, fh;              /* limiter parameters (config_defaults.hpp:24-27) */
   double cs_fac, ca_fac, vv_fac;
-  int source;                 /* 0 EmptySourceTerm, 1 point gravity at the origin */
+  int source;                 /* 0 EmptySourceTerm, 1 point gravity at the origin, 2 a callback, 3 constants */
   double g_grav;              /* its gravitational constant (force -ro g x / |x|^3) */
   /* Boundary: 0 = the mirror / periodic faces above; 1 = the magnetosphere
    * demo's boundary (demo/mhd3d_magnetosphere/src/bc.hpp:39-158): mirror
@@ -47,6 +47,14 @@ typedef struct miso_oracle_desc {
   double ro_floor, pr_floor;         /* floor: ro_floor, pr_floor */
   const double *blend[9];            /* primitive state with ghosts; NULL: zeros */
   int cfl_masked;                    /* 1: the demo's CFL with r <= r_inner masked (timestep.hpp:15-49) */
+  /* source 2: a caller's source functor, evaluated before every stage on
+   * its argument state (the 9 primitive arrays, ghosts included): it fills
+   * src.vx, src.vy, src.vz and src.ei of every cell into s[0..3] (arrays of
+   * the same layout) and returns 0.  source 3: the constants src_const
+   * (vx, vy, vz, ei) in every cell. */
+  int (*src_fn)(void *user, double *const q[9], double *const s[4]);
+  void *src_user;
+  double src_const[4];
 } miso_oracle_desc;
 
 /* Fill every ghost cell of q (9 arrays) from its periodic or mirror image. */

@@ -49,7 +49,31 @@ class Desc(ctypes.Structure):
                 ("sw_vx", ctypes.c_double), ("sw_bz", ctypes.c_double),
                 ("r_inner", ctypes.c_double), ("a0", ctypes.c_double),
                 ("ro_floor", ctypes.c_double), ("pr_floor", ctypes.c_double),
-                ("blend", ctypes.c_void_p * 9), ("cfl_masked", ctypes.c_int)]
+                ("blend", ctypes.c_void_p * 9), ("cfl_masked", ctypes.c_int),
+                ("src_fn", ctypes.c_void_p), ("src_user", ctypes.c_void_p),
+                ("src_const", ctypes.c_double * 4)]
+
+
+# the oracle's source callback: (user, double *const q[9], double *const s[4])
+SOURCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                             ctypes.POINTER(ctypes.c_size_t))
+
+
+def _source_trampoline(fn, shape):
+    """A ctypes callback that hands ``fn`` the argument state (9, I, J, K)
+    and the four source arrays (4, I, J, K) as numpy views."""
+    cells = int(np.prod(shape))
+
+    def view(p):
+        return np.ctypeslib.as_array(ctypes.cast(p, _dp), shape=(cells,)).reshape(shape)
+
+    def tramp(user, q, s):
+        try:
+            fn(np.stack([view(q[f]) for f in range(9)]), [view(s[t]) for t in range(4)])
+            return 0
+        except Exception:
+            return 1
+    return SOURCE_FN(tramp)
 
 
 def make_desc(grid, config, sign=None, blend=None) -> Desc:
@@ -71,8 +95,18 @@ def make_desc(grid, config, sign=None, blend=None) -> Desc:
     d.ep, d.fh = av["ep"], av["fh"]
     d.cs_fac, d.ca_fac, d.vv_fac = av["cs_fac"], av["ca_fac"], av["vv_fac"]
     src = config.get("source") or {}
-    d.source = {"none": 0, "point_gravity": 1}[src.get("kind", "none")]
+    d.source = {"none": 0, "point_gravity": 1, "callback": 2,
+                "constant": 3}[src.get("kind", "none")]
     d.g_grav = float(src.get("g", 0.0))
+    if d.source == 3:
+        for t, v in enumerate(src["values"]):
+            d.src_const[t] = float(v)
+    elif d.source == 2:
+        # fn(q, s): q the stage's argument state (9, I, J, K), s a list of the
+        # four (I, J, K) arrays to fill (src.vx, src.vy, src.vz, src.ei)
+        cb = _source_trampoline(src["fn"], tuple(grid.shape))
+        d.src_fn = ctypes.cast(cb, ctypes.c_void_p).value
+        d._cb = cb  # the callback outlives the call
     bnd = config.get("boundary") or {}
     if bnd.get("kind", "faces") == "magnetosphere":
         sw, ms, fl = config["solar_wind"], config["magnetosphere"], config["floor"]

@@ -205,6 +205,21 @@ struct PointGravity {
   Real ei(mhd::FieldsView<const Real>, int, int, int) const { return 0.0; }
 };
 
+// Four constants as a functor of the reference's Source concept
+// (mhd_model_base.hpp:131-155): src.vx, src.vy, src.vz and src.ei of every
+// cell, whatever the state -- the descriptor's source 3, which pins where
+// update_sc4 adds each term (mhd_integrator_host.hpp:134, 151, 168, 241).
+struct ConstSource {
+  Real c[4];
+  explicit ConstSource(const double *v) {
+    for (int q = 0; q < 4; ++q) c[q] = (Real)v[q];
+  }
+  Real vx(mhd::FieldsView<const Real>, int, int, int) const { return c[0]; }
+  Real vy(mhd::FieldsView<const Real>, int, int, int) const { return c[1]; }
+  Real vz(mhd::FieldsView<const Real>, int, int, int) const { return c[2]; }
+  Real ei(mhd::FieldsView<const Real>, int, int, int) const { return c[3]; }
+};
+
 struct Session {
   std::unique_ptr<Env> env;
   std::string path;
@@ -231,6 +246,8 @@ struct Session {
     with_bc([&](auto &b) {
       if (desc.source == 1)
         integ->update(dt, *eos, b, PointGravity(*grid, (Real)desc.g_grav), qq);
+      else if (desc.source == 3)
+        integ->update(dt, *eos, b, ConstSource(desc.src_const), qq);
       else
         integ->update(dt, *eos, b, src, qq);
     });
@@ -359,6 +376,8 @@ int miso_ref_stage(const miso_oracle_desc *d, double *const orgn[9], double *con
     s.integ->tau_divb = tau_divb;
     if (d->source == 1)
       s.integ->update_sc4(dt, *s.eos, PointGravity(*s.grid, d->g_grav), o, a, r);
+    else if (d->source == 3)
+      s.integ->update_sc4(dt, *s.eos, ConstSource(d->src_const), o, a, r);
     else
       s.integ->update_sc4(dt, *s.eos, s.src, o, a, r);
     from_fields(r, rslt);

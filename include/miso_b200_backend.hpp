@@ -32,8 +32,12 @@
 // split form (FP32 arithmetic, compensated hi/lo state on the device).
 //
 // The equation of state must be eos::IdealEOS<Real> (its gm equal to the
-// config's eos.gm), and the source mhd::EmptySourceTerm<Real> or
-// miso_b200::PointGravity<Real>; any other type is a compile-time error.
+// config's eos.gm).  The source: mhd::EmptySourceTerm<Real> and
+// miso_b200::PointGravity<Real> run on the device; any other functor of the
+// reference's Source concept (vx, vy, vz, ei of (FieldsView<const Real>, i,
+// j, k), mhd_model_base.hpp:131-155) is evaluated, in the FP64 form, on host
+// copies of every stage's argument state (miso_b200_set_source_callback):
+// exact, and slow.  The split form refuses such a functor with an exception.
 //
 // Boundary functors (bc.apply(FieldsView<Real>, GridView<const Real>)):
 //   * mhd::EmptyBoundaryCondition<Real>: every non-degenerate axis must be
@@ -435,8 +439,11 @@ struct Integrator<Real, backend::B200> {
   const void *bc_obj_ = nullptr;
   int bc_path_ = 0;
   std::function<void(FieldsView<Real>)> bc_fn_;
-  int src_kind_ = MISO_B200_SOURCE_NONE;
+  int src_kind_ = MISO_B200_SOURCE_NONE;  // or kSourceFunctor
   double src_g_ = 0.0;
+  static constexpr int kSourceFunctor = -1;  // a caller's functor through the callback
+  const void *src_obj_ = nullptr;
+  std::function<void(const double *const *, double *const *)> src_fn_;
 
   void bind(const Fields<Real, backend::B200> &qq) {
     auto &st = *qq.st;
@@ -459,15 +466,26 @@ struct Integrator<Real, backend::B200> {
       throw miso_b200::Error(MISO_B200_ERR_ARG, "the EOS's gm differs from the config's eos.gm");
   }
 
+  // leave the functor path (before a built-in source is set)
+  void drop_source_functor() {
+    if (src_kind_ != kSourceFunctor) return;
+    miso_b200::detail::check(miso_b200_set_source_callback(h_, nullptr, nullptr, 0), h_,
+                             "miso_b200_set_source_callback");
+    src_kind_ = MISO_B200_SOURCE_NONE;
+    src_obj_ = nullptr;
+  }
+
   template <typename Source>
   void configure_source(const Source &src) {
     if constexpr (std::is_same<Source, EmptySourceTerm<Real>>::value) {
+      drop_source_functor();
       if (src_kind_ != MISO_B200_SOURCE_NONE) {
         miso_b200::detail::check(miso_b200_set_source(h_, MISO_B200_SOURCE_NONE, nullptr, 0), h_,
                                  "miso_b200_set_source");
         src_kind_ = MISO_B200_SOURCE_NONE;
       }
     } else if constexpr (std::is_same<Source, miso_b200::PointGravity<Real>>::value) {
+      drop_source_functor();
       const double g = (double)src.g;
       if (src_kind_ != MISO_B200_SOURCE_POINT_GRAVITY || src_g_ != g) {
         miso_b200::detail::check(
@@ -477,9 +495,52 @@ struct Integrator<Real, backend::B200> {
         src_g_ = g;
       }
     } else {
-      static_assert(miso_b200::detail::always_false<Source>::value,
-                    "the B200 backend takes mhd::EmptySourceTerm<Real> or "
-                    "miso_b200::PointGravity<Real> as the source term");
+      // any other functor of the Source concept: its four terms on host
+      // copies of every stage's argument state (the object must outlive the
+      // steps, as the model's own `src` member does)
+      if (!std::is_same<Real, double>::value || precision_ != MISO_B200_FP64)
+        throw miso_b200::Error(MISO_B200_ERR_STATE,
+                               std::string("source functor ") + typeid(Source).name() +
+                                   " runs on the FP64 form only (Real = double)");
+      if (src_kind_ == kSourceFunctor && src_obj_ == (const void *)&src) return;
+      if (src_kind_ != MISO_B200_SOURCE_NONE && src_kind_ != kSourceFunctor) {
+        miso_b200::detail::check(miso_b200_set_source(h_, MISO_B200_SOURCE_NONE, nullptr, 0), h_,
+                                 "miso_b200_set_source");
+      }
+      const Source *sp = &src;
+      src_fn_ = [this, sp](const double *const *q, double *const *s) {
+        const int n0 = grid.i_total, n1 = grid.j_total, n2 = grid.k_total;
+        auto v = [&](int f) {
+          return Array3D<const Real, backend::B200>(reinterpret_cast<const Real *>(q[f]), n0, n1,
+                                                    n2)
+              .view();
+        };
+        const FieldsView<const Real> qq(v(0), v(1), v(2), v(3), v(4), v(5), v(6), v(7), v(8));
+        for (int i = grid.i_margin; i < n0 - grid.i_margin; ++i)
+          for (int j = grid.j_margin; j < n1 - grid.j_margin; ++j)
+            for (int k = grid.k_margin; k < n2 - grid.k_margin; ++k) {
+              const long c = ((long)i * n1 + j) * n2 + k;
+              s[0][c] = (double)sp->vx(qq, i, j, k);
+              s[1][c] = (double)sp->vy(qq, i, j, k);
+              s[2][c] = (double)sp->vz(qq, i, j, k);
+              s[3][c] = (double)sp->ei(qq, i, j, k);
+            }
+      };
+      miso_b200::detail::check(
+          miso_b200_set_source_callback(h_, &Integrator::src_trampoline, this, 1), h_,
+          "miso_b200_set_source_callback");
+      src_kind_ = kSourceFunctor;
+      src_obj_ = (const void *)&src;
+    }
+  }
+
+  static int src_trampoline(void *user, const double *const q[9], double *const s[4], void *) {
+    auto *self = static_cast<Integrator *>(user);
+    try {
+      self->src_fn_(q, s);
+      return 0;
+    } catch (...) {
+      return 1;
     }
   }
 

@@ -4,7 +4,7 @@
 // tests/cpp/Makefile against the reference's headers where they lie; run by
 // tests/test_cpp_modelbase.py.
 //
-//   modelbase_demo <config.yaml> <initial.bin> <bc> <mode>
+//   modelbase_demo <config.yaml> <initial.bin> <bc> <mode> [const:vx,vy,vz,ei]
 //
 // initial.bin: the 9 primitive arrays (ro .. ph, ghosts included) as raw
 // Real values -- the initial condition functor copies them in, so the host
@@ -16,8 +16,11 @@
 // mirror faces and so runs as a host functor after every pass).  mode:
 // "run" (ModelBase::run: initial condition, the time loop to time.tend with
 // snapshots every time.dt_output) or "update:N" (N calls of
-// ModelBase::update, then one snapshot).  It prints the boundary path the
-// backend chose and exits 0, or prints the exception and exits 3.
+// ModelBase::update, then one snapshot).  The optional last argument gives
+// the model a source functor of its own (four constants as the Source
+// concept's vx, vy, vz, ei), which the backend evaluates on host copies of
+// every stage's argument state.  It prints the boundary path the backend
+// chose and exits 0, or prints the exception and exits 3.
 #include <miso/boundary_condition.hpp>
 #include <miso/mhd_model_base.hpp>
 
@@ -97,24 +100,38 @@ struct LoopBoundaryCondition {
   }
 };
 
-template <class BC>
-struct Model : public mhd::ModelBase<Model<BC>, Real, Backend> {
-  using Base = mhd::ModelBase<Model<BC>, Real, Backend>;
+// A source functor of the model's own: four constants (force per volume
+// along x, y, z and the energy term), in the reference's Source concept
+// (mhd_model_base.hpp:131-155).
+struct ConstSource {
+  Real c[4] = {0, 0, 0, 0};
+  Real vx(mhd::FieldsView<const Real>, int, int, int) const { return c[0]; }
+  Real vy(mhd::FieldsView<const Real>, int, int, int) const { return c[1]; }
+  Real vz(mhd::FieldsView<const Real>, int, int, int) const { return c[2]; }
+  Real ei(mhd::FieldsView<const Real>, int, int, int) const { return c[3]; }
+};
+
+template <class BC> struct MakeBC {
+  static BC make(mpi::Shape &s) { return BC{s}; }
+};
+template <> struct MakeBC<mhd::EmptyBoundaryCondition<Real>> {
+  static mhd::EmptyBoundaryCondition<Real> make(mpi::Shape &) { return {}; }
+};
+
+template <class BC, class Src>
+struct Model : public mhd::ModelBase<Model<BC, Src>, Real, Backend> {
+  using Base = mhd::ModelBase<Model<BC, Src>, Real, Backend>;
   eos::IdealEOS<Real> eos;
   FileInitialCondition ic;
   BC bc;
-  mhd::EmptySourceTerm<Real> src;
-  Model(Config &config, const std::string &init)
-      : Base(config), eos(config), ic{init}, bc{this->mpi_shape}, src() {}
+  Src src;
+  Model(Config &config, const std::string &init, const Src &s)
+      : Base(config), eos(config), ic{init}, bc(MakeBC<BC>::make(this->mpi_shape)), src(s) {}
 };
 
-template <>
-Model<mhd::EmptyBoundaryCondition<Real>>::Model(Config &config, const std::string &init)
-    : Base(config), eos(config), ic{init}, bc(), src() {}
-
-template <class BC>
-int drive(Config &config, const std::string &init, const std::string &mode) {
-  Model<BC> model(config, init);
+template <class BC, class Src>
+int drive(Config &config, const std::string &init, const std::string &mode, const Src &s) {
+  Model<BC, Src> model(config, init, s);
   if (mode == "run") {
     model.run();
   } else {
@@ -137,10 +154,25 @@ int main(int argc, char **argv) {
   Env env(argc, argv);
   Config config(argv[1]);
   const std::string init = argv[2], bc = argv[3], mode = argv[4];
+  const std::string source = argc > 5 ? argv[5] : "none";
   try {
-    if (bc == "empty") return drive<mhd::EmptyBoundaryCondition<Real>>(config, init, mode);
-    if (bc == "mirror") return drive<MirrorBoundaryCondition>(config, init, mode);
-    if (bc == "loop") return drive<LoopBoundaryCondition>(config, init, mode);
+    if (source.rfind("const:", 0) == 0) {
+      ConstSource cs;
+      std::string rest = source.substr(6);
+      for (int t = 0; t < 4; ++t) {
+        const size_t cut = rest.find(',');
+        cs.c[t] = (Real)std::stod(rest.substr(0, cut));
+        rest = cut == std::string::npos ? "" : rest.substr(cut + 1);
+      }
+      if (bc == "empty") return drive<mhd::EmptyBoundaryCondition<Real>>(config, init, mode, cs);
+      if (bc == "mirror") return drive<MirrorBoundaryCondition>(config, init, mode, cs);
+      if (bc == "loop") return drive<LoopBoundaryCondition>(config, init, mode, cs);
+    } else {
+      const mhd::EmptySourceTerm<Real> none{};
+      if (bc == "empty") return drive<mhd::EmptyBoundaryCondition<Real>>(config, init, mode, none);
+      if (bc == "mirror") return drive<MirrorBoundaryCondition>(config, init, mode, none);
+      if (bc == "loop") return drive<LoopBoundaryCondition>(config, init, mode, none);
+    }
   } catch (const std::exception &e) {
     std::printf("error: %s\n", e.what());
     return 3;

@@ -276,6 +276,38 @@ typedef struct miso_b200_halo_ops {
 int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
                        const miso_b200_halo_ops *ops);
 
+/* Halo exchange of a grid decomposed along any of i, j and k: the
+ * reference's full Cartesian decomposition (miso/include/miso/grid.hpp:
+ * 279-313, one box per rank; HaloExchanger::apply exchanging the x, y and z
+ * faces, mhd_halo_exchange.hpp:451-621).  ext[2 * axis + side] marks the
+ * low (side 0) / high (side 1) face of axis 0, 1, 2 (i, j, k) as shared
+ * with a neighbour.  The exchange callback takes the axis and is called
+ * once per axis with a shared face, with the contract of
+ * miso_b200_halo_ops.exchange above.  Along i the pointers are the arrays'
+ * own planes; a j or k face is not contiguous, so the library gathers the
+ * `margin` interior layers next to each shared face (the full extent of the
+ * other two axes, ghosts included, in the arrays' memory order) into
+ * buffers of its own before the call and scatters recv_lo / recv_hi into
+ * the ghost layers after it, on `stream` (the reference's pack_y_send /
+ * unpack_y_recv, mhd_halo_exchange.hpp:303-335, 395-424); `bytes` is one
+ * array's face.  A pass is followed by the exchanges the next pass reads:
+ * every axis after a Runge-Kutta stage and after the step's last viscosity
+ * sweep, j after the x sweep, k after the y sweep.  With a shared k face the
+ * y and z sweeps run as two passes (y sweep variant 3 runs as the line y
+ * sweep and the z sweep the handle's z variant), and the overlapped
+ * exchange is refused (it covers i faces only).  min_all, ops == NULL and
+ * the stepping rules as for miso_b200_set_halo, which is this call with
+ * ext = {ext_lo, ext_hi, 0, 0, 0, 0}. */
+typedef struct miso_b200_halo3_ops {
+  int (*exchange)(void *user, int axis, int narrays, size_t bytes, int ext_lo, int ext_hi,
+                  void *const *send_lo, void *const *send_hi, void *const *recv_lo,
+                  void *const *recv_hi, void *stream);
+  int (*min_all)(void *user, double *value);
+  void *user;
+} miso_b200_halo3_ops;
+
+int miso_b200_set_halo3(miso_b200_handle *h, const int ext[6], const miso_b200_halo3_ops *ops);
+
 /* A source functor of the caller's own for the FP64 form: the reference's
  * Source concept (src.vx, src.vy, src.vz, src.ei evaluated on the stage's
  * argument state, mhd_model_base.hpp:131-155), as update_sc4 uses it

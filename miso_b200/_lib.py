@@ -66,6 +66,18 @@ class HaloOps(ctypes.Structure):
                 ("user", ctypes.c_void_p)]
 
 
+# int exchange(user, axis, narrays, bytes, ext_lo, ext_hi, send_lo, send_hi, recv_lo, recv_hi,
+#              stream)
+HALO3_EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_size_t, ctypes.c_int, ctypes.c_int, _vpp, _vpp, _vpp,
+                                     _vpp, ctypes.c_void_p)
+
+
+class Halo3Ops(ctypes.Structure):
+    _fields_ = [("exchange", HALO3_EXCHANGE_FN), ("min_all", HALO_MIN_FN),
+                ("user", ctypes.c_void_p)]
+
+
 # name -> (restype, argtypes); the exported set must match include/miso_b200.h
 SIGNATURES = {
     "miso_b200_create": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(Params),
@@ -92,6 +104,8 @@ SIGNATURES = {
     "miso_b200_set_blend_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "miso_b200_set_halo": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(HaloOps)]),
+    "miso_b200_set_halo3": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(Halo3Ops)]),
     "miso_b200_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_set_chunks": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "miso_b200_set_monitor_fusion": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

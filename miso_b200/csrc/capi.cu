@@ -310,9 +310,15 @@ struct miso_b200_handle {
   bool bc_host = false;
   double *bc_stage = nullptr;
   double *axc[3] = {};
-  // halo exchange with neighbouring shards along i (miso_b200_set_halo)
+  // halo exchange with neighbouring shards (miso_b200_set_halo along i,
+  // miso_b200_set_halo3 along any axis: callback with the axis); a j or k
+  // face travels through face_buf, four regions of face_region bytes (send
+  // lo, send hi, receive lo, receive hi)
   miso_b200_halo_ops halo_ops{};
-  bool halo_on = false;
+  miso_b200_halo3_ops halo3{};
+  bool halo_on = false, halo_axes = false;
+  char *face_buf = nullptr;
+  size_t face_region = 0;
   // overlap of the exchange with the next pass (miso_b200_set_halo_overlap):
   // the callback runs on `comm` after event ev_pass; the next pass finishes
   // the planes that need no ghost first and waits for ev_xchg before the
@@ -351,7 +357,8 @@ struct miso_b200_handle {
   // y sweep = the y and z sweeps fused into one pass (the z variant unused)
   int rk_var = 3;
   int av_var[3] = {0, 3, 0};  // the y and z sweeps fused by default
-  bool fused_yz() const { return av_var[1] == 3; }
+  // (a shared k face needs the y-swept state exchanged before the z sweep)
+  bool fused_yz() const { return av_var[1] == 3 && !g.ext[2][0] && !g.ext[2][1]; }
   // hi / lo set swaps of one step: one per viscosity pass
   int sweep_passes() const {
     return tiled ? (fused_yz() ? 2 : 3) : g.s[0] + g.s[1] + g.s[2];
@@ -685,11 +692,75 @@ struct miso_b200_handle {
     return split() ? halo_f(hi[cur], lo[cur]) : halo_d(q64[0]);
   }
 
-  // Exchange of the i ghost planes of `n` arrays (element size `elem`) with
-  // the neighbouring shards, through the caller's callback; a no-op for a
-  // single grid.
-  int halo_exchange(void *const *arr, int n, size_t elem) {
+  // Exchange of the ghost layers of `n` arrays (element size `elem`) with
+  // the neighbouring shards along the axes of `axes` (bit a: axis a) that
+  // have a shared face, through the caller's callback; a no-op for a single
+  // grid.
+  int halo_exchange(void *const *arr, int n, size_t elem, unsigned axes = 7u) {
     if (!halo_on) return MISO_B200_OK;
+    for (int a = 0; a < 3; ++a) {
+      if (!((axes >> a) & 1u) || !(g.ext[a][0] || g.ext[a][1])) continue;
+      const int rc = a == 0 ? halo_planes(arr, n, elem) : halo_face(a, arr, n, elem);
+      if (rc) return rc;
+    }
+    return MISO_B200_OK;
+  }
+  int halo_call(int axis, int n, size_t bytes, void **slo, void **shi, void **rlo, void **rhi,
+                cudaStream_t xs) {
+    const int r = halo_axes ? halo3.exchange(halo3.user, axis, n, bytes, g.ext[axis][0],
+                                             g.ext[axis][1], slo, shi, rlo, rhi, (void *)xs)
+                            : halo_ops.exchange(halo_ops.user, n, bytes, g.ext[axis][0],
+                                                g.ext[axis][1], slo, shi, rlo, rhi, (void *)xs);
+    if (r) return fail(MISO_B200_ERR_HALO, "halo exchange callback returned %d", r);
+    return MISO_B200_OK;
+  }
+  // a j or k face: its interior layers gathered into face_buf, the
+  // callback, the received layers scattered into the ghost layers
+  int halo_face(int a, void *const *arr, int n, size_t elem) {
+    FaceArgs f;
+    f.n = n;
+    f.axis = a;
+    f.ext[0] = g.ext[a][0];
+    f.ext[1] = g.ext[a][1];
+    for (int x = 0; x < 3; ++x) {
+      f.d[x] = x == a ? g.m[a] : g.t[x];
+      f.st[x] = g.st[x];
+    }
+    f.face = f.d[0] * f.d[1] * f.d[2];
+    const size_t bytes = (size_t)f.face * elem;
+    if ((size_t)n * bytes > face_region)
+      return fail(MISO_B200_ERR_STATE, "face buffers too small for %d arrays", n);
+    void *slo[2 * NF + 1], *shi[2 * NF + 1], *rlo[2 * NF + 1], *rhi[2 * NF + 1];
+    for (int x = 0; x < n; ++x) {
+      f.arr[x] = arr[x];
+      slo[x] = face_buf + (size_t)x * bytes;
+      shi[x] = face_buf + face_region + (size_t)x * bytes;
+      rlo[x] = face_buf + 2 * face_region + (size_t)x * bytes;
+      rhi[x] = face_buf + 3 * face_region + (size_t)x * bytes;
+    }
+    // interior layers m .. 2m-1 and n .. n+m-1 out; ghost layers 0 .. m-1
+    // and n+m .. n+2m-1 in
+    f.pack = 1;
+    f.start[0] = g.m[a];
+    f.start[1] = g.n[a];
+    f.buf[0] = face_buf;
+    f.buf[1] = face_buf + face_region;
+    launch_face_copy(f, elem, sms, stream);
+    launches++;
+    int rc = check_launch("face_pack");
+    if (!rc) rc = halo_call(a, n, bytes, slo, shi, rlo, rhi, stream);
+    if (rc) return rc;
+    f.pack = 0;
+    f.start[0] = 0;
+    f.start[1] = g.n[a] + g.m[a];
+    f.buf[0] = face_buf + 2 * face_region;
+    f.buf[1] = face_buf + 3 * face_region;
+    launch_face_copy(f, elem, sms, stream);
+    launches++;
+    return check_launch("face_unpack");
+  }
+  // an i face: `margin` whole planes per array, exchanged in place
+  int halo_planes(void *const *arr, int n, size_t elem) {
     const long long plane = (long long)g.t[1] * g.t[2];
     const int m = g.m[0], ni = g.n[0];
     void *slo[2 * NF + 1], *shi[2 * NF + 1], *rlo[2 * NF + 1], *rhi[2 * NF + 1];
@@ -709,9 +780,7 @@ struct miso_b200_handle {
       if (rc) return rc;
       xs = comm;
     }
-    const int r = halo_ops.exchange(halo_ops.user, n, (size_t)m * plane * elem, g.ext[0][0],
-                                    g.ext[0][1], slo, shi, rlo, rhi, (void *)xs);
-    if (r) return fail(MISO_B200_ERR_HALO, "halo exchange callback returned %d", r);
+    if (int rc = halo_call(0, n, (size_t)m * plane * elem, slo, shi, rlo, rhi, xs)) return rc;
     if (comm) {
       int rc = cuda(cudaEventRecord(ev_xchg, comm), "record exchange event");
       if (rc) return rc;
@@ -733,14 +802,15 @@ struct miso_b200_handle {
     for (int f = 0; f < NF; ++f) arr[f] = set[f];
     return halo_exchange(arr, NF, sizeof(double));
   }
-  int halo_f(float *const *a, float *const *b = nullptr, float *c = nullptr) {
+  int halo_f(float *const *a, float *const *b = nullptr, float *c = nullptr,
+             unsigned axes = 7u) {
     void *arr[2 * NF + 1];
     int n = 0;
     for (int f = 0; f < NF; ++f) arr[n++] = a[f];
     if (b)
       for (int f = 0; f < NF; ++f) arr[n++] = b[f];
     if (c) arr[n++] = c;
-    return halo_exchange(arr, n, sizeof(float));
+    return halo_exchange(arr, n, sizeof(float), axes);
   }
 
   // the lo ghost images catch up with the interior before the state leaves
@@ -985,12 +1055,13 @@ struct miso_b200_handle {
           if ((rc = shell(hi[c], SHELL_FACES_I, cc32, SHELL_FACES))) return rc;
         }
       }
-      // a shard's i ghosts of the stage output (and of hi and cc after the
-      // last stage, read by the x sweep; of D when the update is deferred:
-      // the U^n ghosts are current since the last step's exchange) come from
-      // the neighbours
-      if ((rc = st < 3 || defer ? halo_f(stg[defer && st == 3 ? 1 : st & 1])
-                                : halo_f(hi[c], nullptr, cc32)))
+      // a shard's ghosts of the stage output come from the neighbours; after
+      // the last stage only the i ghosts the x sweep reads: of hi and cc, or
+      // of D when the update is deferred (the U^n ghosts are current since
+      // the last step's exchange)
+      if ((rc = st < 3 ? halo_f(stg[st & 1])
+                : defer ? halo_f(stg[1], nullptr, nullptr, 1u)
+                        : halo_f(hi[c], nullptr, cc32, 1u)))
         return rc;
     }
     for (int d = 0; d < 3; ++d) {
@@ -1079,6 +1150,9 @@ struct miso_b200_handle {
         lo_shell_stale = false;
       }
       cur ^= 1;
+      // a shard's j ghosts of the x-swept state and the speed (read by the y
+      // sweep), its k ghosts of the y-swept state and the speed (z sweep)
+      if (d < 2 && (rc = halo_f(hi[cur], lo[cur], cc32, d == 0 ? 2u : 4u))) return rc;
     }
     // a shard: the step's final state (hi and lo, so that a download needs
     // no exchange) takes its i ghosts from the neighbouring shards
@@ -1447,6 +1521,7 @@ int miso_b200_destroy(miso_b200_handle *h) {
   if (h->bc_stage) cudaFreeHost(h->bc_stage);
   if (h->src_stage) cudaFreeHost(h->src_stage);
   if (h->src_dev) cudaFree(h->src_dev);
+  if (h->face_buf) cudaFree(h->face_buf);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
   return MISO_B200_OK;
@@ -1544,8 +1619,9 @@ int miso_b200_cfl(miso_b200_handle *h, double *dt_out) {
   if (v.err & (ERRBIT_NONFINITE | ERRBIT_TIMEOUT)) return h->read_err();
   double dt = v.dt;
   // a shard: the minimum over all shards, as the reference's MPI_Allreduce
-  if (h->halo_on && h->halo_ops.min_all) {
-    const int r = h->halo_ops.min_all(h->halo_ops.user, &dt);
+  int (*min_all)(void *, double *) = h->halo_axes ? h->halo3.min_all : h->halo_ops.min_all;
+  if (h->halo_on && min_all) {
+    const int r = min_all(h->halo_axes ? h->halo3.user : h->halo_ops.user, &dt);
     if (r) return h->fail(MISO_B200_ERR_HALO, "min_all callback returned %d", r);
   }
   *dt_out = dt;
@@ -1764,6 +1840,8 @@ int miso_b200_set_halo_overlap(miso_b200_handle *h, void *comm_stream) {
     return MISO_B200_OK;
   }
   if (!h->halo_on) return h->fail(MISO_B200_ERR_STATE, "no halo exchange is set");
+  if (h->g.ext[1][0] || h->g.ext[1][1] || h->g.ext[2][0] || h->g.ext[2][1])
+    return h->fail(MISO_B200_ERR_STATE, "the overlapped exchange covers shared i faces only");
   if (!h->tiled || h->rk_var < 2 || h->av_var[0] != 0)
     return h->fail(MISO_B200_ERR_STATE,
                    "the overlapped exchange runs on the pipelined split path "
@@ -1778,30 +1856,68 @@ int miso_b200_set_halo_overlap(miso_b200_handle *h, void *comm_stream) {
   return MISO_B200_OK;
 }
 
-int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
-                       const miso_b200_halo_ops *ops) {
-  if (!h) return MISO_B200_ERR_ARG;
+// miso_b200_set_halo (ops, along i) and miso_b200_set_halo3 (ops3, any
+// axis); ext[2 * axis + side]
+static int set_halo_impl(miso_b200_handle *h, const int *ext, const miso_b200_halo_ops *ops,
+                         const miso_b200_halo3_ops *ops3) {
   if (int rc = h->join_xchg()) return rc;
-  if (!ops) h->comm = nullptr;
+  const bool on = ops != nullptr || ops3 != nullptr;
+  if (!on) h->comm = nullptr;
   if (h->bc_cb || h->src_cb)
     return h->fail(MISO_B200_ERR_STATE, "a callback excludes the halo exchange");
-  if (h->split() && h->mag.on && ops)
+  if (h->split() && h->mag.on && on)
     return h->fail(MISO_B200_ERR_STATE,
                    "the split form's magnetosphere boundary runs on a single grid");
   Geom &g = h->g;
-  if (ops && !ops->exchange) return h->fail(MISO_B200_ERR_ARG, "halo ops without exchange");
-  if (ops && !g.s[0]) return h->fail(MISO_B200_ERR_ARG, "halo exchange needs an i axis of size > 1");
-  h->halo_on = ops != nullptr && (ext_lo || ext_hi);
-  h->halo_ops = ops ? *ops : miso_b200_halo_ops{};
-  for (int side = 0; side < 2; ++side) {
-    const bool ext = h->halo_on && (side == 0 ? ext_lo : ext_hi);
-    g.ext[0][side] = ext ? 1 : 0;
-    // no image across a shared face; elsewhere the descriptor's mirror signs
-    g.negmask[0][side] = 0;
-    if (!ext && !g.periodic[0])
-      for (int f = 0; f < NF; ++f)
-        if (g.sign[0][side][f] < 0) g.negmask[0][side] |= (unsigned short)(1u << f);
+  if ((ops && !ops->exchange) || (ops3 && !ops3->exchange))
+    return h->fail(MISO_B200_ERR_ARG, "halo ops without exchange");
+  bool any = false, jk = false;
+  for (int a = 0; a < 3; ++a) {
+    const bool shared = on && (ext[2 * a] || ext[2 * a + 1]);
+    if (shared && !g.s[a])
+      return h->fail(MISO_B200_ERR_ARG, "a shared face needs an axis of size > 1 (axis %d)", a);
+    any = any || shared;
+    jk = jk || (shared && a > 0);
   }
+  if (jk && h->comm)
+    return h->fail(MISO_B200_ERR_STATE, "the overlapped exchange covers shared i faces only");
+  // face buffers: the largest j or k face of the widest exchange (2 * 9 + 1
+  // float arrays, or 9 double arrays), four regions
+  size_t region = 0;
+  if (jk) {
+    const long long fj = (long long)g.t[0] * g.m[1] * g.t[2];
+    const long long fk = (long long)g.t[0] * g.t[1] * g.m[2];
+    const long long face = fj > fk ? fj : fk;
+    region = (size_t)face * (h->split() ? (2 * NF + 1) * sizeof(float) : NF * sizeof(double));
+    region = (region + 255) / 256 * 256;
+  }
+  if (region != h->face_region) {
+    if (h->face_buf) {
+      if (h->stream) cudaStreamSynchronize(h->stream);
+      cudaFree(h->face_buf);
+    }
+    h->face_buf = nullptr;
+    h->face_region = 0;
+    if (region) {
+      if (h->cuda(cudaMalloc((void **)&h->face_buf, 4 * region), "allocate the face buffers"))
+        return MISO_B200_ERR_NOMEM;
+      h->face_region = region;
+    }
+  }
+  h->halo_on = any;
+  h->halo_axes = ops3 != nullptr;
+  h->halo_ops = ops ? *ops : miso_b200_halo_ops{};
+  h->halo3 = ops3 ? *ops3 : miso_b200_halo3_ops{};
+  for (int a = 0; a < 3; ++a)
+    for (int side = 0; side < 2; ++side) {
+      const bool shared = any && ext[2 * a + side];
+      g.ext[a][side] = shared ? 1 : 0;
+      // no image across a shared face; elsewhere the descriptor's mirror signs
+      g.negmask[a][side] = 0;
+      if (!shared && !g.periodic[a])
+        for (int f = 0; f < NF; ++f)
+          if (g.sign[a][side][f] < 0) g.negmask[a][side] |= (unsigned short)(1u << f);
+    }
   if (h->graph_exec) {
     cudaGraphExecDestroy(h->graph_exec);
     cudaGraphDestroy(h->graph);
@@ -1811,6 +1927,20 @@ int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
   }
   h->partials_valid = false;
   return MISO_B200_OK;
+}
+
+int miso_b200_set_halo(miso_b200_handle *h, int ext_lo, int ext_hi,
+                       const miso_b200_halo_ops *ops) {
+  if (!h) return MISO_B200_ERR_ARG;
+  const int ext[6] = {ext_lo, ext_hi, 0, 0, 0, 0};
+  return set_halo_impl(h, ext, ops, nullptr);
+}
+
+int miso_b200_set_halo3(miso_b200_handle *h, const int ext[6], const miso_b200_halo3_ops *ops) {
+  if (!h) return MISO_B200_ERR_ARG;
+  if (ops && !ext) return h->fail(MISO_B200_ERR_ARG, "no face flags");
+  const int none[6] = {0, 0, 0, 0, 0, 0};
+  return set_halo_impl(h, ops ? ext : none, nullptr, ops);
 }
 
 int miso_b200_update(miso_b200_handle *h, double dt) {

@@ -20,6 +20,7 @@
 // The GLM damping keeps the reference's form ph = (ph0 + dt R) exp(-dt/tau).
 #include "common.cuh"
 #include "kernels_s32.h"
+#include "s32_common.cuh"
 
 namespace miso_b200 {
 namespace s32 {
@@ -273,8 +274,8 @@ __device__ __forceinline__ float cfl_cell64(const FieldPtrs<const float> &u,
 
 __global__ void __launch_bounds__(256)
 cfl_partial_kernel(Geom g, FieldPtrs<const float> u, float *__restrict__ partial,
-                   unsigned int *__restrict__ err, float gm, float cfl_dx, Magneto mg,
-                   FieldPtrs<const float> lo) {
+                   unsigned int *__restrict__ err, float gm, float gm1, float cfl_dx,
+                   Magneto mg, FieldPtrs<const float> lo) {
   const long long nint = (long long)g.n[0] * g.n[1] * g.n[2];
   float best = 1.e10f;
   bool bad = false;
@@ -287,16 +288,14 @@ cfl_partial_kernel(Geom g, FieldPtrs<const float> u, float *__restrict__ partial
     if (mg.on) {
       tv = cfl_cell64(u, lo, c, (double)gm, bad);
     } else {
-      const Cons q = load_cons(u, c);
-      const float inv = 1.0f / q.ro;
-      const float mm = q.m[0] * q.m[0] + q.m[1] * q.m[1] + q.m[2] * q.m[2];
-      const float bb = q.b[0] * q.b[0] + q.b[1] * q.b[1] + q.b[2] * q.b[2];
-      const float e = (q.et - 0.5f * mm * inv - bb * FPII8) * inv;
-      const float cs = sqrtf(gm * (gm - 1.0f) * e);
-      const float vv = sqrtf(mm) * inv;
-      const float ca = sqrtf(bb * inv * FPII4);
+      // the speed as the sweeps that fold the CFL minima in form it
+      float q[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) q[f] = u.f[f][c];
+      float cs, vv, ca, e;
+      s32t::speeds(q, gm, gm1, cs, vv, ca, e);
       tv = cs + vv + ca;
-      bad |= !(q.ro > 0.0f) || !(e >= 0.0f) || !isfinite(tv);
+      bad |= !(q[RO] > 0.0f) || !(e >= 0.0f) || !isfinite(tv);
     }
     if (mg.mask_cfl) {
       // the magnetosphere demo's CFL (timestep.hpp:15-49): the sphere
@@ -483,7 +482,7 @@ void launch_s32_cfl_partial(const Geom &g, const FieldPtrs<const float> &u, floa
                             cudaStream_t st, const Magneto &mg,
                             const FieldPtrs<const float> &lo) {
   s32::cfl_partial_kernel<<<nparts, 256, 0, st>>>(g, u, partial, &sc->err, (float)gm,
-                                                  (float)cfl_dx, mg, lo);
+                                                  (float)(gm - 1.0), (float)cfl_dx, mg, lo);
 }
 
 void launch_s32_magneto(const Geom &g, const FieldPtrs<float> &hi, const FieldPtrs<float> &lo,

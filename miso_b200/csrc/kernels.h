@@ -30,4 +30,23 @@ template <typename T>
 void launch_fill_ghosts(const Geom &g, const FieldPtrs<T> &q, int nfields, int sms,
                         cudaStream_t st);
 
+// The j or k face halo of a grid in shards (face_pack.cu): pack = 1 copies
+// the `margin` interior layers next to each shared face (ext[side]) of n
+// arrays into buf[side]; pack = 0 copies buf[side] into the ghost layers.
+// A face of one array is the box d0 x d1 x d2 (the margin on `axis`, the
+// full extent elsewhere) starting at layer start[side] of `axis`.
+struct FaceArgs {
+  void *arr[2 * NF + 1];
+  int n;
+  int axis;
+  int pack;
+  int ext[2];
+  int start[2];
+  long long d[3];
+  long long st[3];
+  long long face;  // elements of one array's face
+  void *buf[2];
+};
+void launch_face_copy(const FaceArgs &f, size_t elem, int sms, cudaStream_t st);
+
 }  // namespace miso_b200

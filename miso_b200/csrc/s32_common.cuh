@@ -25,35 +25,41 @@ struct PrimF {
   float v[3], ptot, e_tot, vb;
 };
 
+// Every product and sum below is rounded as written (no contraction left to
+// the compiler): a point's primitive variables and fluxes then get the same
+// bits wherever a kernel forms them -- for a tile's own points and for its
+// halo rows alike -- so that the step does not depend on where tiles, or the
+// shards of a decomposed grid, begin.
 __device__ __forceinline__ void prim(const float u[NF], float gm1, PrimF &p) {
   const float inv = 1.0f / u[RO];
-  p.v[0] = u[MX] * inv;
-  p.v[1] = u[MY] * inv;
-  p.v[2] = u[MZ] * inv;
-  const float bb = u[BX] * u[BX] + u[BY] * u[BY] + u[BZ] * u[BZ];
-  const float pm = bb * FPII8;
-  const float vm = p.v[0] * u[MX] + p.v[1] * u[MY] + p.v[2] * u[MZ];
-  const float pr = gm1 * (u[ET] - 0.5f * vm - pm);
-  p.ptot = pr + pm;
-  p.e_tot = u[ET] + p.ptot;
-  p.vb = p.v[0] * u[BX] + p.v[1] * u[BY] + p.v[2] * u[BZ];
+  p.v[0] = __fmul_rn(u[MX], inv);
+  p.v[1] = __fmul_rn(u[MY], inv);
+  p.v[2] = __fmul_rn(u[MZ], inv);
+  const float bb = __fmaf_rn(u[BZ], u[BZ], __fmaf_rn(u[BY], u[BY], __fmul_rn(u[BX], u[BX])));
+  const float pm = __fmul_rn(bb, FPII8);
+  const float vm =
+      __fmaf_rn(p.v[2], u[MZ], __fmaf_rn(p.v[1], u[MY], __fmul_rn(p.v[0], u[MX])));
+  // p_tot = (gm - 1) (et - vm / 2 - pm) + pm
+  p.ptot = __fmaf_rn(gm1, __fsub_rn(__fmaf_rn(-0.5f, vm, u[ET]), pm), pm);
+  p.e_tot = __fadd_rn(u[ET], p.ptot);
+  p.vb = __fmaf_rn(p.v[2], u[BZ], __fmaf_rn(p.v[1], u[BY], __fmul_rn(p.v[0], u[BX])));
 }
 
 template <int D>
 __device__ __forceinline__ void flux_dir(const float u[NF], const PrimF &p, float ch2,
                                          float F[NF]) {
   const float vd = p.v[D], bd = u[BX + D];
-  const float bd4 = bd * FPII4;
+  const float bd4 = __fmul_rn(bd, FPII4);
   F[RO] = u[MX + D];
 #pragma unroll
   for (int e = 0; e < 3; ++e) {
-    float fm = u[MX + e] * vd - u[BX + e] * bd4;
-    if (e == D) fm += p.ptot;
+    float fm = __fmaf_rn(u[MX + e], vd, -__fmul_rn(u[BX + e], bd4));
+    if (e == D) fm = __fadd_rn(fm, p.ptot);
     F[MX + e] = fm;
-    F[BX + e] = (e == D) ? u[PH] : (vd * u[BX + e] - p.v[e] * bd);
+    F[BX + e] = (e == D) ? u[PH] : __fmaf_rn(vd, u[BX + e], -__fmul_rn(p.v[e], bd));
   }
-  F[ET] = p.e_tot * vd - p.vb * bd4;
-  F[PH] = ch2 * bd;
+  F[ET] = __fmaf_rn(p.e_tot, vd, -__fmul_rn(p.vb, bd4));
+  F[PH] = __fmul_rn(ch2, bd);
 }
 
 // ---------------------------------------------------------------------------
@@ -140,16 +146,23 @@ __device__ __forceinline__ float char_speed(float ro, float mm, float bb, float 
   return __fmaf_rn(ca, ca_fac, __fmaf_rn(vv, vv_fac, __fmul_rn(cs, cs_fac)));
 }
 
-// characteristic-speed pieces of a conserved state
+// |a|^2 of a 3-vector, rounded as written
+__device__ __forceinline__ float norm2(float x, float y, float z) {
+  return __fmaf_rn(z, z, __fmaf_rn(y, y, __fmul_rn(x, x)));
+}
+
+// characteristic-speed pieces of a conserved state (rounded as written, so
+// that the CFL pass and a sweep that folds the CFL minima in agree)
 __device__ __forceinline__ void speeds(const float s[NF], float gm, float gm1, float &cs,
                                        float &vv, float &ca, float &ein) {
   const float inv = 1.0f / s[RO];
-  const float mm = s[MX] * s[MX] + s[MY] * s[MY] + s[MZ] * s[MZ];
-  const float bb = s[BX] * s[BX] + s[BY] * s[BY] + s[BZ] * s[BZ];
-  ein = (s[ET] - 0.5f * mm * inv - bb * FPII8) * inv;
-  cs = sqrtf(fmaxf(gm * gm1 * ein, 0.0f));
-  vv = sqrtf(mm) * inv;
-  ca = sqrtf(bb * inv * FPII4);
+  const float mm = norm2(s[MX], s[MY], s[MZ]);
+  const float bb = norm2(s[BX], s[BY], s[BZ]);
+  // (et - |m|^2 / (2 ro) - |B|^2 / (8 pi)) / ro
+  ein = __fmul_rn(__fmaf_rn(-bb, FPII8, __fmaf_rn(__fmul_rn(-0.5f, mm), inv, s[ET])), inv);
+  cs = sqrtf(fmaxf(__fmul_rn(__fmul_rn(gm, gm1), ein), 0.0f));
+  vv = __fmul_rn(sqrtf(mm), inv);
+  ca = sqrtf(__fmul_rn(__fmul_rn(bb, inv), FPII4));
 }
 
 // ---------------------------------------------------------------------------
@@ -161,11 +174,11 @@ __device__ __forceinline__ void speeds(const float s[NF], float gm, float gm1, f
 __device__ __forceinline__ void gravity_force(const Source &s, float ro, int i, int j, int k,
                                               float &fx, float &fy, float &fz) {
   const float X = (float)s.x[i], Y = (float)s.y[j], Z = (float)s.z[k];
-  const float rr = sqrtf(X * X + Y * Y + Z * Z);
-  const float a = -ro * (float)s.g / (rr * rr * rr);
-  fx = a * X;
-  fy = a * Y;
-  fz = a * Z;
+  const float rr = sqrtf(norm2(X, Y, Z));
+  const float a = __fmul_rn(-ro, (float)s.g) / __fmul_rn(__fmul_rn(rr, rr), rr);
+  fx = __fmul_rn(a, X);
+  fy = __fmul_rn(a, Y);
+  fz = __fmul_rn(a, Z);
 }
 
 // generalized minmod slope of the centre point (limiter.hpp:11-20)
@@ -211,8 +224,9 @@ __device__ __forceinline__ void limited_vars(const float u[NF], float w[NW]) {
   for (int n = 0; n < 7; ++n) w[n] = u[n];
   w[7] = u[PH];
   const float inv = 1.0f / u[RO];
-  w[8] = u[ET] - 0.5f * (u[MX] * u[MX] + u[MY] * u[MY] + u[MZ] * u[MZ]) * inv -
-         (u[BX] * u[BX] + u[BY] * u[BY] + u[BZ] * u[BZ]) * FPII8;
+  // ro e = et - |m|^2 / (2 ro) - |B|^2 / (8 pi), rounded as written
+  const float et_k = __fmaf_rn(__fmul_rn(-0.5f, norm2(u[MX], u[MY], u[MZ])), inv, u[ET]);
+  w[8] = __fmaf_rn(-norm2(u[BX], u[BY], u[BZ]), FPII8, et_k);
 }
 
 // the limited quantities as pairs (ro, mx) (my, mz) (bx, by) (bz, ph) and

@@ -850,8 +850,8 @@ av_zline_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__
         const ZItem z = z_item(a, it, kblocks);
         // wrap copies for the blocks with lanes across a k face (the last
         // lane of block kb sits at k = kb * ZK + 113)
-        const bool wl = g.periodic[2] && z.kb == 0;
-        const bool wr = g.periodic[2] && z.kb * ZK + 4 * 28 + 1 >= nk;
+        const bool wl = g.periodic[2] && !g.ext[2][0] && z.kb == 0;
+        const bool wr = g.periodic[2] && !g.ext[2][1] && z.kb * ZK + 4 * 28 + 1 >= nk;
         const unsigned tx = ZL_TX + (wl ? ZL_TXW : 0u) + (wr ? ZL_TXW : 0u);
         for (int j = z.t0; j < z.t1; ++j, ++s) {
           const int b = s % ZNB;
@@ -898,7 +898,9 @@ av_zline_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__
     if (kk < 0 || kk >= nk) {
       int side;
       const int img = ghost_src(g, 2, kk, side);
-      if (g.periodic[2]) {
+      if (side < 0) {
+        off = kk - (z.kb * ZK - 2);  // a face shared with a neighbour: its ghost cell
+      } else if (g.periodic[2]) {
         region = kk < 0 ? 1 : 2;
         off = img + 2 - (kk < 0 ? xl : 0);
       } else {
@@ -1083,8 +1085,8 @@ av_yz_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CU
         const ZItem z = z_item(a, it, kblocks);
         // wrap copies for the blocks with lanes across a periodic k face
         // (the last lane of block kb sits at k = kb * ZK + 113)
-        const bool wl = g.periodic[2] && z.kb == 0;
-        const bool wr = g.periodic[2] && z.kb * ZK + 4 * 28 + 1 >= nk;
+        const bool wl = g.periodic[2] && !g.ext[2][0] && z.kb == 0;
+        const bool wr = g.periodic[2] && !g.ext[2][1] && z.kb * ZK + 4 * 28 + 1 >= nk;
         const unsigned tx = ZL_TX + (wl ? YZ_TXW : 0u) + (wr ? YZ_TXW : 0u);
         for (int p = z.t0 - 2; p <= z.t1 + 1; ++p, ++s) {
           const int b = s % YZ_NB;
@@ -1139,7 +1141,9 @@ av_yz_kernel(const __grid_constant__ CUtensorMap thi, const __grid_constant__ CU
     if (kk < 0 || kk >= nk) {
       int side;
       const int img = ghost_src(g, 2, kk, side);
-      if (g.periodic[2]) {
+      if (side < 0) {
+        off = kk - (z.kb * ZK - 2);  // a face shared with a neighbour: its ghost cell
+      } else if (g.periodic[2]) {
         region = kk < 0 ? 1 : 2;
         off = img + 2 - (kk < 0 ? xl : 0);
       } else {

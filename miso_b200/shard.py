@@ -1,14 +1,19 @@
-"""A grid decomposed into shards along i, one Integrator per shard.
+"""A grid decomposed into shards, one Integrator per shard.
 
 The reference runs one grid over many GPUs by Cartesian domain
 decomposition (miso/include/miso/grid.hpp:279-313): every rank owns a box
 of the global grid and, after each pass, swaps face halos with its
 neighbours (HaloExchanger, mhd_halo_exchange.hpp:451-621); the CFL time
-step is reduced over all ranks (mhd_integrator_cuda.cuh:476).  Here the
-decomposition is along i, the slowest axis, so a face halo is ``margin``
-whole planes of each array, contiguous in memory: the library hands the
-plane ranges to an exchange callback (``miso_b200_set_halo``) and nothing
-is packed.  Two transports implement the callback:
+step is reduced over all ranks (mhd_integrator_cuda.cuh:476).  A
+decomposition along i alone (``split_grid``) cuts slabs whose face halo is
+``margin`` whole planes of each array, contiguous in memory: the library
+hands the plane ranges to an exchange callback (``miso_b200_set_halo``) and
+nothing is packed.  The full decomposition over i, j and k
+(``split_grid3``, ranks in the row-major order of their coordinates, as
+MPI_Cart_create numbers them, mpi_util.hpp:69-102) goes through
+``miso_b200_set_halo3``, whose callback is called per axis; the library
+packs the j and k faces into contiguous buffers around it.  Two
+transports implement the callbacks:
 
 * ``LocalHalo``: shards of one process on one GPU, each driven by its own
   host thread, all on one CUDA stream; the planes move by device copies.
@@ -32,14 +37,18 @@ import numpy as np
 from .grid import Grid
 from .integrator import Integrator
 
-__all__ = ["ShardSpec", "split_grid", "split_state", "gather", "LocalHalo", "DistHalo",
-           "run_local_shards"]
+__all__ = ["ShardSpec", "split_grid", "split_grid3", "split_state", "gather", "LocalHalo",
+           "DistHalo", "run_local_shards"]
 
 
 @dataclasses.dataclass
 class ShardSpec:
-    """Shard r of a grid split along i: interior planes [i0, i1) of the
-    global grid, and which i faces it shares with a neighbour."""
+    """Shard r of a decomposed grid: interior planes [i0, i1) of the global
+    grid and which i faces it shares with a neighbour; for a decomposition
+    along j or k as well, its coordinate and the shard counts per axis
+    (``coord``, ``dims``), its interior box [lo, hi) per axis and its shared
+    faces ``ext[axis] = (low, high)`` (for a split along i alone these
+    follow from the i fields)."""
     rank: int
     count: int
     i0: int
@@ -47,6 +56,24 @@ class ShardSpec:
     grid: Grid
     ext_lo: bool
     ext_hi: bool
+    dims: tuple = None
+    coord: tuple = None
+    lo: tuple = None
+    hi: tuple = None
+    ext: tuple = None
+
+    def __post_init__(self):
+        if self.dims is None:
+            self.dims = (self.count, 1, 1)
+            self.coord = (self.rank, 0, 0)
+            self.lo = (self.i0, 0, 0)
+            self.hi = (self.i1, self.grid.j_size, self.grid.k_size)
+            self.ext = ((bool(self.ext_lo), bool(self.ext_hi)), (False, False), (False, False))
+
+    @property
+    def axes3(self) -> bool:
+        """Whether a j or k face is shared (the exchange goes per axis)."""
+        return self.dims[1] > 1 or self.dims[2] > 1
 
 
 def _extent(x0: float, n: int, dx: float) -> float:
@@ -89,19 +116,68 @@ def split_grid(grid: Grid, count: int, periodic_x: bool) -> list[ShardSpec]:
     return out
 
 
+def split_grid3(grid: Grid, dims, periodic) -> list[ShardSpec]:
+    """Split ``grid`` into dims[0] x dims[1] x dims[2] shards, (nearly)
+    equal extents per axis, ranks in the row-major order of their
+    coordinates (k fastest, MPI_Cart_create's order).  The reference
+    requires each global size to divide by its count (grid.hpp:258-276);
+    here the first shards of an axis take one cell less where it does not.
+    Each range is chosen as ``split_grid`` chooses the i ranges, so that
+    every shard steps with the global grid's spacings bit for bit."""
+    sizes = (grid.i_size, grid.j_size, grid.k_size)
+    margins = (grid.i_margin, grid.j_margin, grid.k_margin)
+    bounds = ((grid.x_min, grid.x_max), (grid.y_min, grid.y_max), (grid.z_min, grid.z_max))
+    dims = tuple(int(d) for d in dims)
+    if len(dims) != 3 or min(dims) < 1:
+        raise ValueError("dims needs three counts >= 1")
+    axes = []
+    for a in range(3):
+        n, c = sizes[a], dims[a]
+        if c > 1 and (margins[a] == 0 or n < c * 2 * margins[a]):
+            raise ValueError(f"axis {a}: each shard needs at least 2 * margin interior cells")
+        d = (bounds[a][1] - bounds[a][0]) / n
+        cuts = [n * r // c for r in range(c + 1)]
+        parts, x0 = [], bounds[a][0]
+        for r in range(c):
+            x1 = _extent(x0, cuts[r + 1] - cuts[r], d) if c > 1 else bounds[a][1]
+            parts.append((cuts[r], cuts[r + 1], x0, x1))
+            x0 = x1
+        axes.append(parts)
+    out = []
+    count = dims[0] * dims[1] * dims[2]
+    for rank in range(count):
+        coord = (rank // (dims[1] * dims[2]), (rank // dims[2]) % dims[1], rank % dims[2])
+        box = [axes[a][coord[a]] for a in range(3)]
+        g = Grid(box[0][1] - box[0][0], box[1][1] - box[1][0], box[2][1] - box[2][0],
+                 grid.margin, box[0][2], box[0][3], box[1][2], box[1][3], box[2][2], box[2][3])
+        ext = tuple((dims[a] > 1 and (coord[a] > 0 or bool(periodic[a])),
+                     dims[a] > 1 and (coord[a] < dims[a] - 1 or bool(periodic[a])))
+                    for a in range(3))
+        out.append(ShardSpec(rank, count, box[0][0], box[0][1], g, ext[0][0], ext[0][1],
+                             dims=dims, coord=coord, lo=tuple(b[0] for b in box),
+                             hi=tuple(b[1] for b in box), ext=ext))
+    return out
+
+
+def _box(grid: Grid, spec: ShardSpec):
+    m = (grid.i_margin, grid.j_margin, grid.k_margin)
+    return tuple(slice(spec.lo[a], spec.hi[a] + 2 * m[a]) for a in range(3))
+
+
 def split_state(q: np.ndarray, grid: Grid, spec: ShardSpec) -> np.ndarray:
     """The shard's (9, I, J, K) state, ghosts included, cut from the global
     state (whose ghost layers hold the global boundary)."""
-    m = grid.i_margin
-    return np.ascontiguousarray(q[:, spec.i0:spec.i1 + 2 * m])
+    return np.ascontiguousarray(q[(slice(None),) + _box(grid, spec)])
 
 
 def gather(parts: list[np.ndarray], specs: list[ShardSpec], grid: Grid) -> np.ndarray:
     """The global interior (9, nI, nJ, nK) from the shards' states."""
-    out = []
+    out = np.empty((parts[0].shape[0], grid.i_size, grid.j_size, grid.k_size),
+                   dtype=parts[0].dtype)
     for q, s in zip(parts, specs):
-        out.append(q[(slice(None),) + s.grid.interior])
-    return np.concatenate(out, axis=1)
+        dst = tuple(slice(s.lo[a], s.hi[a]) for a in range(3))
+        out[(slice(None),) + dst] = q[(slice(None),) + s.grid.interior]
+    return out
 
 
 def _cuda_tensor(ptr: int, nbytes: int):
@@ -126,15 +202,18 @@ class _Halo:
         from . import _lib
         self._spec = spec
 
-        def exchange(user, n, nbytes, ext_lo, ext_hi, slo, shi, rlo, rhi, stream):
+        def exchange3(user, axis, n, nbytes, ext_lo, ext_hi, slo, shi, rlo, rhi, stream):
             try:
                 self.exchange(spec.rank, [slo[a] for a in range(n)], [shi[a] for a in range(n)],
                               [rlo[a] for a in range(n)], [rhi[a] for a in range(n)],
-                              int(nbytes), bool(ext_lo), bool(ext_hi), stream or 0)
+                              int(nbytes), bool(ext_lo), bool(ext_hi), stream or 0, axis=axis)
                 return 0
             except Exception as exc:  # reported to the library as MISO_B200_ERR_HALO
                 self.error = exc
                 return 1
+
+        def exchange(user, n, nbytes, ext_lo, ext_hi, slo, shi, rlo, rhi, stream):
+            return exchange3(user, 0, n, nbytes, ext_lo, ext_hi, slo, shi, rlo, rhi, stream)
 
         def min_all(user, value):
             try:
@@ -145,12 +224,35 @@ class _Halo:
                 return 1
 
         self.error = None
-        fn_x = _lib.HALO_EXCHANGE_FN(exchange)
         fn_m = _lib.HALO_MIN_FN(min_all)
-        ops = _lib.HaloOps(fn_x, fn_m, None)
-        integ._halo_keep = (fn_x, fn_m, ops, self)
-        integ._check(integ._lib.miso_b200_set_halo(integ._h, int(spec.ext_lo), int(spec.ext_hi),
-                                                   ctypes.byref(ops)))
+        if spec.axes3:
+            fn_x = _lib.HALO3_EXCHANGE_FN(exchange3)
+            ops = _lib.Halo3Ops(fn_x, fn_m, None)
+            ext = (ctypes.c_int * 6)(*[int(spec.ext[a][sd]) for a in range(3) for sd in range(2)])
+            integ._halo_keep = (fn_x, fn_m, ops, ext, self)
+            integ._check(integ._lib.miso_b200_set_halo3(integ._h, ext, ctypes.byref(ops)))
+        else:
+            fn_x = _lib.HALO_EXCHANGE_FN(exchange)
+            ops = _lib.HaloOps(fn_x, fn_m, None)
+            integ._halo_keep = (fn_x, fn_m, ops, self)
+            integ._check(integ._lib.miso_b200_set_halo(integ._h, int(spec.ext_lo),
+                                                       int(spec.ext_hi), ctypes.byref(ops)))
+
+
+def _neighbour(coord, dims, periodic, axis, d):
+    """Rank of the shard next to ``coord`` along ``axis`` (d = -1 / +1),
+    across a periodic face by the wrap, None past a boundary."""
+    c = list(coord)
+    c[axis] += d
+    if not 0 <= c[axis] < dims[axis]:
+        if not periodic[axis]:
+            return None
+        c[axis] %= dims[axis]
+    return (c[0] * dims[1] + c[1]) * dims[2] + c[2]
+
+
+def _rank_coord(rank, dims):
+    return (rank // (dims[1] * dims[2]), (rank // dims[2]) % dims[1], rank % dims[2])
 
 
 class LocalHalo(_Halo):
@@ -161,9 +263,14 @@ class LocalHalo(_Halo):
     wait again before the next pass is enqueued.  The shared stream orders
     the copies after every shard's pass and before the next."""
 
-    def __init__(self, count: int, periodic_x: bool, timeout: float = 120.0):
+    def __init__(self, count: int, periodic_x: bool, timeout: float = 120.0, dims=None,
+                 periodic=None):
         self.count = count
         self.periodic_x = periodic_x
+        self.dims = tuple(dims) if dims is not None else (count, 1, 1)
+        self.periodic = tuple(periodic) if periodic is not None else (periodic_x, False, False)
+        if self.dims[0] * self.dims[1] * self.dims[2] != count:
+            raise ValueError("dims must multiply to count")
         self._bar = threading.Barrier(count, timeout=timeout)
         self._planes = [None] * count
         self._vals = [0.0] * count
@@ -171,25 +278,24 @@ class LocalHalo(_Halo):
     def attach(self, integ: Integrator, spec: ShardSpec):
         _Halo.attach(self, integ, spec)
 
-    def _peer(self, r: int, d: int):
-        p = r + d
-        if 0 <= p < self.count:
-            return p
-        return p % self.count if self.periodic_x else None
+    def _peer(self, r: int, d: int, axis: int = 0):
+        return _neighbour(_rank_coord(r, self.dims), self.dims, self.periodic, axis, d)
 
-    def exchange(self, r, slo, shi, rlo, rhi, nbytes, ext_lo, ext_hi, stream):
+    def exchange(self, r, slo, shi, rlo, rhi, nbytes, ext_lo, ext_hi, stream, axis=0):
         import torch
-        self._planes[r] = (slo, shi, stream)
+        self._planes[r] = (slo, shi, stream, axis)
         self._bar.wait()
         if any(p[2] != stream for p in self._planes):
             raise RuntimeError("in-process shards must share one CUDA stream")
+        if any(p[3] != axis for p in self._planes):
+            raise RuntimeError("the shards exchange along different axes at once")
         with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
             for a in range(len(rlo)):
                 if ext_lo:
-                    src = self._planes[self._peer(r, -1)][1][a]
+                    src = self._planes[self._peer(r, -1, axis)][1][a]
                     _cuda_tensor(rlo[a], nbytes).copy_(_cuda_tensor(src, nbytes))
                 if ext_hi:
-                    src = self._planes[self._peer(r, +1)][0][a]
+                    src = self._planes[self._peer(r, +1, axis)][0][a]
                     _cuda_tensor(rhi[a], nbytes).copy_(_cuda_tensor(src, nbytes))
         self._bar.wait()
 
@@ -207,7 +313,8 @@ class DistHalo(_Halo):
     stream across GPUs; gloo on host buffers), the time step by an
     all-reduce of the minimum.  With one rank a periodic face is a copy."""
 
-    def __init__(self, periodic_x: bool, device: str = "cuda", group=None):
+    def __init__(self, periodic_x: bool, device: str = "cuda", group=None, dims=None,
+                 periodic=None):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
@@ -215,25 +322,27 @@ class DistHalo(_Halo):
         self.world = dist.get_world_size(group)
         self.periodic_x = periodic_x
         self.device = device
+        self.dims = tuple(dims) if dims is not None else (self.world, 1, 1)
+        self.periodic = tuple(periodic) if periodic is not None else (periodic_x, False, False)
+        if self.dims[0] * self.dims[1] * self.dims[2] != self.world:
+            raise ValueError("dims must multiply to the world size")
 
-    def _peer(self, d: int):
-        p = self.rank + d
-        if 0 <= p < self.world:
-            return p
-        return p % self.world if self.periodic_x else None
+    def _peer(self, d: int, axis: int = 0):
+        return _neighbour(_rank_coord(self.rank, self.dims), self.dims, self.periodic, axis, d)
 
     def _t(self, ptr, nbytes):
         return _cuda_tensor(ptr, nbytes) if self.device == "cuda" else _host_tensor(ptr, nbytes)
 
-    def exchange(self, r, slo, shi, rlo, rhi, nbytes, ext_lo, ext_hi, stream):
+    def exchange(self, r, slo, shi, rlo, rhi, nbytes, ext_lo, ext_hi, stream, axis=0):
         import torch
         dist = self.dist
         ctx = (torch.cuda.stream(torch.cuda.ExternalStream(stream))
                if self.device == "cuda" else _nullcontext())
         with ctx:
-            lo, hi = self._peer(-1), self._peer(+1)
-            if self.world == 1:
-                # one rank: a shared face can only be the periodic wrap
+            lo, hi = self._peer(-1, axis), self._peer(+1, axis)
+            if self.dims[axis] == 1:
+                # one shard along the axis: a shared face can only be the
+                # periodic wrap
                 for a in range(len(rlo)):
                     if ext_lo:
                         self._t(rlo[a], nbytes).copy_(self._t(shi[a], nbytes))
@@ -277,17 +386,26 @@ class _nullcontext:
 
 
 def run_local_shards(prob, count: int, steps: int, precision: str = "fp64", variants=None,
-                     stream=None, overlap: bool = False) -> tuple[np.ndarray, list[float]]:
+                     stream=None, overlap: bool = False,
+                     dims=None) -> tuple[np.ndarray, list[float]]:
     """Advance ``prob`` by ``steps`` host-dt steps (cfl, then update) as
     ``count`` shards on the current GPU, one host thread per shard, all on
     one CUDA stream (``stream``, or a new one); return the gathered global
-    interior and the time steps taken.  With ``overlap`` the exchanges run
-    on a second stream shared by the shards while each next pass finishes
-    the planes that need no ghost (``Integrator.set_halo_overlap``)."""
+    interior and the time steps taken.  ``dims`` (shards per axis, product
+    ``count``) decomposes along j and k too; by default the grid is cut
+    along i.  With ``overlap`` the exchanges run on a second stream shared
+    by the shards while each next pass finishes the planes that need no
+    ghost (``Integrator.set_halo_overlap``; i faces only)."""
     import torch
-    periodic_x = bool(prob.config["domain"]["periodic"]["x"])
-    specs = split_grid(prob.grid, count, periodic_x)
-    halo = LocalHalo(count, periodic_x)
+    per = prob.config["domain"]["periodic"]
+    periodic = (bool(per["x"]), bool(per["y"]), bool(per["z"]))
+    periodic_x = periodic[0]
+    if dims is None:
+        specs = split_grid(prob.grid, count, periodic_x)
+        halo = LocalHalo(count, periodic_x)
+    else:
+        specs = split_grid3(prob.grid, dims, periodic)
+        halo = LocalHalo(count, periodic_x, dims=dims, periodic=periodic)
     # one stream for every shard (a null stream would give each handle its
     # own, and the halo copies would then race with the neighbours' passes)
     keep = None

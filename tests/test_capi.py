@@ -65,6 +65,7 @@ def test_null_arguments():
     assert lib.miso_b200_update(None, 1e-3) == _lib.ERR_ARG
     assert lib.miso_b200_set_source(None, 1, None, 0) == _lib.ERR_ARG
     assert lib.miso_b200_set_halo(None, 1, 1, None) == _lib.ERR_ARG
+    assert lib.miso_b200_set_halo3(None, None, None) == _lib.ERR_ARG
 
 
 def test_cfl_noalloc_refuses_host_arrays_before_any_call():

@@ -1,9 +1,10 @@
-"""A grid decomposed into shards along i, with the face halos exchanged
-between passes through miso_b200_set_halo, advances exactly like the single
-grid: the shards here share one GPU (one host thread each, device copies
-for the halo), and the gathered interior and every time step must be the
-single grid's bit for bit -- the per-cell arithmetic does not depend on
-where a shard ends, and the CFL minimum is exact."""
+"""A grid decomposed into shards -- along i through miso_b200_set_halo, along
+any of i, j and k through miso_b200_set_halo3 -- with the face halos
+exchanged between passes, advances exactly like the single grid: the
+shards here share one GPU (one host thread each, device copies for the
+halo), and the gathered interior and every time step must be the single
+grid's bit for bit -- the per-cell arithmetic does not depend on where a
+shard ends, and the CFL minimum is exact."""
 import numpy as np
 import pytest
 
@@ -136,3 +137,67 @@ def test_dist_halo_one_rank_nccl_equals_single_grid():
         assert np.array_equal(got, ref)
     finally:
         dist.destroy_process_group()
+
+
+# decompositions along j and k (shards per axis), both forms
+CASES3 = [
+    ("turb32_fp64_2x2x1", lambda: P.turbulence(32, seed=3), "fp64", (2, 2, 1), None),
+    ("blast24_fp64_1x2x2", lambda: P.blast(24, seed=2), "fp64", (1, 2, 2), None),
+    ("ot64_fp64_1x2x1", lambda: P.orszag_tang(64), "fp64", (1, 2, 1), None),
+    ("magneto16_fp64_1x2x2", lambda: P.magnetosphere(16, extent=12.0), "fp64", (1, 2, 2), None),
+    ("turb32_split_2x2x2", lambda: P.turbulence(32, seed=3), "fp32_split", (2, 2, 2), None),
+    ("blast32_split_1x2x2", lambda: P.blast(32, seed=1), "fp32_split", (1, 2, 2), None),
+    ("ot64_split_2x2x1", lambda: P.orszag_tang(64), "fp32_split", (2, 2, 1), None),
+    # j only: the fused y and z pass reads the exchanged j ghosts
+    ("turb40_split_1x2x1", lambda: P.turbulence(40, seed=5), "fp32_split", (1, 2, 1), None),
+    # k only, periodic: separate y and z sweeps, no wrap copies at a shared face;
+    # 240 = 2 x (112 + 8): a second, ragged k block on each shard
+    ("turb_16x16x240_split_1x1x2", lambda: P.turbulence(16, seed=2, shape=(16, 16, 240)),
+     "fp32_split", (1, 1, 2), None),
+    ("blast_20x20x36_split_1x1x3", lambda: P.blast(20, seed=6, shape=(20, 20, 36)),
+     "fp32_split", (1, 1, 3), None),
+    # sweep variants that read ghosts directly (flat), march across a face,
+    # or stream k rows (z line)
+    ("turb32_split_flat_1x2x2", lambda: P.turbulence(32, seed=3), "fp32_split", (1, 2, 2),
+     {0: 1, 1: 1, 2: 1, 3: 1}),
+    ("blast32_split_march_2x2x2", lambda: P.blast(32, seed=1), "fp32_split", (2, 2, 2),
+     {0: 0, 1: 2, 2: 2, 3: 2}),
+    ("turb32_split_zline_1x1x2", lambda: P.turbulence(32, seed=4), "fp32_split", (1, 1, 2),
+     {2: 0, 3: 2}),
+]
+
+
+@pytest.mark.parametrize("name,make,precision,dims,variants", CASES3,
+                         ids=[c[0] for c in CASES3])
+def test_shards_along_j_and_k_equal_single_grid(name, make, precision, dims, variants):
+    prob = make()
+    steps = 3
+    ref, dts = single(prob, steps, precision, variants)
+    count = dims[0] * dims[1] * dims[2]
+    got, sdts = run_local_shards(prob, count, steps, precision, variants, dims=dims)
+    assert sdts == dts
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref), float(np.max(np.abs(got - ref)))
+
+
+def test_halo3_refusals():
+    """A shared face on a degenerate axis and the overlapped exchange with a
+    shared j or k face are refused; a decomposition along i through the
+    per-axis call keeps the overlap."""
+    import ctypes
+
+    from miso_b200 import _lib
+    from miso_b200.shard import LocalHalo, split_grid3
+    ot = P.orszag_tang(32)
+    with Integrator(ot.config, ot.grid, precision="fp64") as integ:
+        fn = _lib.HALO3_EXCHANGE_FN(lambda *a: 0)
+        ops = _lib.Halo3Ops(fn, _lib.HALO_MIN_FN(0), None)
+        ext = (ctypes.c_int * 6)(0, 0, 0, 0, 1, 1)  # k has one cell
+        assert integ._lib.miso_b200_set_halo3(integ._h, ext, ctypes.byref(ops)) == _lib.ERR_ARG
+    prob = P.turbulence(32, seed=1)
+    spec = split_grid3(prob.grid, (1, 2, 1), (True, True, True))[0]
+    with Integrator(prob.config, spec.grid, precision="fp32_split") as integ:
+        LocalHalo(2, True, dims=(1, 2, 1), periodic=(True, True, True)).attach(integ, spec)
+        with pytest.raises(_lib.MisoError) as e:
+            integ.set_halo_overlap(1)
+        assert e.value.code == _lib.ERR_STATE

@@ -1,4 +1,4 @@
-"""Host logic of the i decomposition (miso_b200/shard.py) on CPU: shard
+"""Host logic of the decomposition (miso_b200/shard.py) on CPU: shard
 extents and spacings, cutting and gathering states, and the torch.distributed
 halo transport run as two and three gloo ranks on host buffers laid out as
 the library lays out an array (ghost planes, then interior planes)."""
@@ -103,3 +103,95 @@ def test_dist_halo_pairs_faces(tmp_path, world, periodic):
             want_hi = [-1.0] * M if hi is None else [1000 * hi + 100 * a + i for i in range(M)]
             assert d["ghost_lo"][a] == want_lo, (r, a)
             assert d["ghost_hi"][a] == want_hi, (r, a)
+
+
+def _rank3(rank, world, port, dims, periodic, out_dir):
+    """One rank of a decomposition over i, j and k: along each axis with
+    more than one shard it sends face buffers marked with its rank, the
+    axis and the side, as the library calls the exchange once per axis."""
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "MASTER_ADDR": "127.0.0.1",
+                       "MASTER_PORT": str(port)})
+    import datetime
+    import torch.distributed as dist
+    from miso_b200.shard import DistHalo, _rank_coord
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    halo = DistHalo(periodic[0], device="cpu", dims=dims, periodic=periodic)
+    coord = _rank_coord(rank, dims)
+    res = {}
+    for axis in range(3):
+        if dims[axis] == 1:
+            continue
+        ext_lo = periodic[axis] or coord[axis] > 0
+        ext_hi = periodic[axis] or coord[axis] < dims[axis] - 1
+        bufs = {k: [np.full(4, -1.0, dtype=np.float32) for _ in range(NARR)]
+                for k in ("slo", "shi", "rlo", "rhi")}
+        for a in range(NARR):
+            bufs["slo"][a][:] = 1000 * rank + 100 * axis + 10 * a
+            bufs["shi"][a][:] = 1000 * rank + 100 * axis + 10 * a + 1
+        ptr = {k: [x.ctypes.data for x in v] for k, v in bufs.items()}
+        halo.exchange(rank, ptr["slo"], ptr["shi"], ptr["rlo"], ptr["rhi"], 16, ext_lo, ext_hi,
+                      0, axis=axis)
+        res[str(axis)] = {"lo": [float(x[0]) for x in bufs["rlo"]],
+                          "hi": [float(x[0]) for x in bufs["rhi"]]}
+    with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+        json.dump(res, f)
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("dims,periodic", [((1, 2, 2), (False, True, True)),
+                                           ((2, 2, 1), (True, False, False)),
+                                           ((1, 1, 3), (False, False, True))],
+                         ids=["j2k2_periodic", "i2j2_mixed", "k3_periodic"])
+def test_dist_halo_pairs_faces_per_axis(tmp_path, dims, periodic):
+    """The per-axis exchange of a decomposition along j and k: along each
+    axis a rank's low ghosts come from the high face of its low neighbour
+    (the rank one coordinate below, across the wrap on a periodic axis) and
+    its high ghosts from the low face of its high neighbour; two shards on a
+    periodic axis are each other's low and high neighbour."""
+    import torch.multiprocessing as tmp
+    from miso_b200.shard import _neighbour, _rank_coord
+    world = dims[0] * dims[1] * dims[2]
+    tmp.start_processes(_rank3, args=(world, _free_port(), dims, periodic, str(tmp_path)),
+                        nprocs=world, join=True, start_method="spawn")
+    for r in range(world):
+        d = json.load(open(tmp_path / f"r{r}.json"))
+        coord = _rank_coord(r, dims)
+        assert sorted(d) == [str(a) for a in range(3) if dims[a] > 1]
+        for axis in range(3):
+            if dims[axis] == 1:
+                continue
+            lo = _neighbour(coord, dims, periodic, axis, -1)
+            hi = _neighbour(coord, dims, periodic, axis, +1)
+            for a in range(NARR):
+                want_lo = -1.0 if lo is None else 1000 * lo + 100 * axis + 10 * a + 1
+                want_hi = -1.0 if hi is None else 1000 * hi + 100 * axis + 10 * a
+                assert d[str(axis)]["lo"][a] == want_lo, (r, axis, a)
+                assert d[str(axis)]["hi"][a] == want_hi, (r, axis, a)
+
+
+def test_split_grid3_boxes_and_round_trip():
+    """The Cartesian decomposition's boxes: ranks in row-major coordinate
+    order, the reference's spacing on every shard, shared faces where a
+    neighbour or a periodic wrap lies, and cutting then gathering a state
+    gives it back."""
+    from miso_b200.shard import split_grid3
+    prob = P.turbulence(16, seed=1)
+    specs = split_grid3(prob.grid, (2, 2, 2), (True, True, True))
+    assert [s.coord for s in specs][:4] == [(0, 0, 0), (0, 0, 1), (0, 1, 0), (0, 1, 1)]
+    for s in specs:
+        assert (s.grid.dx[0], s.grid.dy[0], s.grid.dz[0]) == \
+            (prob.grid.dx[0], prob.grid.dy[0], prob.grid.dz[0])
+        assert s.ext == ((True, True),) * 3
+    parts = [split_state(prob.q, prob.grid, s) for s in specs]
+    assert np.array_equal(gather(parts, specs, prob.grid),
+                          prob.q[(slice(None),) + prob.grid.interior])
+    blast = P.blast(20, seed=2)  # mirror faces; 20 = 6 + 7 + 7 along k
+    specs = split_grid3(blast.grid, (1, 2, 3), (False, False, False))
+    assert [(s.lo[2], s.hi[2]) for s in specs[:3]] == [(0, 6), (6, 13), (13, 20)]
+    assert specs[0].ext == ((False, False), (False, True), (False, True))
+    assert specs[4].ext == ((False, False), (True, False), (True, True))
+    parts = [split_state(blast.q, blast.grid, s) for s in specs]
+    assert np.array_equal(gather(parts, specs, blast.grid),
+                          blast.q[(slice(None),) + blast.grid.interior])
+    with pytest.raises(ValueError):
+        split_grid3(prob.grid, (1, 5, 1), (True, True, True))

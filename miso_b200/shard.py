@@ -73,7 +73,7 @@ class ShardSpec:
     @property
     def axes3(self) -> bool:
         """Whether a j or k face is shared (the exchange goes per axis)."""
-        return self.dims[1] > 1 or self.dims[2] > 1
+        return self.dims[1] > 1 or self.dims[2] > 1 or any(self.ext[1]) or any(self.ext[2])
 
 
 def _extent(x0: float, n: int, dx: float) -> float:

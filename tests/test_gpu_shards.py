@@ -201,3 +201,43 @@ def test_halo3_refusals():
         with pytest.raises(_lib.MisoError) as e:
             integ.set_halo_overlap(1)
         assert e.value.code == _lib.ERR_STATE
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_split"])
+def test_dist_halo_one_rank_all_faces_equals_single_grid(precision):
+    """One NCCL rank whose six faces are all shared with itself: the j and k
+    faces go through the library's packing, the callback's wrap copy and
+    the unpacking, the i faces in place, dt through an NCCL all-reduce; the
+    periodic box steps like the single grid, bit for bit."""
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+
+    from miso_b200.shard import DistHalo, ShardSpec
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        prob = P.turbulence(24, seed=6, shape=(24, 20, 28))
+        ref, dts = single(prob, 3, precision)
+        integ = Integrator(prob.config, prob.grid, precision=precision)
+        spec = ShardSpec(0, 1, 0, 24, prob.grid, True, True, dims=(1, 1, 1), coord=(0, 0, 0),
+                         lo=(0, 0, 0), hi=(24, 20, 28), ext=((True, True),) * 3)
+        DistHalo(periodic_x=True, device="cuda", periodic=(True, True, True)).attach(integ, spec)
+        integ.upload(prob.q)
+        integ.apply_boundary_condition()
+        got_dts = []
+        for _ in range(3):
+            dt = integ.cfl()
+            integ.update(dt)
+            got_dts.append(dt)
+        got = integ.download()[(slice(None),) + prob.grid.interior]
+        integ.close()
+        assert got_dts == dts
+        assert np.array_equal(got, ref)
+    finally:
+        dist.destroy_process_group()

@@ -481,6 +481,15 @@ const char *miso_b200_last_error(miso_b200_handle *h);
  * GPU, 0 for host memory (pageable or pinned).  Allocates nothing. */
 int miso_b200_pointer_kind(const void *p, int *kind);
 
+/* Memory that host code and device code can both read and write (CUDA
+ * managed memory), for data a device functor of the caller's reads -- the
+ * C++ backend keeps the grid's coordinate arrays there, so a source functor
+ * holding a view of the grid runs on either side.  *ptr = NULL for bytes ==
+ * 0; MISO_B200_ERR_NOMEM when the allocation fails (no GPU, or out of
+ * memory).  miso_b200_free_shared releases such a block (NULL: no-op). */
+int miso_b200_alloc_shared(size_t bytes, void **ptr);
+int miso_b200_free_shared(void *ptr);
+
 /* Library version string. */
 const char *miso_b200_version(void);
 

@@ -11,7 +11,9 @@
 // backend::CUDA (miso/include/miso/backend.hpp:9-13):
 //
 //   backend::B200                       the tag
-//   Grid<Real, backend::B200>           the host grid (grid.hpp:147-450), as is
+//   Grid<Real, backend::B200>           the host grid (grid.hpp:147-450), whose
+//                                       views read a copy of its coordinate
+//                                       arrays in memory host and device share
 //   mhd::Fields<Real, backend::B200>    the state, held on the device by the
 //                                       integrator it is bound to
 //   mhd::ExecContext<Real, backend::B200>
@@ -37,7 +39,19 @@
 // reference's Source concept (vx, vy, vz, ei of (FieldsView<const Real>, i,
 // j, k), mhd_model_base.hpp:131-155) is evaluated, in the FP64 form, on host
 // copies of every stage's argument state (miso_b200_set_source_callback):
-// exact, and slow.  The split form refuses such a functor with an exception.
+// exact, and slow.  Where the model's translation unit is compiled by nvcc
+// and the functor type is declared device-callable --
+//
+//     template <> struct miso_b200::device_source<MySource> : std::true_type {};
+//
+// (its four methods __host__ __device__, the object trivially copyable, and
+// whatever it reads device-accessible: the state, and views of the B200 grid,
+// whose coordinate arrays live in shared memory) -- the functor is evaluated
+// on the device instead: before every stage one kernel of this header, run
+// on the library's stream, fills the four terms of every interior cell from
+// the stage's argument state, as the reference's CUDA integrator evaluates
+// it inside its kernels (mhd_integrator_cuda.cuh:341-392).  The split form
+// refuses such functors with an exception.
 //
 // Boundary functors (bc.apply(FieldsView<Real>, GridView<const Real>)):
 //   * mhd::EmptyBoundaryCondition<Real>: every non-degenerate axis must be
@@ -113,6 +127,11 @@ template <typename Real>
 struct PointGravity {
   Real g;
 };
+
+// A Source functor type the model declares device-callable: specialise to
+// std::true_type (in a translation unit compiled by nvcc).
+template <typename Source>
+struct device_source : std::false_type {};
 
 namespace detail {
 
@@ -200,10 +219,52 @@ void symmetric(backend::B200, Array3DView<Real> arr, GridView<const Real> grid, 
 }  // namespace boundary_condition
 
 /// The grid of the B200 backend is the host grid (its spacings are copied
-/// into the library's descriptor; nothing else lives on the device).
+/// into the library's descriptor).  Its views read a copy of the nine
+/// coordinate and spacing arrays in memory that host and device share
+/// (miso_b200_alloc_shared), so that a functor holding a view of the grid --
+/// a source term that reads the cell centres -- runs on either side.
 template <typename Real>
 struct Grid<Real, backend::B200> : Grid<Real, backend::Host> {
-  explicit Grid(const Grid<Real, backend::Host> &grid) : Grid<Real, backend::Host>(grid) {}
+  using HostGrid = Grid<Real, backend::Host>;
+  explicit Grid(const HostGrid &grid) : HostGrid(grid) { mirror(); }
+  Grid(const Grid &o) : HostGrid(o) { mirror(); }
+  Grid &operator=(const Grid &o) {
+    HostGrid::operator=(o);
+    mirror();
+    return *this;
+  }
+
+  GridView<Real> view() noexcept { return make_view<Real>(); }
+  GridView<const Real> view() const noexcept { return make_view<const Real>(); }
+  GridView<const Real> const_view() const noexcept { return view(); }
+
+ private:
+  std::shared_ptr<Real> shared_;
+  Real *arr_[9] = {};  // x, y, z, dx, dy, dz, dxi, dyi, dzi
+
+  void mirror() {
+    const std::vector<Real> *src[9] = {&this->x,  &this->y,  &this->z,   &this->dx, &this->dy,
+                                       &this->dz, &this->dxi, &this->dyi, &this->dzi};
+    size_t n = 0;
+    for (auto *v : src) n += v->size();
+    void *p = nullptr;
+    const int rc = miso_b200_alloc_shared(n * sizeof(Real), &p);
+    if (rc != MISO_B200_OK)
+      throw miso_b200::Error(rc, "miso_b200_alloc_shared: no memory for the grid's coordinates");
+    shared_.reset(static_cast<Real *>(p), [](Real *q) { miso_b200_free_shared(q); });
+    Real *at = shared_.get();
+    for (int a = 0; a < 9; ++a) {
+      arr_[a] = at;
+      std::memcpy(at, src[a]->data(), src[a]->size() * sizeof(Real));
+      at += src[a]->size();
+    }
+  }
+  template <typename T>
+  GridView<T> make_view() const noexcept {
+    return GridView<T>(this->i_total, this->j_total, this->k_total, this->is, this->js, this->ks,
+                       this->i_margin, this->j_margin, this->k_margin, this->min_dxyz, arr_[0],
+                       arr_[1], arr_[2], arr_[3], arr_[4], arr_[5], arr_[6], arr_[7], arr_[8]);
+  }
 };
 
 namespace mhd {
@@ -325,6 +386,46 @@ struct Fields<Real, backend::B200> {
   Fields(Fields &&) = default;
   Fields &operator=(Fields &&) = default;
 };
+
+}  // namespace mhd
+}  // namespace miso
+
+#if defined(__CUDACC__)
+namespace miso_b200 {
+namespace detail {
+
+// The four terms of a device-callable Source functor at every interior cell
+// of the stage's argument state qq (FP64 arrays of the field layout):
+// s[0..2] the forces per volume src.vx / vy / vz, s[3] the heating src.ei,
+// as the reference's stage kernels call them per cell
+// (mhd_integrator_cuda.cuh:341-392 on mhd_integrator_host.hpp:134, 151,
+// 168, 241).
+template <typename Real, typename Source>
+__global__ void __launch_bounds__(256)
+source_terms_kernel(const Source src, const miso::mhd::FieldsView<const Real> qq, double *s0,
+                    double *s1, double *s2, double *s3, int n1, int n2, int m0, int m1, int m2,
+                    int ni, int nj, int nk) {
+  const long long total = (long long)ni * nj * nk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % nk) + m2;
+    const long long r = t / nk;
+    const int j = (int)(r % nj) + m1;
+    const int i = (int)(r / nj) + m0;
+    const long long c = ((long long)i * n1 + j) * n2 + k;
+    s0[c] = (double)src.vx(qq, i, j, k);
+    s1[c] = (double)src.vy(qq, i, j, k);
+    s2[c] = (double)src.vz(qq, i, j, k);
+    s3[c] = (double)src.ei(qq, i, j, k);
+  }
+}
+
+}  // namespace detail
+}  // namespace miso_b200
+#endif
+
+namespace miso {
+namespace mhd {
 
 /// The reference integrator's interface (mhd_integrator_cuda.cuh:291-501)
 /// over libmiso_b200.so.
@@ -495,9 +596,10 @@ struct Integrator<Real, backend::B200> {
         src_g_ = g;
       }
     } else {
-      // any other functor of the Source concept: its four terms on host
-      // copies of every stage's argument state (the object must outlive the
-      // steps, as the model's own `src` member does)
+      // any other functor of the Source concept: its four terms on the
+      // device (a functor declared device-callable) or on host copies of
+      // every stage's argument state (the object must outlive the steps, as
+      // the model's own `src` member does)
       if (!std::is_same<Real, double>::value || precision_ != MISO_B200_FP64)
         throw miso_b200::Error(MISO_B200_ERR_STATE,
                                std::string("source functor ") + typeid(Source).name() +
@@ -506,6 +608,23 @@ struct Integrator<Real, backend::B200> {
       if (src_kind_ != MISO_B200_SOURCE_NONE && src_kind_ != kSourceFunctor) {
         miso_b200::detail::check(miso_b200_set_source(h_, MISO_B200_SOURCE_NONE, nullptr, 0), h_,
                                  "miso_b200_set_source");
+      }
+      if constexpr (miso_b200::device_source<Source>::value) {
+#if defined(__CUDACC__)
+        static_assert(std::is_trivially_copyable<Source>::value,
+                      "a device source functor is copied into a kernel: it must be trivially "
+                      "copyable");
+        src_obj_ = (const void *)&src;
+        miso_b200::detail::check(
+            miso_b200_set_source_callback(h_, &Integrator::src_device_trampoline<Source>, this,
+                                          0),
+            h_, "miso_b200_set_source_callback");
+        src_kind_ = kSourceFunctor;
+        return;
+#else
+        static_assert(miso_b200::detail::always_false<Source>::value,
+                      "a device source functor needs its translation unit compiled by nvcc");
+#endif
       }
       const Source *sp = &src;
       src_fn_ = [this, sp](const double *const *q, double *const *s) {
@@ -533,6 +652,34 @@ struct Integrator<Real, backend::B200> {
       src_obj_ = (const void *)&src;
     }
   }
+
+#if defined(__CUDACC__)
+  // before every stage: the device-callable functor's terms by one kernel
+  // on the library's stream, from the stage's argument state (device arrays)
+  template <typename Source>
+  static int src_device_trampoline(void *user, const double *const q[9], double *const s[4],
+                                   void *stream) {
+    auto *self = static_cast<Integrator *>(user);
+    const Grid<Real, backend::B200> &g = self->grid;
+    const int n0 = g.i_total, n1 = g.j_total, n2 = g.k_total;
+    auto v = [&](int f) {
+      return Array3D<const Real, backend::B200>(reinterpret_cast<const Real *>(q[f]), n0, n1, n2)
+          .view();
+    };
+    const FieldsView<const Real> qq(v(0), v(1), v(2), v(3), v(4), v(5), v(6), v(7), v(8));
+    const int ni = n0 - 2 * g.i_margin, nj = n1 - 2 * g.j_margin, nk = n2 - 2 * g.k_margin;
+    const long long total = (long long)ni * nj * nk;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    if (blocks < 1) blocks = 1;
+    cudaGetLastError();
+    miso_b200::detail::source_terms_kernel<Real, Source>
+        <<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(
+            *static_cast<const Source *>(self->src_obj_), qq, s[0], s[1], s[2], s[3], n1, n2,
+            g.i_margin, g.j_margin, g.k_margin, ni, nj, nk);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+  }
+#endif
 
   static int src_trampoline(void *user, const double *const q[9], double *const s[4], void *) {
     auto *self = static_cast<Integrator *>(user);

@@ -104,6 +104,8 @@ SIGNATURES = {
     "miso_b200_set_blend_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "miso_b200_set_halo": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(HaloOps)]),
+    "miso_b200_alloc_shared": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
+    "miso_b200_free_shared": (ctypes.c_int, [ctypes.c_void_p]),
     "miso_b200_set_halo3": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(Halo3Ops)]),
     "miso_b200_set_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),

@@ -1213,6 +1213,27 @@ int miso_b200_pointer_kind(const void *p, int *kind) {
   return MISO_B200_OK;
 }
 
+int miso_b200_alloc_shared(size_t bytes, void **ptr) {
+  if (!ptr) return MISO_B200_ERR_ARG;
+  *ptr = nullptr;
+  if (!bytes) return MISO_B200_OK;
+  if (cudaMallocManaged(ptr, bytes, cudaMemAttachGlobal) != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return MISO_B200_ERR_NOMEM;
+  }
+  return MISO_B200_OK;
+}
+
+int miso_b200_free_shared(void *ptr) {
+  if (!ptr) return MISO_B200_OK;
+  if (cudaFree(ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return MISO_B200_ERR_CUDA;
+  }
+  return MISO_B200_OK;
+}
+
 const char *miso_b200_version(void) { return "miso_b200 0.1 (sm_100a)"; }
 
 const char *miso_b200_last_error(miso_b200_handle *h) {

@@ -4,7 +4,7 @@
 // tests/cpp/Makefile against the reference's headers where they lie; run by
 // tests/test_cpp_modelbase.py.
 //
-//   modelbase_demo <config.yaml> <initial.bin> <bc> <mode> [const:vx,vy,vz,ei]
+//   modelbase_demo <config.yaml> <initial.bin> <bc> <mode> [const:vx,vy,vz,ei | grav:g]
 //
 // initial.bin: the 9 primitive arrays (ro .. ph, ghosts included) as raw
 // Real values -- the initial condition functor copies them in, so the host
@@ -17,9 +17,10 @@
 // "run" (ModelBase::run: initial condition, the time loop to time.tend with
 // snapshots every time.dt_output) or "update:N" (N calls of
 // ModelBase::update, then one snapshot).  The optional last argument gives
-// the model a source functor of its own (four constants as the Source
-// concept's vx, vy, vz, ei), which the backend evaluates on host copies of
-// every stage's argument state.  It prints the boundary path the backend
+// the model a source functor of its own: four constants as the Source
+// concept's vx, vy, vz, ei, which the backend evaluates on host copies of
+// every stage's argument state, or the point gravity of constant g, which
+// it evaluates on the device where nvcc built the program.  It prints the boundary path the backend
 // chose and exits 0, or prints the exception and exits 3.
 #include <miso/boundary_condition.hpp>
 #include <miso/mhd_model_base.hpp>
@@ -29,6 +30,7 @@
 #include <cstdio>
 #include <fstream>
 #include <string>
+#include <utility>
 
 using namespace miso;
 
@@ -111,6 +113,34 @@ struct ConstSource {
   Real ei(mhd::FieldsView<const Real>, int, int, int) const { return c[3]; }
 };
 
+// The magnetosphere demo's point gravity written as a model's own Source
+// functor: force per volume -ro g x / |x|^3 about the coordinate origin, no
+// heating.  It keeps a view of the grid for the cell centres.  Built by nvcc,
+// the model declares it device-callable, and the backend evaluates it on the
+// device before every stage; built by the host compiler, on host copies.
+struct GravitySource {
+  GridView<const Real> grid;
+  Real g;
+  __host__ __device__ Real r3(int i, int j, int k) const {
+    return util::pow3(util::sqrt(grid.x[i] * grid.x[i] + grid.y[j] * grid.y[j] +
+                                 grid.z[k] * grid.z[k]));
+  }
+  __host__ __device__ Real vx(mhd::FieldsView<const Real> qq, int i, int j, int k) const {
+    return -qq.ro(i, j, k) * g * grid.x[i] / r3(i, j, k);
+  }
+  __host__ __device__ Real vy(mhd::FieldsView<const Real> qq, int i, int j, int k) const {
+    return -qq.ro(i, j, k) * g * grid.y[j] / r3(i, j, k);
+  }
+  __host__ __device__ Real vz(mhd::FieldsView<const Real> qq, int i, int j, int k) const {
+    return -qq.ro(i, j, k) * g * grid.z[k] / r3(i, j, k);
+  }
+  __host__ __device__ Real ei(mhd::FieldsView<const Real>, int, int, int) const { return 0; }
+};
+#if defined(__CUDACC__)
+template <>
+struct miso_b200::device_source<GravitySource> : std::true_type {};
+#endif
+
 template <class BC> struct MakeBC {
   static BC make(mpi::Shape &s) { return BC{s}; }
 };
@@ -118,20 +148,36 @@ template <> struct MakeBC<mhd::EmptyBoundaryCondition<Real>> {
   static mhd::EmptyBoundaryCondition<Real> make(mpi::Shape &) { return {}; }
 };
 
-template <class BC, class Src>
-struct Model : public mhd::ModelBase<Model<BC, Src>, Real, Backend> {
-  using Base = mhd::ModelBase<Model<BC, Src>, Real, Backend>;
+// the source object from the model's grid (the gravity keeps its view)
+template <class Src> struct MakeSrc {
+  static Src make(const Src &s, Grid<Real, Backend> &) { return s; }
+};
+struct GravitySpec {
+  Real g;
+};
+template <> struct MakeSrc<GravitySpec> {
+  static GravitySource make(const GravitySpec &s, Grid<Real, Backend> &grid) {
+    return GravitySource{grid.const_view(), s.g};
+  }
+};
+
+template <class BC, class Spec>
+struct Model : public mhd::ModelBase<Model<BC, Spec>, Real, Backend> {
+  using Base = mhd::ModelBase<Model<BC, Spec>, Real, Backend>;
+  using Src = decltype(MakeSrc<Spec>::make(std::declval<const Spec &>(),
+                                           std::declval<Grid<Real, Backend> &>()));
   eos::IdealEOS<Real> eos;
   FileInitialCondition ic;
   BC bc;
   Src src;
-  Model(Config &config, const std::string &init, const Src &s)
-      : Base(config), eos(config), ic{init}, bc(MakeBC<BC>::make(this->mpi_shape)), src(s) {}
+  Model(Config &config, const std::string &init, const Spec &s)
+      : Base(config), eos(config), ic{init}, bc(MakeBC<BC>::make(this->mpi_shape)),
+        src(MakeSrc<Spec>::make(s, this->mhd.grid)) {}
 };
 
-template <class BC, class Src>
-int drive(Config &config, const std::string &init, const std::string &mode, const Src &s) {
-  Model<BC, Src> model(config, init, s);
+template <class BC, class Spec>
+int drive(Config &config, const std::string &init, const std::string &mode, const Spec &s) {
+  Model<BC, Spec> model(config, init, s);
   if (mode == "run") {
     model.run();
   } else {
@@ -167,6 +213,11 @@ int main(int argc, char **argv) {
       if (bc == "empty") return drive<mhd::EmptyBoundaryCondition<Real>>(config, init, mode, cs);
       if (bc == "mirror") return drive<MirrorBoundaryCondition>(config, init, mode, cs);
       if (bc == "loop") return drive<LoopBoundaryCondition>(config, init, mode, cs);
+    } else if (source.rfind("grav:", 0) == 0) {
+      const GravitySpec gs{(Real)std::stod(source.substr(5))};
+      if (bc == "empty") return drive<mhd::EmptyBoundaryCondition<Real>>(config, init, mode, gs);
+      if (bc == "mirror") return drive<MirrorBoundaryCondition>(config, init, mode, gs);
+      if (bc == "loop") return drive<LoopBoundaryCondition>(config, init, mode, gs);
     } else {
       const mhd::EmptySourceTerm<Real> none{};
       if (bc == "empty") return drive<mhd::EmptyBoundaryCondition<Real>>(config, init, mode, none);

@@ -5,12 +5,15 @@ unmodified ModelBase::run / ModelBase::update
 (miso/include/miso/mhd_model_base.hpp:57-116); the snapshots the
 reference's Checkpoint writes are compared with the oracle.
 
-CPU: the programs build against the reference's headers, and a source or
-equation of state the backend does not implement is a compile-time error.
+CPU: the programs build against the reference's headers (with the host
+compiler, and with nvcc for device source functors), and an equation of
+state the backend does not implement is a compile-time error.
 GPU: Orszag-Tang (periodic, EmptyBoundaryCondition), Brio-Wu and a 3-D
 blast (the demos' mirror functor, reduced to the library's face fill; the
 same mirror as plain loops, run as a host functor after every pass) equal
-the oracle bit for bit in the FP64 form; Real = float runs the split form;
+the oracle bit for bit in the FP64 form; so do models with source functors
+of their own (constants on host copies; the point gravity on host copies
+and, built by nvcc, on the device); Real = float runs the split form;
 functors and configurations the backend cannot run fail with a message.
 """
 import glob
@@ -44,6 +47,7 @@ def _binary(name):
 def test_modelbase_programs_build():
     assert os.path.exists(_binary("modelbase_fp64"))
     assert os.path.exists(_binary("modelbase_f32"))
+    assert os.path.exists(_binary("modelbase_fp64_cuda"))  # nvcc: device source functors
 
 
 BAD_TU = r"""
@@ -281,6 +285,28 @@ def test_modelbase_user_source_fp64_bit_exact(tmp_path, oracle, mode):
         n_out = 0
     assert r.returncode == 0, r.stdout + r.stderr
     out = _snapshot(tmp_path, base, n_out)
+    a, b = interior(base, out), interior(base, ref)
+    assert int(np.sum(a != b)) == 0, float(np.max(np.abs(a - b)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("exe_name", ["modelbase_fp64", "modelbase_fp64_cuda"],
+                         ids=["host_functor", "device_functor"])
+def test_modelbase_gravity_source_bit_exact(tmp_path, oracle, exe_name):
+    """The point gravity as the model's own Source functor, holding a view
+    of the B200 grid for the cell centres: evaluated on host copies (the
+    host compiler's build) or on the device by the backend's kernel (nvcc's
+    build, the functor declared device-callable), every interior value after
+    ModelBase::update x 4 equals the oracle's built-in gravity -- which
+    equals the reference's own magnetosphere source -- bit for bit."""
+    exe = _binary(exe_name)
+    base = P.blast(12, seed=5)
+    prob = P.with_point_gravity(base, 0.3)
+    ref = prob.q.copy()
+    oracle.run(prob, ref, 4)
+    r = _run(exe, tmp_path, base, "mirror", "update:4", source="grav:0.3")
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = _snapshot(tmp_path, base, 0)
     a, b = interior(base, out), interior(base, ref)
     assert int(np.sum(a != b)) == 0, float(np.max(np.abs(a - b)))
 

@@ -164,6 +164,10 @@ CASES3 = [
      {0: 0, 1: 2, 2: 2, 3: 2}),
     ("turb32_split_zline_1x1x2", lambda: P.turbulence(32, seed=4), "fp32_split", (1, 1, 2),
      {2: 0, 3: 2}),
+    # the thinnest shards: 2 * margin = 4 interior rows / columns each
+    ("turb16_split_1x4x1", lambda: P.turbulence(16, seed=7), "fp32_split", (1, 4, 1), None),
+    ("turb16_split_1x1x4", lambda: P.turbulence(16, seed=7), "fp32_split", (1, 1, 4), None),
+    ("blast16_fp64_2x2x4", lambda: P.blast(16, seed=3), "fp64", (2, 2, 4), None),
 ]
 
 

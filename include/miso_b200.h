@@ -308,7 +308,7 @@ typedef struct miso_b200_halo3_ops {
 
 int miso_b200_set_halo3(miso_b200_handle *h, const int ext[6], const miso_b200_halo3_ops *ops);
 
-/* A source functor of the caller's own for the FP64 form: the reference's
+/* A source functor of the caller's own, for either form: the reference's
  * Source concept (src.vx, src.vy, src.vz, src.ei evaluated on the stage's
  * argument state, mhd_model_base.hpp:131-155), as update_sc4 uses it
  * (mhd_integrator_host.hpp:134, 151, 168: the forces inside the dt factor
@@ -320,9 +320,13 @@ int miso_b200_set_halo3(miso_b200_handle *h, const int ext[6], const miso_b200_h
  * stop the step with MISO_B200_ERR_CALLBACK.  on_host != 0: q and s are
  * host copies that the library stages (exact, and slow); 0: device arrays,
  * with the handle's stream as the last argument.  While set it replaces the
- * built-in source; fn == NULL removes it.  ERR_STATE on the FP32 split form
- * and on a grid in shards; no graph capture (miso_b200_run with use_graph
- * refuses, miso_b200_run_until launches the steps from the host). */
+ * built-in source; fn == NULL removes it.  In the FP32 split form q holds the
+ * stage's argument state converted to FP64 primitives (hi + lo words for the
+ * step's first stage, the FP32 stage buffer otherwise), the terms enter the
+ * FP32 right-hand side, and the grid runs its per-cell kernels while a
+ * callback is set.  ERR_STATE on a grid in shards; no graph capture
+ * (miso_b200_run with use_graph refuses, miso_b200_run_until launches the
+ * steps from the host). */
 typedef int (*miso_b200_source_fn)(void *user, const double *const q[9], double *const s[4],
                                    void *stream);
 int miso_b200_set_source_callback(miso_b200_handle *h, miso_b200_source_fn fn, void *user,

@@ -39,7 +39,9 @@
 // reference's Source concept (vx, vy, vz, ei of (FieldsView<const Real>, i,
 // j, k), mhd_model_base.hpp:131-155) is evaluated, in the FP64 form, on host
 // copies of every stage's argument state (miso_b200_set_source_callback):
-// exact, and slow.  Where the model's translation unit is compiled by nvcc
+// exact, and slow (with b200.precision: fp32_split, the split form hands it
+// the argument state as FP64 primitives and runs its per-cell kernels).
+// Where the model's translation unit is compiled by nvcc
 // and the functor type is declared device-callable --
 //
 //     template <> struct miso_b200::device_source<MySource> : std::true_type {};
@@ -50,8 +52,8 @@
 // on the device instead: before every stage one kernel of this header, run
 // on the library's stream, fills the four terms of every interior cell from
 // the stage's argument state, as the reference's CUDA integrator evaluates
-// it inside its kernels (mhd_integrator_cuda.cuh:341-392).  The split form
-// refuses such functors with an exception.
+// it inside its kernels (mhd_integrator_cuda.cuh:341-392).  Real = float
+// (the split form on FP32 views) refuses such functors with an exception.
 //
 // Boundary functors (bc.apply(FieldsView<Real>, GridView<const Real>)):
 //   * mhd::EmptyBoundaryCondition<Real>: every non-degenerate axis must be
@@ -600,10 +602,11 @@ struct Integrator<Real, backend::B200> {
       // device (a functor declared device-callable) or on host copies of
       // every stage's argument state (the object must outlive the steps, as
       // the model's own `src` member does)
-      if (!std::is_same<Real, double>::value || precision_ != MISO_B200_FP64)
+      if (!std::is_same<Real, double>::value)
         throw miso_b200::Error(MISO_B200_ERR_STATE,
                                std::string("source functor ") + typeid(Source).name() +
-                                   " runs on the FP64 form only (Real = double)");
+                                   " runs with Real = double only (the FP64 form, or the split "
+                                   "form by b200.precision)");
       if (src_kind_ == kSourceFunctor && src_obj_ == (const void *)&src) return;
       if (src_kind_ != MISO_B200_SOURCE_NONE && src_kind_ != kSourceFunctor) {
         miso_b200::detail::check(miso_b200_set_source(h_, MISO_B200_SOURCE_NONE, nullptr, 0), h_,

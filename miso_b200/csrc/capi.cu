@@ -305,6 +305,7 @@ struct miso_b200_handle {
   void *src_user = nullptr;
   bool src_host = false;
   double *src_dev = nullptr, *src_stage = nullptr;  // device terms; host staging (q then s)
+  double *src_arg = nullptr;  // split form: the stage's argument state as FP64 primitives
   miso_b200_boundary_fn bc_cb = nullptr;
   void *bc_user = nullptr;
   bool bc_host = false;
@@ -596,7 +597,19 @@ struct miso_b200_handle {
   }
   // the caller's source functor on the argument state of the stage at hand
   // (set `set`): its four terms into src_dev, which the stage kernel reads
-  int src_callback(int set) {
+  int src_callback(int set) { return src_callback_on(q64[set]); }
+  // the split form: the stage's argument state (hi and, for U^n, lo words;
+  // a stage buffer alone otherwise) as FP64 primitives in the io set first
+  int src_callback_split(const FieldPtrs<const float> &arg, const FieldPtrs<const float> &lo) {
+    FieldPtrs<double> q;
+    double *qp[NF];
+    for (int f = 0; f < NF; ++f) q.f[f] = qp[f] = src_arg + (size_t)f * g.cells;
+    launch_s32_from_split(g.cells, arg, lo, q, sms, stream);
+    launches++;
+    if (int rc = check_launch("from_split")) return rc;
+    return src_callback_on(qp);
+  }
+  int src_callback_on(double *const *qdev) {
     int rc = cuda(cudaStreamSynchronize(stream), "synchronize before the source callback");
     if (rc) return rc;
     const size_t bytes = (size_t)g.cells * sizeof(double);
@@ -605,12 +618,12 @@ struct miso_b200_handle {
     for (int f = 0; f < NF; ++f) {
       if (src_host) {
         double *dst = src_stage + (size_t)f * g.cells;
-        if ((rc = cuda(cudaMemcpyAsync(dst, q64[set][f], bytes, cudaMemcpyDeviceToHost, stream),
+        if ((rc = cuda(cudaMemcpyAsync(dst, qdev[f], bytes, cudaMemcpyDeviceToHost, stream),
                        "stage the fields for the source callback")))
           return rc;
         qp[f] = dst;
       } else {
-        qp[f] = q64[set][f];
+        qp[f] = qdev[f];
       }
     }
     for (int t = 0; t < 4; ++t)
@@ -813,6 +826,13 @@ struct miso_b200_handle {
     return halo_exchange(arr, n, sizeof(float), axes);
   }
 
+  // the pipelined kernels of a 3-D split grid, unless the magnetosphere
+  // boundary or a caller's source needs the per-cell kernels
+  void retile() {
+    const bool t = tiled_ok && !mag.on && !(src_cb && split());
+    if (t != tiled) partials_valid = false;
+    tiled = t;
+  }
   // the lo ghost images catch up with the interior before the state leaves
   // the device
   int fresh_lo_shell() {
@@ -933,6 +953,8 @@ struct miso_b200_handle {
     for (int s = 0; s < 4; ++s) {
       FieldPtrs<const float> prev = s == 0 ? cst(H(c)) : cst(S((s - 1) & 1));
       FieldPtrs<float> out = s < 3 ? S(s & 1) : S(0);
+      if (src_cb && (rc = src_callback_split(prev, s == 0 ? cst(L(c)) : FieldPtrs<const float>{})))
+        return rc;
       const int t = tb();
       launch_s32_rk_stage(g, prev, H(c), L(c), out, sc, s, p.gm, src, sms, stream);
       te(t, "rk_stage", interior() * (s == 0 ? 72.0 : s < 3 ? 108.0 : 180.0));
@@ -1542,6 +1564,7 @@ int miso_b200_destroy(miso_b200_handle *h) {
   if (h->bc_stage) cudaFreeHost(h->bc_stage);
   if (h->src_stage) cudaFreeHost(h->src_stage);
   if (h->src_dev) cudaFree(h->src_dev);
+  if (h->src_arg) cudaFree(h->src_arg);
   if (h->face_buf) cudaFree(h->face_buf);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1680,7 +1703,7 @@ int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, 
   if (kind == MISO_B200_BOUNDARY_FACES) {
     h->mag.on = 0;
     h->mag.mask_cfl = 0;
-    h->tiled = h->tiled_ok;
+    h->retile();
   } else if (kind == MISO_B200_BOUNDARY_MAGNETOSPHERE) {
     if (h->split() && h->halo_on)
       return h->fail(MISO_B200_ERR_STATE,
@@ -1713,7 +1736,8 @@ int miso_b200_set_boundary(miso_b200_handle *h, int kind, const double *params, 
     m.on = 1;
     // the split form runs the per-cell kernels, which read every ghost
     // cell the boundary writes between passes
-    h->tiled = false;
+    if (int rc = h->fresh_lo_shell()) return rc;
+    h->retile();
   } else {
     return h->fail(MISO_B200_ERR_ARG, "unknown boundary kind %d", kind);
   }
@@ -1775,12 +1799,14 @@ int miso_b200_set_source_callback(miso_b200_handle *h, miso_b200_source_fn fn, v
   if (!h) return MISO_B200_ERR_ARG;
   const size_t bytes = (size_t)h->g.cells * sizeof(double);
   if (fn) {
-    if (h->split())
-      return h->fail(MISO_B200_ERR_STATE, "a source callback runs on the FP64 form");
     if (h->halo_on)
       return h->fail(MISO_B200_ERR_STATE, "a source callback runs on a single grid");
     if (!h->src_dev && h->cuda(cudaMalloc((void **)&h->src_dev, 4 * bytes),
                                "allocate the source terms"))
+      return MISO_B200_ERR_NOMEM;
+    // the split form's stage buffers hold no FP64 primitives: a set of its own
+    if (h->split() && !h->src_arg &&
+        h->cuda(cudaMalloc((void **)&h->src_arg, NF * bytes), "allocate the source arguments"))
       return MISO_B200_ERR_NOMEM;
     if (on_host && !h->src_stage &&
         h->cuda(cudaMallocHost((void **)&h->src_stage, (NF + 4) * bytes),
@@ -1796,13 +1822,22 @@ int miso_b200_set_source_callback(miso_b200_handle *h, miso_b200_source_fn fn, v
       cudaStreamSynchronize(h->stream);
       cudaFree(h->src_dev);
     }
+    if (h->src_arg) cudaFree(h->src_arg);
     h->src_stage = nullptr;
     h->src_dev = nullptr;
+    h->src_arg = nullptr;
     if (h->src.kind == 2) h->src.kind = 0;
   }
   h->src_cb = fn;
   h->src_user = user;
   h->src_host = fn && on_host;
+  if (h->split()) {
+    // the split form evaluates a caller's source on the per-cell kernels
+    // (the pipelined stages fuse what the callback must see between them);
+    // they read the lo ghost words, which the pipelined step leaves stale
+    if (int rc = h->fresh_lo_shell()) return rc;
+    h->retile();
+  }
   if (h->graph_exec) {
     cudaGraphExecDestroy(h->graph_exec);
     cudaGraphDestroy(h->graph);

@@ -118,6 +118,9 @@ rk_stage_kernel(Geom g, FieldPtrs<const float> prev, FieldPtrs<float> hi, FieldP
 #pragma unroll
       for (int f = 0; f < NF; ++f) R[f] -= ((M2[f] - P2[f]) + 8.0f * (P1[f] - M1[f])) * w;
     }
+    // a caller's source functor: its heating enters the new total energy
+    // outside the dt factor (mhd_integrator_host.hpp:241)
+    float heat = 0.0f;
     if (src.kind == 1) {  // point gravity on the argument state's density
       const float X = (float)src.x[i], Y = (float)src.y[j], Z = (float)src.z[k];
       const float rr = sqrtf(X * X + Y * Y + Z * Z);
@@ -125,6 +128,11 @@ rk_stage_kernel(Geom g, FieldPtrs<const float> prev, FieldPtrs<float> hi, FieldP
       R[MX] += a * X;
       R[MY] += a * Y;
       R[MZ] += a * Z;
+    } else if (src.kind == 2) {  // the functor's terms, filled before the stage
+      R[MX] += (float)src.arr[0][c];
+      R[MY] += (float)src.arr[1][c];
+      R[MZ] += (float)src.arr[2][c];
+      heat = (float)src.arr[3][c];
     }
     if (stage < 3) {
 #pragma unroll
@@ -132,6 +140,7 @@ rk_stage_kernel(Geom g, FieldPtrs<const float> prev, FieldPtrs<float> hi, FieldP
         const float u0 = hi.f[f][c];
         float v = u0 + dt * R[f];
         if (f == PH) v = (u0 + dt * R[f]) * decay;
+        if (f == ET && src.kind == 2) v += heat;
         out.f[f][c] = v;
       }
     } else {
@@ -146,6 +155,8 @@ rk_stage_kernel(Geom g, FieldPtrs<const float> prev, FieldPtrs<float> hi, FieldP
           const float p = s * decay;
           const float pe = fmaf(s, decay, -p);
           two_sum(p, pe + t * decay, s, e);
+        } else if (f == ET && src.kind == 2) {
+          two_sum(h, (l + dt * R[f]) + heat, s, e);
         } else {
           two_sum(h, l + dt * R[f], s, e);
         }
@@ -426,7 +437,7 @@ from_split_kernel(long long cells, FieldPtrs<const float> hi, FieldPtrs<const fl
        n += (long long)gridDim.x * blockDim.x) {
     double u[NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) u[f] = (double)hi.f[f][n] + (double)lo.f[f][n];
+    for (int f = 0; f < NF; ++f) u[f] = (double)hi.f[f][n] + (lo.f[f] ? (double)lo.f[f][n] : 0.0);
     const double ro = u[RO];
     const double vx = u[MX] / ro, vy = u[MY] / ro, vz = u[MZ] / ro;
     const double bb = u[BX] * u[BX] + u[BY] * u[BY] + u[BZ] * u[BZ];

@@ -310,15 +310,17 @@ class Integrator:
             self._h, ctypes.cast(self._bc_cb, ctypes.c_void_p), None, 1))
 
     def set_source_callback(self, fn, on_host: bool = True):
-        """A source functor of the caller's own (FP64 form; the reference's
-        Source concept, mhd_model_base.hpp:131-155): before every
-        Runge-Kutta stage ``fn(q, s)`` gets the stage's argument state ``q``
-        (the 9 primitive fields with ghosts, (9, I, J, K) float64) and fills
-        ``s`` ((4, I, J, K): src.vx, src.vy, src.vz, src.ei of every
-        interior cell) in place.  With ``on_host`` both are numpy arrays over
-        host copies; otherwise ``fn(q, s, stream)`` gets lists of device
-        addresses (9 and 4) and the cudaStream_t of the handle.
-        ``fn=None`` removes it."""
+        """A source functor of the caller's own (the reference's Source
+        concept, mhd_model_base.hpp:131-155): before every Runge-Kutta stage
+        ``fn(q, s)`` gets the stage's argument state ``q`` (the 9 primitive
+        fields with ghosts, (9, I, J, K) float64) and fills ``s`` ((4, I, J,
+        K): src.vx, src.vy, src.vz, src.ei of every interior cell) in place.
+        With ``on_host`` both are numpy arrays over host copies; otherwise
+        ``fn(q, s, stream)`` gets lists of device addresses (9 and 4) and the
+        cudaStream_t of the handle.  In the split form ``q`` is the argument
+        state converted to FP64 primitives (hi + lo for the step's first
+        stage) and the grid runs its per-cell kernels while a callback is
+        set.  ``fn=None`` removes it."""
         if fn is None:
             self._check(self._lib.miso_b200_set_source_callback(self._h, None, None, 0))
             self._src_cb = None

@@ -245,6 +245,25 @@ def test_modelbase_double_split_form_by_config(tmp_path, oracle):
 
 
 @pytest.mark.gpu
+def test_modelbase_gravity_functor_split_form_by_config(tmp_path, oracle):
+    """Real = double with b200.precision fp32_split: the model's own gravity
+    functor is handed each stage's argument state as FP64 primitives and the
+    split form steps on its per-cell kernels, within 1e-6 in ro and 1e-4 in
+    the momentum (relative L1) of the oracle's gravity."""
+    exe = _binary("modelbase_fp64")
+    base = P.blast(12, seed=5)
+    prob = P.with_point_gravity(base, 0.3)
+    ref = prob.q.copy()
+    oracle.run(prob, ref, 4)
+    r = _run(exe, tmp_path, base, "mirror", "update:4", source="grav:0.3",
+             extra="b200:\n  precision: fp32_split\n")
+    assert r.returncode == 0, r.stdout + r.stderr
+    a, b = interior(base, _snapshot(tmp_path, base, 0)), interior(base, ref)
+    assert rel_l1(a[P.RO], b[P.RO]) < 1e-6
+    assert rel_l1(a[P.RO] * a[P.VX:P.VZ + 1], b[P.RO] * b[P.VX:P.VZ + 1]) < 1e-4
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("exe_name,make,bc,message", [
     ("modelbase_f32", lambda: P.brio_wu(64), "loop", "not a set of mirror faces"),
     ("modelbase_fp64", lambda: P.brio_wu(64), "empty", "EmptyBoundaryCondition leaves"),
@@ -312,10 +331,10 @@ def test_modelbase_gravity_source_bit_exact(tmp_path, oracle, exe_name):
 
 
 @pytest.mark.gpu
-def test_modelbase_user_source_refused_in_split_form(tmp_path):
+def test_modelbase_user_source_refused_with_float(tmp_path):
     exe = _binary("modelbase_f32")
     prob = P.blast(12, seed=5)
     r = _run(exe, tmp_path, prob, "mirror", "update:1", real=np.float32,
              source="const:0,0,0,0")
     assert r.returncode == 3, r.stdout + r.stderr
-    assert "FP64 form only" in r.stdout
+    assert "Real = double only" in r.stdout

@@ -72,7 +72,8 @@
 //     functor is refused with an exception.
 //
 // Single rank: a decomposition over several MPI ranks is refused (use the
-// slab interface of the C ABI, miso_b200_set_halo).  Errors are thrown as
+// halo interface of the C ABI, miso_b200_set_halo / miso_b200_set_halo3).
+// Errors are thrown as
 // miso_b200::Error (std::runtime_error).
 #ifndef MISO_B200_BACKEND_HPP
 #define MISO_B200_BACKEND_HPP

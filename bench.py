@@ -59,10 +59,12 @@ def parse():
                     help="turbulence: one 3-D grid (the headline); the batch workloads run "
                          "many instances through the batched solver")
     ap.add_argument("--count", type=int, default=0, help="instances of a batch workload")
-    ap.add_argument("--decomp", choices=["replicas", "slab"], default="replicas",
+    ap.add_argument("--decomp", choices=["replicas", "slab", "box"], default="replicas",
                     help="turbulence under torchrun: independent n^3 grids per rank "
-                         "(replicas), or one (n*N) x n x n periodic grid cut into N slabs "
-                         "along x with the face halos exchanged over NCCL after every pass")
+                         "(replicas), one (n*N) x n x n periodic grid cut into N slabs "
+                         "along x (slab), or one periodic grid of N n^3 boxes cut along "
+                         "x, y and z (box: N's prime factors shared out over z, y, x), with "
+                         "the face halos exchanged over NCCL after every pass")
     return ap.parse_args()
 
 
@@ -469,6 +471,23 @@ def roofline_of(report: dict, precision: str, value_per_gpu: float) -> dict:
     return out
 
 
+def box_dims(world):
+    """Shards per axis (x, y, z) for N ranks: N's prime factors, largest
+    first, each to the axis that has the fewest shards so far (z, then y,
+    then x on a tie)."""
+    f, n, p = [], world, 2
+    while n > 1:
+        while n % p == 0:
+            f.append(p)
+            n //= p
+        p += 1
+    dims = [1, 1, 1]
+    for q in sorted(f, reverse=True):
+        a = min((2, 1, 0), key=lambda ax: dims[ax])
+        dims[a] *= q
+    return tuple(dims)
+
+
 def run_slab(args):
     """One periodic grid of (n * N) x n x n cells over N GPUs, cut into N
     slabs along x (miso_b200.shard): every pass's i ghost planes travel to
@@ -477,7 +496,8 @@ def run_slab(args):
     sequence cfl() -> update(dt).  Every slab holds the unit cube's
     turbulence field (its Fourier modes have period 1 in x, so the stacked
     field is the periodic field of the long box).  Weak scaling: n^3 cells
-    per GPU."""
+    per GPU.  With --decomp box the N cubes are stacked along x, y and z
+    (box_dims) and the j and k faces travel too, packed by the library."""
     import torch
 
     from miso_b200 import problems as P
@@ -499,9 +519,16 @@ def run_slab(args):
         from miso_b200.autotune import autotune
         tuning = autotune(integ)  # the tuner steps with run(): before the halo is attached
         integ.upload(prob.q)
+    box = args.decomp == "box"
+    dims = box_dims(world) if box else (world, 1, 1)
     if world > 1:
-        DistHalo(periodic_x=True, device="cuda").attach(
-            integ, ShardSpec(rank, world, 0, n, prob.grid, True, True))
+        coord = (rank // (dims[1] * dims[2]), (rank // dims[2]) % dims[1], rank % dims[2])
+        ext = tuple((dims[a] > 1, dims[a] > 1) for a in range(3))
+        spec = ShardSpec(rank, world, 0, n, prob.grid, ext[0][0], ext[0][1], dims=dims,
+                         coord=coord, lo=tuple(c * n for c in coord),
+                         hi=tuple((c + 1) * n for c in coord), ext=ext)
+        DistHalo(periodic_x=True, device="cuda", dims=dims,
+                 periodic=(True, True, True)).attach(integ, spec)
     integ.apply_boundary_condition()
 
     def steps(k):
@@ -550,11 +577,16 @@ def run_slab(args):
             "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.precision == "fp32_split" else "f64",
             "data": "synthetic (seeded solenoidal Fourier modes)",
-            "config": {"workload": f"3D decaying MHD turbulence ({n}*{world})x{n}x{n} periodic, "
-                                   f"one grid in {world} slabs along x, {args.precision}",
+            "config": {"workload": (f"3D decaying MHD turbulence ({n}*{dims[0]})x({n}*{dims[1]})"
+                                    f"x({n}*{dims[2]}) periodic, one grid in "
+                                    f"{dims[0]}x{dims[1]}x{dims[2]} boxes, {args.precision}"
+                                    if box else
+                                    f"3D decaying MHD turbulence ({n}*{world})x{n}x{n} periodic, "
+                                    f"one grid in {world} slabs along x, {args.precision}"),
                        "precision": args.precision, "cells_per_gpu": cells,
                        "l2": "inputs larger than L2 (state > 1 GB)",
-                       "parallelism": f"slab x{world} (NCCL halo exchange)"},
+                       "parallelism": (f"box {dims[0]}x{dims[1]}x{dims[2]}" if box
+                                       else f"slab x{world}") + " (NCCL halo exchange)"},
             "timed_path": "Integrator.cfl() -> update(dt) per step, dt all-reduced over ranks",
             "tuning": tuning, "gpu_launches": launches,
             "kernels": {k: {"launches": v["launches"], "ms_per_step": v["ms"] / 2}
@@ -734,7 +766,7 @@ def main():
         run_reference(args)
     elif args.workload != "turbulence":
         run_batch(args)
-    elif args.decomp == "slab":
+    elif args.decomp in ("slab", "box"):
         run_slab(args)
     else:
         run_b200(args)

@@ -195,3 +195,14 @@ def test_split_grid3_boxes_and_round_trip():
                           blast.q[(slice(None),) + blast.grid.interior])
     with pytest.raises(ValueError):
         split_grid3(prob.grid, (1, 5, 1), (True, True, True))
+
+
+def test_bench_box_dims():
+    """bench.py --decomp box: N ranks as shards per axis whose product is N,
+    the counts as even as N's prime factors allow, z first."""
+    from bench import box_dims
+    assert [box_dims(n) for n in (1, 2, 4, 8, 12)] == \
+        [(1, 1, 1), (1, 1, 2), (1, 2, 2), (2, 2, 2), (2, 2, 3)]
+    for n in range(1, 33):
+        d = box_dims(n)
+        assert d[0] * d[1] * d[2] == n

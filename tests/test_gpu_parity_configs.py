@@ -141,3 +141,40 @@ def test_batch_stated_config_vs_oracle(name):
                     tol = 1e-5 if name.startswith("brio") else 1e-6
                     assert e_ro <= tol, (name, i, int(sizes[i]), e_ro)
                     assert e_p <= 1e-5 and e_b <= 1e-5, (name, i, e_p, e_b)
+
+
+def test_blast384_sharp_matches_reference_record():
+    """The blast configuration as stated (384^3, sharp pressure edge, seed
+    0) in the FP64 form: its time step and its FP64 sum of ei over the
+    interior equal the reference host integrator's at every one of steps
+    1-21, bit for bit (tests/golden/blast384_sharp_reference.json, made by
+    tests/golden/make_blast384_record.py), and, like the reference's, its
+    step 22 leaves non-finite values, which the next CFL pass reports."""
+    import json
+    import os
+
+    from miso_b200 import _lib
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                        "blast384_sharp_reference.json")
+    rec = json.load(open(path))["steps"]
+    assert len(rec) == 22 and not np.isfinite(rec[21]["sum_ei"])
+    prob = P.blast(384, seed=0)
+    g = prob.grid
+    integ = Integrator(prob.config, g, sign=prob.sign, precision="fp64")
+    integ.upload(prob.q)
+    integ.apply_boundary_condition()
+    out = np.empty((9,) + tuple(g.shape))
+    for r in rec:
+        dt = integ.cfl()
+        assert dt == r["dt"], r["step"]
+        integ.update(dt)
+        integ.download(out=out)
+        total = float(np.sum(out[P.EI][g.interior], dtype=np.float64))
+        if np.isfinite(r["sum_ei"]):
+            assert total == r["sum_ei"], r["step"]
+        else:
+            assert not np.isfinite(total)
+    with pytest.raises(_lib.MisoError) as e:
+        integ.cfl()
+    assert e.value.code == _lib.ERR_NONFINITE
+    integ.close()

@@ -323,8 +323,9 @@ int miso_b200_set_halo3(miso_b200_handle *h, const int ext[6], const miso_b200_h
  * built-in source; fn == NULL removes it.  In the FP32 split form q holds the
  * stage's argument state converted to FP64 primitives (hi + lo words for the
  * step's first stage, the FP32 stage buffer otherwise), the terms enter the
- * FP32 right-hand side, and the grid runs its per-cell kernels while a
- * callback is set.  ERR_STATE on a grid in shards; no graph capture
+ * FP32 right-hand side, and the last stage's update is not deferred into the
+ * x sweep while a callback is set.  ERR_STATE on a grid in shards; no graph
+ * capture
  * (miso_b200_run with use_graph refuses, miso_b200_run_until launches the
  * steps from the host). */
 typedef int (*miso_b200_source_fn)(void *user, const double *const q[9], double *const s[4],

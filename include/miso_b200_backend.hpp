@@ -40,7 +40,7 @@
 // j, k), mhd_model_base.hpp:131-155) is evaluated, in the FP64 form, on host
 // copies of every stage's argument state (miso_b200_set_source_callback):
 // exact, and slow (with b200.precision: fp32_split, the split form hands it
-// the argument state as FP64 primitives and runs its per-cell kernels).
+// the argument state as FP64 primitives).
 // Where the model's translation unit is compiled by nvcc
 // and the functor type is declared device-callable --
 //

@@ -829,7 +829,7 @@ struct miso_b200_handle {
   // the pipelined kernels of a 3-D split grid, unless the magnetosphere
   // boundary or a caller's source needs the per-cell kernels
   void retile() {
-    const bool t = tiled_ok && !mag.on && !(src_cb && split());
+    const bool t = tiled_ok && !mag.on;
     if (t != tiled) partials_valid = false;
     tiled = t;
   }
@@ -1002,7 +1002,9 @@ struct miso_b200_handle {
     return items < av_grid ? items : av_grid;
   }
   bool defer_last() const {
-    return rk_var == 3 && av_var[0] == 0 && av_var[1] != 1 && av_var[2] != 1;
+    // (a caller's source heats the new total energy, which the deferred
+    // update, formed in the x sweep, does not add)
+    return rk_var == 3 && av_var[0] == 0 && av_var[1] != 1 && av_var[2] != 1 && src.kind != 2;
   }
 
   int enqueue_update_tiled() {
@@ -1010,6 +1012,14 @@ struct miso_b200_handle {
     const int c = cur;
     const bool defer = defer_last();
     for (int st = 0; st < 4; ++st) {
+      if (src_cb) {
+        // the caller's source on the stage's argument state (U^n with the
+        // lo images current, or the last stage's output)
+        if (st == 0 && (rc = fresh_lo_shell())) return rc;
+        if ((rc = src_callback_split(st == 0 ? cst(H(c)) : cst(S((st - 1) & 1)),
+                                     st == 0 ? cst(L(c)) : FieldPtrs<const float>{})))
+          return rc;
+      }
       RkArgs a;
       a.g = g;
       a.u0 = cfs(hi[c]);
@@ -1831,13 +1841,7 @@ int miso_b200_set_source_callback(miso_b200_handle *h, miso_b200_source_fn fn, v
   h->src_cb = fn;
   h->src_user = user;
   h->src_host = fn && on_host;
-  if (h->split()) {
-    // the split form evaluates a caller's source on the per-cell kernels
-    // (the pipelined stages fuse what the callback must see between them);
-    // they read the lo ghost words, which the pipelined step leaves stale
-    if (int rc = h->fresh_lo_shell()) return rc;
-    h->retile();
-  }
+
   if (h->graph_exec) {
     cudaGraphExecDestroy(h->graph_exec);
     cudaGraphDestroy(h->graph);

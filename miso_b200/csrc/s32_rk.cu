@@ -286,11 +286,21 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
       D.p[i] = sub2(R2.p[i], mul2(k.wx2, N));
     }
     D.s = __fsub_rn(R2.s, __fmul_rn(k.wx, fmaf(-8.f, F1.s, Fn.s)));
+    // a caller's source functor: its heating enters the new total energy
+    // outside the dt factor (mhd_integrator_host.hpp:241)
+    float heat = 0.0f;
     if (SRC) {
       // the source's force enters the momentum RHS: D -= force
-      const float ro = STAGE == 0 ? A0[RO] : __ldg(a.src_ro + cell);
       float fx, fy, fz;
-      gravity_force(a.src, ro, c + g.m[0], jg + g.m[1], kg + g.m[2], fx, fy, fz);
+      if (a.src.kind == 2) {  // the functor's terms, filled before the stage
+        fx = (float)__ldg(a.src.arr[0] + cell);
+        fy = (float)__ldg(a.src.arr[1] + cell);
+        fz = (float)__ldg(a.src.arr[2] + cell);
+        heat = (float)__ldg(a.src.arr[3] + cell);
+      } else {
+        const float ro = STAGE == 0 ? A0[RO] : __ldg(a.src_ro + cell);
+        gravity_force(a.src, ro, c + g.m[0], jg + g.m[1], kg + g.m[2], fx, fy, fz);
+      }
       D.p[0].y -= fx;  // (ro, mx)
       D.p[1].x -= fy;  // (my, mz)
       D.p[1].y -= fz;
@@ -307,7 +317,8 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
 #pragma unroll
       for (int i = 0; i < NPAIR; ++i) {
         const float2 u0 = f2(A0[2 * i], A0[2 * i + 1]);
-        const float2 v = fma2(k.mdt2, D.p[i], u0);
+        float2 v = fma2(k.mdt2, D.p[i], u0);
+        if (SRC && i == 3) v.y = __fadd_rn(v.y, heat);  // (bz, et)
         a.out.f[2 * i][cell] = v.x;
         a.out.f[2 * i + 1][cell] = v.y;
       }
@@ -323,7 +334,8 @@ __device__ __forceinline__ bool plane_step(const RkArgs &a, PipeSmem &sm, const 
         float *h0 = a.hi.f[2 * i], *h1 = a.hi.f[2 * i + 1];
         float *l0 = a.lo.f[2 * i], *l1 = a.lo.f[2 * i + 1];
         const float2 h = f2(A0[2 * i], A0[2 * i + 1]);
-        const float2 b = fma2(k.mdt2, D.p[i], f2(A1[2 * i], A1[2 * i + 1]));
+        float2 b = fma2(k.mdt2, D.p[i], f2(A1[2 * i], A1[2 * i + 1]));
+        if (SRC && i == 3) b.y = __fadd_rn(b.y, heat);  // (bz, et)
         const float2 sm2 = add2(h, b);
         const float2 bb = sub2(sm2, h);
         const float2 e = add2(sub2(h, sub2(sm2, bb)), sub2(b, bb));

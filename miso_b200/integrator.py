@@ -319,8 +319,7 @@ class Integrator:
         ``fn(q, s, stream)`` gets lists of device addresses (9 and 4) and the
         cudaStream_t of the handle.  In the split form ``q`` is the argument
         state converted to FP64 primitives (hi + lo for the step's first
-        stage) and the grid runs its per-cell kernels while a callback is
-        set.  ``fn=None`` removes it."""
+        stage).  ``fn=None`` removes it."""
         if fn is None:
             self._check(self._lib.miso_b200_set_source_callback(self._h, None, None, 0))
             self._src_cb = None

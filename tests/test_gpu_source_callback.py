@@ -168,10 +168,10 @@ def _device_gravity(grid, gconst):
 def test_split_form_callback_gravity(make, nsteps, on_host):
     """The split form with the gravity as a caller's callback -- the stage's
     argument state handed over as FP64 primitives (hi + lo for U^n), the
-    grid on its per-cell kernels -- follows the FP64 form with the built-in
-    gravity stepped with the same dt sequence: relative L1 of ro <= 1e-6 and
-    of the momentum <= 1e-4, while dropping the source moves the momentum by
-    more than 100x that."""
+    terms read by the pipelined RK stage (3-D) or the per-cell one (2-D) --
+    follows the FP64 form with the built-in gravity stepped with the same dt
+    sequence: relative L1 of ro <= 1e-6 and of the momentum <= 1e-4, while
+    dropping the source moves the momentum by more than 100x that."""
     prob = make()
     g = prob.config["source"]["g"]
     ref = Integrator(prob.config, prob.grid, sign=prob.sign, precision="fp64")

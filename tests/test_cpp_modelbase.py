@@ -248,8 +248,8 @@ def test_modelbase_double_split_form_by_config(tmp_path, oracle):
 def test_modelbase_gravity_functor_split_form_by_config(tmp_path, oracle):
     """Real = double with b200.precision fp32_split: the model's own gravity
     functor is handed each stage's argument state as FP64 primitives and the
-    split form steps on its per-cell kernels, within 1e-6 in ro and 1e-4 in
-    the momentum (relative L1) of the oracle's gravity."""
+    split form adds its terms, within 1e-6 in ro and 1e-4 in the momentum
+    (relative L1) of the oracle's gravity."""
     exe = _binary("modelbase_fp64")
     base = P.blast(12, seed=5)
     prob = P.with_point_gravity(base, 0.3)

@@ -245,12 +245,15 @@ def test_modelbase_double_split_form_by_config(tmp_path, oracle):
 
 
 @pytest.mark.gpu
-def test_modelbase_gravity_functor_split_form_by_config(tmp_path, oracle):
+@pytest.mark.parametrize("exe_name", ["modelbase_fp64", "modelbase_fp64_cuda"],
+                         ids=["host_functor", "device_functor"])
+def test_modelbase_gravity_functor_split_form_by_config(tmp_path, oracle, exe_name):
     """Real = double with b200.precision fp32_split: the model's own gravity
-    functor is handed each stage's argument state as FP64 primitives and the
-    split form adds its terms, within 1e-6 in ro and 1e-4 in the momentum
-    (relative L1) of the oracle's gravity."""
-    exe = _binary("modelbase_fp64")
+    functor (on host copies, or on the device from nvcc's build) is handed
+    each stage's argument state as FP64 primitives and the split form adds
+    its terms, within 1e-6 in ro and 1e-4 in the momentum (relative L1) of
+    the oracle's gravity."""
+    exe = _binary(exe_name)
     base = P.blast(12, seed=5)
     prob = P.with_point_gravity(base, 0.3)
     ref = prob.q.copy()

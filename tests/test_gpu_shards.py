@@ -245,3 +245,33 @@ def test_dist_halo_one_rank_all_faces_equals_single_grid(precision):
         assert np.array_equal(got, ref)
     finally:
         dist.destroy_process_group()
+
+
+def test_halo3_callback_error_stops_the_step():
+    """An exchange callback that fails on the k faces stops the step with
+    MISO_B200_ERR_HALO (the error is reported, nothing aborts); the i and j
+    exchanges before it went through the same callback."""
+    import ctypes
+
+    from miso_b200 import _lib
+    prob = P.turbulence(16, seed=2)
+    calls = []
+
+    def exchange(user, axis, n, nbytes, ext_lo, ext_hi, slo, shi, rlo, rhi, stream):
+        calls.append(axis)
+        return 1 if axis == 2 else 0
+    with Integrator(prob.config, prob.grid, precision="fp32_split") as integ:
+        fn = _lib.HALO3_EXCHANGE_FN(exchange)
+        ops = _lib.Halo3Ops(fn, _lib.HALO_MIN_FN(0), None)
+        ext = (ctypes.c_int * 6)(1, 1, 1, 1, 1, 1)
+        assert integ._lib.miso_b200_set_halo3(integ._h, ext, ctypes.byref(ops)) == _lib.OK
+        integ.upload(prob.q)
+        with pytest.raises(_lib.MisoError) as e:
+            integ.apply_boundary_condition()
+        assert e.value.code == _lib.ERR_HALO
+        assert calls == [0, 1, 2]
+        # back to a single grid
+        assert integ._lib.miso_b200_set_halo3(integ._h, None, None) == _lib.OK
+        integ.upload(prob.q)
+        integ.apply_boundary_condition()
+        integ.update(integ.cfl())

@@ -382,9 +382,10 @@ class MHD:
     """Fields + integrator for one grid (miso/include/miso/mhd.hpp:15-50)."""
 
     def __init__(self, config: dict, grid: Grid, sign=None, precision: str = "fp64",
-                 blend=None):
+                 blend=None, stream=None):
         self.grid = grid
-        self.integrator = Integrator(config, grid, sign=sign, precision=precision, blend=blend)
+        self.integrator = Integrator(config, grid, sign=sign, precision=precision, blend=blend,
+                                     stream=stream)
 
     def apply_initial_condition(self, q):
         """Upload initial fields and fill the ghosts (mhd.hpp:28-35)."""

@@ -13,6 +13,13 @@ that follow it.
 Configuration keys, as the reference reads them: ``time.tend``,
 ``time.dt_output``, ``io.enabled``, ``io.continue``, ``io.save_dir``.
 
+A model of a decomposed grid (``shard``, a ShardSpec of miso_b200.shard,
+with ``halo``, its LocalHalo or DistHalo) steps its own box of the global
+grid -- the halos exchanged after every pass and dt reduced over all ranks,
+as the reference's ModelBase does with MPI -- and writes its snapshots in
+the reference's multi-rank layout (one mhd file per rank, coords.csv);
+``run_local_models`` runs such a decomposition as threads on one GPU.
+
 ``run(device_loop=True)`` keeps the steps between two outputs on the device:
 one ``Integrator.run_until`` call -- a CUDA graph whose WHILE node runs
 steps until the device-held time reaches the next output time or
@@ -36,7 +43,7 @@ class Model:
     """One grid's model: fields, integrator, time and output."""
 
     def __init__(self, config: dict, grid: Grid, initial_state: np.ndarray, sign=None,
-                 precision: str = "fp64", blend=None):
+                 precision: str = "fp64", blend=None, shard=None, halo=None, stream=None):
         t = config.get("time") or {}
         if "tend" not in t or "dt_output" not in t:
             raise KeyError("config needs time.tend and time.dt_output")
@@ -49,9 +56,23 @@ class Model:
         self.resume = bool(io.get("continue", False))
         self.config = config
         self.grid = grid
+        self.shard = shard
+        box = grid
+        if shard is not None:
+            from .shard import split_state
+            if halo is None:
+                raise ValueError("a shard needs its halo exchange")
+            box = shard.grid
+            initial_state = split_state(initial_state, grid, shard)
+            if blend is not None:
+                blend = split_state(blend, grid, shard)
         self.q0 = initial_state
-        self.mhd = MHD(config, grid, sign=sign, precision=precision, blend=blend)
-        self.output = (Output(io.get("save_dir", "data/"), config, grid)
+        self.mhd = MHD(config, box, sign=sign, precision=precision, blend=blend, stream=stream)
+        if shard is not None:
+            halo.attach(self.mhd.integrator, shard)
+        self.output = (Output(io.get("save_dir", "data/"), config, grid,
+                              rank=shard.rank if shard is not None else 0,
+                              dims=shard.dims if shard is not None else (1, 1, 1), box=box)
                        if self.io_enabled else None)
         # Time::initialize (time.hpp:37-41)
         self.time = 0.0
@@ -86,7 +107,10 @@ class Model:
             self.n_output += 1
 
     def run(self, device_loop: bool = False):
-        """ModelBase::run (mhd_model_base.hpp:88-116)."""
+        """ModelBase::run (mhd_model_base.hpp:88-116).  A shard steps from
+        the host (its dt is reduced over the ranks)."""
+        if device_loop and self.shard is not None:
+            raise ValueError("a shard steps from the host: device_loop=False")
         self.mhd.apply_initial_condition(self.q0)
         if (self.resume and self.output is not None and
                 os.path.exists(os.path.join(self.output.time_dir, "n_output.txt"))):
@@ -114,3 +138,47 @@ class Model:
         if self.output is not None:
             self.output.wait()
         self.mhd.integrator.close()
+
+
+def run_local_models(config: dict, grid: Grid, initial_state: np.ndarray, dims, sign=None,
+                     precision: str = "fp64", blend=None, stream=None):
+    """ModelBase::run of one grid decomposed into dims[0] x dims[1] x dims[2]
+    boxes, each a Model on the current GPU driven by its own host thread
+    (all on one CUDA stream, the halos moved by device copies: LocalHalo).
+    The snapshots land in the reference's multi-rank layout under
+    ``io.save_dir``.  Returns the models (closed)."""
+    import threading
+
+    import torch
+
+    from .shard import LocalHalo, split_grid3
+    per = config["domain"]["periodic"]
+    periodic = (bool(per["x"]), bool(per["y"]), bool(per["z"]))
+    specs = split_grid3(grid, dims, periodic)
+    count = len(specs)
+    halo = LocalHalo(count, periodic[0], dims=dims, periodic=periodic)
+    keep = None
+    if stream is None:
+        keep = torch.cuda.Stream()
+        stream = keep.cuda_stream
+    models = [Model(config, grid, initial_state, sign=sign, precision=precision, blend=blend,
+                    shard=s, halo=halo, stream=stream) for s in specs]
+    errors = []
+
+    def drive(r):
+        try:
+            models[r].run()
+        except Exception as exc:
+            errors.append(exc)
+            halo._bar.abort()
+
+    threads = [threading.Thread(target=drive, args=(r,)) for r in range(count)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for m in models:
+        m.close()
+    if errors:
+        raise errors[0]
+    return models

@@ -121,3 +121,37 @@ def test_async_snapshot_and_restart(tmp_path):
         again.update(again.cfl())
     assert np.array_equal(again.download(), full)
     again.close()
+
+
+@pytest.mark.skipif(not os.path.isdir(PYMISO_SRC), reason="pymiso sources not present")
+@pytest.mark.parametrize("make,dims", [(lambda: P.orszag_tang(24), (2, 3, 1)),
+                                       (lambda: P.turbulence(8, seed=2), (2, 2, 2))],
+                         ids=["ot2d_2x3", "turb3d_2x2x2"])
+def test_pymiso_reads_decomposed_output(tmp_path, monkeypatch, make, dims):
+    """A run directory of a grid in boxes (one mhd file per rank, every
+    rank's coordinates in coords.csv, the global grid in grid.bin and
+    config.yaml) is read by pymiso as the global field, and by our own
+    load_global alike."""
+    from miso_b200.shard import split_grid3, split_state
+    prob = make()
+    save_dir = str(tmp_path / "data")
+    per = prob.config["domain"]["periodic"]
+    specs = split_grid3(prob.grid, dims, (per["x"], per["y"], per["z"]))
+    outs = [Output(save_dir, prob.config, prob.grid, rank=s.rank, dims=dims, box=s.grid)
+            for s in specs]
+    for o in outs:
+        o.write_setup()
+    for o, s in zip(outs, specs):
+        o.save(_FakeHandle(split_state(prob.q, prob.grid, s)), time=0.25, n_output=1, n_step=9)
+    inner = prob.q[(slice(None),) + prob.grid.interior]
+    assert np.array_equal(outs[0].load_global(1), inner)
+    monkeypatch.setitem(sys.modules, "box", _box_module())
+    monkeypatch.syspath_prepend(PYMISO_SRC)
+    for name in [m for m in sys.modules if m == "pymiso" or m.startswith("pymiso.")]:
+        monkeypatch.delitem(sys.modules, name)
+    import pymiso
+    d = pymiso.Data(save_dir)
+    d.load(1)
+    assert d.time.time == 0.25
+    for v, name in enumerate(("ro", "vx", "vy", "vz", "bx", "by", "bz", "ei", "ph")):
+        assert np.array_equal(getattr(d, name), np.squeeze(inner[v])), name

@@ -148,58 +148,129 @@ monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
 }
 
 // |div B| of the split state (the monitors with their sums folded into the
-// z sweep), the monitor kernel's difference in FP64 from hi + lo, by quads
-// of 4 cells along k that start on a 16-byte boundary (tiled grids: k_total
-// a multiple of 4, margin 2): every neighbour row is one float4 of hi and
-// one of lo, bz takes three per array; lanes on ghost cells of the quad
-// contribute nothing.  The ghost layers must be current (the caller
-// refreshes the lo images first).  Writes slots 5 and 6 of the monitor
-// kernel's per-block layout.
-__device__ __forceinline__ void quad64(const float *h, const float *l, long long c, double v[4]) {
-  const float4 a = __ldg(reinterpret_cast<const float4 *>(h + c));
-  const float4 b = __ldg(reinterpret_cast<const float4 *>(l + c));
-  v[0] = (double)a.x + (double)b.x;
-  v[1] = (double)a.y + (double)b.y;
-  v[2] = (double)a.z + (double)b.z;
-  v[3] = (double)a.w + (double)b.w;
+// z sweep), the monitor kernel's difference in FP64 from hi + lo, by a march
+// along i.  A work item is a tile of DBM_TJ x DBM_TK (j, k) cells over a run
+// of DBM_L planes; a thread owns two neighbouring k cells (one float2 of hi
+// and one of lo per array, tiled grids having k_total a multiple of 4).  bx
+// of the planes i-2 .. i+2 stays in a register ring, so each bx word is read
+// and widened to FP64 once per run (plus the four planes before it); by and
+// bz of plane i go to shared memory as FP64, halo rows and columns included,
+// and the y and z neighbours are read from there: about 7 widenings per cell
+// instead of the 22 of a kernel that widens every neighbour it loads.  The
+// next plane's words are loaded into registers before the plane's barrier,
+// and the shared planes alternate between two buffers, so one barrier per
+// plane suffices.  The ghost layers of bx, by and bz (hi and lo) must be
+// current.  Writes slots 5 and 6 of the monitor kernel's per-block layout;
+// the grid is at most 3 CTAs per SM, all resident, each taking every
+// gridDim-th item.
+constexpr int DBM_TJ = 8, DBM_TK = 64, DBM_L = 64;
+
+struct Raw2 {
+  float2 h, l;
+};
+__device__ __forceinline__ Raw2 ld_raw2(const float *h, const float *l, long long c) {
+  return Raw2{__ldg(reinterpret_cast<const float2 *>(h + c)),
+              __ldg(reinterpret_cast<const float2 *>(l + c))};
+}
+__device__ __forceinline__ double2 widen2(const Raw2 &r) {
+  return make_double2((double)r.h.x + (double)r.l.x, (double)r.h.y + (double)r.l.y);
 }
 
-__global__ void __launch_bounds__(256)
-divb_quad_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
-                 double *__restrict__ partial) {
-  const int nq = g.t[2] / 4;
-  const long long work = (long long)g.n[0] * g.n[1] * nq;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+__global__ void __launch_bounds__(256, 3)
+divb_march_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
+                  double *__restrict__ partial) {
+  __shared__ __align__(16) double sby[2][DBM_TJ + 4][DBM_TK];
+  __shared__ __align__(16) double sbz[2][DBM_TJ][DBM_TK + 4];
+  const int lane = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  const int njt = (n1 + DBM_TJ - 1) / DBM_TJ, nkt = (n2 + DBM_TK - 1) / DBM_TK;
+  const int items = (n0 + DBM_L - 1) / DBM_L * njt * nkt;
+  const float *bxh = hi.f[BX], *bxl = lo.f[BX], *byh = hi.f[BY], *byl = lo.f[BY];
+  const float *bzh = hi.f[BZ], *bzl = lo.f[BZ];
+  // halo duty: warps 0-3 load the by rows j0-2, j0-1, j0+8, j0+9; lanes
+  // 0-15 of warp 4 the bz pairs at k0-2 and k0+64 of the tile's 8 rows
+  const int hy_row = ty < 2 ? ty - 2 : ty + DBM_TJ - 2;  // tile-relative j of a by halo row
+  const int hz_row = lane >> 1, hz_side = lane & 1;
   double sum = 0.0, mx = 0.0;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < work; w += stride) {
-    const int q = (int)(w % nq);
-    const long long r = w / nq;
-    const int j = (int)(r % g.n[1]);
-    const int i = (int)(r / g.n[1]);
-    const long long c = (long long)(i + g.m[0]) * g.st[0] + (long long)(j + g.m[1]) * g.st[1] +
-                        4 * q;  // total k = 4q .. 4q+3
-    double xm2[4], xm1[4], xp1[4], xp2[4], ym2[4], ym1[4], yp1[4], yp2[4], z[12];
-    quad64(hi.f[BX], lo.f[BX], c - 2 * g.st[0], xm2);
-    quad64(hi.f[BX], lo.f[BX], c - g.st[0], xm1);
-    quad64(hi.f[BX], lo.f[BX], c + g.st[0], xp1);
-    quad64(hi.f[BX], lo.f[BX], c + 2 * g.st[0], xp2);
-    quad64(hi.f[BY], lo.f[BY], c - 2 * g.st[1], ym2);
-    quad64(hi.f[BY], lo.f[BY], c - g.st[1], ym1);
-    quad64(hi.f[BY], lo.f[BY], c + g.st[1], yp1);
-    quad64(hi.f[BY], lo.f[BY], c + 2 * g.st[1], yp2);
-    quad64(hi.f[BZ], lo.f[BZ], c - 4, z);
-    quad64(hi.f[BZ], lo.f[BZ], c, z + 4);
-    quad64(hi.f[BZ], lo.f[BZ], c + 4, z + 8);
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int kk = 4 * q + t - g.m[2];  // interior k of this lane of the quad
-      if (kk < 0 || kk >= g.n[2]) continue;
-      double divb = 0.0;
-      divb += (-xp2[t] + 8.0 * xp1[t] - 8.0 * xm1[t] + xm2[t]) * INV12 * g.dsi[0];
-      divb += (-yp2[t] + 8.0 * yp1[t] - 8.0 * ym1[t] + ym2[t]) * INV12 * g.dsi[1];
-      divb += (-z[t + 6] + 8.0 * z[t + 5] - 8.0 * z[t + 3] + z[t + 2]) * INV12 * g.dsi[2];
-      sum += fabs(divb);
-      mx = fmax(mx, fabs(divb));
+  int par = 0;  // shared buffer of the current plane; flips once per plane
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    int r = it;
+    const int kt = r % nkt;
+    r /= nkt;
+    const int jt = r % njt;
+    const int i0 = r / njt * DBM_L;
+    const int i1 = min(i0 + DBM_L, n0);
+    const int j0 = jt * DBM_TJ, k0 = kt * DBM_TK;
+    const int j = j0 + ty, k = k0 + 2 * lane;  // interior (j, k) of this thread's pair
+    const bool own = j < n1 && k < n2;         // n2 is a multiple of 4: k + 1 < n2 too
+    const bool yv = j <= n1 + 1 && k < n2;     // by pair that an owned cell reads
+    const bool zv = j < n1 && k <= n2;         // bz pair that an owned cell reads
+    const int jh = j0 + hy_row, kh = hz_side ? k0 + DBM_TK : k0 - 2, jz = j0 + hz_row;
+    const bool hy = ty < 4 && jh <= n1 + 1 && k < n2;
+    const bool hz = ty == 4 && lane < 16 && jz < n1 && kh <= n2;
+    const long long cj = (long long)(j + g.m[1]) * g.st[1] + (k + g.m[2]);
+    const long long ch = hy ? (long long)(jh + g.m[1]) * g.st[1] + (k + g.m[2])
+                            : (long long)(jz + g.m[1]) * g.st[1] + (kh + g.m[2]);
+    double2 x0 = make_double2(0.0, 0.0), x1 = x0, x3 = x0;  // bx of planes i-2, i-1, i+1
+    double2 x2 = x0;                                        // bx of plane i (not in the stencil)
+    if (own) {
+      const long long c = (long long)(i0 + g.m[0]) * g.st[0] + cj;
+      x0 = widen2(ld_raw2(bxh, bxl, c - 2 * g.st[0]));
+      x1 = widen2(ld_raw2(bxh, bxl, c - g.st[0]));
+      x2 = widen2(ld_raw2(bxh, bxl, c));
+      x3 = widen2(ld_raw2(bxh, bxl, c + g.st[0]));
+    }
+    Raw2 px{}, py{}, pz{}, ph{};  // plane i's words: bx at i+2, by, bz, halo
+    {
+      const long long ci = (long long)(i0 + g.m[0]) * g.st[0];
+      if (own) px = ld_raw2(bxh, bxl, ci + 2 * g.st[0] + cj);
+      if (yv) py = ld_raw2(byh, byl, ci + cj);
+      if (zv) pz = ld_raw2(bzh, bzl, ci + cj);
+      if (hy) ph = ld_raw2(byh, byl, ci + ch);
+      if (hz) ph = ld_raw2(bzh, bzl, ci + ch);
+    }
+    for (int i = i0; i < i1; ++i, par ^= 1) {
+      if (yv) *reinterpret_cast<double2 *>(&sby[par][ty + 2][2 * lane]) = widen2(py);
+      if (zv) *reinterpret_cast<double2 *>(&sbz[par][ty][2 * lane + 2]) = widen2(pz);
+      if (hy) *reinterpret_cast<double2 *>(&sby[par][hy_row + 2][2 * lane]) = widen2(ph);
+      if (hz)
+        *reinterpret_cast<double2 *>(&sbz[par][hz_row][hz_side ? DBM_TK + 2 : 0]) = widen2(ph);
+      const double2 x4 = own ? widen2(px) : make_double2(0.0, 0.0);
+      if (i + 1 < i1) {  // the next plane's words, in flight across the barrier
+        const long long ci = (long long)(i + 1 + g.m[0]) * g.st[0];
+        if (own) px = ld_raw2(bxh, bxl, ci + 2 * g.st[0] + cj);
+        if (yv) py = ld_raw2(byh, byl, ci + cj);
+        if (zv) pz = ld_raw2(bzh, bzl, ci + cj);
+        if (hy) ph = ld_raw2(byh, byl, ci + ch);
+        if (hz) ph = ld_raw2(bzh, bzl, ci + ch);
+      }
+      __syncthreads();
+      if (own) {
+        const double2 ym2 = *reinterpret_cast<const double2 *>(&sby[par][ty][2 * lane]);
+        const double2 ym1 = *reinterpret_cast<const double2 *>(&sby[par][ty + 1][2 * lane]);
+        const double2 yp1 = *reinterpret_cast<const double2 *>(&sby[par][ty + 3][2 * lane]);
+        const double2 yp2 = *reinterpret_cast<const double2 *>(&sby[par][ty + 4][2 * lane]);
+        // bz of k-2 .. k+3
+        const double2 za = *reinterpret_cast<const double2 *>(&sbz[par][ty][2 * lane]);
+        const double2 zb = *reinterpret_cast<const double2 *>(&sbz[par][ty][2 * lane + 2]);
+        const double2 zc = *reinterpret_cast<const double2 *>(&sbz[par][ty][2 * lane + 4]);
+        double divb = 0.0;
+        divb += (-x4.x + 8.0 * x3.x - 8.0 * x1.x + x0.x) * INV12 * g.dsi[0];
+        divb += (-yp2.x + 8.0 * yp1.x - 8.0 * ym1.x + ym2.x) * INV12 * g.dsi[1];
+        divb += (-zc.x + 8.0 * zb.y - 8.0 * za.y + za.x) * INV12 * g.dsi[2];
+        sum += fabs(divb);
+        mx = fmax(mx, fabs(divb));
+        divb = 0.0;
+        divb += (-x4.y + 8.0 * x3.y - 8.0 * x1.y + x0.y) * INV12 * g.dsi[0];
+        divb += (-yp2.y + 8.0 * yp1.y - 8.0 * ym1.y + ym2.y) * INV12 * g.dsi[1];
+        divb += (-zc.y + 8.0 * zc.x - 8.0 * zb.x + za.y) * INV12 * g.dsi[2];
+        sum += fabs(divb);
+        mx = fmax(mx, fabs(divb));
+      }
+      x0 = x1;
+      x1 = x2;
+      x2 = x3;
+      x3 = x4;
     }
   }
 #pragma unroll
@@ -208,10 +279,9 @@ divb_quad_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
     mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   }
   __shared__ double red[8][2];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (lane == 0) {
-    red[wid][0] = sum;
-    red[wid][1] = mx;
+    red[ty][0] = sum;
+    red[ty][1] = mx;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -350,6 +420,7 @@ struct miso_b200_handle {
   int z_parts = 0;  // CFL partial minima written by the last z sweep
   bool partials_valid = false;  // `partial` holds CFL minima of the current state
   bool lo_shell_stale = false;  // the lo ghost images lag the interior (filled on download)
+  bool lo_b_fresh = false;      // while stale: those of bx, by and bz are current
   // kernel variant per class on the 3-D split path: 0 = tiled (TMA plane
   // tiles / streaming lines), 1 = flat (one thread per cell); 2: RK =
   // pipelined TMA planes with packed FP32x2 differences (default), x / y
@@ -841,6 +912,27 @@ struct miso_b200_handle {
     lo_shell_stale = false;
     return shell(lo[cur], SHELL_ALL);
   }
+  // the same for bx, by and bz alone (the div B stencil of the monitors);
+  // the other lo images stay stale until a download
+  int fresh_lo_b() {
+    if (!lo_shell_stale || lo_b_fresh) return MISO_B200_OK;
+    lo_b_fresh = true;
+    ShellArgs sa;
+    sa.n = 0;
+    for (int f = BX; f <= BZ; ++f) {
+      sa.p[sa.n] = lo[cur][f];
+      sa.f[sa.n] = f;
+      sa.m[sa.n++] = SHELL_ALL;
+    }
+    sa.slab = -1;
+    const long long cells = s32_shell_count(g, sa.slab);
+    long long grid = (cells + 255) / 256;
+    if (grid > 8LL * sms) grid = 8LL * sms;
+    const int t = tb();
+    launch_s32_shell(g, sa, (int)grid, stream);
+    te(t, "ghost_shell", (double)cells * 8.0 * sa.n);
+    return check_launch("ghost_shell");
+  }
 
   // ghost images of the interior shell: the 9 arrays of `set` with image
   // mask `mset`, and (when given) cc with mask `mcc`
@@ -1135,6 +1227,7 @@ struct miso_b200_handle {
         if ((rc = check_launch("av_yz"))) return rc;
         if ((rc = shell(hi[cur ^ 1], SHELL_ALL))) return rc;
         lo_shell_stale = true;
+        lo_b_fresh = false;
         cur ^= 1;
         break;
       }
@@ -1179,6 +1272,7 @@ struct miso_b200_handle {
           if ((rc = shell(hi[cur ^ 1], m))) return rc;
         }
         lo_shell_stale = true;
+        lo_b_fresh = false;
       } else {
         lo_shell_stale = false;
       }
@@ -2283,14 +2377,19 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
     if (h->g.s[a]) dv *= 1.0 / h->g.dsi[a];
   if (h->split() && h->mon_valid) {
     // the last z sweep summed the state; only |div B| is left to reduce (its
-    // stencil reads lo ghost words, which lag the interior until refreshed)
-    if ((rc = h->fresh_lo_shell())) return rc;
-    divb_quad_kernel<<<h->mon_blocks, 256, 0, h->stream>>>(
-        h->g, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)), h->mon_partial);
+    // stencil reads the lo ghost words of bx, by and bz, which lag the
+    // interior until refreshed)
+    if ((rc = h->fresh_lo_b())) return rc;
+    const Geom &g = h->g;
+    const long long items = (long long)((g.n[0] + DBM_L - 1) / DBM_L) *
+                            ((g.n[1] + DBM_TJ - 1) / DBM_TJ) * ((g.n[2] + DBM_TK - 1) / DBM_TK);
+    const int nb = items < 3LL * h->sms ? (int)items : 3 * h->sms;  // <= mon_blocks
+    divb_march_kernel<<<nb, 256, 0, h->stream>>>(g, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)),
+                                                 h->mon_partial);
     h->launches++;
     if ((rc = h->check_launch("divb"))) return rc;
     // per-block sums of the sweep that left them (z_parts blocks)
-    std::vector<double> zs((size_t)h->z_parts * 6), db((size_t)h->mon_blocks * 8);
+    std::vector<double> zs((size_t)h->z_parts * 6), db((size_t)nb * 8);
     if ((rc = h->cuda(cudaMemcpyAsync(zs.data(), h->mon_z, zs.size() * sizeof(double),
                                       cudaMemcpyDeviceToHost, h->stream),
                       "read monitors")) ||
@@ -2303,7 +2402,7 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
     const int map[6] = {0, 1, 2, 3, 4, 7};  // ro, mx, my, mz, et, ph^2
     for (int b = 0; b < h->z_parts; ++b)
       for (int q = 0; q < 6; ++q) out[map[q]] += zs[(size_t)b * 6 + q];
-    for (int b = 0; b < h->mon_blocks; ++b) {
+    for (int b = 0; b < nb; ++b) {
       out[5] += db[(size_t)b * 8 + 5];
       out[6] = std::fmax(out[6], db[(size_t)b * 8 + 6]);
     }

@@ -150,20 +150,21 @@ monitor_kernel(Geom g, FieldPtrs<const double> q, FieldPtrs<const float> hi,
 // |div B| of the split state (the monitors with their sums folded into the
 // z sweep), the monitor kernel's difference in FP64 from hi + lo, by a march
 // along i.  A work item is a tile of DBM_TJ x DBM_TK (j, k) cells over a run
-// of DBM_L planes; a thread owns two neighbouring k cells (one float2 of hi
-// and one of lo per array, tiled grids having k_total a multiple of 4).  bx
-// of the planes i-2 .. i+2 stays in a register ring, so each bx word is read
-// and widened to FP64 once per run (plus the four planes before it); by and
-// bz of plane i go to shared memory as FP64, halo rows and columns included,
-// and the y and z neighbours are read from there: about 7 widenings per cell
-// instead of the 22 of a kernel that widens every neighbour it loads.  The
-// next plane's words are loaded into registers before the plane's barrier,
-// and the shared planes alternate between two buffers, so one barrier per
-// plane suffices.  The ghost layers of bx, by and bz (hi and lo) must be
-// current.  Writes slots 5 and 6 of the monitor kernel's per-block layout;
-// the grid is at most 3 CTAs per SM, all resident, each taking every
-// gridDim-th item.
-constexpr int DBM_TJ = 8, DBM_TK = 64, DBM_L = 64;
+// of DBM_L planes; a thread owns DBM_NP pairs of neighbouring k cells, 64
+// cells apart (one float2 of hi and one of lo per array and pair, tiled
+// grids having k_total a multiple of 4).  bx of the planes i-2 .. i+2 stays
+// in a register ring, so each bx word is read and widened to FP64 once per
+// run (plus the four planes before it); by and bz of plane i go to shared
+// memory as FP64, halo rows and columns included, and the y and z
+// neighbours are read from there: about 7 widenings per cell instead of the
+// 22 of a kernel that widens every neighbour it loads.  The next plane's
+// words are loaded into registers before the plane's barrier, and the
+// shared planes alternate between two buffers, so one barrier per plane
+// suffices; two pairs per thread halve the barriers per cell.  The ghost
+// layers of bx, by and bz (hi and lo) must be current.  Writes slots 5 and 6
+// of the monitor kernel's per-block layout; the grid is at most 2 CTAs per
+// SM, all resident, each taking every gridDim-th item.
+constexpr int DBM_NP = 2, DBM_TJ = 8, DBM_TK = 64 * DBM_NP, DBM_L = 64;
 
 struct Raw2 {
   float2 h, l;
@@ -176,7 +177,7 @@ __device__ __forceinline__ double2 widen2(const Raw2 &r) {
   return make_double2((double)r.h.x + (double)r.l.x, (double)r.h.y + (double)r.l.y);
 }
 
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 2)
 divb_march_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
                   double *__restrict__ partial) {
   __shared__ __align__(16) double sby[2][DBM_TJ + 4][DBM_TK];
@@ -188,7 +189,7 @@ divb_march_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
   const float *bxh = hi.f[BX], *bxl = lo.f[BX], *byh = hi.f[BY], *byl = lo.f[BY];
   const float *bzh = hi.f[BZ], *bzl = lo.f[BZ];
   // halo duty: warps 0-3 load the by rows j0-2, j0-1, j0+8, j0+9; lanes
-  // 0-15 of warp 4 the bz pairs at k0-2 and k0+64 of the tile's 8 rows
+  // 0-15 of warp 4 the bz pairs at k0-2 and k0+DBM_TK of the tile's 8 rows
   const int hy_row = ty < 2 ? ty - 2 : ty + DBM_TJ - 2;  // tile-relative j of a by halo row
   const int hz_row = lane >> 1, hz_side = lane & 1;
   double sum = 0.0, mx = 0.0;
@@ -201,76 +202,102 @@ divb_march_kernel(Geom g, FieldPtrs<const float> hi, FieldPtrs<const float> lo,
     const int i0 = r / njt * DBM_L;
     const int i1 = min(i0 + DBM_L, n0);
     const int j0 = jt * DBM_TJ, k0 = kt * DBM_TK;
-    const int j = j0 + ty, k = k0 + 2 * lane;  // interior (j, k) of this thread's pair
-    const bool own = j < n1 && k < n2;         // n2 is a multiple of 4: k + 1 < n2 too
-    const bool yv = j <= n1 + 1 && k < n2;     // by pair that an owned cell reads
-    const bool zv = j < n1 && k <= n2;         // bz pair that an owned cell reads
-    const int jh = j0 + hy_row, kh = hz_side ? k0 + DBM_TK : k0 - 2, jz = j0 + hz_row;
-    const bool hy = ty < 4 && jh <= n1 + 1 && k < n2;
+    const int j = j0 + ty;
+    const int jh = j0 + hy_row, jz = j0 + hz_row, kh = hz_side ? k0 + DBM_TK : k0 - 2;
     const bool hz = ty == 4 && lane < 16 && jz < n1 && kh <= n2;
-    const long long cj = (long long)(j + g.m[1]) * g.st[1] + (k + g.m[2]);
-    const long long ch = hy ? (long long)(jh + g.m[1]) * g.st[1] + (k + g.m[2])
-                            : (long long)(jz + g.m[1]) * g.st[1] + (kh + g.m[2]);
-    double2 x0 = make_double2(0.0, 0.0), x1 = x0, x3 = x0;  // bx of planes i-2, i-1, i+1
-    double2 x2 = x0;                                        // bx of plane i (not in the stencil)
-    if (own) {
-      const long long c = (long long)(i0 + g.m[0]) * g.st[0] + cj;
-      x0 = widen2(ld_raw2(bxh, bxl, c - 2 * g.st[0]));
-      x1 = widen2(ld_raw2(bxh, bxl, c - g.st[0]));
-      x2 = widen2(ld_raw2(bxh, bxl, c));
-      x3 = widen2(ld_raw2(bxh, bxl, c + g.st[0]));
+    const long long chz = (long long)(jz + g.m[1]) * g.st[1] + (kh + g.m[2]);
+    bool own[DBM_NP], yv[DBM_NP], hy[DBM_NP];
+    long long cj[DBM_NP], chy[DBM_NP];
+#pragma unroll
+    for (int h = 0; h < DBM_NP; ++h) {
+      const int k = k0 + 64 * h + 2 * lane;  // interior k of this pair
+      own[h] = j < n1 && k < n2;             // n2 is a multiple of 4: k + 1 < n2 too
+      yv[h] = j <= n1 + 1 && k < n2;         // by pair that an owned cell reads
+      hy[h] = ty < 4 && jh <= n1 + 1 && k < n2;
+      cj[h] = (long long)(j + g.m[1]) * g.st[1] + (k + g.m[2]);
+      chy[h] = (long long)(jh + g.m[1]) * g.st[1] + (k + g.m[2]);
     }
-    Raw2 px{}, py{}, pz{}, ph{};  // plane i's words: bx at i+2, by, bz, halo
+    // bz pair that an owned cell reads: k <= n2
+    bool zv[DBM_NP];
+#pragma unroll
+    for (int h = 0; h < DBM_NP; ++h) zv[h] = j < n1 && k0 + 64 * h + 2 * lane <= n2;
+    // bx of planes i-2, i-1, i (not in the stencil), i+1 per pair
+    double2 x0[DBM_NP], x1[DBM_NP], x2[DBM_NP], x3[DBM_NP];
+    Raw2 px[DBM_NP], py[DBM_NP], pz[DBM_NP], ph[DBM_NP], pq{};  // plane i's words
     {
       const long long ci = (long long)(i0 + g.m[0]) * g.st[0];
-      if (own) px = ld_raw2(bxh, bxl, ci + 2 * g.st[0] + cj);
-      if (yv) py = ld_raw2(byh, byl, ci + cj);
-      if (zv) pz = ld_raw2(bzh, bzl, ci + cj);
-      if (hy) ph = ld_raw2(byh, byl, ci + ch);
-      if (hz) ph = ld_raw2(bzh, bzl, ci + ch);
+#pragma unroll
+      for (int h = 0; h < DBM_NP; ++h) {
+        x0[h] = x1[h] = x2[h] = x3[h] = make_double2(0.0, 0.0);
+        px[h] = py[h] = pz[h] = ph[h] = Raw2{};
+        if (own[h]) {
+          const long long c = ci + cj[h];
+          x0[h] = widen2(ld_raw2(bxh, bxl, c - 2 * g.st[0]));
+          x1[h] = widen2(ld_raw2(bxh, bxl, c - g.st[0]));
+          x2[h] = widen2(ld_raw2(bxh, bxl, c));
+          x3[h] = widen2(ld_raw2(bxh, bxl, c + g.st[0]));
+          px[h] = ld_raw2(bxh, bxl, c + 2 * g.st[0]);
+        }
+        if (yv[h]) py[h] = ld_raw2(byh, byl, ci + cj[h]);
+        if (zv[h]) pz[h] = ld_raw2(bzh, bzl, ci + cj[h]);
+        if (hy[h]) ph[h] = ld_raw2(byh, byl, ci + chy[h]);
+      }
+      if (hz) pq = ld_raw2(bzh, bzl, ci + chz);
     }
     for (int i = i0; i < i1; ++i, par ^= 1) {
-      if (yv) *reinterpret_cast<double2 *>(&sby[par][ty + 2][2 * lane]) = widen2(py);
-      if (zv) *reinterpret_cast<double2 *>(&sbz[par][ty][2 * lane + 2]) = widen2(pz);
-      if (hy) *reinterpret_cast<double2 *>(&sby[par][hy_row + 2][2 * lane]) = widen2(ph);
+      double2 x4[DBM_NP];
+#pragma unroll
+      for (int h = 0; h < DBM_NP; ++h) {
+        const int c = 64 * h + 2 * lane;  // tile-relative k of the pair
+        if (yv[h]) *reinterpret_cast<double2 *>(&sby[par][ty + 2][c]) = widen2(py[h]);
+        if (zv[h]) *reinterpret_cast<double2 *>(&sbz[par][ty][c + 2]) = widen2(pz[h]);
+        if (hy[h]) *reinterpret_cast<double2 *>(&sby[par][hy_row + 2][c]) = widen2(ph[h]);
+        x4[h] = own[h] ? widen2(px[h]) : make_double2(0.0, 0.0);
+      }
       if (hz)
-        *reinterpret_cast<double2 *>(&sbz[par][hz_row][hz_side ? DBM_TK + 2 : 0]) = widen2(ph);
-      const double2 x4 = own ? widen2(px) : make_double2(0.0, 0.0);
+        *reinterpret_cast<double2 *>(&sbz[par][hz_row][hz_side ? DBM_TK + 2 : 0]) = widen2(pq);
       if (i + 1 < i1) {  // the next plane's words, in flight across the barrier
         const long long ci = (long long)(i + 1 + g.m[0]) * g.st[0];
-        if (own) px = ld_raw2(bxh, bxl, ci + 2 * g.st[0] + cj);
-        if (yv) py = ld_raw2(byh, byl, ci + cj);
-        if (zv) pz = ld_raw2(bzh, bzl, ci + cj);
-        if (hy) ph = ld_raw2(byh, byl, ci + ch);
-        if (hz) ph = ld_raw2(bzh, bzl, ci + ch);
+#pragma unroll
+        for (int h = 0; h < DBM_NP; ++h) {
+          if (own[h]) px[h] = ld_raw2(bxh, bxl, ci + 2 * g.st[0] + cj[h]);
+          if (yv[h]) py[h] = ld_raw2(byh, byl, ci + cj[h]);
+          if (zv[h]) pz[h] = ld_raw2(bzh, bzl, ci + cj[h]);
+          if (hy[h]) ph[h] = ld_raw2(byh, byl, ci + chy[h]);
+        }
+        if (hz) pq = ld_raw2(bzh, bzl, ci + chz);
       }
       __syncthreads();
-      if (own) {
-        const double2 ym2 = *reinterpret_cast<const double2 *>(&sby[par][ty][2 * lane]);
-        const double2 ym1 = *reinterpret_cast<const double2 *>(&sby[par][ty + 1][2 * lane]);
-        const double2 yp1 = *reinterpret_cast<const double2 *>(&sby[par][ty + 3][2 * lane]);
-        const double2 yp2 = *reinterpret_cast<const double2 *>(&sby[par][ty + 4][2 * lane]);
-        // bz of k-2 .. k+3
-        const double2 za = *reinterpret_cast<const double2 *>(&sbz[par][ty][2 * lane]);
-        const double2 zb = *reinterpret_cast<const double2 *>(&sbz[par][ty][2 * lane + 2]);
-        const double2 zc = *reinterpret_cast<const double2 *>(&sbz[par][ty][2 * lane + 4]);
-        double divb = 0.0;
-        divb += (-x4.x + 8.0 * x3.x - 8.0 * x1.x + x0.x) * INV12 * g.dsi[0];
-        divb += (-yp2.x + 8.0 * yp1.x - 8.0 * ym1.x + ym2.x) * INV12 * g.dsi[1];
-        divb += (-zc.x + 8.0 * zb.y - 8.0 * za.y + za.x) * INV12 * g.dsi[2];
-        sum += fabs(divb);
-        mx = fmax(mx, fabs(divb));
-        divb = 0.0;
-        divb += (-x4.y + 8.0 * x3.y - 8.0 * x1.y + x0.y) * INV12 * g.dsi[0];
-        divb += (-yp2.y + 8.0 * yp1.y - 8.0 * ym1.y + ym2.y) * INV12 * g.dsi[1];
-        divb += (-zc.y + 8.0 * zc.x - 8.0 * zb.x + za.y) * INV12 * g.dsi[2];
-        sum += fabs(divb);
-        mx = fmax(mx, fabs(divb));
+#pragma unroll
+      for (int h = 0; h < DBM_NP; ++h) {
+        if (own[h]) {
+          const int c = 64 * h + 2 * lane;
+          const double2 ym2 = *reinterpret_cast<const double2 *>(&sby[par][ty][c]);
+          const double2 ym1 = *reinterpret_cast<const double2 *>(&sby[par][ty + 1][c]);
+          const double2 yp1 = *reinterpret_cast<const double2 *>(&sby[par][ty + 3][c]);
+          const double2 yp2 = *reinterpret_cast<const double2 *>(&sby[par][ty + 4][c]);
+          // bz of k-2 .. k+3
+          const double2 za = *reinterpret_cast<const double2 *>(&sbz[par][ty][c]);
+          const double2 zb = *reinterpret_cast<const double2 *>(&sbz[par][ty][c + 2]);
+          const double2 zc = *reinterpret_cast<const double2 *>(&sbz[par][ty][c + 4]);
+          double divb = 0.0;
+          divb += (-x4[h].x + 8.0 * x3[h].x - 8.0 * x1[h].x + x0[h].x) * INV12 * g.dsi[0];
+          divb += (-yp2.x + 8.0 * yp1.x - 8.0 * ym1.x + ym2.x) * INV12 * g.dsi[1];
+          divb += (-zc.x + 8.0 * zb.y - 8.0 * za.y + za.x) * INV12 * g.dsi[2];
+          sum += fabs(divb);
+          mx = fmax(mx, fabs(divb));
+          divb = 0.0;
+          divb += (-x4[h].y + 8.0 * x3[h].y - 8.0 * x1[h].y + x0[h].y) * INV12 * g.dsi[0];
+          divb += (-yp2.y + 8.0 * yp1.y - 8.0 * ym1.y + ym2.y) * INV12 * g.dsi[1];
+          divb += (-zc.y + 8.0 * zc.x - 8.0 * zb.x + za.y) * INV12 * g.dsi[2];
+          sum += fabs(divb);
+          mx = fmax(mx, fabs(divb));
+        }
+        x0[h] = x1[h];
+        x1[h] = x2[h];
+        x2[h] = x3[h];
+        x3[h] = x4[h];
       }
-      x0 = x1;
-      x1 = x2;
-      x2 = x3;
-      x3 = x4;
     }
   }
 #pragma unroll
@@ -2383,7 +2410,7 @@ int miso_b200_monitors(miso_b200_handle *h, double out[8]) {
     const Geom &g = h->g;
     const long long items = (long long)((g.n[0] + DBM_L - 1) / DBM_L) *
                             ((g.n[1] + DBM_TJ - 1) / DBM_TJ) * ((g.n[2] + DBM_TK - 1) / DBM_TK);
-    const int nb = items < 3LL * h->sms ? (int)items : 3 * h->sms;  // <= mon_blocks
+    const int nb = items < 2LL * h->sms ? (int)items : 2 * h->sms;  // <= mon_blocks
     divb_march_kernel<<<nb, 256, 0, h->stream>>>(g, h->cst(h->H(h->cur)), h->cst(h->L(h->cur)),
                                                  h->mon_partial);
     h->launches++;

@@ -305,10 +305,10 @@ def run_b200(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     # the monitors' read-back: the last sweep's per-block sums (6 doubles per
     # block of the fused y and z pass, 3 CTAs per SM, or of the z sweep, 8
-    # per SM) and the div B march's (8 doubles per block, 3 per SM); the
+    # per SM) and the div B march's (8 doubles per block, 2 per SM); the
     # unfused monitor kernel's (8 doubles per block, 4 per SM)
     zparts = (3 if tuning.get("av_y") == 3 else 8) * sms
-    d2h_mon = (6 * zparts + 8 * 3 * sms) * 8 if fused else 8 * 4 * sms * 8
+    d2h_mon = (6 * zparts + 8 * 2 * sms) * 8 if fused else 8 * 4 * sms * 8
     e2e = {"value": world * cells * K / e2e_s / 1e9, "unit": UNIT,
            "h2d_bytes_per_step": 96, "d2h_bytes_per_step": 96 + d2h_mon,
            "monitors_fused": fused,
